@@ -1,0 +1,211 @@
+// Internal declarations shared by the libhfm translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/hfm.h"
+
+namespace hfm {
+
+// ------------------------------------------------------------------ error reporting
+void set_error(const std::string &msg);
+int fail(int status, const std::string &msg);
+int cuda_status(cudaError_t e, const char *what);
+
+#define HFM_CUDA(call)                                                    \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess) return ::hfm::cuda_status(e_, #call);          \
+  } while (0)
+
+// Counts every kernel the library enqueues: direct launches here, graph launches by the
+// number of kernel nodes of the graph (launches made while capturing are not counted).
+void note_launch();
+void note_graph_launch(int64_t kernel_nodes);
+void set_capturing(bool on);
+
+#define HFM_CHECK_LAUNCH(what)                                            \
+  do {                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                  \
+    if (e_ != cudaSuccess) return ::hfm::cuda_status(e_, what);           \
+    ::hfm::note_launch();                                                 \
+  } while (0)
+
+int sm_count();  // SMs of the current device (cached per device)
+
+// ------------------------------------------------------------------ storage types
+template <class T> struct St;
+template <> struct St<float> {
+  static __device__ __forceinline__ float ld(const float *p) { return __ldg(p); }
+  static __device__ __forceinline__ float to(float v) { return v; }
+  static __device__ __forceinline__ float from(float v) { return v; }
+};
+template <> struct St<__nv_bfloat16> {
+  static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) {
+    return __bfloat162float(__ldg(p));
+  }
+  static __device__ __forceinline__ __nv_bfloat16 from(float v) { return __float2bfloat16(v); }
+  static __device__ __forceinline__ float to(__nv_bfloat16 v) { return __bfloat162float(v); }
+};
+template <> struct St<__half> {
+  static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
+  static __device__ __forceinline__ __half from(float v) { return __float2half(v); }
+  static __device__ __forceinline__ float to(__half v) { return __half2float(v); }
+};
+
+// ------------------------------------------------------------------ operator on device
+// Resolved operator for one level: `coef` point at instance 0, instance i is at
+// coef + i * coef_stride.  `k` already includes `scale` (coefficients for CONST7/K27),
+// and `scale` is kept for the array forms (SIGMA7 / DIR7) whose coefficients are in memory.
+struct DevOp {
+  float k[27];
+  float c[3];  // cz, cy, cx
+  float scale;
+  const void *coef[7];
+  int64_t coef_stride;
+};
+
+DevOp make_devop(const hfm_operator &op, int64_t coef_stride);
+
+// phi'(cell) = base(cell) + corr_sign * corr(cell or its parent), optionally zero on x = X-1.
+template <class T> struct PhiSrc {
+  const T *base;
+  const T *corr;
+  int64_t base_stride, corr_stride;
+  float corr_sign;
+  int corr_coarse;  // corr lives on the coarse grid (Zc, Yc, Xc) = fine / 2
+  int Yc, Xc;
+  int zero_xend;
+  __device__ __forceinline__ float operator()(int64_t inst, int z, int y, int x, int Y,
+                                              int X) const {
+    if (zero_xend && x == X - 1) return 0.f;
+    float v = 0.f;
+    if (base) v = St<T>::ld(base + inst * base_stride + ((int64_t)z * Y + y) * X + x);
+    if (corr) {
+      int64_t ci = corr_coarse ? (((int64_t)(z >> 1) * Yc + (y >> 1)) * Xc + (x >> 1))
+                               : (((int64_t)z * Y + y) * X + x);
+      v += corr_sign * St<T>::ld(corr + inst * corr_stride + ci);
+    }
+    return v;
+  }
+};
+
+// Evaluate (A phi')(z,y,x) and the Jacobi diagonal for operator KIND.
+template <int KIND, class T, class F>
+__device__ __forceinline__ float op_apply_at(const DevOp &op, const F &phi, int64_t inst,
+                                             int z, int y, int x, int Z, int Y, int X,
+                                             float *diag) {
+  auto P = [&](int zz, int yy, int xx) -> float {
+    if (zz < 0 || zz >= Z || yy < 0 || yy >= Y || xx < 0 || xx >= X) return 0.f;
+    return phi(inst, zz, yy, xx, Y, X);
+  };
+  if (KIND == HFM_OP_K27) {
+    float acc = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float w = op.k[9 * a + 3 * b + c];
+          if (w != 0.f) acc += w * P(z + a - 1, y + b - 1, x + c - 1);
+        }
+    *diag = op.k[13];
+    return acc;
+  } else if (KIND == HFM_OP_CONST7) {
+    const float kz = op.k[0], ky = op.k[1], kx = op.k[2];
+    const float d = 2.f * (kz + ky + kx);
+    float pc = P(z, y, x);
+    *diag = d;
+    return d * pc - kz * (P(z - 1, y, x) + P(z + 1, y, x)) - ky * (P(z, y - 1, x) + P(z, y + 1, x)) -
+           kx * (P(z, y, x - 1) + P(z, y, x + 1));
+  } else if (KIND == HFM_OP_SIGMA7) {
+    const T *sx = (const T *)op.coef[0] + inst * op.coef_stride;
+    const T *sy = (const T *)op.coef[1] + inst * op.coef_stride;
+    const T *sz = (const T *)op.coef[2] + inst * op.coef_stride;
+    const int64_t i = ((int64_t)z * Y + y) * X + x;
+    const float s = op.scale;
+    const float cz = op.c[0] * s, cy = op.c[1] * s, cx = op.c[2] * s;
+    float pc = P(z, y, x);
+    float vx = St<T>::ld(sx + i), vy = St<T>::ld(sy + i), vz = St<T>::ld(sz + i);
+    float axm = cx * (x > 0 ? 0.5f * (vx + St<T>::ld(sx + i - 1)) : vx);
+    float axp = cx * (x < X - 1 ? 0.5f * (vx + St<T>::ld(sx + i + 1)) : vx);
+    float aym = cy * (y > 0 ? 0.5f * (vy + St<T>::ld(sy + i - X)) : vy);
+    float ayp = cy * (y < Y - 1 ? 0.5f * (vy + St<T>::ld(sy + i + X)) : vy);
+    const int64_t P2 = (int64_t)X * Y;
+    float azm = cz * (z > 0 ? 0.5f * (vz + St<T>::ld(sz + i - P2)) : vz);
+    float azp = cz * (z < Z - 1 ? 0.5f * (vz + St<T>::ld(sz + i + P2)) : vz);
+    *diag = axm + axp + aym + ayp + azm + azp;
+    return axm * (pc - P(z, y, x - 1)) + axp * (pc - P(z, y, x + 1)) +
+           aym * (pc - P(z, y - 1, x)) + ayp * (pc - P(z, y + 1, x)) +
+           azm * (pc - P(z - 1, y, x)) + azp * (pc - P(z + 1, y, x));
+  } else {  // HFM_OP_DIR7
+    const int64_t i = ((int64_t)z * Y + y) * X + x + inst * op.coef_stride;
+    const float s = op.scale;
+    float pc = P(z, y, x);
+    auto A = [&](int d) { return s * St<T>::ld((const T *)op.coef[d] + i); };
+    *diag = A(6);
+    return A(0) * (pc - P(z, y, x - 1)) + A(1) * (pc - P(z, y, x + 1)) +
+           A(2) * (pc - P(z, y - 1, x)) + A(3) * (pc - P(z, y + 1, x)) +
+           A(4) * (pc - P(z - 1, y, x)) + A(5) * (pc - P(z + 1, y, x));
+  }
+}
+
+// ------------------------------------------------------------------ generic launchers
+// (ops_generic.cu).  All take instance strides in elements and an optional per-instance
+// `active` mask (nullptr = all instances) and optional per-block float64 partial sums of the
+// squared output (`partials`, laid out [inst][block]); `nblk_out` returns blocks per instance.
+struct Grid3 {
+  int Z, Y, X;
+  int64_t n() const { return (int64_t)Z * Y * X; }
+};
+
+template <class T>
+int launch_smooth(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
+                  int64_t rhs_stride, T *out, int64_t out_stride, int B, Grid3 g, float omega,
+                  unsigned flags, const int *active, cudaStream_t s);
+template <class T>
+int launch_residual(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *b,
+                    int64_t b_stride, T *r, int64_t r_stride, int B, Grid3 g, unsigned flags,
+                    const int *active, double *partials, int *nblk_out, cudaStream_t s);
+template <class T>
+int launch_apply(int kind, const DevOp &op, const PhiSrc<T> &phi, T *out, int64_t out_stride,
+                 int B, Grid3 g, const int *active, cudaStream_t s);
+// Fused residual + restriction on an even grid g (fine).  r_fine may be null.
+template <class T>
+int launch_residual_restrict(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *b,
+                             int64_t b_stride, T *r_fine, int64_t rf_stride, T *r_coarse,
+                             int64_t rc_stride, int B, Grid3 g, unsigned flags,
+                             const int *active, double *partials, int *nblk_out,
+                             cudaStream_t s);
+template <class T>
+int launch_restrict(const T *fine, int64_t f_stride, T *coarse, int64_t c_stride, int B,
+                    Grid3 g, const int *active, cudaStream_t s);
+template <class T>
+int launch_prolong(const T *coarse, int64_t c_stride, T *fine, int64_t f_stride, int B,
+                   Grid3 gc, const int *active, cudaStream_t s);
+// Jacobi sweeps on a small grid held in shared memory, one block per instance.
+template <class T>
+int launch_coarse_jacobi(int kind, const DevOp &op, const T *rhs, int64_t rhs_stride,
+                         const T *phi0, T *out, int64_t stride, int B, Grid3 g, float omega,
+                         int sweeps, const int *active, cudaStream_t s);
+int coarse_smem_limit();  // max cells for launch_coarse_jacobi
+
+// Reductions (reduce.cu)
+template <class T>
+int launch_sumsq_partials(const T *x, int64_t n, int64_t stride, int B, double *partials,
+                          int *nblk_out, const int *active, cudaStream_t s);
+int launch_finalize_sum(const double *partials, int nblk, int B, double *out_sum,
+                        cudaStream_t s);
+int reduce_blocks_for(int64_t n);
+
+template <class T>
+int launch_convert(const void *src, int src_dtype, T *dst, int64_t n, cudaStream_t s);
+template <class T>
+int launch_convert_out(const T *src, float *dst, int64_t n, cudaStream_t s);
+
+}  // namespace hfm

@@ -1,0 +1,914 @@
+// Multigrid handle: resident hierarchies for `slots` same-size instances, device-side
+// convergence control and CUDA graphs of whole cycles.
+//
+// Cycle forms (sign convention r = A phi - b, phi -= P w, as in the reference):
+//   SAWTOOTH  the reference loop (Anisotropic_3d_Multigrid_7point.ipynb:406-449,
+//             BGS_multigrid_v1.ipynb cell 42, naiver_stokes_3D.py:646-703);
+//   V / F     textbook cycles with nu_pre / nu_post weighted-Jacobi sweeps and a Jacobi
+//             solve on the coarsest level;
+//   accel CG  the V / F cycle (symmetric: nu_pre == nu_post) preconditions conjugate
+//             gradients on the fine level.
+// Every slot carries its own state on the device; a slot whose relative residual falls
+// below tol (or that fails, or reaches max_cycles) is switched off by the check kernel and
+// every later kernel skips it, so the host only polls between graph launches.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <type_traits>
+#include <vector>
+
+#include "hfm_internal.cuh"
+
+namespace hfm {
+
+struct SlotState {
+  int status;
+  int cycles;
+  int sol_buf;
+  int pad;
+  double norm_b;
+  double rel;
+  double rz;
+  double pq;
+};
+
+namespace {
+
+constexpr int kMaxLevels = 24;
+
+__global__ void k_init_state(SlotState *st, int *active, int slot, const double *sumsq_b,
+                             int status_if_zero) {
+  double nb = sqrt(sumsq_b[0]);
+  SlotState s;
+  s.status = HFM_OK;
+  s.cycles = 0;
+  s.sol_buf = 0;
+  s.pad = 0;
+  s.norm_b = nb;
+  s.rel = 1.0;
+  s.rz = 0.0;
+  s.pq = 0.0;
+  int act = 1;
+  if (!(nb > 0.0)) {
+    s.rel = 0.0;
+    act = 0;
+    if (nb != nb) s.status = HFM_ERR_NAN;
+    else s.status = status_if_zero;
+  }
+  st[slot] = s;
+  active[slot] = act;
+}
+
+// Sum the residual partials of each slot, update its state, switch it off when done.
+__global__ void k_check(const double *__restrict__ partials, int nblk, SlotState *st,
+                        int *active, double tol, int max_cycles, int which_buf) {
+  const int inst = blockIdx.x;
+  if (!active[inst]) return;
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) acc += partials[(int64_t)inst * nblk + i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sh[w];
+    SlotState s = st[inst];
+    double rel = sqrt(tot) / s.norm_b;
+    s.rel = rel;
+    if (!(rel == rel) || isinf(rel)) {
+      s.status = HFM_ERR_NAN;
+      s.sol_buf = which_buf;
+      active[inst] = 0;
+    } else if (rel < tol) {
+      s.status = HFM_OK;
+      s.sol_buf = which_buf;
+      active[inst] = 0;
+    } else if (s.cycles >= max_cycles) {
+      s.status = HFM_ERR_NOT_CONVERGED;
+      s.sol_buf = which_buf;
+      active[inst] = 0;
+    } else {
+      s.cycles += 1;
+    }
+    st[inst] = s;
+  }
+}
+
+template <class T>
+__global__ void k_fetch(const T *__restrict__ b0, const T *__restrict__ b1,
+                        const float *__restrict__ bx, int64_t n, const SlotState *st,
+                        const int *active, int slot, float *__restrict__ out) {
+  const int which = active[slot] ? 0 : st[slot].sol_buf;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float v;
+    if (bx) v = bx[i];
+    else v = St<T>::to(which ? b1[i] : b0[i]);
+    out[i] = v;
+  }
+}
+
+// ----------------------------------------------------------------- CG vector kernels
+template <class TZ>
+__global__ void k_dot_partials(const float *__restrict__ a, const TZ *__restrict__ b,
+                               int64_t n, int64_t sa, int64_t sb, double *partials,
+                               const int *active) {
+  __shared__ double sh[32];
+  const int64_t inst = blockIdx.y;
+  if (!active[inst]) return;
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    acc += (double)a[inst * sa + i] * (double)St<TZ>::ld(b + inst * sb + i);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    partials[inst * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// which: 0 -> rz (new), 1 -> pq
+__global__ void k_scalar_sum(const double *__restrict__ partials, int nblk, SlotState *st,
+                             const int *active, int which, double *rz_new) {
+  const int inst = blockIdx.x;
+  if (!active[inst]) return;
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) acc += partials[(int64_t)inst * nblk + i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    if (which == 0) rz_new[inst] = t;
+    else st[inst].pq = t;
+  }
+}
+
+// p = z + beta p (beta = rz_new / rz; first iteration p = z); rz <- rz_new.
+template <class TZ>
+__global__ void k_cg_p(const TZ *__restrict__ z, float *__restrict__ p, int64_t n, int64_t sz,
+                       int64_t sp, SlotState *st, const double *rz_new, const int *active) {
+  const int64_t inst = blockIdx.y;
+  if (!active[inst]) return;
+  const SlotState s = st[inst];
+  const double rzn = rz_new[inst];
+  const float beta = (s.cycles == 0 || s.rz == 0.0) ? 0.f : (float)(rzn / s.rz);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[inst * sp + i] = St<TZ>::ld(z + inst * sz + i) + beta * p[inst * sp + i];
+}
+
+__global__ void k_cg_commit_rz(SlotState *st, const double *rz_new, const int *active, int B) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < B && active[i]) st[i].rz = rz_new[i];
+}
+
+// x += alpha p, r -= alpha q, partial sums of r^2.
+__global__ void k_cg_xr(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
+                        const float *__restrict__ q, int64_t n, int64_t stride,
+                        const SlotState *st, double *partials, const int *active) {
+  __shared__ double sh[32];
+  const int64_t inst = blockIdx.y;
+  if (!active[inst]) return;
+  const SlotState s = st[inst];
+  const float alpha = (s.pq != 0.0) ? (float)(s.rz / s.pq) : 0.f;
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t k = inst * stride + i;
+    x[k] += alpha * p[k];
+    float rv = r[k] - alpha * q[k];
+    r[k] = rv;
+    acc += (double)rv * rv;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    partials[inst * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// r = b - A x computed as -(A x - b): negate in place.
+__global__ void k_negate(float *__restrict__ v, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = -v[i];
+}
+
+template <class T>
+__global__ void k_to_storage(const float *__restrict__ a, T *__restrict__ b, int64_t n,
+                             const int *active, int64_t stride) {
+  const int64_t inst = blockIdx.y;
+  if (!active[inst]) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[inst * stride + i] = St<T>::from(a[inst * stride + i]);
+}
+
+int vec_blocks(int64_t n, int B) {
+  int64_t want = (int64_t)sm_count() * 8 / std::max(B, 1);
+  int64_t need = (n + 255) / 256;
+  int64_t b = std::min(std::max<int64_t>(want, 1), need);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 65535));
+}
+
+size_t dtype_size(int dt) { return dt == HFM_F32 ? 4 : 2; }
+
+}  // namespace
+
+struct Level {
+  int Z, Y, X;
+  int64_t n;
+  void *phi = nullptr, *tmp = nullptr, *rhs = nullptr;
+  void *coef[3] = {nullptr, nullptr, nullptr};
+  DevOp op;
+};
+
+class EngineBase {
+ public:
+  virtual ~EngineBase() {}
+  virtual int emit_cycles(int cycles, cudaStream_t s) = 0;
+  virtual int load(int slot, const float *rhs, const float *phi0, cudaStream_t s) = 0;
+  virtual int fetch(int slot, float *out, cudaStream_t s) = 0;
+  virtual int set_operator(int slot, const hfm_operator &op, cudaStream_t s) = 0;
+  virtual int read_level(int slot, int level, int which, float *out, cudaStream_t s) = 0;
+  virtual bool cycle_flips_parity() const = 0;
+};
+
+}  // namespace hfm
+
+struct hfm_mg {
+  hfm_mg_config cfg;
+  int Z, Y, X, slots, L;
+  std::vector<hfm::Level> lv;
+  float *cg[4] = {nullptr, nullptr, nullptr, nullptr};  // x, r, p, q (CG) / w, r (sawtooth)
+  void *fine_b = nullptr;   // b for CG (rhs[0] holds r in storage type)
+  void *saw[2] = {nullptr, nullptr};  // sawtooth: r, w in storage type
+  int *active = nullptr;
+  hfm::SlotState *state = nullptr;
+  double *partials = nullptr;
+  int64_t partials_per_slot = 0;
+  double *scal = nullptr;  // per-slot scratch scalars (rz_new), and ||b||^2 at load
+  hfm_operator fine_desc;
+  cudaStream_t cap = nullptr;
+  std::map<int, cudaGraphExec_t> graphs;
+  std::map<int, int64_t> graph_kernels;
+  std::vector<void *> allocs;
+  std::unique_ptr<hfm::EngineBase> eng;
+};
+
+namespace hfm {
+
+template <class T>
+class Engine : public EngineBase {
+ public:
+  explicit Engine(hfm_mg *m) : m_(m) {}
+
+  bool cycle_flips_parity() const override {
+    const hfm_mg_config &c = m_->cfg;
+    if (c.accel == HFM_ACCEL_CG) return false;
+    if (c.cycle == HFM_CYCLE_SAWTOOTH) return true;
+    int post = std::max(c.nu_post, 1);
+    return ((c.nu_pre + post) & 1) != 0;
+  }
+
+  // ----------------------------------------------------------------- helpers
+  T *buf(int l, int which) { return (T *)(which ? m_->lv[l].tmp : m_->lv[l].phi); }
+  T *rhs(int l) { return (T *)m_->lv[l].rhs; }
+  Grid3 g(int l) { return Grid3{m_->lv[l].Z, m_->lv[l].Y, m_->lv[l].X}; }
+  int64_t n(int l) { return m_->lv[l].n; }
+  int kind() { return m_->cfg.op_kind; }
+
+  PhiSrc<T> src(const T *base, int64_t stride) {
+    PhiSrc<T> p;
+    memset(&p, 0, sizeof(p));
+    p.base = base;
+    p.base_stride = stride;
+    return p;
+  }
+  PhiSrc<T> with_coarse(PhiSrc<T> p, int lc, const T *corr, float sign) {
+    p.corr = corr;
+    p.corr_stride = n(lc);
+    p.corr_coarse = 1;
+    p.corr_sign = sign;
+    p.Yc = m_->lv[lc].Y;
+    p.Xc = m_->lv[lc].X;
+    return p;
+  }
+
+  int smooth(int l, const PhiSrc<T> &p, const T *f, T *out, float omega, unsigned flags,
+             cudaStream_t s) {
+    return launch_smooth<T>(kind(), m_->lv[l].op, p, f, n(l), out, n(l), m_->slots, g(l),
+                            omega, flags, m_->active, s);
+  }
+
+  int check(int nblk, int which, cudaStream_t s) {
+    k_check<<<m_->slots, 256, 0, s>>>(m_->partials, nblk, m_->state, m_->active, m_->cfg.tol,
+                                      m_->cfg.max_cycles, which);
+    HFM_CHECK_LAUNCH("k_check");
+    return HFM_OK;
+  }
+
+  // ----------------------------------------------------------------- V / F cycles
+  int coarse_solve(int l, cudaStream_t s) {
+    cur_[l] = 0;
+    if (n(l) <= coarse_smem_limit())
+      return launch_coarse_jacobi<T>(kind(), m_->lv[l].op, rhs(l), n(l), nullptr, buf(l, 0),
+                                     n(l), m_->slots, g(l), m_->cfg.coarse_omega,
+                                     m_->cfg.coarse_sweeps, m_->active, s);
+    // large coarsest level: global-memory sweeps
+    for (int k = 0; k < m_->cfg.coarse_sweeps; ++k) {
+      PhiSrc<T> p = src(k == 0 ? nullptr : buf(l, cur_[l]), n(l));
+      int st = smooth(l, p, rhs(l), buf(l, cur_[l] ^ 1), m_->cfg.coarse_omega, 0u, s);
+      if (st) return st;
+      cur_[l] ^= 1;
+    }
+    return HFM_OK;
+  }
+
+  // Approximately solve A_l phi = rhs(l); `zero` says the current iterate is zero.
+  int vcycle(int l, bool zero, bool fcycle, int check_level0, cudaStream_t s) {
+    const hfm_mg_config &c = m_->cfg;
+    int st;
+    if (l == m_->L - 1) return coarse_solve(l, s);
+    if (zero) cur_[l] = 0;
+    for (int k = 0; k < c.nu_pre; ++k) {
+      PhiSrc<T> p = src((zero && k == 0) ? nullptr : buf(l, cur_[l]), n(l));
+      if ((st = smooth(l, p, rhs(l), buf(l, cur_[l] ^ 1), c.omega, 0u, s))) return st;
+      cur_[l] ^= 1;
+    }
+    const bool still_zero = zero && c.nu_pre == 0;
+    int nblk = 0;
+    const bool chk = (l == 0 && check_level0);
+    PhiSrc<T> p = src(still_zero ? nullptr : buf(l, cur_[l]), n(l));
+    if ((st = launch_residual_restrict<T>(kind(), m_->lv[l].op, p, rhs(l), n(l), nullptr, 0,
+                                          rhs(l + 1), n(l + 1), m_->slots, g(l), 0u,
+                                          m_->active, chk ? m_->partials : nullptr, &nblk, s)))
+      return st;
+    if (chk && (st = check(nblk, cur_[0], s))) return st;
+    if (fcycle) {
+      if ((st = vcycle(l + 1, true, true, 0, s))) return st;
+      if ((st = vcycle(l + 1, false, false, 0, s))) return st;
+    } else {
+      if ((st = vcycle(l + 1, true, false, 0, s))) return st;
+    }
+    // correction fused with the first post-smoothing sweep (omega = 0 when nu_post == 0)
+    const int post = std::max(c.nu_post, 1);
+    for (int k = 0; k < post; ++k) {
+      PhiSrc<T> q = src(still_zero && k == 0 ? nullptr : buf(l, cur_[l]), n(l));
+      if (k == 0) q = with_coarse(q, l + 1, buf(l + 1, cur_[l + 1]), -1.f);
+      float om = c.nu_post == 0 ? 0.f : c.omega;
+      if ((st = smooth(l, q, rhs(l), buf(l, cur_[l] ^ 1), om, 0u, s))) return st;
+      cur_[l] ^= 1;
+    }
+    return HFM_OK;
+  }
+
+  // ----------------------------------------------------------------- sawtooth
+  int sawtooth(cudaStream_t s) {
+    const hfm_mg_config &c = m_->cfg;
+    const int L = m_->L;
+    T *r0 = (T *)m_->saw[0], *w0 = (T *)m_->saw[1];
+    int st, nblk = 0;
+    const unsigned xend = c.flags & HFM_FLAG_ZERO_XEND;
+    // 1. r = A phi - b (NS: r[..., X-1] = 0), residual norm for the stopping test
+    if ((st = launch_residual<T>(kind(), m_->lv[0].op, src(buf(0, cur_[0]), n(0)), rhs(0), n(0),
+                                 r0, n(0), m_->slots, g(0), xend, m_->active, m_->partials,
+                                 &nblk, s)))
+      return st;
+    if ((st = check(nblk, cur_[0], s))) return st;
+    // 2. restriction chain r -> r_1 -> ... -> r_{L-1} (coarse rhs buffers)
+    for (int l = 1; l < L; ++l) {
+      const T *f = l == 1 ? r0 : rhs(l - 1);
+      if ((st = launch_restrict<T>(f, n(l - 1), rhs(l), n(l), m_->slots, g(l - 1), m_->active, s)))
+        return st;
+    }
+    // 3. coarsest: one Jacobi sweep from w = 0
+    if ((st = smooth(L - 1, src(nullptr, n(L - 1)), rhs(L - 1), buf(L - 1, 0), c.omega, 0u, s)))
+      return st;
+    // 4. coarse levels: w = P w; one Jacobi
+    for (int l = L - 2; l >= 1; --l) {
+      PhiSrc<T> p = with_coarse(src(nullptr, n(l)), l + 1, buf(l + 1, 0), 1.f);
+      if ((st = smooth(l, p, rhs(l), buf(l, 0), c.omega, 0u, s))) return st;
+    }
+    // 5. fine: w = P w (+ one Jacobi against r in the 7-point form)
+    if (c.sawtooth_fine_smooth) {
+      PhiSrc<T> p = with_coarse(src(nullptr, n(0)), 1, buf(1, 0), 1.f);
+      if ((st = smooth(0, p, r0, w0, c.omega, 0u, s))) return st;
+    } else {
+      if ((st = launch_prolong<T>(buf(1, 0), n(1), w0, n(0), m_->slots, g(1), m_->active, s)))
+        return st;
+    }
+    // 6. phi = J(phi - w) against b (NS: phi[..., X-1] = 0 before the sweep; _BC: top copy)
+    PhiSrc<T> p = src(buf(0, cur_[0]), n(0));
+    p.corr = w0;
+    p.corr_stride = n(0);
+    p.corr_sign = -1.f;
+    p.zero_xend = xend ? 1 : 0;
+    if ((st = smooth(0, p, rhs(0), buf(0, cur_[0] ^ 1), c.omega, c.flags & HFM_FLAG_TOP_COPY, s)))
+      return st;
+    cur_[0] ^= 1;
+    return HFM_OK;
+  }
+
+  // ----------------------------------------------------------------- PCG iteration
+  int cg_iteration(cudaStream_t s) {
+    const int B = m_->slots;
+    const int64_t nf = n(0);
+    float *x = m_->cg[0], *r = m_->cg[1], *p = m_->cg[2], *q = m_->cg[3];
+    const int vb = vec_blocks(nf, B);
+    int st;
+    // z = M r  (rhs(0) holds r in the storage type)
+    if (!std::is_same<T, float>::value) {
+      k_to_storage<T><<<dim3(vb, B), 256, 0, s>>>(r, rhs(0), nf, m_->active, nf);
+      HFM_CHECK_LAUNCH("k_to_storage");
+    }
+    if ((st = vcycle(0, true, m_->cfg.cycle == HFM_CYCLE_F, 0, s))) return st;
+    const T *z = buf(0, cur_[0]);
+    // rz_new = r . z ; p = z + beta p
+    k_dot_partials<T><<<dim3(vb, B), 256, 0, s>>>(r, z, nf, nf, nf, m_->partials, m_->active);
+    HFM_CHECK_LAUNCH("k_dot_partials");
+    k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 0, m_->scal);
+    k_cg_p<T><<<dim3(vb, B), 256, 0, s>>>(z, p, nf, nf, nf, m_->state, m_->scal, m_->active);
+    k_cg_commit_rz<<<(B + 127) / 128, 128, 0, s>>>(m_->state, m_->scal, m_->active, B);
+    HFM_CHECK_LAUNCH("k_cg_p");
+    // q = A p ; pq = p . q   (FP32 operator on the fine level)
+    PhiSrc<float> pp;
+    memset(&pp, 0, sizeof(pp));
+    pp.base = p;
+    pp.base_stride = nf;
+    if ((st = launch_apply<float>(kind(), fine32_, pp, q, nf, B, g(0), m_->active, s))) return st;
+    k_dot_partials<float><<<dim3(vb, B), 256, 0, s>>>(p, q, nf, nf, nf, m_->partials, m_->active);
+    k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 1, m_->scal);
+    // x += alpha p ; r -= alpha q ; ||r||
+    k_cg_xr<<<dim3(vb, B), 256, 0, s>>>(x, r, p, q, nf, nf, m_->state, m_->partials, m_->active);
+    HFM_CHECK_LAUNCH("k_cg_xr");
+    return check(vb, 0, s);
+  }
+
+  int emit_cycles(int cycles, cudaStream_t s) override {
+    int st;
+    for (int k = 0; k < kMaxLevels; ++k) cur_[k] = 0;
+    for (int i = 0; i < cycles; ++i) {
+      const hfm_mg_config &c = m_->cfg;
+      if (c.accel == HFM_ACCEL_CG) st = cg_iteration(s);
+      else if (c.cycle == HFM_CYCLE_SAWTOOTH) st = sawtooth(s);
+      else st = vcycle(0, false, c.cycle == HFM_CYCLE_F, 1, s);
+      if (st) return st;
+    }
+    if (m_->cfg.accel != HFM_ACCEL_CG && cur_[0] != 0)
+      return fail(HFM_ERR_BAD_ARG, "internal: odd number of fine-level sweeps in a launch");
+    return HFM_OK;
+  }
+
+  // ----------------------------------------------------------------- slots
+  int set_operator(int slot, const hfm_operator &op, cudaStream_t s) override {
+    const int k = m_->cfg.op_kind;
+    if (op.kind != k) return fail(HFM_ERR_BAD_ARG, "operator kind differs from the handle's");
+    m_->fine_desc = op;
+    if (k == HFM_OP_CONST7 || k == HFM_OP_K27) {
+      float sc = 1.f;
+      for (int l = 0; l < m_->L; ++l) {
+        hfm_operator o = op;
+        o.scale = (op.scale == 0.f ? 1.f : op.scale) * sc;
+        m_->lv[l].op = make_devop(o, 0);
+        sc *= m_->cfg.coarse_scale;
+      }
+      fine32_ = m_->lv[0].op;
+      return HFM_OK;
+    }
+    if (k != HFM_OP_SIGMA7) return fail(HFM_ERR_UNSUPPORTED, "handle supports CONST7, SIGMA7, K27");
+    if (op.coef_dtype != HFM_F32 && op.coef_dtype != HFM_F64)
+      return fail(HFM_ERR_BAD_ARG, "coefficients must be float32 or float64");
+    int lo = slot < 0 ? 0 : slot, hi = slot < 0 ? m_->slots : slot + 1;
+    for (int sl = lo; sl < hi; ++sl) {
+      for (int a = 0; a < 3; ++a) {
+        if (!op.coef[a]) return fail(HFM_ERR_BAD_ARG, "SIGMA7 needs sx, sy, sz");
+        const size_t esz = op.coef_dtype == HFM_F64 ? 8 : 4;
+        const void *srcp = (const char *)op.coef[a] + (slot < 0 ? (size_t)sl * n(0) * esz : 0);
+        int st = launch_convert<T>(srcp, op.coef_dtype, (T *)m_->lv[0].coef[a] + sl * n(0), n(0), s);
+        if (st) return st;
+        if (fine32_coef_[a] && (st = launch_convert<float>(srcp, op.coef_dtype,
+                                                           fine32_coef_[a] + sl * n(0), n(0), s)))
+          return st;
+        for (int l = 1; l < m_->L; ++l) {
+          st = launch_restrict<T>((T *)m_->lv[l - 1].coef[a] + sl * n(l - 1), n(l - 1),
+                                  (T *)m_->lv[l].coef[a] + sl * n(l), n(l), 1, g(l - 1),
+                                  nullptr, s);
+          if (st) return st;
+        }
+      }
+    }
+    float sc = 1.f;
+    for (int l = 0; l < m_->L; ++l) {
+      hfm_operator o = op;
+      o.scale = (op.scale == 0.f ? 1.f : op.scale) * sc;
+      for (int a = 0; a < 3; ++a) o.coef[a] = m_->lv[l].coef[a];
+      m_->lv[l].op = make_devop(o, n(l));
+      sc *= m_->cfg.coarse_scale;
+    }
+    fine32_ = m_->lv[0].op;
+    if (fine32_coef_[0])
+      for (int a = 0; a < 3; ++a) fine32_.coef[a] = fine32_coef_[a];
+    return HFM_OK;
+  }
+
+  int load(int slot, const float *b, const float *phi0, cudaStream_t s) override {
+    const int64_t nf = n(0);
+    int st;
+    const bool cg = m_->cfg.accel == HFM_ACCEL_CG;
+    if (cg) {
+      float *x = m_->cg[0] + slot * nf, *r = m_->cg[1] + slot * nf, *bb = (float *)m_->fine_b + slot * nf;
+      HFM_CUDA(cudaMemcpyAsync(bb, b, nf * 4, cudaMemcpyDeviceToDevice, s));
+      if (phi0) {
+        HFM_CUDA(cudaMemcpyAsync(x, phi0, nf * 4, cudaMemcpyDeviceToDevice, s));
+        DevOp d = fine32_;
+        for (int a = 0; a < 3; ++a)
+          if (d.coef[a]) d.coef[a] = (const char *)d.coef[a] + (size_t)slot * nf * 4;
+        PhiSrc<float> p;
+        memset(&p, 0, sizeof(p));
+        p.base = x;
+        p.base_stride = nf;
+        if (!std::is_same<T, float>::value && m_->cfg.op_kind == HFM_OP_SIGMA7 && !fine32_coef_[0])
+          return fail(HFM_ERR_UNSUPPORTED, "initial guess with reduced-precision CG");
+        if ((st = launch_residual<float>(kind(), d, p, bb, nf, r, nf, 1, g(0), 0u, nullptr,
+                                         nullptr, nullptr, s)))
+          return st;
+        k_negate<<<vec_blocks(nf, 1), 256, 0, s>>>(r, nf);
+      } else {
+        HFM_CUDA(cudaMemsetAsync(x, 0, nf * 4, s));
+        HFM_CUDA(cudaMemcpyAsync(r, b, nf * 4, cudaMemcpyDeviceToDevice, s));
+      }
+      HFM_CUDA(cudaMemsetAsync(m_->cg[2] + slot * nf, 0, nf * 4, s));
+    } else {
+      if ((st = launch_convert<T>(b, HFM_F32, rhs(0) + slot * nf, nf, s))) return st;
+      if (phi0) {
+        if ((st = launch_convert<T>(phi0, HFM_F32, buf(0, 0) + slot * nf, nf, s))) return st;
+      } else {
+        HFM_CUDA(cudaMemsetAsync(buf(0, 0) + slot * nf, 0, nf * sizeof(T), s));
+      }
+    }
+    int nb = 0;
+    if ((st = launch_sumsq_partials<float>(b, nf, nf, 1, m_->partials, &nb, nullptr, s))) return st;
+    if ((st = launch_finalize_sum(m_->partials, nb, 1, m_->scal + m_->slots, s))) return st;
+    k_init_state<<<1, 1, 0, s>>>(m_->state, m_->active, slot, m_->scal + m_->slots, HFM_OK);
+    HFM_CHECK_LAUNCH("k_init_state");
+    return HFM_OK;
+  }
+
+  int fetch(int slot, float *out, cudaStream_t s) override {
+    const int64_t nf = n(0);
+    const float *bx = m_->cfg.accel == HFM_ACCEL_CG ? m_->cg[0] + slot * nf : nullptr;
+    k_fetch<T><<<vec_blocks(nf, 1), 256, 0, s>>>(buf(0, 0) + slot * nf, buf(0, 1) + slot * nf,
+                                                bx, nf, m_->state, m_->active, slot, out);
+    HFM_CHECK_LAUNCH("k_fetch");
+    return HFM_OK;
+  }
+
+  int read_level(int slot, int level, int which, float *out, cudaStream_t s) override {
+    if (level < 0 || level >= m_->L) return fail(HFM_ERR_BAD_ARG, "level out of range");
+    const T *src_p;
+    if (m_->cfg.cycle == HFM_CYCLE_SAWTOOTH && level == 0 && m_->cfg.accel != HFM_ACCEL_CG)
+      src_p = (const T *)(which ? m_->saw[0] : m_->saw[1]);
+    else
+      src_p = which ? rhs(level) : buf(level, 0);
+    return launch_convert_out<T>(src_p + slot * n(level), out, n(level), s);
+  }
+
+  DevOp fine32_;
+  float *fine32_coef_[3] = {nullptr, nullptr, nullptr};
+
+ private:
+  hfm_mg *m_;
+  int cur_[kMaxLevels] = {0};
+};
+
+}  // namespace hfm
+
+using namespace hfm;
+
+namespace {
+
+void *dalloc(hfm_mg *m, size_t bytes, int *st) {
+  if (*st) return nullptr;
+  void *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *st = fail(HFM_ERR_OOM, "cudaMalloc failed while creating a multigrid handle");
+    return nullptr;
+  }
+  m->allocs.push_back(p);
+  return p;
+}
+
+std::vector<Grid3> plan_levels(const hfm_mg_config &c, int Z, int Y, int X) {
+  std::vector<Grid3> v{Grid3{Z, Y, X}};
+  const int want = c.n_levels > 0 ? c.n_levels : kMaxLevels;
+  while ((int)v.size() < want) {
+    Grid3 t = v.back();
+    bool even = !(t.Z & 1) && !(t.Y & 1) && !(t.X & 1);
+    if (c.n_levels > 0) {
+      // explicit depth: the reference's VALID restriction floors odd extents
+      if (t.Z < 2 && t.Y < 2 && t.X < 2) break;
+      v.push_back(Grid3{std::max(t.Z / 2, 1), std::max(t.Y / 2, 1), std::max(t.X / 2, 1)});
+      continue;
+    }
+    if (!even || std::min(t.Z, std::min(t.Y, t.X)) <= c.min_coarse_edge) break;
+    v.push_back(Grid3{t.Z / 2, t.Y / 2, t.X / 2});
+  }
+  return v;
+}
+
+int validate_cfg(const hfm_mg_config &c, int Z, int Y, int X, int slots) {
+  if (Z <= 0 || Y <= 0 || X <= 0 || slots <= 0 || slots > 65535)
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: bad extents or slot count");
+  if (c.op_kind != HFM_OP_CONST7 && c.op_kind != HFM_OP_SIGMA7 && c.op_kind != HFM_OP_K27)
+    return fail(HFM_ERR_UNSUPPORTED, "hfm_mg_create: operator kind must be CONST7, SIGMA7 or K27");
+  if (c.storage != HFM_F32 && c.storage != HFM_BF16 && c.storage != HFM_F16)
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: storage must be F32, BF16 or F16");
+  if (c.cycle < 0 || c.cycle > 2 || c.accel < 0 || c.accel > 1)
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: bad cycle / accel");
+  if (c.cycle == HFM_CYCLE_SAWTOOTH && c.accel == HFM_ACCEL_CG)
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: the sawtooth cycle is not symmetric; use V or F with CG");
+  if (c.accel == HFM_ACCEL_CG && c.nu_pre != c.nu_post)
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: CG needs a symmetric cycle (nu_pre == nu_post)");
+  if (c.nu_pre < 0 || c.nu_post < 0 || c.coarse_sweeps < 1 || c.max_cycles < 1)
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: bad sweep counts");
+  if (!(c.omega > 0.f) || !(c.tol > 0.0)) return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: bad omega / tol");
+  return HFM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void hfm_mg_config_default(hfm_mg_config *c) {
+  if (!c) return;
+  memset(c, 0, sizeof(*c));
+  c->op_kind = HFM_OP_SIGMA7;
+  c->cycle = HFM_CYCLE_V;
+  c->accel = HFM_ACCEL_NONE;
+  c->n_levels = 0;
+  c->min_coarse_edge = 4;
+  c->nu_pre = 2;
+  c->nu_post = 2;
+  c->coarse_sweeps = 32;
+  c->omega = 2.f / 3.f;
+  c->coarse_omega = 2.f / 3.f;
+  c->coarse_scale = 0.5f;
+  c->sawtooth_fine_smooth = 1;
+  c->flags = 0;
+  c->storage = HFM_F32;
+  c->tol = 1e-6;
+  c->max_cycles = 500;
+  c->cycles_per_launch = 4;
+}
+
+size_t hfm_mg_footprint_bytes(const hfm_mg_config *c, int Z, int Y, int X, int slots) {
+  if (!c) return 0;
+  std::vector<Grid3> lv = plan_levels(*c, Z, Y, X);
+  const size_t es = dtype_size(c->storage);
+  size_t tot = 0;
+  for (size_t l = 0; l < lv.size(); ++l) {
+    size_t nl = (size_t)lv[l].n();
+    size_t fields = 3 + (c->op_kind == HFM_OP_SIGMA7 ? 3 : 0);
+    tot += nl * fields * es;
+  }
+  const size_t nf = (size_t)Z * Y * X;
+  if (c->accel == HFM_ACCEL_CG) {
+    tot += nf * 5 * 4;  // x r p q b
+    if (c->op_kind == HFM_OP_SIGMA7 && c->storage != HFM_F32) tot += nf * 3 * 4;
+  } else if (c->cycle == HFM_CYCLE_SAWTOOTH) {
+    tot += nf * 2 * es;
+  }
+  tot *= (size_t)slots;
+  tot += (size_t)slots * (sizeof(SlotState) + 64) + (size_t)slots * 4096 * 8;
+  return tot;
+}
+
+int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_mg **out) {
+  if (!cfg || !out) return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: NULL argument");
+  *out = nullptr;
+  int st = validate_cfg(*cfg, Z, Y, X, slots);
+  if (st) return st;
+  std::unique_ptr<hfm_mg> m(new hfm_mg());
+  m->cfg = *cfg;
+  if (m->cfg.cycles_per_launch < 1) m->cfg.cycles_per_launch = 1;
+  m->Z = Z;
+  m->Y = Y;
+  m->X = X;
+  m->slots = slots;
+  std::vector<Grid3> lv = plan_levels(*cfg, Z, Y, X);
+  m->L = (int)lv.size();
+  if (m->L < 2 && cfg->cycle == HFM_CYCLE_SAWTOOTH)
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: the sawtooth cycle needs at least two levels");
+  if (lv.back().n() > coarse_smem_limit() && cfg->cycle != HFM_CYCLE_SAWTOOTH && m->L > 1 &&
+      cfg->coarse_sweeps > 64)
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: coarsest level too large");
+  const size_t es = dtype_size(cfg->storage);
+  m->lv.resize(m->L);
+  for (int l = 0; l < m->L; ++l) {
+    Level &L = m->lv[l];
+    L.Z = lv[l].Z;
+    L.Y = lv[l].Y;
+    L.X = lv[l].X;
+    L.n = lv[l].n();
+    const size_t b = (size_t)L.n * slots * es;
+    L.phi = dalloc(m.get(), b, &st);
+    L.tmp = dalloc(m.get(), b, &st);
+    L.rhs = dalloc(m.get(), b, &st);
+    if (cfg->op_kind == HFM_OP_SIGMA7)
+      for (int a = 0; a < 3; ++a) L.coef[a] = dalloc(m.get(), b, &st);
+  }
+  const size_t nf = (size_t)Z * Y * X * slots;
+  if (cfg->accel == HFM_ACCEL_CG) {
+    for (int i = 0; i < 4; ++i) m->cg[i] = (float *)dalloc(m.get(), nf * 4, &st);
+    m->fine_b = dalloc(m.get(), nf * 4, &st);
+  } else if (cfg->cycle == HFM_CYCLE_SAWTOOTH) {
+    m->saw[0] = dalloc(m.get(), nf * es, &st);
+    m->saw[1] = dalloc(m.get(), nf * es, &st);
+  }
+  m->partials_per_slot = 4096;
+  m->partials = (double *)dalloc(m.get(), (size_t)slots * m->partials_per_slot * 8, &st);
+  m->active = (int *)dalloc(m.get(), (size_t)slots * 4, &st);
+  m->state = (SlotState *)dalloc(m.get(), (size_t)slots * sizeof(SlotState), &st);
+  m->scal = (double *)dalloc(m.get(), (size_t)(slots + 1) * 8, &st);
+  if (!st) {
+    if (cudaMemset(m->active, 0, (size_t)slots * 4) != cudaSuccess ||
+        cudaMemset(m->state, 0, (size_t)slots * sizeof(SlotState)) != cudaSuccess)
+      st = fail(HFM_ERR_CUDA, "cudaMemset failed");
+  }
+  if (!st && cudaStreamCreateWithFlags(&m->cap, cudaStreamNonBlocking) != cudaSuccess)
+    st = fail(HFM_ERR_CUDA, "cudaStreamCreate failed");
+  if (!st) {
+    switch (cfg->storage) {
+      case HFM_F32: m->eng.reset(new Engine<float>(m.get())); break;
+      case HFM_BF16: m->eng.reset(new Engine<__nv_bfloat16>(m.get())); break;
+      default: m->eng.reset(new Engine<__half>(m.get())); break;
+    }
+    // CG runs its outer vectors and fine operator in float32: keep float32 conductivities.
+    if (cfg->accel == HFM_ACCEL_CG && cfg->op_kind == HFM_OP_SIGMA7 && cfg->storage != HFM_F32) {
+      float **fc = nullptr;
+      switch (cfg->storage) {
+        case HFM_BF16: fc = ((Engine<__nv_bfloat16> *)m->eng.get())->fine32_coef_; break;
+        default: fc = ((Engine<__half> *)m->eng.get())->fine32_coef_; break;
+      }
+      for (int a = 0; a < 3; ++a) fc[a] = (float *)dalloc(m.get(), nf * 4, &st);
+    }
+  }
+  if (st) {
+    for (void *p : m->allocs) cudaFree(p);
+    if (m->cap) cudaStreamDestroy(m->cap);
+    return st;
+  }
+  // default constant operator so that CONST7 / K27 handles work after set_operator only
+  *out = m.release();
+  return HFM_OK;
+}
+
+int hfm_mg_destroy(hfm_mg *m) {
+  if (!m) return HFM_OK;
+  for (auto &kv : m->graphs) cudaGraphExecDestroy(kv.second);
+  if (m->cap) {
+    cudaStreamSynchronize(m->cap);
+    cudaStreamDestroy(m->cap);
+  }
+  cudaDeviceSynchronize();
+  for (void *p : m->allocs) cudaFree(p);
+  delete m;
+  return HFM_OK;
+}
+
+int hfm_mg_num_levels(const hfm_mg *m) { return m ? m->L : 0; }
+
+int hfm_mg_level_shape(const hfm_mg *m, int level, int *Z, int *Y, int *X) {
+  if (!m || level < 0 || level >= m->L || !Z || !Y || !X) return fail(HFM_ERR_BAD_ARG, "bad level");
+  *Z = m->lv[level].Z;
+  *Y = m->lv[level].Y;
+  *X = m->lv[level].X;
+  return HFM_OK;
+}
+
+int hfm_mg_set_operator(hfm_mg *m, int slot, const hfm_operator *op, hfm_stream_t stream) {
+  if (!m || !op || slot >= m->slots || slot < -1) return fail(HFM_ERR_BAD_ARG, "hfm_mg_set_operator: bad argument");
+  return m->eng->set_operator(slot, *op, (cudaStream_t)stream);
+}
+
+int hfm_mg_load(hfm_mg *m, int slot, const float *rhs, const float *phi0, hfm_stream_t stream) {
+  if (!m || !rhs || slot < 0 || slot >= m->slots) return fail(HFM_ERR_BAD_ARG, "hfm_mg_load: bad argument");
+  return m->eng->load(slot, rhs, phi0, (cudaStream_t)stream);
+}
+
+int hfm_mg_run(hfm_mg *m, int cycles, hfm_stream_t stream) {
+  if (!m || cycles < 1) return fail(HFM_ERR_BAD_ARG, "hfm_mg_run: bad argument");
+  if (m->eng->cycle_flips_parity() && (cycles & 1)) cycles += 1;
+  cudaGraphExec_t exec = nullptr;
+  auto it = m->graphs.find(cycles);
+  if (it != m->graphs.end()) {
+    exec = it->second;
+  } else {
+    cudaGraph_t graph = nullptr;
+    HFM_CUDA(cudaStreamBeginCapture(m->cap, cudaStreamCaptureModeRelaxed));
+    set_capturing(true);
+    int st = m->eng->emit_cycles(cycles, m->cap);
+    set_capturing(false);
+    cudaError_t e = cudaStreamEndCapture(m->cap, &graph);
+    if (st) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+    size_t nn = 0;
+    int64_t nk = 0;
+    if (cudaGraphGetNodes(graph, nullptr, &nn) == cudaSuccess && nn) {
+      std::vector<cudaGraphNode_t> nodes(nn);
+      if (cudaGraphGetNodes(graph, nodes.data(), &nn) == cudaSuccess)
+        for (size_t i = 0; i < nn; ++i) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nk;
+        }
+    }
+    m->graph_kernels[cycles] = nk;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+    m->graphs[cycles] = exec;
+  }
+  HFM_CUDA(cudaGraphLaunch(exec, (cudaStream_t)stream));
+  note_graph_launch(m->graph_kernels[cycles]);
+  return HFM_OK;
+}
+
+int hfm_mg_query(hfm_mg *m, hfm_slot_stats *out, hfm_stream_t stream) {
+  if (!m || !out) return fail(HFM_ERR_BAD_ARG, "hfm_mg_query: bad argument");
+  std::vector<SlotState> st(m->slots);
+  std::vector<int> act(m->slots);
+  cudaStream_t s = (cudaStream_t)stream;
+  HFM_CUDA(cudaMemcpyAsync(st.data(), m->state, m->slots * sizeof(SlotState), cudaMemcpyDeviceToHost, s));
+  HFM_CUDA(cudaMemcpyAsync(act.data(), m->active, m->slots * 4, cudaMemcpyDeviceToHost, s));
+  HFM_CUDA(cudaStreamSynchronize(s));
+  for (int i = 0; i < m->slots; ++i) {
+    out[i].active = act[i];
+    out[i].status = st[i].status;
+    out[i].cycles = st[i].cycles;
+    out[i].reserved = 0;
+    out[i].norm_b = st[i].norm_b;
+    out[i].rel_resid = st[i].rel;
+  }
+  return HFM_OK;
+}
+
+int hfm_mg_fetch(hfm_mg *m, int slot, float *out, hfm_stream_t stream) {
+  if (!m || !out || slot < 0 || slot >= m->slots) return fail(HFM_ERR_BAD_ARG, "hfm_mg_fetch: bad argument");
+  return m->eng->fetch(slot, out, (cudaStream_t)stream);
+}
+
+int hfm_mg_cancel(hfm_mg *m, int slot, hfm_stream_t stream) {
+  if (!m || slot < 0 || slot >= m->slots) return fail(HFM_ERR_BAD_ARG, "hfm_mg_cancel: bad argument");
+  HFM_CUDA(cudaMemsetAsync(m->active + slot, 0, 4, (cudaStream_t)stream));
+  return HFM_OK;
+}
+
+int hfm_mg_read_level(hfm_mg *m, int slot, int level, int which, float *out, hfm_stream_t stream) {
+  if (!m || !out || slot < 0 || slot >= m->slots) return fail(HFM_ERR_BAD_ARG, "hfm_mg_read_level: bad argument");
+  return m->eng->read_level(slot, level, which, out, (cudaStream_t)stream);
+}
+
+int hfm_mg_solve(hfm_mg *m, const float *rhs, float *phi, hfm_slot_stats *stats_host,
+                 hfm_stream_t stream) {
+  if (!m || !rhs || !phi) return fail(HFM_ERR_BAD_ARG, "hfm_mg_solve: bad argument");
+  const int64_t nf = (int64_t)m->Z * m->Y * m->X;
+  int st;
+  for (int s = 0; s < m->slots; ++s)
+    if ((st = hfm_mg_load(m, s, rhs + s * nf, nullptr, stream))) return st;
+  std::vector<hfm_slot_stats> tmp(m->slots);
+  hfm_slot_stats *ss = stats_host ? stats_host : tmp.data();
+  const int per = m->cfg.cycles_per_launch;
+  for (int done = 0; done <= m->cfg.max_cycles + per; done += per) {
+    if ((st = hfm_mg_run(m, per, stream))) return st;
+    if ((st = hfm_mg_query(m, ss, stream))) return st;
+    bool any = false;
+    for (int s = 0; s < m->slots; ++s) any |= ss[s].active != 0;
+    if (!any) break;
+  }
+  for (int s = 0; s < m->slots; ++s)
+    if ((st = hfm_mg_fetch(m, s, phi + s * nf, stream))) return st;
+  HFM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  int worst = HFM_OK;
+  for (int s = 0; s < m->slots; ++s)
+    if (ss[s].status != HFM_OK) worst = ss[s].status;
+  return worst;
+}
+
+}  // extern "C"

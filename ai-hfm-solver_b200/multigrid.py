@@ -1,0 +1,175 @@
+"""Multigrid solver handle over ``libhfm`` (``hfm_mg_*``).
+
+``SolverConfig`` holds the knobs the reference keeps as module-level constants
+(``multi_itr``, ``j_itr``, the level list and the Jacobi diagonal,
+``Anisotropic_3d_Multigrid_7point.ipynb:402-405``) plus the textbook cycle parameters of the
+solver configurations.  ``Multigrid`` owns the resident hierarchy of ``slots`` same-size
+instances; slots are loaded, advanced together by CUDA graphs of whole cycles, polled and
+fetched independently, which is what the serving layer builds on.
+"""
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .ops import Operator, _check_field, _stream
+
+_CYCLES = {"sawtooth": L.CYCLE_SAWTOOTH, "V": L.CYCLE_V, "F": L.CYCLE_F}
+_ACCEL = {None: L.ACCEL_NONE, "none": L.ACCEL_NONE, "cg": L.ACCEL_CG}
+_STORAGE = {"f32": L.F32, "bf16": L.BF16, "f16": L.F16}
+
+
+@dataclass
+class SolverConfig:
+    cycle: str = "V"            # "sawtooth" (reference), "V" or "F"
+    accel: str = "none"         # "none" (stationary cycles) or "cg" (cycle preconditions CG)
+    n_levels: int = 0           # 0: halve while every extent is even and > min_coarse_edge
+    min_coarse_edge: int = 4
+    nu_pre: int = 2
+    nu_post: int = 2
+    coarse_sweeps: int = 32
+    omega: float = 2.0 / 3.0
+    coarse_omega: float = 2.0 / 3.0
+    coarse_scale: float = 0.5   # operator on level l scaled by coarse_scale**l (1 = reference)
+    sawtooth_fine_smooth: bool = True
+    top_copy: bool = False      # boundary_condition_top after each reference cycle
+    zero_xend: bool = False     # NS pressure form: r and phi zero on x = X-1
+    storage: str = "f32"
+    tol: float = 1e-6
+    max_cycles: int = 500
+    cycles_per_launch: int = 4
+
+    @staticmethod
+    def reference(n_levels, fine_smooth=True, top_copy=False, zero_xend=False, cycles=1000):
+        """The reference sawtooth cycle: omega 1, one Jacobi per level, same operator on every
+        level (``Anisotropic_3d_Multigrid_7point.ipynb:402-449``)."""
+        return SolverConfig(cycle="sawtooth", n_levels=n_levels, nu_pre=0, nu_post=1,
+                            omega=1.0, coarse_omega=1.0, coarse_scale=1.0,
+                            sawtooth_fine_smooth=fine_smooth, top_copy=top_copy,
+                            zero_xend=zero_xend, tol=1e-300, max_cycles=cycles,
+                            cycles_per_launch=2)
+
+    def struct(self, op_kind):
+        c = L.HfmMgConfig()
+        L.lib().hfm_mg_config_default(C.byref(c))
+        c.op_kind = op_kind
+        c.cycle = _CYCLES[self.cycle]
+        c.accel = _ACCEL[self.accel]
+        c.n_levels = self.n_levels
+        c.min_coarse_edge = self.min_coarse_edge
+        c.nu_pre, c.nu_post = self.nu_pre, self.nu_post
+        c.coarse_sweeps = self.coarse_sweeps
+        c.omega, c.coarse_omega = self.omega, self.coarse_omega
+        c.coarse_scale = self.coarse_scale
+        c.sawtooth_fine_smooth = int(self.sawtooth_fine_smooth)
+        c.flags = (L.FLAG_TOP_COPY if self.top_copy else 0) | (L.FLAG_ZERO_XEND if self.zero_xend else 0)
+        c.storage = _STORAGE[self.storage]
+        c.tol = self.tol
+        c.max_cycles = self.max_cycles
+        c.cycles_per_launch = self.cycles_per_launch
+        return c
+
+
+def footprint_bytes(cfg, op_kind, shape, slots):
+    s = cfg.struct(op_kind)
+    return int(L.lib().hfm_mg_footprint_bytes(C.byref(s), shape[0], shape[1], shape[2], slots))
+
+
+class Multigrid:
+    """Resident multigrid hierarchy for ``slots`` instances of extent ``shape`` (Z, Y, X)."""
+
+    def __init__(self, shape, op_kind, cfg=None, slots=1):
+        self.cfg = cfg or SolverConfig()
+        self.shape = tuple(int(v) for v in shape)
+        self.slots = int(slots)
+        self.op_kind = op_kind
+        self._s = self.cfg.struct(op_kind)
+        h = C.c_void_p()
+        Z, Y, X = self.shape
+        L.call("hfm_mg_create", C.byref(self._s), Z, Y, X, self.slots, C.byref(h))
+        self._h = h
+        self._stats = (L.HfmSlotStats * self.slots)()
+
+    # ------------------------------------------------------------------ lifetime
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            torch.cuda.synchronize()
+            L.lib().hfm_mg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------ queries
+    @property
+    def levels(self):
+        out = []
+        for l in range(L.lib().hfm_mg_num_levels(self._h)):
+            z, y, x = C.c_int(), C.c_int(), C.c_int()
+            L.call("hfm_mg_level_shape", self._h, l, C.byref(z), C.byref(y), C.byref(x))
+            out.append((z.value, y.value, x.value))
+        return out
+
+    # ------------------------------------------------------------------ slots
+    def set_operator(self, op, slot=-1):
+        """Install the fine operator (and its coefficient hierarchy) for ``slot`` (-1: all;
+        SIGMA7 coefficient tensors then hold every slot, ``(slots, Z, Y, X)``)."""
+        if not isinstance(op, Operator):
+            raise TypeError("op must be an ops.Operator")
+        s = op.struct()
+        self._op_keep = op
+        L.call("hfm_mg_set_operator", self._h, int(slot), C.byref(s), _stream())
+
+    def load(self, slot, rhs, phi0=None):
+        _check_field(rhs, "rhs")
+        if phi0 is not None:
+            _check_field(phi0, "phi0")
+        L.call("hfm_mg_load", self._h, int(slot), C.c_void_p(rhs.data_ptr()),
+               C.c_void_p(phi0.data_ptr() if phi0 is not None else 0), _stream())
+
+    def run(self, cycles):
+        L.call("hfm_mg_run", self._h, int(cycles), _stream())
+
+    def query(self):
+        L.call("hfm_mg_query", self._h, self._stats, _stream())
+        return [dict(active=s.active, status=s.status, cycles=s.cycles, norm_b=s.norm_b,
+                     rel_resid=s.rel_resid) for s in self._stats]
+
+    def fetch(self, slot, out=None):
+        out = torch.empty(self.shape, dtype=torch.float32, device="cuda") if out is None else out
+        L.call("hfm_mg_fetch", self._h, int(slot), C.c_void_p(out.data_ptr()), _stream())
+        return out
+
+    def cancel(self, slot):
+        L.call("hfm_mg_cancel", self._h, int(slot), _stream())
+
+    def read_level(self, slot, level, which):
+        shp = self.levels[level]
+        out = torch.empty(shp, dtype=torch.float32, device="cuda")
+        L.call("hfm_mg_read_level", self._h, int(slot), int(level), int(which),
+               C.c_void_p(out.data_ptr()), _stream())
+        return out
+
+    def solve(self, rhs):
+        """Solve every slot for ``rhs`` of shape ``(slots, Z, Y, X)``; returns (phi, stats).
+        A slot that does not reach tolerance keeps its status in stats (no exception)."""
+        _check_field(rhs, "rhs")
+        phi = torch.empty_like(rhs)
+        st = L.lib().hfm_mg_solve(self._h, C.c_void_p(rhs.data_ptr()), C.c_void_p(phi.data_ptr()),
+                                  self._stats, _stream())
+        if st not in (L.OK, L.ERR_NOT_CONVERGED, L.ERR_NAN):
+            L.check(st, "hfm_mg_solve")
+        stats = [dict(active=s.active, status=s.status, cycles=s.cycles, norm_b=s.norm_b,
+                      rel_resid=s.rel_resid) for s in self._stats]
+        return phi, stats

@@ -1,0 +1,244 @@
+/*
+ * hfm.h - C ABI of libhfm, the B200 (sm_100a) stencil + geometric-multigrid library that
+ * replaces the frozen-weight TensorFlow layers and the Python multigrid loops of
+ * bc1chen/AI-HFM-Solver ("AI4CFD").
+ *
+ * Conventions shared by every entry point
+ *   - Fields are float32 (unless stated) in C order [B][Z][Y][X], X fastest: the reference
+ *     tensor (1, Z, Y, X, 1) with the batch of B independent instances stacked in front.
+ *     All pointers are device pointers unless the name says "host".
+ *   - A 3x3x3 kernel w27 is indexed (dz, dy, dx) row-major, w27[9*a + 3*b + c] applying to
+ *     phi[z+a-1][y+b-1][x+c-1] (cross-correlation, like TF Conv3D).  Samples outside the
+ *     grid are zero (TF 'SAME' zero padding = homogeneous Dirichlet ghost cells).
+ *   - Residual sign follows the reference: r = A phi - b, and corrections are subtracted.
+ *   - Every call returns an hfm_status; hfm_last_error() gives a message for the calling
+ *     thread.  Calls enqueue work on `stream` (a cudaStream_t) and return without
+ *     synchronising, unless documented otherwise.  No stateless call allocates memory.
+ */
+#ifndef HFM_H_
+#define HFM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HFM_ABI_VERSION 1
+
+typedef void *hfm_stream_t; /* cudaStream_t */
+
+typedef enum {
+  HFM_OK = 0,
+  HFM_ERR_BAD_ARG = 1,       /* malformed shape, null pointer, unsupported combination */
+  HFM_ERR_OOM = 2,           /* device allocation failed (handles only) */
+  HFM_ERR_NOT_CONVERGED = 3, /* max_cycles reached above tolerance (the reference's guard) */
+  HFM_ERR_NAN = 4,           /* NaN/Inf found in a residual norm */
+  HFM_ERR_TIMEOUT = 5,       /* a bounded device-side wait expired */
+  HFM_ERR_CUDA = 6,          /* CUDA runtime error (message in hfm_last_error) */
+  HFM_ERR_UNSUPPORTED = 7
+} hfm_status;
+
+typedef enum { HFM_F32 = 0, HFM_BF16 = 1, HFM_F16 = 2, HFM_F64 = 3 } hfm_dtype;
+
+/* Operator kinds. */
+typedef enum {
+  HFM_OP_CONST7 = 0, /* anisotropic 7-point, constant coefficients kz, ky, kx (7point.ipynb w2) */
+  HFM_OP_SIGMA7 = 1, /* 7-point from per-cell conductivities sx, sy, sz (face means) */
+  HFM_OP_DIR7 = 2,   /* six per-cell directional coefficient arrays + diagonal (BGS form) */
+  HFM_OP_K27 = 3     /* arbitrary frozen 3x3x3 kernel (27-point pressure / diffusion) */
+} hfm_op_kind;
+
+/* Flags for residual / smoothing calls. */
+#define HFM_FLAG_ZERO_XEND 1u  /* NS pressure form: residual / corrected phi zero on plane x = X-1 */
+#define HFM_FLAG_TOP_COPY 2u   /* after smoothing copy plane z = 1 onto z = 0 (boundary_condition_top) */
+#define HFM_FLAG_ZERO_GUESS 4u /* the input phi is identically zero (not read) */
+
+/* Operator descriptor (plain data, copied by value into each launch).
+ *   CONST7: k[0..2] = (kz, ky, kx) = (Dz/dz^2, Dy/dy^2, Dx/dx^2); diagonal 2(kz+ky+kx).
+ *   SIGMA7: coef[0..2] = sx, sy, sz ([B][Z][Y][X] each); c[0..2] = (cz, cy, cx) = 1/h^2.
+ *           Face coefficient between cells i, j on axis d: c_d (s_i + s_j)/2; a wall face
+ *           uses c_d s_i.  (Anisotropic Resistivity Tomography/README:14-26)
+ *   DIR7:   coef[0..6] = A_xm, A_xp, A_ym, A_yp, A_zm, A_zp, A_tot (BGS_multigrid_v1 cell 38),
+ *           (A phi)_c = sum_d A_d (phi_c - phi_nb(d)), diagonal A_tot.
+ *   K27:    k[0..26] = w27; Jacobi diagonal = k[13].
+ *   scale multiplies the operator (1 = reference; coarse levels of a handle use
+ *   coarse_scale^level).  coef_dtype is the storage type of coef arrays (HFM_F32 for the
+ *   stateless calls). */
+typedef struct {
+  int kind;
+  int coef_dtype;
+  float k[27];
+  float c[3];
+  float scale;
+  const void *coef[7];
+} hfm_operator;
+
+/* ---------------------------------------------------------------- library information */
+int hfm_abi_version(void);
+const char *hfm_status_string(int status);
+const char *hfm_last_error(void);
+int hfm_device_sm_count(int *sm_count); /* current device's SM count */
+/* Kernels this library has enqueued since load (a CUDA-graph launch counts its kernel nodes). */
+int64_t hfm_kernel_launch_count(void);
+
+/* ------------------------------------------------ stateless operators (drop-in layers) */
+/* Conv3D(1, kernel_size=3, strides=1, padding='SAME') with frozen weights and zero bias:
+ * replaces every `keras.models.Sequential([... Conv3D(k=3, 'SAME')])` callable, e.g.
+ * CNN3D_A_<n> (Anisotropic_3d_Multigrid_7point.ipynb cell 7, lines 124-183),
+ * CNN3D_central_2nd_{dif,xadv,yadv,zadv}, CNN3D_{Su,Sv,Sw,pu,pv,pw} (naiver_stokes_3D.py:166-236). */
+int hfm_conv3d_k3(const float *x, float *y, int B, int Z, int Y, int X, const float *w27_host,
+                  hfm_stream_t stream);
+
+/* Conv3D(1, kernel_size=2, strides=2, padding='VALID') with weights 0.125 = CNN3D_res_<n>
+ * (Anisotropic_3d_Multigrid_7point.ipynb cell 9, lines 194-240).  Output extent floor(n/2). */
+int hfm_restrict_avg(const float *fine, float *coarse, int B, int Z, int Y, int X,
+                     hfm_stream_t stream);
+
+/* UpSampling3D(size=(2,2,2)) = CNN3D_prol_<n> (Anisotropic_3d_Multigrid_7point.ipynb cell 11,
+ * lines 251-289).  (Zc, Yc, Xc) are the coarse extents; the fine output is twice each. */
+int hfm_prolong_nearest(const float *coarse, float *fine, int B, int Zc, int Yc, int Xc,
+                        hfm_stream_t stream);
+
+/* out = A phi (operator descriptor form): CNN3D_A_<n>(phi) / A_operator_<n>(phi)
+ * (BGS_multigrid_v1.ipynb cell 40). */
+int hfm_op_apply(const hfm_operator *op, const float *phi, float *out, int B, int Z, int Y,
+                 int X, hfm_stream_t stream);
+
+/* r = A phi - b (Anisotropic_3d_Multigrid_7point.ipynb:409; naiver_stokes_3D.py:649-651 with
+ * HFM_FLAG_ZERO_XEND). */
+int hfm_op_residual(const hfm_operator *op, const float *phi, const float *b, float *r, int B,
+                    int Z, int Y, int X, unsigned flags, hfm_stream_t stream);
+
+/* `sweeps` weighted-Jacobi sweeps phi <- phi + omega (rhs - A phi) / diag
+ * (reference form w - A(w)/d + r/d with omega = 1, 7point.ipynb:424-449).  The result is in
+ * `out`; for sweeps > 1 the sweeps ping-pong between `out` and `tmp` (caller memory, same
+ * size; may be NULL when sweeps == 1).  phi may alias neither out nor tmp. */
+int hfm_op_jacobi(const hfm_operator *op, const float *phi, const float *rhs, float *out,
+                  float *tmp, int B, int Z, int Y, int X, float omega, int sweeps,
+                  unsigned flags, hfm_stream_t stream);
+
+/* Fused residual + restriction: r_coarse = R (A phi - b) on the even grid (Z, Y, X), and
+ * r_fine = A phi - b when r_fine is not NULL (7point.ipynb:409-419). */
+int hfm_residual_restrict(const hfm_operator *op, const float *phi, const float *b,
+                          float *r_fine, float *r_coarse, int B, int Z, int Y, int X,
+                          unsigned flags, hfm_stream_t stream);
+
+/* Fused prolongation + correction + one smoothing sweep:
+ * out = J(phi - P w_coarse) against rhs (7point.ipynb:443-449; phi may be NULL = zero, which
+ * gives the sawtooth "w_n = prol(w); Jacobi" step). (Z, Y, X) are the fine extents. */
+int hfm_prolong_correct_smooth(const hfm_operator *op, const float *phi,
+                               const float *w_coarse, const float *rhs, float *out, int B,
+                               int Z, int Y, int X, float omega, unsigned flags,
+                               hfm_stream_t stream);
+
+/* Named wrappers: constant-coefficient 7-point (A1), per-cell sigma 7-point
+ * (A2) and 27-point (B1-B4) forms of apply / residual / jacobi. */
+int hfm_stencil7_const_apply(const float *phi, float *out, int B, int Z, int Y, int X,
+                             float kz, float ky, float kx, hfm_stream_t stream);
+int hfm_stencil7_const_residual(const float *phi, const float *b, float *r, int B, int Z,
+                                int Y, int X, float kz, float ky, float kx, unsigned flags,
+                                hfm_stream_t stream);
+int hfm_stencil7_const_jacobi(const float *phi, const float *rhs, float *out, float *tmp,
+                              int B, int Z, int Y, int X, float kz, float ky, float kx,
+                              float omega, int sweeps, unsigned flags, hfm_stream_t stream);
+int hfm_stencil7_var_apply(const float *phi, float *out, const float *sx, const float *sy,
+                           const float *sz, int B, int Z, int Y, int X, float cz, float cy,
+                           float cx, hfm_stream_t stream);
+int hfm_stencil7_var_residual(const float *phi, const float *b, float *r, const float *sx,
+                              const float *sy, const float *sz, int B, int Z, int Y, int X,
+                              float cz, float cy, float cx, unsigned flags,
+                              hfm_stream_t stream);
+int hfm_stencil7_var_jacobi(const float *phi, const float *rhs, float *out, float *tmp,
+                            const float *sx, const float *sy, const float *sz, int B, int Z,
+                            int Y, int X, float cz, float cy, float cx, float omega,
+                            int sweeps, unsigned flags, hfm_stream_t stream);
+int hfm_stencil27_apply(const float *phi, float *out, int B, int Z, int Y, int X,
+                        const float *w27_host, hfm_stream_t stream);
+int hfm_stencil27_residual(const float *phi, const float *b, float *r, int B, int Z, int Y,
+                           int X, const float *w27_host, unsigned flags, hfm_stream_t stream);
+int hfm_stencil27_jacobi(const float *phi, const float *rhs, float *out, float *tmp, int B,
+                         int Z, int Y, int X, const float *w27_host, float omega, int sweeps,
+                         unsigned flags, hfm_stream_t stream);
+
+/* ------------------------------------------------------------------------ reductions */
+/* Per-instance reductions over n elements of each of B instances (HFM3 diagnostics
+ * np.max(w), np.max(r): Urban Modelling/AI_HFM_v3.ipynb:2622-2627).  Results land in device
+ * memory (B values).  `scratch` is caller device memory of hfm_reduce_scratch_bytes(n, B)
+ * bytes; the summation order is fixed, so results do not depend on other work in flight. */
+size_t hfm_reduce_scratch_bytes(int64_t n, int B);
+int hfm_norm2_f64(const float *x, int64_t n, int B, double *out, void *scratch,
+                  hfm_stream_t stream); /* sqrt(sum x^2), accumulated in float64 */
+int hfm_max_abs(const float *x, int64_t n, int B, float *out, void *scratch,
+                hfm_stream_t stream);
+
+/* ------------------------------------------------------------------ multigrid handle */
+typedef enum { HFM_CYCLE_SAWTOOTH = 0, HFM_CYCLE_V = 1, HFM_CYCLE_F = 2 } hfm_cycle;
+typedef enum { HFM_ACCEL_NONE = 0, HFM_ACCEL_CG = 1 } hfm_accel;
+
+typedef struct {
+  int op_kind;            /* hfm_op_kind: CONST7, SIGMA7, K27 (DIR7 via stateless calls) */
+  int cycle;              /* hfm_cycle */
+  int accel;              /* hfm_accel: NONE = stationary cycles, CG = cycle preconditions CG */
+  int n_levels;           /* 0 = automatic (halve while extents even and min > min_coarse_edge) */
+  int min_coarse_edge;    /* default 4 */
+  int nu_pre, nu_post;    /* V/F smoothing sweeps (default 2, 2) */
+  int coarse_sweeps;      /* Jacobi sweeps on the coarsest level (V/F; sawtooth uses 1) */
+  float omega;            /* smoother weight (default 2/3; sawtooth reference 1) */
+  float coarse_omega;
+  float coarse_scale;     /* level l operator scaled by coarse_scale^l (1 = reference) */
+  int sawtooth_fine_smooth; /* 1: Jacobi on w at the fine level (7point), 0: NS form */
+  unsigned flags;         /* HFM_FLAG_TOP_COPY / HFM_FLAG_ZERO_XEND applied as the reference does */
+  int storage;            /* hfm_dtype of inner fields and coefficients: F32, BF16, F16 */
+  double tol;             /* relative residual ||b - A phi|| / ||b|| (default 1e-6) */
+  int max_cycles;         /* NOT_CONVERGED after this many cycles / CG iterations */
+  int cycles_per_launch;  /* cycles captured in one CUDA graph between host checks (default 4) */
+} hfm_mg_config;
+
+typedef struct {
+  int active;       /* 1 while the slot is still iterating */
+  int status;       /* hfm_status of the finished solve */
+  int cycles;       /* cycles (or CG iterations) done */
+  int reserved;
+  double norm_b;    /* ||b||_2 */
+  double rel_resid; /* last ||b - A phi|| / ||b|| */
+} hfm_slot_stats;
+
+typedef struct hfm_mg hfm_mg;
+
+void hfm_mg_config_default(hfm_mg_config *cfg);
+/* Device bytes a handle of this configuration holds (admission control). */
+size_t hfm_mg_footprint_bytes(const hfm_mg_config *cfg, int Z, int Y, int X, int slots);
+int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_mg **out);
+int hfm_mg_destroy(hfm_mg *mg);
+int hfm_mg_num_levels(const hfm_mg *mg);
+int hfm_mg_level_shape(const hfm_mg *mg, int level, int *Z, int *Y, int *X);
+
+/* Install the fine operator for one slot (slot = -1: every slot) and build the coefficient
+ * hierarchy by the reference restriction (BGS_multigrid_v1.ipynb cell 38, lines 16-33).
+ * SIGMA7 coefficient arrays hold one instance each ([Z][Y][X]); they are copied. */
+int hfm_mg_set_operator(hfm_mg *mg, int slot, const hfm_operator *op, hfm_stream_t stream);
+/* Copy rhs (and phi0, NULL = zero) into a slot, compute ||b|| and mark it active. */
+int hfm_mg_load(hfm_mg *mg, int slot, const float *rhs, const float *phi0, hfm_stream_t stream);
+/* Advance every active slot by `cycles` cycles (CUDA graph; slots that converge, fail or
+ * hit max_cycles stop on the device and do no more work). */
+int hfm_mg_run(hfm_mg *mg, int cycles, hfm_stream_t stream);
+/* Copy per-slot statistics to host memory (synchronises `stream`). */
+int hfm_mg_query(hfm_mg *mg, hfm_slot_stats *stats_host, hfm_stream_t stream);
+/* Copy a slot's current solution into phi_out (device, [Z][Y][X] float32). */
+int hfm_mg_fetch(hfm_mg *mg, int slot, float *phi_out, hfm_stream_t stream);
+/* Stop a slot (request cancelled); its memory can be reloaded at once. */
+int hfm_mg_cancel(hfm_mg *mg, int slot, hfm_stream_t stream);
+/* Convenience: load all slots from rhs/phi ([slots][Z][Y][X]), run to completion, fetch the
+ * solutions into phi, fill stats_host (may be NULL).  Synchronises `stream`. */
+int hfm_mg_solve(hfm_mg *mg, const float *rhs, float *phi, hfm_slot_stats *stats_host,
+                 hfm_stream_t stream);
+/* Read an internal level buffer of a slot (0 = phi / w, 1 = rhs / r) for per-level checks. */
+int hfm_mg_read_level(hfm_mg *mg, int slot, int level, int which, float *out,
+                      hfm_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HFM_H_ */

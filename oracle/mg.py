@@ -1,0 +1,345 @@
+"""Multigrid oracle: discrete operators, Jacobi, and the reference / textbook cycles.
+
+Sign convention (the reference's, ``Anisotropic_3d_Multigrid_7point.ipynb:409,448``): the
+residual is ``r = A phi - b``, the coarse problems solve ``A w = r`` and the correction is
+``phi -= P w``.  Every function works on arrays shaped ``(..., Z, Y, X)``; ``dtype`` selects
+float32 (the reference's arithmetic) or float64 (the "FP64 oracle of the same discrete
+operators").
+"""
+import numpy as np
+
+from . import tfops
+from . import weights as W
+
+
+# --------------------------------------------------------------------------------------
+# Operators.  Each exposes apply(x), diag (scalar or array) and coarsen() -> next level.
+# --------------------------------------------------------------------------------------
+class Stencil27:
+    """A frozen 3x3x3 Conv3D used as a matrix (``CNN3D_A_<n>``,
+    ``Anisotropic_3d_Multigrid_7point.ipynb`` cell 7; ``naiver_stokes_3D.py:239-307``).
+    The Jacobi diagonal is the centre weight ``w[0,1,1,1,0]`` (``7point.ipynb:424``).
+    The reference uses the same weights on every level (no coarse rescaling); ``scale``
+    multiplies the whole operator (1 reproduces the reference)."""
+
+    def __init__(self, K, scale=1.0, dtype=np.float32):
+        self.dtype = dtype
+        self.K = np.asarray(K, dtype=np.float64).reshape(3, 3, 3) * scale
+        self.diag = dtype(self.K[1, 1, 1])
+
+    def apply(self, x):
+        return tfops.conv3d_same(x, self.K, self.dtype)
+
+    def coarsen(self, coarse_scale=1.0):
+        return Stencil27(self.K * coarse_scale, 1.0, self.dtype)
+
+
+def const7(kz, ky, kx, scale=1.0, dtype=np.float32):
+    """Constant-coefficient anisotropic 7-point operator with ``kz = Dz/dz**2`` etc.: the
+    reference ``w2`` (``Anisotropic_3d_Multigrid_7point.ipynb:75-90``)."""
+    return Stencil27(W.w2_7point(Dx=kx, Dy=ky, Dz=kz), scale, dtype)
+
+
+class Sigma7:
+    """Variable-coefficient 7-point operator from per-cell conductivities (sx, sy, sz).
+
+    ``(A phi)_c = sum_d a_d(c) (phi_c - phi_nb(d))`` over the six neighbours, the operator
+    form of ``BGS_multigrid_v1.ipynb`` cell 40 (directional differences times coefficients).
+    Face coefficients follow the README face formula (``Anisotropic Resistivity
+    Tomography/README:14-26``) with uniform spacing: ``a = cx * (sx_c + sx_nb) / 2``; at a
+    wall the ghost conductivity equals the interior one (``a = cx * sx_c``) and the ghost
+    potential is zero (SAME zero padding).  The diagonal is the sum of the six faces
+    (``A_MAT_TOT``, ``BGS_multigrid_v1.ipynb`` cell 38).  Coarse levels average the
+    conductivities with the reference restriction (cell 38, lines 16-33), with no
+    rescaling unless ``coarse_scale != 1``.
+    """
+
+    def __init__(self, sx, sy, sz, c=(1.0, 1.0, 1.0), scale=1.0, dtype=np.float32):
+        self.dtype = dtype
+        self.s = [np.asarray(a, dtype=dtype) for a in (sx, sy, sz)]
+        self.c = tuple(float(v) for v in c)  # (cz, cy, cx) multipliers 1/h^2, as the C ABI
+        self.scale = float(scale)
+        self._faces()
+
+    def _faces(self):
+        dt = self.dtype
+        sx, sy, sz = self.s
+        cz, cy, cx = (dt(v * self.scale) for v in self.c)
+        half = dt(0.5)
+        faces = []
+        for arr, ax, cc in ((sx, -1, cx), (sy, -2, cy), (sz, -3, cz)):
+            lo = arr.copy()
+            hi = arr.copy()
+            n = arr.shape[ax]
+            if n > 1:
+                a = [slice(None)] * arr.ndim
+                b = [slice(None)] * arr.ndim
+                a[ax] = slice(1, None)
+                b[ax] = slice(None, -1)
+                lo[tuple(a)] = half * (arr[tuple(a)] + arr[tuple(b)])
+                hi[tuple(b)] = half * (arr[tuple(b)] + arr[tuple(a)])
+            faces.append((cc * lo, cc * hi))
+        self.faces = faces  # [(x-, x+), (y-, y+), (z-, z+)]
+        d = np.zeros_like(sx)
+        for lo, hi in faces:
+            d = d + lo + hi
+        self.diag = d
+
+    def apply(self, x):
+        x = np.asarray(x, dtype=self.dtype)
+        Z, Y, X = x.shape[-3:]
+        pad = [(0, 0)] * (x.ndim - 3) + [(1, 1)] * 3
+        xp = np.pad(x, pad)
+        c = xp[..., 1:Z + 1, 1:Y + 1, 1:X + 1]
+        nb = {
+            (0, 0): xp[..., 1:Z + 1, 1:Y + 1, 0:X],
+            (0, 1): xp[..., 1:Z + 1, 1:Y + 1, 2:X + 2],
+            (1, 0): xp[..., 1:Z + 1, 0:Y, 1:X + 1],
+            (1, 1): xp[..., 1:Z + 1, 2:Y + 2, 1:X + 1],
+            (2, 0): xp[..., 0:Z, 1:Y + 1, 1:X + 1],
+            (2, 1): xp[..., 2:Z + 2, 1:Y + 1, 1:X + 1],
+        }
+        out = np.zeros_like(x)
+        for axis, (lo, hi) in enumerate(self.faces):
+            out = out + lo * (c - nb[(axis, 0)]) + hi * (c - nb[(axis, 1)])
+        return out
+
+    def coarsen(self, coarse_scale=1.0):
+        s = [tfops.restrict_avg(a, self.dtype) for a in self.s]
+        return Sigma7(*s, c=self.c, scale=self.scale * coarse_scale, dtype=self.dtype)
+
+
+class Dir7:
+    """The reference's variable-coefficient form verbatim: six per-cell coefficient arrays
+    ``A_MAT_{xm1,xp1,ym1,yp1,zm1,zp1}`` and their sum ``A_MAT_TOT``
+    (``BGS_multigrid_v1.ipynb`` cells 38 and 40).  ``apply`` evaluates
+    ``sum_d conv_d(v) * A_d`` in the reference's order (cell 40); ``coarsen`` restricts all
+    seven arrays with the averaging conv (cell 38, lines 16-33)."""
+
+    ORDER = ("xm", "xp", "ym", "yp", "zm", "zp")
+
+    def __init__(self, coeffs, tot=None, dtype=np.float32):
+        self.dtype = dtype
+        self.A = [np.asarray(coeffs[k], dtype=dtype) for k in self.ORDER]
+        if tot is None:
+            tot = self.A[0] + self.A[2] + self.A[4] + self.A[1] + self.A[3] + self.A[5]
+        self.diag = np.asarray(tot, dtype=dtype)
+        self._K = W.directional_kernels()
+
+    def apply(self, x):
+        k = self._K
+        A = self.A
+        c = lambda i: tfops.conv3d_same(x, k[i], self.dtype)
+        return (c(0) * A[0] + c(1) * A[1] + c(2) * A[2] + c(3) * A[3]
+                + c(4) * A[4] + c(5) * A[5])
+
+    def coarsen(self, coarse_scale=1.0):
+        d = {k: tfops.restrict_avg(a, self.dtype) * self.dtype(coarse_scale)
+             for k, a in zip(self.ORDER, self.A)}
+        return Dir7(d, tfops.restrict_avg(self.diag, self.dtype) * self.dtype(coarse_scale),
+                    self.dtype)
+
+
+def bgs_coefficients(D, mesh_x, mesh_y, mesh_z, mesh_x_p1, mesh_y_p1, mesh_z_p1):
+    """``A_MAT_* = D / mesh**2`` (``BGS_multigrid_v1.ipynb`` cell 38, lines 5-11)."""
+    return {
+        "xm": D / mesh_x ** 2, "ym": D / mesh_y ** 2, "zm": D / mesh_z ** 2,
+        "xp": D / mesh_x_p1 ** 2, "yp": D / mesh_y_p1 ** 2, "zp": D / mesh_z_p1 ** 2,
+    }
+
+
+def hierarchy(op0, n_levels, coarse_scale=1.0):
+    ops = [op0]
+    for _ in range(n_levels - 1):
+        ops.append(ops[-1].coarsen(coarse_scale))
+    return ops
+
+
+def level_shapes(shape, min_edge=4, max_levels=32):
+    """Coarsening rule for the solver configurations: halve while every extent is even and
+    the smallest extent exceeds ``min_edge`` (the reference's VALID restriction floors odd
+    extents, which would break the prolongation shape, so odd grids stop coarsening)."""
+    shapes = [tuple(shape)]
+    while len(shapes) < max_levels:
+        z, y, x = shapes[-1]
+        if z % 2 or y % 2 or x % 2 or min(z, y, x) <= min_edge:
+            break
+        shapes.append((z // 2, y // 2, x // 2))
+    return shapes
+
+
+# --------------------------------------------------------------------------------------
+# Jacobi and residual
+# --------------------------------------------------------------------------------------
+def jacobi_ref(op, w, r):
+    """One reference Jacobi sweep ``w - A(w)/d + r/d`` in the reference's operation order
+    (``Anisotropic_3d_Multigrid_7point.ipynb:424``; ``BGS_multigrid_v1.ipynb`` cell 42)."""
+    dt = op.dtype
+    d = op.diag
+    return (np.asarray(w, dt) - op.apply(w) / d) + np.asarray(r, dt) / d
+
+
+def jacobi(op, w, r, omega=1.0):
+    """Weighted Jacobi ``w + omega (r - A w) / d``; equals ``jacobi_ref`` for omega = 1 up to
+    rounding."""
+    dt = op.dtype
+    w = np.asarray(w, dt)
+    return w + dt(omega) * (np.asarray(r, dt) - op.apply(w)) / op.diag
+
+
+def residual(op, phi, b):
+    """``r = A phi - b`` (``Anisotropic_3d_Multigrid_7point.ipynb:409``)."""
+    return op.apply(phi) - np.asarray(b, op.dtype)
+
+
+# --------------------------------------------------------------------------------------
+# Reference sawtooth cycle (8(a) A8)
+# --------------------------------------------------------------------------------------
+def sawtooth_cycle(ops, phi, b, fine_smooth=True, zero_xend=False, top_copy=False,
+                   coarse_zero_shape=None, keep=None):
+    """One cycle of the reference multigrid (``Anisotropic_3d_Multigrid_7point.ipynb:
+    406-449``; ``BGS_multigrid_v1.ipynb`` cell 42; pressure form ``naiver_stokes_3D.py:
+    646-703``).
+
+    1. ``r = A phi - b`` (NS form: ``r[..., X-1] = 0``);
+    2. restrict ``r`` level by level down to ``ops[-1]``;
+    3. coarsest: ``w = 0`` then one Jacobi against its residual;
+    4. every finer coarse level: ``w = P w`` then one Jacobi;
+    5. fine: ``w = P w`` then (unless ``fine_smooth`` is False, the NS form) one Jacobi
+       against ``r``;
+    6. ``phi = phi - w`` (NS: ``phi[..., X-1] = 0``), one Jacobi of ``phi`` against ``b``;
+       ``top_copy`` applies ``boundary_condition_top`` (``phi[0] = phi[1]``,
+       ``Anisotropic_3d_Multigrid_7point_BC.ipynb:340-344,470``).
+
+    ``keep`` (a dict) receives the per-level residuals and corrections for per-level
+    comparisons.
+    """
+    dt = ops[0].dtype
+    L = len(ops)
+    r = residual(ops[0], phi, b)
+    if zero_xend:
+        r[..., -1] = 0
+    rs = [r]
+    for l in range(1, L):
+        rs.append(tfops.restrict_avg(rs[-1], dt))
+    w = np.zeros_like(rs[-1])
+    w = jacobi_ref(ops[-1], w, rs[-1])
+    ws = {L - 1: w}
+    for l in range(L - 2, 0, -1):
+        w = tfops.prolong_nearest(w, dt)
+        w = jacobi_ref(ops[l], w, rs[l])
+        ws[l] = w
+    w = tfops.prolong_nearest(w, dt)
+    if fine_smooth:
+        w = jacobi_ref(ops[0], w, rs[0])
+    ws[0] = w
+    phi = np.asarray(phi, dt) - w
+    if zero_xend:
+        phi[..., -1] = 0
+    phi = jacobi_ref(ops[0], phi, b)
+    if top_copy:
+        phi[..., 0, :, :] = phi[..., 1, :, :]
+    if keep is not None:
+        keep["r"] = rs
+        keep["w"] = ws
+    return phi
+
+
+# --------------------------------------------------------------------------------------
+# Textbook cycles used by the solver configurations (8(a) A9)
+# --------------------------------------------------------------------------------------
+class CycleConfig:
+    def __init__(self, nu_pre=2, nu_post=2, omega=2.0 / 3.0, coarse_sweeps=32,
+                 coarse_omega=None):
+        self.nu_pre = nu_pre
+        self.nu_post = nu_post
+        self.omega = omega
+        self.coarse_sweeps = coarse_sweeps
+        self.coarse_omega = omega if coarse_omega is None else coarse_omega
+
+
+def _coarse_solve(op, f, cfg):
+    w = np.zeros_like(np.asarray(f, op.dtype))
+    for _ in range(cfg.coarse_sweeps):
+        w = jacobi(op, w, f, cfg.coarse_omega)
+    return w
+
+
+def vcycle(ops, l, phi, f, cfg):
+    """V(nu_pre, nu_post) cycle on level ``l`` for ``A_l phi = f``."""
+    op = ops[l]
+    if l == len(ops) - 1:
+        return _coarse_solve(op, f, cfg)
+    for _ in range(cfg.nu_pre):
+        phi = jacobi(op, phi, f, cfg.omega)
+    fc = tfops.restrict_avg(residual(op, phi, f), op.dtype)
+    wc = vcycle(ops, l + 1, np.zeros_like(fc), fc, cfg)
+    phi = phi - tfops.prolong_nearest(wc, op.dtype)
+    for _ in range(cfg.nu_post):
+        phi = jacobi(op, phi, f, cfg.omega)
+    return phi
+
+
+def fcycle(ops, l, phi, f, cfg):
+    """F-cycle: the coarse correction is one recursive F-cycle followed by one V-cycle
+    from its result."""
+    op = ops[l]
+    if l == len(ops) - 1:
+        return _coarse_solve(op, f, cfg)
+    for _ in range(cfg.nu_pre):
+        phi = jacobi(op, phi, f, cfg.omega)
+    fc = tfops.restrict_avg(residual(op, phi, f), op.dtype)
+    wc = fcycle(ops, l + 1, np.zeros_like(fc), fc, cfg)
+    wc = vcycle(ops, l + 1, wc, fc, cfg)
+    phi = phi - tfops.prolong_nearest(wc, op.dtype)
+    for _ in range(cfg.nu_post):
+        phi = jacobi(op, phi, f, cfg.omega)
+    return phi
+
+
+def rel_residual(op, phi, b):
+    """``||b - A phi||_2 / ||b||_2`` accumulated in float64."""
+    r = residual(op, phi, b).astype(np.float64)
+    nb = np.linalg.norm(np.asarray(b, np.float64).ravel())
+    return float(np.linalg.norm(r.ravel()) / nb) if nb > 0 else float(np.linalg.norm(r))
+
+
+def solve(ops, b, cfg, cycle="V", tol=1e-6, max_cycles=200, phi0=None):
+    """Cycle until the relative residual drops below ``tol``.  Returns (phi, history)."""
+    dt = ops[0].dtype
+    phi = np.zeros_like(np.asarray(b, dt)) if phi0 is None else np.asarray(phi0, dt).copy()
+    fn = vcycle if cycle == "V" else fcycle
+    hist = [rel_residual(ops[0], phi, b)]
+    while hist[-1] >= tol and len(hist) <= max_cycles:
+        phi = fn(ops, 0, phi, b, cfg)
+        hist.append(rel_residual(ops[0], phi, b))
+    return phi, hist
+
+
+def pcg_solve(ops, b, cfg, cycle="V", tol=1e-6, max_iter=500):
+    """Conjugate gradients preconditioned by one V (or F) cycle with zero initial guess
+    (symmetric when nu_pre == nu_post).  Returns (x, history of ||r||/||b||)."""
+    dt = ops[0].dtype
+    b = np.asarray(b, dt)
+    fn = vcycle if cycle == "V" else fcycle
+    x = np.zeros_like(b)
+    r = b.copy()
+    nb = float(np.linalg.norm(b.astype(np.float64).ravel()))
+    hist = [1.0 if nb > 0 else 0.0]
+    if nb == 0:
+        return x, hist
+    p = np.zeros_like(b)
+    rz_old = None
+    for it in range(max_iter):
+        z = fn(ops, 0, np.zeros_like(r), r, cfg)
+        rz = float((r.astype(np.float64) * z).sum())
+        p = z + (dt(rz / rz_old) if rz_old else dt(0)) * p
+        rz_old = rz
+        q = ops[0].apply(p)
+        alpha = dt(rz / float((p.astype(np.float64) * q).sum()))
+        x = x + alpha * p
+        r = r - alpha * q
+        hist.append(float(np.linalg.norm(r.astype(np.float64).ravel())) / nb)
+        if hist[-1] < tol:
+            break
+    return x, hist

@@ -1,0 +1,71 @@
+"""The C-ABI library loads and exports every symbol include/hfm.h declares (no GPU calls)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "hfm.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(hfm_[a-z0-9_]+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib(pkg):
+    return pkg._lib.lib()
+
+
+def test_header_declares_api():
+    syms = declared_symbols()
+    for must in ("hfm_conv3d_k3", "hfm_restrict_avg", "hfm_prolong_nearest", "hfm_op_jacobi",
+                 "hfm_residual_restrict", "hfm_prolong_correct_smooth", "hfm_norm2_f64",
+                 "hfm_mg_create", "hfm_mg_solve", "hfm_stencil7_var_jacobi",
+                 "hfm_stencil27_residual"):
+        assert must in syms
+
+
+def test_every_declared_symbol_is_exported(lib):
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header(pkg):
+    assert set(declared_symbols()) == set(pkg._lib.SIGNATURES)
+
+
+def test_host_only_calls(lib, pkg):
+    L = pkg._lib
+    assert lib.hfm_abi_version() == 1
+    assert lib.hfm_status_string(L.ERR_NOT_CONVERGED) == b"HFM_ERR_NOT_CONVERGED"
+    cfg = L.HfmMgConfig()
+    lib.hfm_mg_config_default(C.byref(cfg))
+    assert cfg.nu_pre == 2 and cfg.nu_post == 2 and abs(cfg.omega - 2 / 3) < 1e-7
+    assert cfg.tol == 1e-6 and cfg.min_coarse_edge == 4
+    f64 = lib.hfm_mg_footprint_bytes(C.byref(cfg), 64, 64, 64, 1)
+    f128 = lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1)
+    assert 64 ** 3 * 24 < f64 < 64 ** 3 * 40
+    assert 6 < f128 / f64 < 9
+    assert lib.hfm_mg_footprint_bytes(C.byref(cfg), 64, 64, 64, 10) > 9 * f64
+    assert lib.hfm_reduce_scratch_bytes(0, 1) == 0
+
+
+def test_bad_arguments_fail_without_gpu(lib, pkg):
+    """Argument validation happens on the host before any CUDA call."""
+    L = pkg._lib
+    st = lib.hfm_restrict_avg(None, None, 1, 4, 4, 4, None)
+    assert st == L.ERR_BAD_ARG
+    assert b"NULL" in lib.hfm_last_error()
+    st = lib.hfm_conv3d_k3(None, None, 0, 4, 4, 4, None, None)
+    assert st == L.ERR_BAD_ARG
+    cfg = L.HfmMgConfig()
+    lib.hfm_mg_config_default(C.byref(cfg))
+    cfg.accel = L.ACCEL_CG
+    cfg.nu_post = 1
+    h = C.c_void_p()
+    assert lib.hfm_mg_create(C.byref(cfg), 8, 8, 8, 1, C.byref(h)) == L.ERR_BAD_ARG
+    assert b"symmetric" in lib.hfm_last_error()

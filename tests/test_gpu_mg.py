@@ -1,0 +1,230 @@
+"""GPU parity of the multigrid handle (hfm_mg_* through the C ABI) against the oracle.
+
+Reference-mode (sawtooth) parity: float32 fields within 1e-5 relative (to the field max) of
+the float32 oracle after 1, 2, 3 and 10 cycles.  Config-mode cycles: same bar per cycle;
+solves: relative residual below tol, error against the float64 oracle stated.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mg, tfops, weights as W
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def close(got, ref, rtol=1e-5):
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    err = np.abs(got - ref).max() / max(np.abs(ref).max(), 1e-30)
+    assert err <= rtol, "max rel err %.3e > %.1e" % (err, rtol)
+    return err
+
+
+@pytest.fixture(scope="module")
+def T(hfm):
+    import torch
+    return torch
+
+
+def dev(T, a):
+    return T.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
+
+
+def run_sawtooth(hfm, T, K, b, phi0, n_levels, cycles, **kw):
+    M = hfm.multigrid
+    cfg = M.SolverConfig.reference(n_levels=n_levels, cycles=cycles + 2, **kw)
+    with M.Multigrid(b.shape, hfm._lib.OP_K27, cfg, slots=1) as h:
+        h.set_operator(hfm.ops.Stencil27(K))
+        h.load(0, dev(T, b), dev(T, phi0))
+        outs = []
+        for _ in range(cycles // 2):
+            h.run(2)
+            outs.append(h.fetch(0).cpu().numpy())
+        return outs, h.levels
+
+
+def test_sawtooth_7point_golden(hfm, T):
+    g = np.load(os.path.join(GOLD, "oracle_small.npz"))
+    b = g["saw7_b"]
+    M = hfm.multigrid
+    cfg = M.SolverConfig.reference(n_levels=5, cycles=10)
+    cfg.cycles_per_launch = 1
+    with M.Multigrid(b.shape, hfm._lib.OP_K27, cfg, slots=1) as h:
+        h.set_operator(hfm.ops.Stencil27(W.w2_7point()))
+        assert h.levels == [(16, 16, 16), (8, 8, 8), (4, 4, 4), (2, 2, 2), (1, 1, 1)]
+        h.load(0, dev(T, b), dev(T, b))
+        h.run(2)
+        close(h.fetch(0).cpu(), g["saw7_after_2"])
+
+
+def test_sawtooth_7point_10_cycles_and_levels(hfm, T):
+    """7point.ipynb cycle on 32^3 (6 levels down to 1^3): fields and per-level w after
+    10 cycles."""
+    n = 32
+    b = np.zeros((n, n, n), np.float32)
+    b[11:21, 11:21, 11:21] = 1.0
+    K = W.w2_7point()
+    ops = mg.hierarchy(mg.Stencil27(K), 6)
+    ref = b.copy()
+    refs = []
+    keep = {}
+    for c in range(10):
+        ref = mg.sawtooth_cycle(ops, ref, b, keep=keep)
+        refs.append(ref)
+    M = hfm.multigrid
+    cfg = M.SolverConfig.reference(n_levels=6, cycles=20)
+    with M.Multigrid(b.shape, hfm._lib.OP_K27, cfg, slots=1) as h:
+        h.set_operator(hfm.ops.Stencil27(K))
+        h.load(0, dev(T, b), dev(T, b))
+        for k in range(5):
+            h.run(2)
+            close(h.fetch(0).cpu(), refs[2 * k + 1])
+        # the last cycle's corrections and residuals, level by level
+        for l in range(1, 6):
+            close(h.read_level(0, l, 0).cpu(), keep["w"][l], rtol=1e-4)
+            close(h.read_level(0, l, 1).cpu(), keep["r"][l], rtol=1e-4)
+
+
+def test_sawtooth_neumann_top(hfm, T):
+    """Anisotropic_3d_Multigrid_7point_BC.ipynb: boundary_condition_top after each cycle."""
+    n = 16
+    b = np.zeros((n, n, n), np.float32)
+    b[5:10, 5:10, 5:10] = 1.0
+    K = W.w2_7point()
+    ops = mg.hierarchy(mg.Stencil27(K), 5)
+    ref = b.copy()
+    for _ in range(4):
+        ref = mg.sawtooth_cycle(ops, ref, b, top_copy=True)
+    outs, _ = run_sawtooth(hfm, T, K, b, b, 5, 4, top_copy=True)
+    close(outs[-1], ref)
+    np.testing.assert_array_equal(outs[-1][0], outs[-1][1])
+
+
+def test_sawtooth_ns_pressure_golden(hfm, T):
+    """naiver_stokes_3D.py:646-703 pressure cycle: 27-point w5, coarsest 2^3, no fine-level
+    Jacobi on w, residual and pressure zeroed on x = X-1."""
+    g = np.load(os.path.join(GOLD, "oracle_small.npz"))
+    pb = g["sawns_b"]
+    outs, levels = run_sawtooth(hfm, T, W.w5_pressure27(), pb, np.zeros_like(pb), 4, 2,
+                                fine_smooth=False, zero_xend=True)
+    assert levels[-1] == (2, 2, 2)
+    close(outs[-1], g["sawns_after_2"])
+
+
+def test_sawtooth_rectangular(hfm, T):
+    """Anisotropic_3d_Multigrid_7point_BC_Rec.ipynb: (nz, ny, nx) = (5*m, m, m) grids with
+    dz = 5 coarsen to a 5x1x1 coarsest level."""
+    b = np.zeros((40, 8, 8), np.float32)
+    b[10:20, 2:6, 2:6] = 1.0
+    K = W.w2_7point(dz=5.0)
+    ops = mg.hierarchy(mg.Stencil27(K), 4)
+    ref = b.copy()
+    for _ in range(2):
+        ref = mg.sawtooth_cycle(ops, ref, b)
+    outs, levels = run_sawtooth(hfm, T, K, b, b, 4, 2)
+    assert levels[-1] == (5, 1, 1)
+    close(outs[-1], ref)
+
+
+def _problem(hfm, n, seed, log_std=1.0):
+    sig = hfm.problems.anisotropic_sigma((n, n, n), seed=seed, log_std=log_std)
+    f = hfm.problems.dipole((n, n, n), seed=seed)
+    return sig, f
+
+
+@pytest.mark.parametrize("cycle", ["V", "F"])
+def test_config_cycles_match_oracle(hfm, T, cycle):
+    n = 32
+    sig, f = _problem(hfm, n, 5)
+    oop = mg.Sigma7(sig[0], sig[1], sig[2], dtype=np.float32)
+    shapes = mg.level_shapes((n, n, n))
+    ops = mg.hierarchy(oop, len(shapes), 0.5)
+    ccfg = mg.CycleConfig(2, 2, 2.0 / 3.0, 32)
+    M = hfm.multigrid
+    cfg = M.SolverConfig(cycle=cycle, tol=1e-300, max_cycles=50, cycles_per_launch=1)
+    with M.Multigrid((n, n, n), hfm._lib.OP_SIGMA7, cfg, slots=1) as h:
+        assert h.levels == shapes
+        h.set_operator(hfm.ops.Sigma7(*(dev(T, sig[k]) for k in range(3))))
+        h.load(0, dev(T, f))
+        ref = np.zeros_like(f)
+        fn = mg.vcycle if cycle == "V" else mg.fcycle
+        for c in range(3):
+            ref = fn(ops, 0, ref, f, ccfg)
+            h.run(1)
+            close(h.fetch(0).cpu(), ref)
+
+
+@pytest.mark.parametrize("accel,cycle", [("cg", "V"), ("none", "V"), ("cg", "F")])
+def test_solve_to_tolerance(hfm, T, accel, cycle):
+    n = 32
+    sig, f = _problem(hfm, n, 6)
+    M = hfm.multigrid
+    cfg = M.SolverConfig(cycle=cycle, accel=accel, tol=1e-6, max_cycles=400)
+    with M.Multigrid((n, n, n), hfm._lib.OP_SIGMA7, cfg, slots=1) as h:
+        h.set_operator(hfm.ops.Sigma7(*(dev(T, sig[k]) for k in range(3))))
+        phi, st = h.solve(dev(T, f[None]))
+    assert st[0]["status"] == 0, st
+    oop = mg.Sigma7(sig[0], sig[1], sig[2], dtype=np.float64)
+    p = phi[0].double().cpu().numpy()
+    rel = mg.rel_residual(oop, p, f)
+    assert rel < 1.5e-6
+    assert abs(rel - st[0]["rel_resid"]) < 1e-6
+    # error against the float64 oracle solution of the same discrete system
+    ops64 = mg.hierarchy(oop, len(mg.level_shapes((n, n, n))), 0.5)
+    x64, _ = mg.solve(ops64, f.astype(np.float64), mg.CycleConfig(), "V", 1e-12, 2000)
+    err = np.linalg.norm(p - x64) / np.linalg.norm(x64)
+    assert err < 1e-3, err
+
+
+def test_slots_alone_and_in_the_mix(hfm, T):
+    """Each slot's result is identical whether it is solved alone or with others."""
+    n = 16
+    M = hfm.multigrid
+    cfg = M.SolverConfig(cycle="V", accel="cg", tol=1e-6)
+    probs = [_problem(hfm, n, s, 0.5 + 0.5 * s) for s in range(3)]
+    sig = np.stack([p[0] for p in probs], axis=1)  # (3, slots, n, n, n)
+    f = np.stack([p[1] for p in probs])
+    with M.Multigrid((n, n, n), hfm._lib.OP_SIGMA7, cfg, slots=3) as h:
+        h.set_operator(hfm.ops.Sigma7(*(dev(T, sig[k]) for k in range(3))))
+        phi, st = h.solve(dev(T, f))
+        mix = phi.cpu().numpy()
+    for s in range(3):
+        with M.Multigrid((n, n, n), hfm._lib.OP_SIGMA7, cfg, slots=1) as h:
+            h.set_operator(hfm.ops.Sigma7(*(dev(T, sig[k, s]) for k in range(3))))
+            phi1, st1 = h.solve(dev(T, f[s:s + 1]))
+        assert st1[0]["cycles"] == st[s]["cycles"]
+        np.testing.assert_array_equal(phi1[0].cpu().numpy(), mix[s])
+
+
+def test_failure_statuses(hfm, T):
+    n = 16
+    sig, f = _problem(hfm, n, 8)
+    M, L = hfm.multigrid, hfm._lib
+    cfg = M.SolverConfig(cycle="V", tol=1e-12, max_cycles=2)
+    with M.Multigrid((n, n, n), L.OP_SIGMA7, cfg, slots=3) as h:
+        h.set_operator(hfm.ops.Sigma7(*(dev(T, np.broadcast_to(sig[k], (3, n, n, n))) for k in range(3))))
+        bad = f.copy()
+        bad[3, 3, 3] = np.nan
+        rhs = np.stack([f, bad, np.zeros_like(f)])
+        phi, st = h.solve(dev(T, rhs))
+    assert st[0]["status"] == L.ERR_NOT_CONVERGED and st[0]["cycles"] == 2
+    assert st[1]["status"] == L.ERR_NAN
+    assert st[2]["status"] == L.OK and np.all(phi[2].cpu().numpy() == 0)
+
+
+def test_cancel_frees_slot(hfm, T):
+    n = 16
+    sig, f = _problem(hfm, n, 9)
+    M = hfm.multigrid
+    cfg = M.SolverConfig(cycle="V", accel="cg", tol=1e-6)
+    with M.Multigrid((n, n, n), hfm._lib.OP_SIGMA7, cfg, slots=1) as h:
+        h.set_operator(hfm.ops.Sigma7(*(dev(T, sig[k]) for k in range(3))))
+        h.load(0, dev(T, f))
+        h.run(1)
+        h.cancel(0)
+        assert h.query()[0]["active"] == 0
+        phi, st = h.solve(dev(T, f[None]))
+        assert st[0]["status"] == 0

@@ -1,0 +1,155 @@
+"""CPU checks of the oracle: reference known-answers, TF layer semantics, golden fixtures."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mg, tfops, weights as W
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def pins():
+    with open(os.path.join(GOLD, "reference_pins.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(os.path.join(GOLD, "oracle_small.npz"))
+
+
+def test_reference_printed_kernel(pins):
+    """Multigrid_3d_7point_source.ipynb cells 4, 5, 6, 10 at dt=0.1, D=(200,100,50)."""
+    K = W.w2_7point(Dx=200.0, Dy=100.0, Dz=50.0, dt=0.1)
+    assert K.sum() == pytest.approx(pins["sum_w2"], abs=1e-12)
+    np.testing.assert_allclose(K[1], np.array(pins["centre_plane"]), atol=1e-12)
+    assert K[1, 1, 1] == pytest.approx(pins["centre_weight"])
+    np.testing.assert_allclose(K, np.array(pins["kernel_3x3x3"]), atol=1e-12)
+
+
+def test_product_weights_match_oracle(pkg):
+    w = pkg.weights
+    np.testing.assert_allclose(w.anisotropic7(), W.w2_7point(), rtol=1e-7)
+    np.testing.assert_allclose(w.anisotropic7(dt=0.1), W.w2_7point(dt=0.1), rtol=1e-6)
+    np.testing.assert_allclose(w.pressure27(), W.w5_pressure27(), rtol=1e-6)
+    np.testing.assert_allclose(w.diffusion27(0.1, 0.25), W.w1_diffusion27(0.1, 0.25), rtol=1e-6)
+    for a, b in zip(w.advection(0.4, factor=0.5), W.advection_kernels(0.4, factor=0.5)):
+        np.testing.assert_allclose(a, b, rtol=1e-6)
+    for a, b in zip(w.divergence(0.1), W.divergence_kernels(0.1)):
+        np.testing.assert_allclose(a, b, rtol=1e-6)
+    assert w.pressure27()[1, 1, 1] == pytest.approx(88 / 26, rel=1e-6)
+
+
+def test_param_counts(pins, pkg):
+    """Keras summaries: 28 params for a 3x3x3 conv + bias, 9 for the 2x2x2 restriction."""
+    ops = pytest.importorskip("torch") and pkg.ops
+    assert ops.Conv3DSame(W.w2_7point()).count_params() == pins["params_conv3x3x3"]
+    assert ops.Restriction().count_params() == pins["params_restrict2x2x2"]
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 3, 4), (5, 4, 7), (8, 8, 8)])
+def test_conv_is_cross_correlation_with_zero_pad(shape):
+    """Independent second opinion: torch CPU conv3d (cross-correlation, zero padding)."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(shape)
+    K = rng.standard_normal((3, 3, 3))
+    ref = torch.nn.functional.conv3d(torch.from_numpy(x)[None, None],
+                                     torch.from_numpy(K)[None, None], padding=1)[0, 0].numpy()
+    np.testing.assert_allclose(tfops.conv3d_same(x, K, np.float64), ref, rtol=1e-12, atol=1e-12)
+
+
+def test_restrict_prolong_semantics():
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((7, 6, 9))
+    ref = torch.nn.functional.avg_pool3d(torch.from_numpy(x)[None, None], 2)[0, 0].numpy()
+    np.testing.assert_allclose(tfops.restrict_avg(x, np.float64), ref, rtol=1e-12)
+    y = tfops.prolong_nearest(x[:3, :3, :3], np.float64)
+    assert y.shape == (6, 6, 6)
+    assert y[5, 4, 3] == x[2, 2, 1]
+    # restriction is 1/8 of the prolongation's transpose
+    a = rng.standard_normal((4, 4, 4))
+    c = rng.standard_normal((2, 2, 2))
+    lhs = (tfops.restrict_avg(a, np.float64) * c).sum()
+    rhs = (a * tfops.prolong_nearest(c, np.float64)).sum() / 8.0
+    assert lhs == pytest.approx(rhs, rel=1e-12)
+
+
+def test_sigma_form_equals_directional_form():
+    """Sigma7 (face means) equals the reference's six-array form with the same faces."""
+    rng = np.random.default_rng(3)
+    s = np.exp(rng.standard_normal((3, 5, 6, 7)))
+    op = mg.Sigma7(s[0], s[1], s[2], dtype=np.float64)
+    (xl, xh), (yl, yh), (zl, zh) = op.faces
+    d = mg.Dir7({"xm": xl, "xp": xh, "ym": yl, "yp": yh, "zm": zl, "zp": zh}, op.diag, np.float64)
+    x = rng.standard_normal((5, 6, 7))
+    np.testing.assert_allclose(op.apply(x), d.apply(x), rtol=1e-12)
+    # symmetric positive definite
+    y = rng.standard_normal((5, 6, 7))
+    assert (op.apply(x) * y).sum() == pytest.approx((x * op.apply(y)).sum(), rel=1e-10)
+    assert (op.apply(x) * x).sum() > 0
+
+
+def test_const7_is_sigma7_with_constant_sigma():
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal((6, 5, 4))
+    ones = np.ones((6, 5, 4))
+    a = mg.Sigma7(200 * ones, 100 * ones, 50 * ones, dtype=np.float64).apply(x)
+    b = mg.const7(50.0, 100.0, 200.0, dtype=np.float64).apply(x)
+    # wall faces differ: SAME zero padding puts the ghost at distance h on both forms
+    np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-9)
+
+
+def test_golden_fixtures_reproduce(gold):
+    """The oracle reproduces its committed fixtures bit-for-bit (regression pin)."""
+    K7 = W.w2_7point()
+    K27 = W.w5_pressure27()
+    Kr = gold["kr"].astype(np.float64)
+    for i in range(6):
+        x, b, sig = gold["x_%d" % i], gold["b_%d" % i], gold["sig_%d" % i]
+        np.testing.assert_array_equal(tfops.conv3d_same(x, K7), gold["conv_k7_%d" % i])
+        np.testing.assert_array_equal(tfops.conv3d_same(x, K27), gold["conv_k27_%d" % i])
+        np.testing.assert_allclose(tfops.conv3d_same(x, Kr), gold["conv_kr_%d" % i], rtol=1e-6, atol=1e-6)
+        op = mg.Sigma7(sig[0], sig[1], sig[2])
+        np.testing.assert_array_equal(op.apply(x), gold["sigma_apply_%d" % i])
+        np.testing.assert_array_equal(mg.jacobi(op, x, b, 2.0 / 3.0), gold["sigma_jacobi_%d" % i])
+        if "restrict_%d" % i in gold:
+            np.testing.assert_array_equal(tfops.restrict_avg(x), gold["restrict_%d" % i])
+        np.testing.assert_array_equal(tfops.prolong_nearest(x), gold["prolong_%d" % i])
+    b = gold["saw7_b"]
+    ops = mg.hierarchy(mg.Stencil27(K7), 5)
+    phi = b.copy()
+    for c in range(3):
+        phi = mg.sawtooth_cycle(ops, phi, b)
+        np.testing.assert_array_equal(phi, gold["saw7_after_%d" % (c + 1)])
+
+
+def test_sawtooth_first_cycle_by_hand():
+    """On 2^3 with two levels the reference cycle can be written out by hand."""
+    K = W.w2_7point()
+    d = K[1, 1, 1]
+    b = np.arange(8, dtype=np.float64).reshape(2, 2, 2)
+    ops = mg.hierarchy(mg.Stencil27(K, dtype=np.float64), 2)
+    phi = b.copy()
+    r = tfops.conv3d_same(phi, K, np.float64) - b
+    w1 = r.mean() / d                     # restriction of the 2^3 block then J from zero on 1^3
+    w = np.full((2, 2, 2), w1)
+    w = w - tfops.conv3d_same(w, K, np.float64) / d + r / d
+    p = phi - w
+    p = p - tfops.conv3d_same(p, K, np.float64) / d + b / d
+    np.testing.assert_allclose(mg.sawtooth_cycle(ops, phi, b), p, rtol=1e-12)
+
+
+def test_vcycle_converges_and_pcg_faster(pkg):
+    n = 16
+    sig = pkg.problems.anisotropic_sigma((n, n, n), seed=0, log_std=1.0).astype(np.float64)
+    f = pkg.problems.dipole((n, n, n), seed=0).astype(np.float64)
+    op = mg.Sigma7(sig[0], sig[1], sig[2], dtype=np.float64)
+    ops = mg.hierarchy(op, len(mg.level_shapes((n, n, n))), 0.5)
+    _, h = mg.solve(ops, f, mg.CycleConfig(), "V", 1e-6, 400)
+    assert h[-1] < 1e-6
+    assert all(b < a for a, b in zip(h, h[1:]))
