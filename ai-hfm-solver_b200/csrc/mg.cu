@@ -727,7 +727,9 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
     const size_t b = (size_t)L.n * slots * es;
     L.phi = dalloc(m.get(), b, &st);
     L.tmp = dalloc(m.get(), b, &st);
-    L.rhs = dalloc(m.get(), b, &st);
+    // float32 CG: the fine-level cycle reads the CG residual in place (set below)
+    if (!(l == 0 && cfg->accel == HFM_ACCEL_CG && cfg->storage == HFM_F32))
+      L.rhs = dalloc(m.get(), b, &st);
     if (cfg->op_kind == HFM_OP_SIGMA7)
       for (int a = 0; a < 3; ++a) L.coef[a] = dalloc(m.get(), b, &st);
   }
@@ -735,6 +737,7 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
   if (cfg->accel == HFM_ACCEL_CG) {
     for (int i = 0; i < 4; ++i) m->cg[i] = (float *)dalloc(m.get(), nf * 4, &st);
     m->fine_b = dalloc(m.get(), nf * 4, &st);
+    if (cfg->storage == HFM_F32) m->lv[0].rhs = m->cg[1];
   } else if (cfg->cycle == HFM_CYCLE_SAWTOOTH) {
     m->saw[0] = dalloc(m.get(), nf * es, &st);
     m->saw[1] = dalloc(m.get(), nf * es, &st);
