@@ -85,6 +85,7 @@ SIGNATURES = {
     "hfm_reduce_scratch_bytes": (C.c_size_t, [I64, I]),
     "hfm_norm2_f64": (I, [P, I64, I, P, P, P]),
     "hfm_max_abs": (I, [P, I64, I, P, P, P]),
+    "hfm_norm2_f64_noalloc": (I, [P, I64, I, P, P]),
     "hfm_mg_config_default": (None, [C.POINTER(HfmMgConfig)]),
     "hfm_mg_footprint_bytes": (C.c_size_t, [C.POINTER(HfmMgConfig), I, I, I, I]),
     "hfm_mg_create": (I, [C.POINTER(HfmMgConfig), I, I, I, I, C.POINTER(P)]),

@@ -1,7 +1,15 @@
 // Per-instance reductions with a fixed summation order, dtype conversions.
+#include <mutex>
+#include <vector>
+
 #include "hfm_internal.cuh"
 
 namespace hfm {
+
+// Block partial sums for hfm_norm2_f64_noalloc.  Every GPU that loads the library holds
+// this array (HFM_NORM2_NOALLOC_SCRATCH_BYTES) until the process exits.
+static __device__ __align__(256) double g_norm2_noalloc_scratch[HFM_NORM2_NOALLOC_SCRATCH_BYTES /
+                                                                sizeof(double)];
 
 namespace {
 constexpr int kThreads = 256;
@@ -193,6 +201,56 @@ extern "C" int hfm_norm2_f64(const float *x, int64_t n, int B, double *out, void
   int st = launch_sumsq_partials<float>(x, n, n, B, (double *)scratch, &nb, nullptr, s);
   if (st) return st;
   if ((st = launch_finalize_sum((double *)scratch, nb, B, out, s))) return st;
+  k_sqrt_inplace<<<(B + 127) / 128, 128, 0, s>>>(out, B);
+  HFM_CHECK_LAUNCH("k_sqrt_inplace");
+  return HFM_OK;
+}
+
+namespace {
+
+// Device address of g_norm2_noalloc_scratch on the current device.  In host code the
+// array's name only stands for the symbol, so the address is looked up with
+// cudaGetSymbolAddress once per device (with that device current) and cached.
+int noalloc_scratch(double **out) {
+  static std::mutex mu;
+  static std::vector<double *> ptrs;
+  int dev = 0;
+  HFM_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)ptrs.size() <= dev) ptrs.resize(dev + 1, nullptr);
+  if (!ptrs[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_norm2_noalloc_scratch);
+    if (e != cudaSuccess || !p) return cuda_status(e, "cudaGetSymbolAddress(norm2 scratch)");
+    ptrs[dev] = (double *)p;
+  }
+  *out = ptrs[dev];
+  return HFM_OK;
+}
+
+}  // namespace
+
+// Same kernels and summation order as hfm_norm2_f64, with the block partial sums kept in
+// the library's static device array instead of caller memory.
+extern "C" int hfm_norm2_f64_noalloc(const float *x, int64_t n, int B, double *out,
+                                     hfm_stream_t stream) {
+  if (!x || !out || n <= 0 || B <= 0) return fail(HFM_ERR_BAD_ARG, "hfm_norm2_f64_noalloc: bad argument");
+  const size_t need = hfm_reduce_scratch_bytes(n, B);
+  if (need > HFM_NORM2_NOALLOC_SCRATCH_BYTES)
+    return fail(HFM_ERR_BAD_ARG,
+                "hfm_norm2_f64_noalloc: needs " + std::to_string(need) +
+                    " bytes of partial sums (B x blocks x 8), more than the library's static " +
+                    std::to_string((size_t)HFM_NORM2_NOALLOC_SCRATCH_BYTES) +
+                    "-byte array; use hfm_norm2_f64 with caller scratch");
+  double *scratch = nullptr;
+  int st = noalloc_scratch(&scratch);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  int nb = 0;
+  // every partial the finalize step reads is written by this call's first kernel, so the
+  // array needs no clearing between calls
+  if ((st = launch_sumsq_partials<float>(x, n, n, B, scratch, &nb, nullptr, s))) return st;
+  if ((st = launch_finalize_sum(scratch, nb, B, out, s))) return st;
   k_sqrt_inplace<<<(B + 127) / 128, 128, 0, s>>>(out, B);
   HFM_CHECK_LAUNCH("k_sqrt_inplace");
   return HFM_OK;

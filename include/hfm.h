@@ -173,6 +173,23 @@ int hfm_norm2_f64(const float *x, int64_t n, int B, double *out, void *scratch,
 int hfm_max_abs(const float *x, int64_t n, int B, float *out, void *scratch,
                 hfm_stream_t stream);
 
+/* hfm_norm2_f64 for callers that cannot allocate device memory: no counterpart in the
+ * reference.  Some callers have no way to obtain scratch - a C or Fortran host code that
+ * owns no device allocator, or a time-stepping loop under a fixed device-memory budget where
+ * a cudaMalloc (which may synchronise the whole device) is not allowed.  This variant keeps
+ * its block partial sums in a static device array of HFM_NORM2_NOALLOC_SCRATCH_BYTES inside
+ * the library, so it allocates nothing; the caller still passes x and out (device, B
+ * doubles).  Limit: hfm_reduce_scratch_bytes(n, B) must not exceed that size (512 KiB, e.g.
+ * up to 221 instances of any size, more for small n); larger requests return
+ * HFM_ERR_BAD_ARG.  Every GPU that loads the library holds the array until the process
+ * exits.  The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) and caches it; make that first call before any stream capture.
+ * All calls share the one array: calls whose kernels overlap on the GPU (different streams
+ * without ordering) race and may return wrong sums; order them on one stream.  Results are
+ * bitwise equal to hfm_norm2_f64's. */
+#define HFM_NORM2_NOALLOC_SCRATCH_BYTES (512u * 1024u)
+int hfm_norm2_f64_noalloc(const float *x, int64_t n, int B, double *out, hfm_stream_t stream);
+
 /* ------------------------------------------------------------------ multigrid handle */
 typedef enum { HFM_CYCLE_SAWTOOTH = 0, HFM_CYCLE_V = 1, HFM_CYCLE_F = 2 } hfm_cycle;
 typedef enum { HFM_ACCEL_NONE = 0, HFM_ACCEL_CG = 1 } hfm_accel;
