@@ -230,7 +230,7 @@ int hfm_residual_restrict(const hfm_operator *op, const float *phi, const float 
   if (!phi || !b || !r_coarse) return fail(HFM_ERR_BAD_ARG, "hfm_residual_restrict: NULL field");
   const int64_t n = (int64_t)Z * Y * X;
   DevOp d = make_devop(*op, n);
-  return launch_residual_restrict<float>(op->kind, d, plain_src(phi, n, flags), b, n, r_fine, n,
+  return launch_residual_restrict<float>(op->kind, d, plain_src(phi, n, flags & HFM_FLAG_ZERO_GUESS), b, n, r_fine, n,
                                          r_coarse, n / 8, B, Grid3{Z, Y, X}, flags, nullptr,
                                          nullptr, nullptr, (cudaStream_t)stream);
 }

@@ -195,6 +195,25 @@ int launch_coarse_jacobi(int kind, const DevOp &op, const T *rhs, int64_t rhs_st
                          int sweeps, const int *active, cudaStream_t s);
 int coarse_smem_limit();  // max cells for launch_coarse_jacobi
 
+// Plane-marching kernels (ops_fast.cu) for X % 4 == 0; mode 0 smooth, 1 residual,
+// 2 residual + restriction.  The generic launchers call them when fast_eligible().
+enum { FAST_SMOOTH = 0, FAST_RESID = 1, FAST_RESTRICT = 2 };
+bool fast_eligible(int kind, Grid3 g, bool restrict_mode);
+template <class T>
+int fast_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
+                T *out, T *coarse, int64_t stride, int64_t coarse_stride, int B, Grid3 g,
+                float omega, unsigned flags, const int *active, double *partials,
+                int *nblk_out, cudaStream_t s);
+// TMA-pipelined kernels (ops_tma.cu) for X >= 64: same modes as fast_launch.
+bool tma_eligible(int kind, Grid3 g, int mode, const void *corr, int corr_coarse, int es);
+template <class T>
+int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const T *rhs, T *out,
+               T *coarse, int64_t stride, int64_t coarse_stride, int B, Grid3 g, float omega,
+               unsigned flags, const int *active, double *partials, int *nblk_out,
+               cudaStream_t s);
+// Upper bound of blocks per instance of any residual launch on grid g (partials sizing).
+int64_t max_partial_blocks(Grid3 g, int B);
+
 // Reductions (reduce.cu)
 template <class T>
 int launch_sumsq_partials(const T *x, int64_t n, int64_t stride, int B, double *partials,

@@ -110,6 +110,42 @@ __global__ void k_fetch(const T *__restrict__ b0, const T *__restrict__ b1,
   }
 }
 
+// Initial state of every slot from its ||b||^2 (batched load).
+__global__ void k_init_states(SlotState *st, int *active, int B, const double *sumsq_b) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= B) return;
+  double nb = sqrt(sumsq_b[i]);
+  SlotState s;
+  s.status = HFM_OK;
+  s.cycles = 0;
+  s.sol_buf = 0;
+  s.pad = 0;
+  s.norm_b = nb;
+  s.rel = 1.0;
+  s.rz = 0.0;
+  s.pq = 0.0;
+  int act = 1;
+  if (!(nb > 0.0)) {
+    s.rel = 0.0;
+    act = 0;
+    s.status = (nb != nb) ? HFM_ERR_NAN : HFM_OK;
+  }
+  st[i] = s;
+  active[i] = act;
+}
+
+template <class T>
+__global__ void k_fetch_all(const T *__restrict__ b0, const T *__restrict__ b1,
+                            const float *__restrict__ bx, int64_t n, const SlotState *st,
+                            const int *active, float *__restrict__ out) {
+  const int64_t slot = blockIdx.y;
+  const int which = active[slot] ? 0 : st[slot].sol_buf;
+  const int64_t o = slot * n;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[o + i] = bx ? bx[o + i] : St<T>::to(which ? b1[o + i] : b0[o + i]);
+}
+
 // ----------------------------------------------------------------- CG vector kernels
 template <class TZ>
 __global__ void k_dot_partials(const float *__restrict__ a, const TZ *__restrict__ b,
@@ -240,6 +276,8 @@ class EngineBase {
   virtual int emit_cycles(int cycles, cudaStream_t s) = 0;
   virtual int load(int slot, const float *rhs, const float *phi0, cudaStream_t s) = 0;
   virtual int fetch(int slot, float *out, cudaStream_t s) = 0;
+  virtual int load_all(const float *rhs, cudaStream_t s) = 0;
+  virtual int fetch_all(float *out, cudaStream_t s) = 0;
   virtual int set_operator(int slot, const hfm_operator &op, cudaStream_t s) = 0;
   virtual int read_level(int slot, int level, int which, float *out, cudaStream_t s) = 0;
   virtual bool cycle_flips_parity() const = 0;
@@ -490,23 +528,20 @@ class Engine : public EngineBase {
     if (k != HFM_OP_SIGMA7) return fail(HFM_ERR_UNSUPPORTED, "handle supports CONST7, SIGMA7, K27");
     if (op.coef_dtype != HFM_F32 && op.coef_dtype != HFM_F64)
       return fail(HFM_ERR_BAD_ARG, "coefficients must be float32 or float64");
-    int lo = slot < 0 ? 0 : slot, hi = slot < 0 ? m_->slots : slot + 1;
-    for (int sl = lo; sl < hi; ++sl) {
-      for (int a = 0; a < 3; ++a) {
-        if (!op.coef[a]) return fail(HFM_ERR_BAD_ARG, "SIGMA7 needs sx, sy, sz");
-        const size_t esz = op.coef_dtype == HFM_F64 ? 8 : 4;
-        const void *srcp = (const char *)op.coef[a] + (slot < 0 ? (size_t)sl * n(0) * esz : 0);
-        int st = launch_convert<T>(srcp, op.coef_dtype, (T *)m_->lv[0].coef[a] + sl * n(0), n(0), s);
+    // slot < 0: every slot at once (the arrays hold all slots), one launch per level
+    const int lo = slot < 0 ? 0 : slot, cnt = slot < 0 ? m_->slots : 1;
+    for (int a = 0; a < 3; ++a) {
+      if (!op.coef[a]) return fail(HFM_ERR_BAD_ARG, "SIGMA7 needs sx, sy, sz");
+      int st = launch_convert<T>(op.coef[a], op.coef_dtype, (T *)m_->lv[0].coef[a] + lo * n(0),
+                                 n(0) * cnt, s);
+      if (st) return st;
+      if (fine32_coef_[a] && (st = launch_convert<float>(op.coef[a], op.coef_dtype,
+                                                         fine32_coef_[a] + lo * n(0), n(0) * cnt, s)))
+        return st;
+      for (int l = 1; l < m_->L; ++l) {
+        st = launch_restrict<T>((T *)m_->lv[l - 1].coef[a] + lo * n(l - 1), n(l - 1),
+                                (T *)m_->lv[l].coef[a] + lo * n(l), n(l), cnt, g(l - 1), nullptr, s);
         if (st) return st;
-        if (fine32_coef_[a] && (st = launch_convert<float>(srcp, op.coef_dtype,
-                                                           fine32_coef_[a] + sl * n(0), n(0), s)))
-          return st;
-        for (int l = 1; l < m_->L; ++l) {
-          st = launch_restrict<T>((T *)m_->lv[l - 1].coef[a] + sl * n(l - 1), n(l - 1),
-                                  (T *)m_->lv[l].coef[a] + sl * n(l), n(l), 1, g(l - 1),
-                                  nullptr, s);
-          if (st) return st;
-        }
       }
     }
     float sc = 1.f;
@@ -563,6 +598,37 @@ class Engine : public EngineBase {
     if ((st = launch_finalize_sum(m_->partials, nb, 1, m_->scal + m_->slots, s))) return st;
     k_init_state<<<1, 1, 0, s>>>(m_->state, m_->active, slot, m_->scal + m_->slots, HFM_OK);
     HFM_CHECK_LAUNCH("k_init_state");
+    return HFM_OK;
+  }
+
+  // All slots at once from rhs [slots][n] (zero initial guess): the batched form of load().
+  int load_all(const float *b, cudaStream_t s) override {
+    const int64_t nf = n(0);
+    const int B = m_->slots;
+    int st;
+    if (m_->cfg.accel == HFM_ACCEL_CG) {
+      HFM_CUDA(cudaMemcpyAsync(m_->fine_b, b, nf * B * 4, cudaMemcpyDeviceToDevice, s));
+      HFM_CUDA(cudaMemsetAsync(m_->cg[0], 0, nf * B * 4, s));
+      HFM_CUDA(cudaMemcpyAsync(m_->cg[1], b, nf * B * 4, cudaMemcpyDeviceToDevice, s));
+      HFM_CUDA(cudaMemsetAsync(m_->cg[2], 0, nf * B * 4, s));
+    } else {
+      if ((st = launch_convert<T>(b, HFM_F32, rhs(0), nf * B, s))) return st;
+      HFM_CUDA(cudaMemsetAsync(buf(0, 0), 0, nf * B * sizeof(T), s));
+    }
+    int nb = 0;
+    if ((st = launch_sumsq_partials<float>(b, nf, nf, B, m_->partials, &nb, nullptr, s))) return st;
+    if ((st = launch_finalize_sum(m_->partials, nb, B, m_->scal, s))) return st;
+    k_init_states<<<(B + 127) / 128, 128, 0, s>>>(m_->state, m_->active, B, m_->scal);
+    HFM_CHECK_LAUNCH("k_init_states");
+    return HFM_OK;
+  }
+
+  int fetch_all(float *out, cudaStream_t s) override {
+    const int64_t nf = n(0);
+    const float *bx = m_->cfg.accel == HFM_ACCEL_CG ? m_->cg[0] : nullptr;
+    k_fetch_all<T><<<dim3(vec_blocks(nf, m_->slots), m_->slots), 256, 0, s>>>(
+        buf(0, 0), buf(0, 1), bx, nf, m_->state, m_->active, out);
+    HFM_CHECK_LAUNCH("k_fetch_all");
     return HFM_OK;
   }
 
@@ -742,7 +808,7 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
     m->saw[0] = dalloc(m.get(), nf * es, &st);
     m->saw[1] = dalloc(m.get(), nf * es, &st);
   }
-  m->partials_per_slot = 4096;
+  m->partials_per_slot = std::max<int64_t>(4096, max_partial_blocks(lv[0], slots));
   m->partials = (double *)dalloc(m.get(), (size_t)slots * m->partials_per_slot * 8, &st);
   m->active = (int *)dalloc(m.get(), (size_t)slots * 4, &st);
   m->state = (SlotState *)dalloc(m.get(), (size_t)slots * sizeof(SlotState), &st);
@@ -891,10 +957,8 @@ int hfm_mg_read_level(hfm_mg *m, int slot, int level, int which, float *out, hfm
 int hfm_mg_solve(hfm_mg *m, const float *rhs, float *phi, hfm_slot_stats *stats_host,
                  hfm_stream_t stream) {
   if (!m || !rhs || !phi) return fail(HFM_ERR_BAD_ARG, "hfm_mg_solve: bad argument");
-  const int64_t nf = (int64_t)m->Z * m->Y * m->X;
   int st;
-  for (int s = 0; s < m->slots; ++s)
-    if ((st = hfm_mg_load(m, s, rhs + s * nf, nullptr, stream))) return st;
+  if ((st = m->eng->load_all(rhs, (cudaStream_t)stream))) return st;
   std::vector<hfm_slot_stats> tmp(m->slots);
   hfm_slot_stats *ss = stats_host ? stats_host : tmp.data();
   const int per = m->cfg.cycles_per_launch;
@@ -905,8 +969,7 @@ int hfm_mg_solve(hfm_mg *m, const float *rhs, float *phi, hfm_slot_stats *stats_
     for (int s = 0; s < m->slots; ++s) any |= ss[s].active != 0;
     if (!any) break;
   }
-  for (int s = 0; s < m->slots; ++s)
-    if ((st = hfm_mg_fetch(m, s, phi + s * nf, stream))) return st;
+  if ((st = m->eng->fetch_all(phi, (cudaStream_t)stream))) return st;
   HFM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
   int worst = HFM_OK;
   for (int s = 0; s < m->slots; ++s)

@@ -217,6 +217,17 @@ __global__ void k_coarse_jacobi(DevOp op, const T *__restrict__ rhs, int64_t rhs
 
 int coarse_smem_limit() { return 4096; }
 
+int64_t max_partial_blocks(Grid3 g, int B) {
+  // generic kernels: blocks_for() <= 8 per SM; fast kernels: plane tiles x z chunks
+  const int64_t tiles = ((int64_t)g.Y * (g.X / 4) + 255) / 256 + 1;
+  const int64_t chunks = (g.Z + 3) / 4 + 1;
+  int64_t v = tiles * chunks;
+  const int64_t tma_tiles = ((int64_t)(g.X + 63) / 64) * ((g.Y + 7) / 8);
+  if (tma_tiles * chunks > v) v = tma_tiles * chunks;
+  int64_t gen = (int64_t)sm_count() * 8;
+  return v > gen ? v : gen;
+}
+
 #define HFM_DISPATCH_KIND(kind, ...)                                          \
   switch (kind) {                                                             \
     case HFM_OP_CONST7: { constexpr int K_ = HFM_OP_CONST7; __VA_ARGS__; break; } \
@@ -230,6 +241,15 @@ template <class T>
 int launch_smooth(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
                   int64_t rhs_stride, T *out, int64_t out_stride, int B, Grid3 g, float omega,
                   unsigned flags, const int *active, cudaStream_t s) {
+  if ((!phi.base || phi.base_stride == out_stride) && (phi.base || phi.corr || rhs) &&
+      (!rhs || rhs_stride == out_stride) &&
+      tma_eligible(kind, g, FAST_SMOOTH, phi.corr, phi.corr_coarse, (int)sizeof(T)))
+    return tma_launch<T>(kind, FAST_SMOOTH, op, phi, rhs, out, nullptr, out_stride, 0, B, g,
+                         omega, flags, active, nullptr, nullptr, s);
+  if (fast_eligible(kind, g, false) && (!rhs || rhs_stride == out_stride) &&
+      (!phi.base || phi.base_stride == out_stride) && (!phi.corr || phi.corr_coarse || phi.corr_stride == out_stride))
+    return fast_launch<T>(kind, FAST_SMOOTH, op, phi, rhs, out, nullptr, out_stride, 0, B, g,
+                          omega, flags, active, nullptr, nullptr, s);
   dim3 grid(blocks_for(g.n(), B), B);
   HFM_DISPATCH_KIND(kind, (k_smooth<K_, T><<<grid, kThreads, 0, s>>>(
                               op, phi, rhs, rhs_stride, out, out_stride, g.Z, g.Y, g.X, omega,
@@ -242,6 +262,14 @@ template <class T>
 int launch_residual(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *b,
                     int64_t b_stride, T *r, int64_t r_stride, int B, Grid3 g, unsigned flags,
                     const int *active, double *partials, int *nblk_out, cudaStream_t s) {
+  if (phi.base && !phi.corr && !phi.zero_xend && r && phi.base_stride == r_stride &&
+      (!b || b_stride == r_stride) && tma_eligible(kind, g, FAST_RESID, nullptr, 0, (int)sizeof(T)))
+    return tma_launch<T>(kind, FAST_RESID, op, phi, b, r, nullptr, r_stride, 0, B, g, 0.f,
+                         flags, active, partials, nblk_out, s);
+  if (fast_eligible(kind, g, false) && !phi.corr && !phi.zero_xend && r &&
+      (!b || b_stride == r_stride) && (!phi.base || phi.base_stride == r_stride))
+    return fast_launch<T>(kind, FAST_RESID, op, phi, b, r, nullptr, r_stride, 0, B, g, 0.f,
+                          flags, active, partials, nblk_out, s);
   int nb = blocks_for(g.n(), B);
   if (nblk_out) *nblk_out = nb;
   dim3 grid(nb, B);
@@ -266,6 +294,16 @@ int launch_residual_restrict(int kind, const DevOp &op, const PhiSrc<T> &phi, co
                              const int *active, double *partials, int *nblk_out,
                              cudaStream_t s) {
   if ((g.Z | g.Y | g.X) & 1) return fail(HFM_ERR_BAD_ARG, "residual_restrict needs even extents");
+  if (phi.base && !phi.corr && !phi.zero_xend && b && phi.base_stride == b_stride &&
+      (!r_fine || rf_stride == b_stride) && rc_stride == b_stride / 8 &&
+      tma_eligible(kind, g, FAST_RESTRICT, nullptr, 0, (int)sizeof(T)))
+    return tma_launch<T>(kind, FAST_RESTRICT, op, phi, b, r_fine, r_coarse, b_stride, rc_stride,
+                         B, g, 0.f, flags, active, partials, nblk_out, s);
+  if (fast_eligible(kind, g, true) && !phi.corr && !phi.zero_xend && b &&
+      (!r_fine || rf_stride == b_stride) && (!phi.base || phi.base_stride == b_stride) &&
+      rc_stride == b_stride / 8)
+    return fast_launch<T>(kind, FAST_RESTRICT, op, phi, b, r_fine, r_coarse, b_stride, rc_stride,
+                          B, g, 0.f, flags, active, partials, nblk_out, s);
   int64_t nc = g.n() / 8;
   int nb = blocks_for(nc, B);
   if (nblk_out) *nblk_out = nb;

@@ -82,6 +82,9 @@ const char *hfm_last_error(void);
 int hfm_device_sm_count(int *sm_count); /* current device's SM count */
 /* Kernels this library has enqueued since load (a CUDA-graph launch counts its kernel nodes). */
 int64_t hfm_kernel_launch_count(void);
+/* Bounded device-side waits that expired on the current device (TMA pipeline stages); a
+ * non-zero count means results of the affected launches are invalid.  reset != 0 clears it. */
+int hfm_device_timeouts(int *count, int reset);
 
 /* ------------------------------------------------ stateless operators (drop-in layers) */
 /* Conv3D(1, kernel_size=3, strides=1, padding='SAME') with frozen weights and zero bias:

@@ -88,17 +88,18 @@ def test_sawtooth_7point_10_cycles_and_levels(hfm, T):
             close(h.read_level(0, l, 1).cpu(), keep["r"][l], rtol=1e-4)
 
 
-def test_sawtooth_neumann_top(hfm, T):
+@pytest.mark.parametrize("n", [16, 64])
+def test_sawtooth_neumann_top(hfm, T, n):
     """Anisotropic_3d_Multigrid_7point_BC.ipynb: boundary_condition_top after each cycle."""
-    n = 16
     b = np.zeros((n, n, n), np.float32)
-    b[5:10, 5:10, 5:10] = 1.0
+    b[n // 3:n // 2, n // 3:n // 2, n // 3:n // 2] = 1.0
     K = W.w2_7point()
-    ops = mg.hierarchy(mg.Stencil27(K), 5)
+    nl = int(np.log2(n)) + 1
+    ops = mg.hierarchy(mg.Stencil27(K), nl)
     ref = b.copy()
     for _ in range(4):
         ref = mg.sawtooth_cycle(ops, ref, b, top_copy=True)
-    outs, _ = run_sawtooth(hfm, T, K, b, b, 5, 4, top_copy=True)
+    outs, _ = run_sawtooth(hfm, T, K, b, b, nl, 4, top_copy=True)
     close(outs[-1], ref)
     np.testing.assert_array_equal(outs[-1][0], outs[-1][1])
 
@@ -135,9 +136,8 @@ def _problem(hfm, n, seed, log_std=1.0):
     return sig, f
 
 
-@pytest.mark.parametrize("cycle", ["V", "F"])
-def test_config_cycles_match_oracle(hfm, T, cycle):
-    n = 32
+@pytest.mark.parametrize("cycle,n", [("V", 32), ("F", 32), ("V", 64)])
+def test_config_cycles_match_oracle(hfm, T, cycle, n):
     sig, f = _problem(hfm, n, 5)
     oop = mg.Sigma7(sig[0], sig[1], sig[2], dtype=np.float32)
     shapes = mg.level_shapes((n, n, n))
@@ -157,9 +157,9 @@ def test_config_cycles_match_oracle(hfm, T, cycle):
             close(h.fetch(0).cpu(), ref)
 
 
-@pytest.mark.parametrize("accel,cycle", [("cg", "V"), ("none", "V"), ("cg", "F")])
-def test_solve_to_tolerance(hfm, T, accel, cycle):
-    n = 32
+@pytest.mark.parametrize("accel,cycle,n", [("cg", "V", 32), ("none", "V", 32), ("cg", "F", 32),
+                                           ("cg", "V", 64)])
+def test_solve_to_tolerance(hfm, T, accel, cycle, n):
     sig, f = _problem(hfm, n, 6)
     M = hfm.multigrid
     cfg = M.SolverConfig(cycle=cycle, accel=accel, tol=1e-6, max_cycles=400)
@@ -172,11 +172,12 @@ def test_solve_to_tolerance(hfm, T, accel, cycle):
     rel = mg.rel_residual(oop, p, f)
     assert rel < 1.5e-6
     assert abs(rel - st[0]["rel_resid"]) < 1e-6
-    # error against the float64 oracle solution of the same discrete system
-    ops64 = mg.hierarchy(oop, len(mg.level_shapes((n, n, n))), 0.5)
-    x64, _ = mg.solve(ops64, f.astype(np.float64), mg.CycleConfig(), "V", 1e-12, 2000)
-    err = np.linalg.norm(p - x64) / np.linalg.norm(x64)
-    assert err < 1e-3, err
+    if n <= 32:
+        # error against the float64 oracle solution of the same discrete system
+        ops64 = mg.hierarchy(oop, len(mg.level_shapes((n, n, n))), 0.5)
+        x64, _ = mg.pcg_solve(ops64, f.astype(np.float64), mg.CycleConfig(), tol=1e-11)
+        err = np.linalg.norm(p - x64) / np.linalg.norm(x64)
+        assert err < 1e-3, err
 
 
 def test_slots_alone_and_in_the_mix(hfm, T):
@@ -228,3 +229,25 @@ def test_cancel_frees_slot(hfm, T):
         assert h.query()[0]["active"] == 0
         phi, st = h.solve(dev(T, f[None]))
         assert st[0]["status"] == 0
+
+
+def test_ns_pressure_form_64(hfm, T):
+    """NS pressure cycle on 64^3 (27-point operator, x-end zeroing) through the large-grid
+    kernels."""
+    rng = np.random.default_rng(21)
+    n = 64
+    pb = rng.standard_normal((n, n, n)).astype(np.float32)
+    K = W.w5_pressure27()
+    ops27 = mg.hierarchy(mg.Stencil27(K), 6)
+    p = np.zeros_like(pb)
+    for _ in range(2):
+        p = mg.sawtooth_cycle(ops27, p, pb, fine_smooth=False, zero_xend=True)
+    outs, _ = run_sawtooth(hfm, T, K, pb, np.zeros_like(pb), 6, 2, fine_smooth=False, zero_xend=True)
+    close(outs[-1], p)
+
+
+def test_no_device_timeouts(hfm, T):
+    import ctypes as C
+    cnt = C.c_int(-1)
+    hfm._lib.call("hfm_device_timeouts", C.byref(cnt), 0)
+    assert cnt.value == 0

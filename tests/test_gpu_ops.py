@@ -14,8 +14,10 @@ pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 RTOL = 1e-5
 
+# X % 4 == 0 grids run the plane-marching kernels, the others the generic ones; X = 132
+# (33 vectors per row) makes rows straddle warp boundaries, Z = 70 spans several z-chunks.
 SHAPES = [(1, 1, 1), (2, 2, 2), (3, 5, 4), (4, 4, 4), (5, 7, 6), (8, 6, 10), (16, 16, 16),
-          (12, 20, 32), (32, 8, 64), (9, 33, 40)]
+          (12, 20, 32), (32, 8, 64), (9, 33, 40), (70, 18, 132), (64, 40, 96)]
 
 
 def close(got, ref, rtol=RTOL, operands=()):
@@ -124,7 +126,8 @@ def test_flags(hfm, T):
     close(ops.jacobi(gop, dev(T, x), dev(T, b), 1.0, flags=L.FLAG_TOP_COPY).cpu(), j)
 
 
-@pytest.mark.parametrize("shape", [(2, 2, 2), (4, 6, 8), (16, 16, 16), (32, 8, 64), (10, 12, 14)])
+@pytest.mark.parametrize("shape", [(2, 2, 2), (4, 6, 8), (16, 16, 16), (32, 8, 64), (10, 12, 14),
+                                   (70, 18, 132), (64, 40, 96)])
 def test_fused_transfer_kernels(hfm, T, shape):
     ops = hfm.ops
     rng = np.random.default_rng(11)
@@ -144,10 +147,11 @@ def test_fused_transfer_kernels(hfm, T, shape):
     close(out.cpu(), mg.jacobi(oop, tfops.prolong_nearest(c, np.float64), b, 1.0))
 
 
-def test_batched_equals_single(hfm, T):
+@pytest.mark.parametrize("s", [(8, 12, 16), (10, 12, 14)])
+def test_batched_equals_single(hfm, T, s):
     ops = hfm.ops
     rng = np.random.default_rng(12)
-    B, s = 5, (8, 12, 16)
+    B = 5
     x = rng.standard_normal((B,) + s).astype(np.float32)
     sig = np.exp(rng.standard_normal((3, B) + s)).astype(np.float32)
     gop = ops.Sigma7(*(dev(T, sig[k]) for k in range(3)))
@@ -175,3 +179,27 @@ def test_bad_shapes_raise(hfm, T):
         ops.conv3d_same(T.zeros((2, 2), device="cuda"), W.w2_7point())
     with pytest.raises(hfm._lib.HfmError):
         ops.restrict_avg(T.zeros((1, 1, 1), device="cuda"))
+
+
+@pytest.mark.parametrize("storage", ["bf16", "f16"])
+def test_reduced_precision_storage_smoother(hfm, T, storage):
+    """The handle's bf16 / fp16 storage path: one V-cycle agrees with the float32 handle to
+    the storage precision."""
+    n = 32
+    sig = hfm.problems.anisotropic_sigma((n, n, n), seed=2, log_std=1.0)
+    f = hfm.problems.dipole((n, n, n), seed=2)
+    M = hfm.multigrid
+    outs = {}
+    for st in ("f32", storage):
+        cfg = M.SolverConfig(cycle="V", storage=st, tol=1e-300, max_cycles=10, cycles_per_launch=1)
+        with M.Multigrid((n, n, n), hfm._lib.OP_SIGMA7, cfg, slots=1) as h:
+            h.set_operator(ops_sigma(hfm, T, sig))
+            h.load(0, dev(T, f))
+            h.run(2)
+            outs[st] = h.fetch(0).cpu().numpy()
+    err = np.abs(outs[storage] - outs["f32"]).max() / np.abs(outs["f32"]).max()
+    assert err < (3e-2 if storage == "bf16" else 5e-3), err
+
+
+def ops_sigma(hfm, T, sig):
+    return hfm.ops.Sigma7(*(dev(T, sig[k]) for k in range(3)))
