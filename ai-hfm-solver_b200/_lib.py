@@ -19,7 +19,7 @@ OP_CONST7, OP_SIGMA7, OP_DIR7, OP_K27 = range(4)
 FLAG_ZERO_XEND, FLAG_TOP_COPY, FLAG_ZERO_GUESS = 1, 2, 4
 # hfm_cycle / hfm_accel
 CYCLE_SAWTOOTH, CYCLE_V, CYCLE_F = range(3)
-ACCEL_NONE, ACCEL_CG = range(2)
+ACCEL_NONE, ACCEL_CG, ACCEL_IR = range(3)
 
 
 class HfmOperator(C.Structure):
@@ -33,12 +33,13 @@ class HfmMgConfig(C.Structure):
                 ("nu_post", C.c_int), ("coarse_sweeps", C.c_int), ("omega", C.c_float),
                 ("coarse_omega", C.c_float), ("coarse_scale", C.c_float),
                 ("sawtooth_fine_smooth", C.c_int), ("flags", C.c_uint), ("storage", C.c_int),
-                ("tol", C.c_double), ("max_cycles", C.c_int), ("cycles_per_launch", C.c_int)]
+                ("tol", C.c_double), ("max_cycles", C.c_int), ("cycles_per_launch", C.c_int),
+                ("inner_tol", C.c_double), ("inner_max_cycles", C.c_int), ("reserved_cfg", C.c_int)]
 
 
 class HfmSlotStats(C.Structure):
     _fields_ = [("active", C.c_int), ("status", C.c_int), ("cycles", C.c_int),
-                ("reserved", C.c_int), ("norm_b", C.c_double), ("rel_resid", C.c_double)]
+                ("outer", C.c_int), ("norm_b", C.c_double), ("rel_resid", C.c_double)]
 
 
 class HfmError(RuntimeError):
@@ -101,6 +102,8 @@ SIGNATURES = {
     "hfm_mg_cancel": (I, [P, I, P]),
     "hfm_mg_solve": (I, [P, P, P, C.POINTER(HfmSlotStats), P]),
     "hfm_mg_read_level": (I, [P, I, I, I, P, P]),
+    "hfm_mg_load_f64": (I, [P, I, P, P, P]),
+    "hfm_mg_fetch_f64": (I, [P, I, P, P]),
 }
 
 _lib = None

@@ -24,13 +24,17 @@ namespace hfm {
 
 struct SlotState {
   int status;
-  int cycles;
+  int cycles;        // cycles (stationary) or CG iterations (in total, for refinement)
   int sol_buf;
-  int pad;
+  int inner_cycles;  // CG iterations of the current (inner) solve
   double norm_b;
-  double rel;
+  double rel;        // last relative residual (outer residual for refinement)
   double rz;
   double pq;
+  double rr;         // last ||r||^2 of the CG residual (scales the preconditioner input)
+  double inner_norm; // refinement: ||b - A x|| when the current inner solve started
+  int outer;         // refinement steps taken
+  int first;         // refinement: the next outer step has no correction to add yet
 };
 
 namespace {
@@ -38,17 +42,22 @@ namespace {
 constexpr int kMaxLevels = 24;
 
 __global__ void k_init_state(SlotState *st, int *active, int slot, const double *sumsq_b,
-                             int status_if_zero) {
+                             int status_if_zero, int *outer_mask) {
   double nb = sqrt(sumsq_b[0]);
   SlotState s;
   s.status = HFM_OK;
   s.cycles = 0;
   s.sol_buf = 0;
-  s.pad = 0;
+
   s.norm_b = nb;
   s.rel = 1.0;
   s.rz = 0.0;
   s.pq = 0.0;
+  s.inner_cycles = 0;
+  s.rr = sumsq_b[0];
+  s.inner_norm = nb;
+  s.outer = 0;
+  s.first = 1;
   int act = 1;
   if (!(nb > 0.0)) {
     s.rel = 0.0;
@@ -57,7 +66,12 @@ __global__ void k_init_state(SlotState *st, int *active, int slot, const double 
     else s.status = status_if_zero;
   }
   st[slot] = s;
-  active[slot] = act;
+  if (outer_mask) {  // refinement starts with an outer step (residual of x0 in float64)
+    outer_mask[slot] = act;
+    active[slot] = 0;
+  } else {
+    active[slot] = act;
+  }
 }
 
 // Sum the residual partials of each slot, update its state, switch it off when done.
@@ -77,6 +91,7 @@ __global__ void k_check(const double *__restrict__ partials, int nblk, SlotState
     SlotState s = st[inst];
     double rel = sqrt(tot) / s.norm_b;
     s.rel = rel;
+    s.rr = tot;
     if (!(rel == rel) || isinf(rel)) {
       s.status = HFM_ERR_NAN;
       s.sol_buf = which_buf;
@@ -91,8 +106,168 @@ __global__ void k_check(const double *__restrict__ partials, int nblk, SlotState
       active[inst] = 0;
     } else {
       s.cycles += 1;
+      s.inner_cycles += 1;
     }
     st[inst] = s;
+  }
+}
+
+// End of one inner CG iteration of the refinement: the inner solve stops when its residual
+// reaches max(inner_tol * ||r0||, 0.3 tol ||b||) or after inner_max iterations, and hands
+// the slot to the outer (float64) step.
+__global__ void k_check_inner(const double *__restrict__ partials, int nblk, SlotState *st,
+                              int *active, int *outer_mask, double tol, double inner_tol,
+                              int inner_max) {
+  const int inst = blockIdx.x;
+  if (!active[inst]) return;
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) acc += partials[(int64_t)inst * nblk + i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sh[w];
+    SlotState s = st[inst];
+    s.rr = tot;
+    s.cycles += 1;
+    s.inner_cycles += 1;
+    const double r = sqrt(tot);
+    const double target = fmax(inner_tol * s.inner_norm, 0.3 * tol * s.norm_b);
+    if (!(r == r) || isinf(r)) {
+      s.status = HFM_ERR_NAN;
+      active[inst] = 0;
+    } else if (r < target || s.inner_cycles >= inner_max) {
+      active[inst] = 0;
+      outer_mask[inst] = 1;
+    }
+    st[inst] = s;
+  }
+}
+
+// Outer step bookkeeping: relative residual of the float64 solution; finish, or start the
+// next inner solve from its residual.
+__global__ void k_check_outer(const double *__restrict__ partials, int nblk, SlotState *st,
+                              int *active, int *outer_mask, double tol, int max_cycles) {
+  const int inst = blockIdx.x;
+  if (!outer_mask[inst]) return;
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) acc += partials[(int64_t)inst * nblk + i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sh[w];
+    SlotState s = st[inst];
+    const double r = sqrt(tot);
+    const double rel = r / s.norm_b;
+    s.rel = rel;
+    s.outer += 1;
+    s.first = 0;
+    outer_mask[inst] = 0;
+    if (!(rel == rel) || isinf(rel)) {
+      s.status = HFM_ERR_NAN;
+    } else if (rel < tol) {
+      s.status = HFM_OK;
+    } else if (s.cycles >= max_cycles) {
+      s.status = HFM_ERR_NOT_CONVERGED;
+    } else {
+      s.inner_norm = r;
+      s.rr = tot;
+      s.rz = 0.0;
+      s.inner_cycles = 0;
+      active[inst] = 1;
+    }
+    st[inst] = s;
+  }
+}
+
+// x64 += x_in for slots whose outer step is due (not before the first inner solve).
+__global__ void k_ir_update(double *__restrict__ x64, const float *__restrict__ xin, int64_t n,
+                            const SlotState *st, const int *outer_mask) {
+  const int64_t inst = blockIdx.y;
+  if (!outer_mask[inst] || st[inst].first) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x64[inst * n + i] += (double)xin[inst * n + i];
+}
+
+// A new inner solve starts from x_in = 0.
+__global__ void k_ir_start_inner(float *__restrict__ xin, int64_t n, const SlotState *st,
+                                 const int *active) {
+  const int64_t inst = blockIdx.y;
+  if (!active[inst] || st[inst].inner_cycles != 0) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    xin[inst * n + i] = 0.f;
+}
+
+// float64 outer residual r = b - A x (sigma / kernel read as float32), partial sums of r^2.
+template <int KIND>
+__global__ void k_residual64(DevOp op, const double *__restrict__ x, const double *__restrict__ b,
+                             float *__restrict__ rout, int Z, int Y, int X,
+                             const int *__restrict__ mask, double *__restrict__ partials) {
+  __shared__ double sh[32];
+  const int64_t inst = blockIdx.y;
+  if (!mask[inst]) return;
+  const int64_t n = (int64_t)Z * Y * X;
+  const double *xi = x + inst * n;
+  auto P = [&](int zz, int yy, int xx) -> double {
+    if (zz < 0 || zz >= Z || yy < 0 || yy >= Y || xx < 0 || xx >= X) return 0.0;
+    return xi[((int64_t)zz * Y + yy) * X + xx];
+  };
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int xx = (int)(i % X);
+    const int64_t t = i / X;
+    const int yy = (int)(t % Y), zz = (int)(t / Y);
+    double ax;
+    if (KIND == HFM_OP_K27) {
+      ax = 0.0;
+      for (int a = 0; a < 3; ++a)
+        for (int bb = 0; bb < 3; ++bb)
+          for (int c = 0; c < 3; ++c) {
+            const float w = op.k[9 * a + 3 * bb + c];
+            if (w != 0.f) ax += (double)w * P(zz + a - 1, yy + bb - 1, xx + c - 1);
+          }
+    } else if (KIND == HFM_OP_CONST7) {
+      const double kz = op.k[0], ky = op.k[1], kx = op.k[2];
+      ax = 2.0 * (kz + ky + kx) * P(zz, yy, xx) - kz * (P(zz - 1, yy, xx) + P(zz + 1, yy, xx)) -
+           ky * (P(zz, yy - 1, xx) + P(zz, yy + 1, xx)) - kx * (P(zz, yy, xx - 1) + P(zz, yy, xx + 1));
+    } else {
+      const float *sx = (const float *)op.coef[0] + inst * op.coef_stride;
+      const float *sy = (const float *)op.coef[1] + inst * op.coef_stride;
+      const float *sz = (const float *)op.coef[2] + inst * op.coef_stride;
+      const double sc = op.scale;
+      const double cz = op.c[0] * sc, cy = op.c[1] * sc, cx = op.c[2] * sc;
+      const double vx = sx[i], vy = sy[i], vz = sz[i];
+      const int64_t PL = (int64_t)X * Y;
+      const double axm = cx * (xx > 0 ? 0.5 * (vx + sx[i - 1]) : vx);
+      const double axp = cx * (xx < X - 1 ? 0.5 * (vx + sx[i + 1]) : vx);
+      const double aym = cy * (yy > 0 ? 0.5 * (vy + sy[i - X]) : vy);
+      const double ayp = cy * (yy < Y - 1 ? 0.5 * (vy + sy[i + X]) : vy);
+      const double azm = cz * (zz > 0 ? 0.5 * (vz + sz[i - PL]) : vz);
+      const double azp = cz * (zz < Z - 1 ? 0.5 * (vz + sz[i + PL]) : vz);
+      const double pc = P(zz, yy, xx);
+      ax = axm * (pc - P(zz, yy, xx - 1)) + axp * (pc - P(zz, yy, xx + 1)) +
+           aym * (pc - P(zz, yy - 1, xx)) + ayp * (pc - P(zz, yy + 1, xx)) +
+           azm * (pc - P(zz - 1, yy, xx)) + azp * (pc - P(zz + 1, yy, xx));
+    }
+    const double r = b[inst * n + i] - ax;
+    rout[inst * n + i] = (float)r;
+    acc += r * r;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    partials[inst * gridDim.x + blockIdx.x] = t;
   }
 }
 
@@ -110,8 +285,40 @@ __global__ void k_fetch(const T *__restrict__ b0, const T *__restrict__ b1,
   }
 }
 
+__global__ void k_to_f64(const void *__restrict__ src, int dt, double *__restrict__ dst, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = dt == HFM_F64 ? ((const double *)src)[i] : (double)((const float *)src)[i];
+}
+
+__global__ void k_f64_to_f32(const double *__restrict__ src, float *__restrict__ dst, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+
+__global__ void k_sumsq64(const double *__restrict__ x, int64_t n, double *__restrict__ partials) {
+  __shared__ double sh[32];
+  const int64_t inst = blockIdx.y;
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = x[inst * n + i];
+    acc += v * v;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    partials[inst * gridDim.x + blockIdx.x] = t;
+  }
+}
+
 // Initial state of every slot from its ||b||^2 (batched load).
-__global__ void k_init_states(SlotState *st, int *active, int B, const double *sumsq_b) {
+__global__ void k_init_states(SlotState *st, int *active, int B, const double *sumsq_b,
+                              int *outer_mask) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= B) return;
   double nb = sqrt(sumsq_b[i]);
@@ -119,11 +326,16 @@ __global__ void k_init_states(SlotState *st, int *active, int B, const double *s
   s.status = HFM_OK;
   s.cycles = 0;
   s.sol_buf = 0;
-  s.pad = 0;
+
   s.norm_b = nb;
   s.rel = 1.0;
   s.rz = 0.0;
   s.pq = 0.0;
+  s.inner_cycles = 0;
+  s.rr = sumsq_b[i];
+  s.inner_norm = nb;
+  s.outer = 0;
+  s.first = 1;
   int act = 1;
   if (!(nb > 0.0)) {
     s.rel = 0.0;
@@ -131,7 +343,12 @@ __global__ void k_init_states(SlotState *st, int *active, int B, const double *s
     s.status = (nb != nb) ? HFM_ERR_NAN : HFM_OK;
   }
   st[i] = s;
-  active[i] = act;
+  if (outer_mask) {
+    outer_mask[i] = act;
+    active[i] = 0;
+  } else {
+    active[i] = act;
+  }
 }
 
 template <class T>
@@ -147,17 +364,25 @@ __global__ void k_fetch_all(const T *__restrict__ b0, const T *__restrict__ b1,
 }
 
 // ----------------------------------------------------------------- CG vector kernels
+// Scale of the preconditioner input for 16-bit storage: the cycle solves for r / s with
+// s = RMS(r), so its fields stay O(1) in bf16 / fp16 whatever the residual's size; z = s M(r/s).
+__device__ __forceinline__ float pc_scale(const SlotState &s, int64_t n, int scaled) {
+  return (scaled && s.rr > 0.0) ? (float)sqrt(s.rr / (double)n) : 1.f;
+}
+
 template <class TZ>
 __global__ void k_dot_partials(const float *__restrict__ a, const TZ *__restrict__ b,
                                int64_t n, int64_t sa, int64_t sb, double *partials,
-                               const int *active) {
+                               const int *active, const SlotState *st, int scaled) {
   __shared__ double sh[32];
   const int64_t inst = blockIdx.y;
   if (!active[inst]) return;
+  const double zs = st ? pc_scale(st[inst], n, scaled) : 1.0;
   double acc = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     acc += (double)a[inst * sa + i] * (double)St<TZ>::ld(b + inst * sb + i);
+  acc *= zs;
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
   __syncthreads();
@@ -190,15 +415,20 @@ __global__ void k_scalar_sum(const double *__restrict__ partials, int nblk, Slot
 // p = z + beta p (beta = rz_new / rz; first iteration p = z); rz <- rz_new.
 template <class TZ>
 __global__ void k_cg_p(const TZ *__restrict__ z, float *__restrict__ p, int64_t n, int64_t sz,
-                       int64_t sp, SlotState *st, const double *rz_new, const int *active) {
+                       int64_t sp, SlotState *st, const double *rz_new, const int *active,
+                       int scaled) {
   const int64_t inst = blockIdx.y;
   if (!active[inst]) return;
   const SlotState s = st[inst];
   const double rzn = rz_new[inst];
-  const float beta = (s.cycles == 0 || s.rz == 0.0) ? 0.f : (float)(rzn / s.rz);
+  const bool first = s.inner_cycles == 0 || s.rz == 0.0;
+  const float beta = first ? 0.f : (float)(rzn / s.rz);
+  const float zs = pc_scale(s, n, scaled);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    p[inst * sp + i] = St<TZ>::ld(z + inst * sz + i) + beta * p[inst * sp + i];
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float zv = zs * St<TZ>::ld(z + inst * sz + i);
+    p[inst * sp + i] = first ? zv : zv + beta * p[inst * sp + i];
+  }
 }
 
 __global__ void k_cg_commit_rz(SlotState *st, const double *rz_new, const int *active, int B) {
@@ -243,12 +473,14 @@ __global__ void k_negate(float *__restrict__ v, int64_t n) {
 
 template <class T>
 __global__ void k_to_storage(const float *__restrict__ a, T *__restrict__ b, int64_t n,
-                             const int *active, int64_t stride) {
+                             const int *active, int64_t stride, const SlotState *st,
+                             int scaled) {
   const int64_t inst = blockIdx.y;
   if (!active[inst]) return;
+  const float inv = 1.f / pc_scale(st[inst], n, scaled);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    b[inst * stride + i] = St<T>::from(a[inst * stride + i]);
+    b[inst * stride + i] = St<T>::from(a[inst * stride + i] * inv);
 }
 
 int vec_blocks(int64_t n, int B) {
@@ -277,6 +509,8 @@ class EngineBase {
   virtual int load(int slot, const float *rhs, const float *phi0, cudaStream_t s) = 0;
   virtual int fetch(int slot, float *out, cudaStream_t s) = 0;
   virtual int load_all(const float *rhs, cudaStream_t s) = 0;
+  virtual int load64(int slot, const double *rhs, const double *phi0, cudaStream_t s) = 0;
+  virtual int fetch64(int slot, double *out, cudaStream_t s) = 0;
   virtual int fetch_all(float *out, cudaStream_t s) = 0;
   virtual int set_operator(int slot, const hfm_operator &op, cudaStream_t s) = 0;
   virtual int read_level(int slot, int level, int which, float *out, cudaStream_t s) = 0;
@@ -293,6 +527,9 @@ struct hfm_mg {
   void *fine_b = nullptr;   // b for CG (rhs[0] holds r in storage type)
   void *saw[2] = {nullptr, nullptr};  // sawtooth: r, w in storage type
   int *active = nullptr;
+  int *outer = nullptr;     // refinement: slots whose float64 outer step is due
+  double *x64 = nullptr;    // refinement: float64 solution and right-hand side
+  double *b64 = nullptr;
   hfm::SlotState *state = nullptr;
   double *partials = nullptr;
   int64_t partials_per_slot = 0;
@@ -314,7 +551,7 @@ class Engine : public EngineBase {
 
   bool cycle_flips_parity() const override {
     const hfm_mg_config &c = m_->cfg;
-    if (c.accel == HFM_ACCEL_CG) return false;
+    if (c.accel != HFM_ACCEL_NONE) return false;
     if (c.cycle == HFM_CYCLE_SAWTOOTH) return true;
     int post = std::max(c.nu_post, 1);
     return ((c.nu_pre + post) & 1) != 0;
@@ -460,24 +697,60 @@ class Engine : public EngineBase {
   }
 
   // ----------------------------------------------------------------- PCG iteration
-  int cg_iteration(cudaStream_t s) {
+  // float64 outer step of the refinement for the slots whose inner solve ended:
+  // x64 += x_in; r = b - A x64 (float64); finish or restart the inner solve from r.
+  int outer_step(cudaStream_t s) {
+    const int B = m_->slots;
+    const int64_t nf = n(0);
+    const int vb = vec_blocks(nf, B);
+    k_ir_update<<<dim3(vb, B), 256, 0, s>>>(m_->x64, m_->cg[0], nf, m_->state, m_->outer);
+    HFM_CHECK_LAUNCH("k_ir_update");
+    DevOp d = fine32_;
+    switch (kind()) {
+      case HFM_OP_SIGMA7:
+        k_residual64<HFM_OP_SIGMA7><<<dim3(vb, B), 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1],
+                                                                g(0).Z, g(0).Y, g(0).X, m_->outer,
+                                                                m_->partials);
+        break;
+      case HFM_OP_CONST7:
+        k_residual64<HFM_OP_CONST7><<<dim3(vb, B), 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1],
+                                                                g(0).Z, g(0).Y, g(0).X, m_->outer,
+                                                                m_->partials);
+        break;
+      default:
+        k_residual64<HFM_OP_K27><<<dim3(vb, B), 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1],
+                                                             g(0).Z, g(0).Y, g(0).X, m_->outer,
+                                                             m_->partials);
+    }
+    HFM_CHECK_LAUNCH("k_residual64");
+    k_check_outer<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
+                                    m_->cfg.tol, m_->cfg.max_cycles);
+    HFM_CHECK_LAUNCH("k_check_outer");
+    k_ir_start_inner<<<dim3(vb, B), 256, 0, s>>>(m_->cg[0], nf, m_->state, m_->active);
+    HFM_CHECK_LAUNCH("k_ir_start_inner");
+    return HFM_OK;
+  }
+
+  int cg_iteration(cudaStream_t s, bool ir) {
     const int B = m_->slots;
     const int64_t nf = n(0);
     float *x = m_->cg[0], *r = m_->cg[1], *p = m_->cg[2], *q = m_->cg[3];
     const int vb = vec_blocks(nf, B);
+    const int scaled = std::is_same<T, float>::value ? 0 : 1;
     int st;
-    // z = M r  (rhs(0) holds r in the storage type)
+    // z = M r  (rhs(0) holds r / s in the storage type; float32 storage reads r in place)
     if (!std::is_same<T, float>::value) {
-      k_to_storage<T><<<dim3(vb, B), 256, 0, s>>>(r, rhs(0), nf, m_->active, nf);
+      k_to_storage<T><<<dim3(vb, B), 256, 0, s>>>(r, rhs(0), nf, m_->active, nf, m_->state, scaled);
       HFM_CHECK_LAUNCH("k_to_storage");
     }
     if ((st = vcycle(0, true, m_->cfg.cycle == HFM_CYCLE_F, 0, s))) return st;
     const T *z = buf(0, cur_[0]);
     // rz_new = r . z ; p = z + beta p
-    k_dot_partials<T><<<dim3(vb, B), 256, 0, s>>>(r, z, nf, nf, nf, m_->partials, m_->active);
+    k_dot_partials<T><<<dim3(vb, B), 256, 0, s>>>(r, z, nf, nf, nf, m_->partials, m_->active,
+                                                  m_->state, scaled);
     HFM_CHECK_LAUNCH("k_dot_partials");
     k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 0, m_->scal);
-    k_cg_p<T><<<dim3(vb, B), 256, 0, s>>>(z, p, nf, nf, nf, m_->state, m_->scal, m_->active);
+    k_cg_p<T><<<dim3(vb, B), 256, 0, s>>>(z, p, nf, nf, nf, m_->state, m_->scal, m_->active, scaled);
     k_cg_commit_rz<<<(B + 127) / 128, 128, 0, s>>>(m_->state, m_->scal, m_->active, B);
     HFM_CHECK_LAUNCH("k_cg_p");
     // q = A p ; pq = p . q   (FP32 operator on the fine level)
@@ -486,12 +759,17 @@ class Engine : public EngineBase {
     pp.base = p;
     pp.base_stride = nf;
     if ((st = launch_apply<float>(kind(), fine32_, pp, q, nf, B, g(0), m_->active, s))) return st;
-    k_dot_partials<float><<<dim3(vb, B), 256, 0, s>>>(p, q, nf, nf, nf, m_->partials, m_->active);
+    k_dot_partials<float><<<dim3(vb, B), 256, 0, s>>>(p, q, nf, nf, nf, m_->partials, m_->active,
+                                                      nullptr, 0);
     k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 1, m_->scal);
     // x += alpha p ; r -= alpha q ; ||r||
     k_cg_xr<<<dim3(vb, B), 256, 0, s>>>(x, r, p, q, nf, nf, m_->state, m_->partials, m_->active);
     HFM_CHECK_LAUNCH("k_cg_xr");
-    return check(vb, 0, s);
+    if (!ir) return check(vb, 0, s);
+    k_check_inner<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
+                                    m_->cfg.tol, m_->cfg.inner_tol, m_->cfg.inner_max_cycles);
+    HFM_CHECK_LAUNCH("k_check_inner");
+    return HFM_OK;
   }
 
   int emit_cycles(int cycles, cudaStream_t s) override {
@@ -499,12 +777,15 @@ class Engine : public EngineBase {
     for (int k = 0; k < kMaxLevels; ++k) cur_[k] = 0;
     for (int i = 0; i < cycles; ++i) {
       const hfm_mg_config &c = m_->cfg;
-      if (c.accel == HFM_ACCEL_CG) st = cg_iteration(s);
+      if (c.accel == HFM_ACCEL_IR) {
+        if ((st = outer_step(s))) return st;
+        st = cg_iteration(s, true);
+      } else if (c.accel == HFM_ACCEL_CG) st = cg_iteration(s, false);
       else if (c.cycle == HFM_CYCLE_SAWTOOTH) st = sawtooth(s);
       else st = vcycle(0, false, c.cycle == HFM_CYCLE_F, 1, s);
       if (st) return st;
     }
-    if (m_->cfg.accel != HFM_ACCEL_CG && cur_[0] != 0)
+    if (m_->cfg.accel == HFM_ACCEL_NONE && cur_[0] != 0)
       return fail(HFM_ERR_BAD_ARG, "internal: odd number of fine-level sweeps in a launch");
     return HFM_OK;
   }
@@ -558,9 +839,45 @@ class Engine : public EngineBase {
     return HFM_OK;
   }
 
+  // Refinement: float64 right-hand side / initial guess (from float32 or float64 input).
+  int load_ir(int slot, int count, const void *b, const void *phi0, int dt, cudaStream_t s) {
+    const int64_t nf = n(0) * count;
+    double *bb = m_->b64 + (int64_t)slot * n(0), *xx = m_->x64 + (int64_t)slot * n(0);
+    const int vb = vec_blocks(nf, 1);
+    k_to_f64<<<vb, 256, 0, s>>>(b, dt, bb, nf);
+    if (phi0) k_to_f64<<<vb, 256, 0, s>>>(phi0, dt, xx, nf);
+    else HFM_CUDA(cudaMemsetAsync(xx, 0, nf * 8, s));
+    HFM_CHECK_LAUNCH("k_to_f64");
+    HFM_CUDA(cudaMemsetAsync(m_->cg[0] + (int64_t)slot * n(0), 0, nf * 4, s));
+    const int nb = vec_blocks(n(0), count);
+    k_sumsq64<<<dim3(nb, count), 256, 0, s>>>(bb, n(0), m_->partials);
+    HFM_CHECK_LAUNCH("k_sumsq64");
+    int st;
+    if ((st = launch_finalize_sum(m_->partials, nb, count, m_->scal + (count == 1 ? m_->slots : 0), s)))
+      return st;
+    if (count == 1)
+      k_init_state<<<1, 1, 0, s>>>(m_->state, m_->active, slot, m_->scal + m_->slots, HFM_OK, m_->outer);
+    else
+      k_init_states<<<(count + 127) / 128, 128, 0, s>>>(m_->state, m_->active, count, m_->scal, m_->outer);
+    HFM_CHECK_LAUNCH("k_init_state");
+    return HFM_OK;
+  }
+
+  int load64(int slot, const double *b, const double *phi0, cudaStream_t s) override {
+    if (m_->cfg.accel != HFM_ACCEL_IR) return fail(HFM_ERR_UNSUPPORTED, "float64 load needs accel = IR");
+    return load_ir(slot, 1, b, phi0, HFM_F64, s);
+  }
+
+  int fetch64(int slot, double *out, cudaStream_t s) override {
+    if (m_->cfg.accel != HFM_ACCEL_IR) return fail(HFM_ERR_UNSUPPORTED, "float64 fetch needs accel = IR");
+    HFM_CUDA(cudaMemcpyAsync(out, m_->x64 + (int64_t)slot * n(0), n(0) * 8, cudaMemcpyDeviceToDevice, s));
+    return HFM_OK;
+  }
+
   int load(int slot, const float *b, const float *phi0, cudaStream_t s) override {
     const int64_t nf = n(0);
     int st;
+    if (m_->cfg.accel == HFM_ACCEL_IR) return load_ir(slot, 1, b, phi0, HFM_F32, s);
     const bool cg = m_->cfg.accel == HFM_ACCEL_CG;
     if (cg) {
       float *x = m_->cg[0] + slot * nf, *r = m_->cg[1] + slot * nf, *bb = (float *)m_->fine_b + slot * nf;
@@ -596,7 +913,7 @@ class Engine : public EngineBase {
     int nb = 0;
     if ((st = launch_sumsq_partials<float>(b, nf, nf, 1, m_->partials, &nb, nullptr, s))) return st;
     if ((st = launch_finalize_sum(m_->partials, nb, 1, m_->scal + m_->slots, s))) return st;
-    k_init_state<<<1, 1, 0, s>>>(m_->state, m_->active, slot, m_->scal + m_->slots, HFM_OK);
+    k_init_state<<<1, 1, 0, s>>>(m_->state, m_->active, slot, m_->scal + m_->slots, HFM_OK, nullptr);
     HFM_CHECK_LAUNCH("k_init_state");
     return HFM_OK;
   }
@@ -606,6 +923,7 @@ class Engine : public EngineBase {
     const int64_t nf = n(0);
     const int B = m_->slots;
     int st;
+    if (m_->cfg.accel == HFM_ACCEL_IR) return load_ir(0, B, b, nullptr, HFM_F32, s);
     if (m_->cfg.accel == HFM_ACCEL_CG) {
       HFM_CUDA(cudaMemcpyAsync(m_->fine_b, b, nf * B * 4, cudaMemcpyDeviceToDevice, s));
       HFM_CUDA(cudaMemsetAsync(m_->cg[0], 0, nf * B * 4, s));
@@ -618,13 +936,18 @@ class Engine : public EngineBase {
     int nb = 0;
     if ((st = launch_sumsq_partials<float>(b, nf, nf, B, m_->partials, &nb, nullptr, s))) return st;
     if ((st = launch_finalize_sum(m_->partials, nb, B, m_->scal, s))) return st;
-    k_init_states<<<(B + 127) / 128, 128, 0, s>>>(m_->state, m_->active, B, m_->scal);
+    k_init_states<<<(B + 127) / 128, 128, 0, s>>>(m_->state, m_->active, B, m_->scal, nullptr);
     HFM_CHECK_LAUNCH("k_init_states");
     return HFM_OK;
   }
 
   int fetch_all(float *out, cudaStream_t s) override {
     const int64_t nf = n(0);
+    if (m_->cfg.accel == HFM_ACCEL_IR) {
+      k_f64_to_f32<<<vec_blocks(nf * m_->slots, 1), 256, 0, s>>>(m_->x64, out, nf * m_->slots);
+      HFM_CHECK_LAUNCH("k_f64_to_f32");
+      return HFM_OK;
+    }
     const float *bx = m_->cfg.accel == HFM_ACCEL_CG ? m_->cg[0] : nullptr;
     k_fetch_all<T><<<dim3(vec_blocks(nf, m_->slots), m_->slots), 256, 0, s>>>(
         buf(0, 0), buf(0, 1), bx, nf, m_->state, m_->active, out);
@@ -634,6 +957,11 @@ class Engine : public EngineBase {
 
   int fetch(int slot, float *out, cudaStream_t s) override {
     const int64_t nf = n(0);
+    if (m_->cfg.accel == HFM_ACCEL_IR) {
+      k_f64_to_f32<<<vec_blocks(nf, 1), 256, 0, s>>>(m_->x64 + slot * nf, out, nf);
+      HFM_CHECK_LAUNCH("k_f64_to_f32");
+      return HFM_OK;
+    }
     const float *bx = m_->cfg.accel == HFM_ACCEL_CG ? m_->cg[0] + slot * nf : nullptr;
     k_fetch<T><<<vec_blocks(nf, 1), 256, 0, s>>>(buf(0, 0) + slot * nf, buf(0, 1) + slot * nf,
                                                 bx, nf, m_->state, m_->active, slot, out);
@@ -644,7 +972,7 @@ class Engine : public EngineBase {
   int read_level(int slot, int level, int which, float *out, cudaStream_t s) override {
     if (level < 0 || level >= m_->L) return fail(HFM_ERR_BAD_ARG, "level out of range");
     const T *src_p;
-    if (m_->cfg.cycle == HFM_CYCLE_SAWTOOTH && level == 0 && m_->cfg.accel != HFM_ACCEL_CG)
+    if (m_->cfg.cycle == HFM_CYCLE_SAWTOOTH && level == 0 && m_->cfg.accel == HFM_ACCEL_NONE)
       src_p = (const T *)(which ? m_->saw[0] : m_->saw[1]);
     else
       src_p = which ? rhs(level) : buf(level, 0);
@@ -703,11 +1031,11 @@ int validate_cfg(const hfm_mg_config &c, int Z, int Y, int X, int slots) {
     return fail(HFM_ERR_UNSUPPORTED, "hfm_mg_create: operator kind must be CONST7, SIGMA7 or K27");
   if (c.storage != HFM_F32 && c.storage != HFM_BF16 && c.storage != HFM_F16)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: storage must be F32, BF16 or F16");
-  if (c.cycle < 0 || c.cycle > 2 || c.accel < 0 || c.accel > 1)
+  if (c.cycle < 0 || c.cycle > 2 || c.accel < 0 || c.accel > 2)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: bad cycle / accel");
-  if (c.cycle == HFM_CYCLE_SAWTOOTH && c.accel == HFM_ACCEL_CG)
+  if (c.cycle == HFM_CYCLE_SAWTOOTH && c.accel != HFM_ACCEL_NONE)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: the sawtooth cycle is not symmetric; use V or F with CG");
-  if (c.accel == HFM_ACCEL_CG && c.nu_pre != c.nu_post)
+  if (c.accel != HFM_ACCEL_NONE && c.nu_pre != c.nu_post)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: CG needs a symmetric cycle (nu_pre == nu_post)");
   if (c.nu_pre < 0 || c.nu_post < 0 || c.coarse_sweeps < 1 || c.max_cycles < 1)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: bad sweep counts");
@@ -739,6 +1067,8 @@ void hfm_mg_config_default(hfm_mg_config *c) {
   c->tol = 1e-6;
   c->max_cycles = 500;
   c->cycles_per_launch = 4;
+  c->inner_tol = 1e-6;
+  c->inner_max_cycles = 200;
 }
 
 size_t hfm_mg_footprint_bytes(const hfm_mg_config *c, int Z, int Y, int X, int slots) {
@@ -752,8 +1082,9 @@ size_t hfm_mg_footprint_bytes(const hfm_mg_config *c, int Z, int Y, int X, int s
     tot += nl * fields * es;
   }
   const size_t nf = (size_t)Z * Y * X;
-  if (c->accel == HFM_ACCEL_CG) {
+  if (c->accel != HFM_ACCEL_NONE) {
     tot += nf * 5 * 4;  // x r p q b
+    if (c->accel == HFM_ACCEL_IR) tot += nf * 2 * 8;  // float64 x, b
     if (c->op_kind == HFM_OP_SIGMA7 && c->storage != HFM_F32) tot += nf * 3 * 4;
   } else if (c->cycle == HFM_CYCLE_SAWTOOTH) {
     tot += nf * 2 * es;
@@ -794,13 +1125,18 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
     L.phi = dalloc(m.get(), b, &st);
     L.tmp = dalloc(m.get(), b, &st);
     // float32 CG: the fine-level cycle reads the CG residual in place (set below)
-    if (!(l == 0 && cfg->accel == HFM_ACCEL_CG && cfg->storage == HFM_F32))
+    if (!(l == 0 && cfg->accel != HFM_ACCEL_NONE && cfg->storage == HFM_F32))
       L.rhs = dalloc(m.get(), b, &st);
     if (cfg->op_kind == HFM_OP_SIGMA7)
       for (int a = 0; a < 3; ++a) L.coef[a] = dalloc(m.get(), b, &st);
   }
   const size_t nf = (size_t)Z * Y * X * slots;
-  if (cfg->accel == HFM_ACCEL_CG) {
+  if (cfg->accel == HFM_ACCEL_IR) {
+    m->x64 = (double *)dalloc(m.get(), nf * 8, &st);
+    m->b64 = (double *)dalloc(m.get(), nf * 8, &st);
+  }
+  m->outer = (int *)dalloc(m.get(), (size_t)slots * 4, &st);
+  if (cfg->accel != HFM_ACCEL_NONE) {
     for (int i = 0; i < 4; ++i) m->cg[i] = (float *)dalloc(m.get(), nf * 4, &st);
     m->fine_b = dalloc(m.get(), nf * 4, &st);
     if (cfg->storage == HFM_F32) m->lv[0].rhs = m->cg[1];
@@ -815,6 +1151,7 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
   m->scal = (double *)dalloc(m.get(), (size_t)(slots + 1) * 8, &st);
   if (!st) {
     if (cudaMemset(m->active, 0, (size_t)slots * 4) != cudaSuccess ||
+        cudaMemset(m->outer, 0, (size_t)slots * 4) != cudaSuccess ||
         cudaMemset(m->state, 0, (size_t)slots * sizeof(SlotState)) != cudaSuccess)
       st = fail(HFM_ERR_CUDA, "cudaMemset failed");
   }
@@ -827,7 +1164,7 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
       default: m->eng.reset(new Engine<__half>(m.get())); break;
     }
     // CG runs its outer vectors and fine operator in float32: keep float32 conductivities.
-    if (cfg->accel == HFM_ACCEL_CG && cfg->op_kind == HFM_OP_SIGMA7 && cfg->storage != HFM_F32) {
+    if (cfg->accel != HFM_ACCEL_NONE && cfg->op_kind == HFM_OP_SIGMA7 && cfg->storage != HFM_F32) {
       float **fc = nullptr;
       switch (cfg->storage) {
         case HFM_BF16: fc = ((Engine<__nv_bfloat16> *)m->eng.get())->fine32_coef_; break;
@@ -922,16 +1259,17 @@ int hfm_mg_run(hfm_mg *m, int cycles, hfm_stream_t stream) {
 int hfm_mg_query(hfm_mg *m, hfm_slot_stats *out, hfm_stream_t stream) {
   if (!m || !out) return fail(HFM_ERR_BAD_ARG, "hfm_mg_query: bad argument");
   std::vector<SlotState> st(m->slots);
-  std::vector<int> act(m->slots);
+  std::vector<int> act(m->slots), outer(m->slots);
   cudaStream_t s = (cudaStream_t)stream;
   HFM_CUDA(cudaMemcpyAsync(st.data(), m->state, m->slots * sizeof(SlotState), cudaMemcpyDeviceToHost, s));
   HFM_CUDA(cudaMemcpyAsync(act.data(), m->active, m->slots * 4, cudaMemcpyDeviceToHost, s));
+  HFM_CUDA(cudaMemcpyAsync(outer.data(), m->outer, m->slots * 4, cudaMemcpyDeviceToHost, s));
   HFM_CUDA(cudaStreamSynchronize(s));
   for (int i = 0; i < m->slots; ++i) {
-    out[i].active = act[i];
+    out[i].active = act[i] | outer[i];
     out[i].status = st[i].status;
     out[i].cycles = st[i].cycles;
-    out[i].reserved = 0;
+    out[i].outer = st[i].outer;
     out[i].norm_b = st[i].norm_b;
     out[i].rel_resid = st[i].rel;
   }
@@ -946,7 +1284,19 @@ int hfm_mg_fetch(hfm_mg *m, int slot, float *out, hfm_stream_t stream) {
 int hfm_mg_cancel(hfm_mg *m, int slot, hfm_stream_t stream) {
   if (!m || slot < 0 || slot >= m->slots) return fail(HFM_ERR_BAD_ARG, "hfm_mg_cancel: bad argument");
   HFM_CUDA(cudaMemsetAsync(m->active + slot, 0, 4, (cudaStream_t)stream));
+  HFM_CUDA(cudaMemsetAsync(m->outer + slot, 0, 4, (cudaStream_t)stream));
   return HFM_OK;
+}
+
+int hfm_mg_load_f64(hfm_mg *m, int slot, const double *rhs, const double *phi0,
+                    hfm_stream_t stream) {
+  if (!m || !rhs || slot < 0 || slot >= m->slots) return fail(HFM_ERR_BAD_ARG, "hfm_mg_load_f64: bad argument");
+  return m->eng->load64(slot, rhs, phi0, (cudaStream_t)stream);
+}
+
+int hfm_mg_fetch_f64(hfm_mg *m, int slot, double *phi_out, hfm_stream_t stream) {
+  if (!m || !phi_out || slot < 0 || slot >= m->slots) return fail(HFM_ERR_BAD_ARG, "hfm_mg_fetch_f64: bad argument");
+  return m->eng->fetch64(slot, phi_out, (cudaStream_t)stream);
 }
 
 int hfm_mg_read_level(hfm_mg *m, int slot, int level, int which, float *out, hfm_stream_t stream) {

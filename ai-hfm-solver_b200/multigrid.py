@@ -17,14 +17,15 @@ from . import _lib as L
 from .ops import Operator, _check_field, _stream
 
 _CYCLES = {"sawtooth": L.CYCLE_SAWTOOTH, "V": L.CYCLE_V, "F": L.CYCLE_F}
-_ACCEL = {None: L.ACCEL_NONE, "none": L.ACCEL_NONE, "cg": L.ACCEL_CG}
+_ACCEL = {None: L.ACCEL_NONE, "none": L.ACCEL_NONE, "cg": L.ACCEL_CG, "ir": L.ACCEL_IR}
 _STORAGE = {"f32": L.F32, "bf16": L.BF16, "f16": L.F16}
 
 
 @dataclass
 class SolverConfig:
     cycle: str = "V"            # "sawtooth" (reference), "V" or "F"
-    accel: str = "none"         # "none" (stationary cycles) or "cg" (cycle preconditions CG)
+    accel: str = "none"         # "none" (stationary cycles), "cg" (cycle preconditions CG) or
+                                # "ir" (float64 iterative refinement around CG)
     n_levels: int = 0           # 0: halve while every extent is even and > min_coarse_edge
     min_coarse_edge: int = 4
     nu_pre: int = 2
@@ -40,6 +41,8 @@ class SolverConfig:
     tol: float = 1e-6
     max_cycles: int = 500
     cycles_per_launch: int = 4
+    inner_tol: float = 1e-6     # "ir": inner CG stops at max(inner_tol ||r0||, 0.3 tol ||b||)
+    inner_max_cycles: int = 200
 
     @staticmethod
     def reference(n_levels, fine_smooth=True, top_copy=False, zero_xend=False, cycles=1000):
@@ -69,6 +72,8 @@ class SolverConfig:
         c.tol = self.tol
         c.max_cycles = self.max_cycles
         c.cycles_per_launch = self.cycles_per_launch
+        c.inner_tol = self.inner_tol
+        c.inner_max_cycles = self.inner_max_cycles
         return c
 
 
@@ -143,12 +148,25 @@ class Multigrid:
 
     def query(self):
         L.call("hfm_mg_query", self._h, self._stats, _stream())
-        return [dict(active=s.active, status=s.status, cycles=s.cycles, norm_b=s.norm_b,
-                     rel_resid=s.rel_resid) for s in self._stats]
+        return [dict(active=s.active, status=s.status, cycles=s.cycles, outer=s.outer,
+                     norm_b=s.norm_b, rel_resid=s.rel_resid) for s in self._stats]
 
     def fetch(self, slot, out=None):
         out = torch.empty(self.shape, dtype=torch.float32, device="cuda") if out is None else out
         L.call("hfm_mg_fetch", self._h, int(slot), C.c_void_p(out.data_ptr()), _stream())
+        return out
+
+    def load_f64(self, slot, rhs, phi0=None):
+        """float64 right-hand side / initial guess (accel="ir")."""
+        for t in (rhs, phi0):
+            if t is not None and (t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous()):
+                raise TypeError("load_f64 takes contiguous float64 CUDA tensors")
+        L.call("hfm_mg_load_f64", self._h, int(slot), C.c_void_p(rhs.data_ptr()),
+               C.c_void_p(phi0.data_ptr() if phi0 is not None else 0), _stream())
+
+    def fetch_f64(self, slot, out=None):
+        out = torch.empty(self.shape, dtype=torch.float64, device="cuda") if out is None else out
+        L.call("hfm_mg_fetch_f64", self._h, int(slot), C.c_void_p(out.data_ptr()), _stream())
         return out
 
     def cancel(self, slot):
@@ -170,6 +188,6 @@ class Multigrid:
                                   self._stats, _stream())
         if st not in (L.OK, L.ERR_NOT_CONVERGED, L.ERR_NAN):
             L.check(st, "hfm_mg_solve")
-        stats = [dict(active=s.active, status=s.status, cycles=s.cycles, norm_b=s.norm_b,
-                      rel_resid=s.rel_resid) for s in self._stats]
+        stats = [dict(active=s.active, status=s.status, cycles=s.cycles, outer=s.outer,
+                      norm_b=s.norm_b, rel_resid=s.rel_resid) for s in self._stats]
         return phi, stats

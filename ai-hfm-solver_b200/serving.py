@@ -1,0 +1,253 @@
+"""Continuous-batching server for anisotropic forward solves of mixed grid sizes.
+
+Requests (sigma, f, arrival time) of different cubic edges arrive over time.  The server
+keeps one resident multigrid handle per edge ("bucket") with a fixed number of slots whose
+hierarchies live in HBM, sized so the buckets fit an HBM budget (admission by footprint,
+``hfm_mg_footprint_bytes``).  The serving loop
+
+1. admits every request that has arrived into a free slot of its bucket (coefficient
+   hierarchy + right-hand side loaded into that slot; requests wait in a queue while their
+   bucket is full);
+2. advances every bucket that holds work by a few cycles (one CUDA-graph launch per bucket,
+   each bucket on its own stream so the buckets overlap on the GPU); inside the graph every
+   slot runs on its own: a slot that converges, fails or hits its cycle cap switches itself
+   off and the remaining kernels skip it;
+3. polls the buckets, retires finished slots (solution copied out, latency recorded) and
+   frees them for the next arrivals.
+
+A request that arrives while others are on the GPU therefore joins the next launch of its
+bucket: iteration-level continuous batching, not a queue that waits for a batch to drain.
+Each slot's arithmetic depends only on its own data (fixed-order per-slot reductions), so a
+result is the same alone and in the mix.
+
+The plain baseline (``solve_one_at_a_time``) is the same solver with one slot per handle,
+one request at a time, float32 storage.
+"""
+import collections
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .multigrid import Multigrid, SolverConfig, footprint_bytes
+from .ops import Sigma7
+
+EDGES = (32, 48, 64, 96, 128)
+
+
+@dataclass
+class SolveRequest:
+    rid: int
+    n: int
+    arrival: float                 # seconds after the stream starts
+    sigma: torch.Tensor            # (3, n, n, n) float32 (device, or pinned host for e2e)
+    rhs: torch.Tensor              # (n, n, n) float32
+    log_std: float = 1.0
+
+
+@dataclass
+class SolveResult:
+    rid: int
+    n: int
+    status: int
+    cycles: int
+    outer: int
+    rel_resid: float
+    admitted: float
+    done: float
+    latency: float
+    phi: torch.Tensor = None
+
+
+def sigma_field(n, gen, log_std, device):
+    """Seeded log-normal conductivity: iid N(0,1) per axis, 5^3 box filter with reflected
+    edges, rescaled to mean 0 / std ``log_std``, exponentiated (same recipe as
+    ``problems.anisotropic_sigma``, generated on the device)."""
+    g = torch.randn((3, 1, n, n, n), device=device, generator=gen)
+    g = torch.nn.functional.pad(g, (2, 2, 2, 2, 2, 2), mode="reflect")
+    g = torch.nn.functional.avg_pool3d(g, 5, stride=1)[:, 0]
+    m = g.mean(dim=(1, 2, 3), keepdim=True)
+    s = g.std(dim=(1, 2, 3), keepdim=True)
+    return torch.exp((g - m) / (s + 1e-30) * log_std).contiguous()
+
+
+def dipole_field(n, rng, device, margin=4):
+    f = torch.zeros((n, n, n), device=device)
+    lo, hi = margin, n - margin
+    p = tuple(int(v) for v in rng.integers(lo, hi, 3))
+    q = p
+    while q == p:
+        q = tuple(int(v) for v in rng.integers(lo, hi, 3))
+    f[p] = 1.0
+    f[q] = -1.0
+    return f
+
+
+def make_stream(count=1024, rate=2000.0, edges=EDGES, log_std=(0.5, 2.0), seed=0,
+                device="cuda"):
+    """The serving workload: ``count`` requests, edge uniform over ``edges``, log-std uniform
+    in ``log_std``, own sigma and dipole each, Poisson arrivals at ``rate`` per second."""
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device)
+    t = 0.0
+    reqs = []
+    for i in range(count):
+        t += rng.exponential(1.0 / rate)
+        n = int(rng.choice(edges))
+        ls = float(rng.uniform(*log_std))
+        gen.manual_seed(seed * 1000003 + i)
+        reqs.append(SolveRequest(i, n, t, sigma_field(n, gen, ls, device),
+                                 dipole_field(n, rng, device), ls))
+    return reqs
+
+
+class _Bucket:
+    def __init__(self, n, cfg, slots, keep_solutions):
+        self.n = n
+        self.slots = slots
+        self.mg = Multigrid((n, n, n), L.OP_SIGMA7, cfg, slots=slots)
+        self.stream = torch.cuda.Stream()
+        self.free = list(range(slots - 1, -1, -1))
+        self.busy = {}  # slot -> (request, admitted time)
+        self.keep = keep_solutions
+        self.dev_in = None
+
+    def admit(self, req, now):
+        slot = self.free.pop()
+        with torch.cuda.stream(self.stream):
+            sig, rhs = req.sigma, req.rhs
+            if not sig.is_cuda:  # end-to-end mode: host -> device copy is part of the request
+                sig = sig.to("cuda", non_blocking=True)
+                rhs = rhs.to("cuda", non_blocking=True)
+            self.mg.set_operator(Sigma7(sig[0], sig[1], sig[2]), slot=slot)
+            self.mg.load(slot, rhs)
+            if not req.sigma.is_cuda:
+                # keep the staging tensors alive until the stream has consumed them
+                self.busy[slot] = (req, now, (sig, rhs))
+                return
+        self.busy[slot] = (req, now, None)
+
+    def launch(self, cycles):
+        if self.busy:
+            with torch.cuda.stream(self.stream):
+                self.mg.run(cycles)
+
+    def poll(self, clock, t0, host_out):
+        if not self.busy:
+            return []
+        with torch.cuda.stream(self.stream):
+            stats = self.mg.query()  # synchronises this bucket's stream
+            done = []
+            for slot, (req, adm, _) in list(self.busy.items()):
+                s = stats[slot]
+                if s["active"]:
+                    continue
+                phi = None
+                if self.keep or host_out:
+                    phi = self.mg.fetch_f64(slot) if self.mg.cfg.accel == "ir" else self.mg.fetch(slot)
+                    if host_out:
+                        phi = phi.to("cpu", non_blocking=False)
+                now = clock() - t0
+                done.append(SolveResult(req.rid, req.n, s["status"], s["cycles"], s["outer"],
+                                        s["rel_resid"], adm, now, now - req.arrival, phi))
+                del self.busy[slot]
+                self.free.append(slot)
+        return done
+
+
+class SolveServer:
+    """Buckets per edge sized to an HBM budget; ``serve`` runs a request stream."""
+
+    def __init__(self, cfg=None, edges=EDGES, slots=64, budget_bytes=120e9,
+                 cycles_per_tick=4, keep_solutions=False):
+        self.cfg = cfg or SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6,
+                                       max_cycles=600)
+        self.cycles_per_tick = cycles_per_tick
+        per = {n: footprint_bytes(self.cfg, L.OP_SIGMA7, (n, n, n), 1) for n in edges}
+        want = {n: (slots[n] if isinstance(slots, dict) else slots) for n in edges}
+        # admission by footprint: shrink the largest buckets until everything fits the budget
+        while sum(per[n] * want[n] for n in edges) > budget_bytes:
+            big = max(edges, key=lambda n: per[n] * want[n])
+            if want[big] <= 1:
+                raise ValueError("HBM budget too small for one slot per edge")
+            want[big] = max(1, want[big] // 2)
+        self.footprint = {n: per[n] * want[n] for n in edges}
+        self.buckets = {n: _Bucket(n, self.cfg, want[n], keep_solutions) for n in edges}
+
+    def close(self):
+        for b in self.buckets.values():
+            b.mg.close()
+
+    def serve(self, requests, realtime=True, host_out=False):
+        """Serve ``requests`` (sorted by arrival).  With ``realtime`` a request is admitted only
+        once its arrival time has passed on the wall clock.  Returns the list of results."""
+        clock = time.perf_counter
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        queued = {n: collections.deque() for n in self.buckets}
+        results = []
+        torch.cuda.synchronize()
+        t0 = clock()
+        total = len(pending)
+        while len(results) < total:
+            now = clock() - t0
+            while pending and (not realtime or pending[0].arrival <= now):
+                r = pending.popleft()
+                queued[r.n].append(r)
+            for n, q in queued.items():
+                b = self.buckets[n]
+                while q and b.free:
+                    b.admit(q.popleft(), clock() - t0)
+            for b in self.buckets.values():
+                b.launch(self.cycles_per_tick)
+            for b in self.buckets.values():
+                results.extend(b.poll(clock, t0, host_out))
+            if realtime and not any(b.busy for b in self.buckets.values()) and pending:
+                wait = pending[0].arrival - (clock() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 1e-3))
+        return results
+
+
+def solve_one_at_a_time(requests, cfg=None, time_budget_s=None, keep_solutions=False):
+    """The plain path: one request at a time through a single-slot float32 handle per edge.
+    Returns (results, seconds)."""
+    cfg = cfg or SolverConfig(cycle="V", accel="ir", storage="f32", tol=1e-6, max_cycles=600)
+    handles = {}
+    results = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in requests:
+        h = handles.get(r.n)
+        if h is None:
+            h = handles[r.n] = Multigrid((r.n, r.n, r.n), L.OP_SIGMA7, cfg, slots=1)
+        sig = r.sigma if r.sigma.is_cuda else r.sigma.cuda()
+        rhs = r.rhs if r.rhs.is_cuda else r.rhs.cuda()
+        ts = time.perf_counter() - t0
+        h.set_operator(Sigma7(sig[0], sig[1], sig[2]))
+        h.load(0, rhs)
+        while True:
+            h.run(cfg.cycles_per_launch)
+            s = h.query()[0]
+            if not s["active"]:
+                break
+        phi = h.fetch_f64(0) if cfg.accel == "ir" else h.fetch(0)
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        results.append(SolveResult(r.rid, r.n, s["status"], s["cycles"], s["outer"],
+                                   s["rel_resid"], ts, te, te - ts,
+                                   phi if keep_solutions else None))
+        if time_budget_s is not None and te > time_budget_s:
+            break
+    dt = time.perf_counter() - t0
+    for h in handles.values():
+        h.close()
+    return results, dt
+
+
+def latency_stats(results):
+    lat = np.array([r.latency for r in results]) * 1e3
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max())}

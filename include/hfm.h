@@ -195,7 +195,9 @@ int hfm_norm2_f64_noalloc(const float *x, int64_t n, int B, double *out, hfm_str
 
 /* ------------------------------------------------------------------ multigrid handle */
 typedef enum { HFM_CYCLE_SAWTOOTH = 0, HFM_CYCLE_V = 1, HFM_CYCLE_F = 2 } hfm_cycle;
-typedef enum { HFM_ACCEL_NONE = 0, HFM_ACCEL_CG = 1 } hfm_accel;
+/* NONE: stationary cycles; CG: the cycle preconditions conjugate gradients; IR: float64
+ * iterative refinement (outer residual, norm and update in float64) around CG. */
+typedef enum { HFM_ACCEL_NONE = 0, HFM_ACCEL_CG = 1, HFM_ACCEL_IR = 2 } hfm_accel;
 
 typedef struct {
   int op_kind;            /* hfm_op_kind: CONST7, SIGMA7, K27 (DIR7 via stateless calls) */
@@ -214,13 +216,16 @@ typedef struct {
   double tol;             /* relative residual ||b - A phi|| / ||b|| (default 1e-6) */
   int max_cycles;         /* NOT_CONVERGED after this many cycles / CG iterations */
   int cycles_per_launch;  /* cycles captured in one CUDA graph between host checks (default 4) */
+  double inner_tol;       /* IR: an inner CG solve stops at max(inner_tol ||r0||, 0.3 tol ||b||) */
+  int inner_max_cycles;   /* IR: iteration cap of one inner solve (default 200) */
+  int reserved_cfg;
 } hfm_mg_config;
 
 typedef struct {
   int active;       /* 1 while the slot is still iterating */
   int status;       /* hfm_status of the finished solve */
   int cycles;       /* cycles (or CG iterations) done */
-  int reserved;
+  int outer;        /* float64 refinement steps done (IR) */
   double norm_b;    /* ||b||_2 */
   double rel_resid; /* last ||b - A phi|| / ||b|| */
 } hfm_slot_stats;
@@ -254,6 +259,10 @@ int hfm_mg_cancel(hfm_mg *mg, int slot, hfm_stream_t stream);
  * solutions into phi, fill stats_host (may be NULL).  Synchronises `stream`. */
 int hfm_mg_solve(hfm_mg *mg, const float *rhs, float *phi, hfm_slot_stats *stats_host,
                  hfm_stream_t stream);
+/* float64 right-hand side / initial guess (NULL = zero) and solution of a slot (accel = IR). */
+int hfm_mg_load_f64(hfm_mg *mg, int slot, const double *rhs, const double *phi0,
+                    hfm_stream_t stream);
+int hfm_mg_fetch_f64(hfm_mg *mg, int slot, double *phi_out, hfm_stream_t stream);
 /* Read an internal level buffer of a slot (0 = phi / w, 1 = rhs / r) for per-level checks. */
 int hfm_mg_read_level(hfm_mg *mg, int slot, int level, int which, float *out,
                       hfm_stream_t stream);
