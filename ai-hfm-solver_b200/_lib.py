@@ -73,6 +73,7 @@ SIGNATURES = {
     "hfm_op_apply": (I, [P, P, P, I, I, I, I, P]),
     "hfm_op_residual": (I, [P, P, P, P, I, I, I, I, U, P]),
     "hfm_op_jacobi": (I, [P, P, P, P, P, I, I, I, I, F, I, U, P]),
+    "hfm_op_jacobi_typed": (I, [P, I, P, P, P, I, I, I, I, F, U, P]),
     "hfm_residual_restrict": (I, [P, P, P, P, P, I, I, I, I, U, P]),
     "hfm_prolong_correct_smooth": (I, [P, P, P, P, P, I, I, I, I, F, U, P]),
     "hfm_stencil7_const_apply": (I, [P, P, I, I, I, I, F, F, F, P]),

@@ -222,6 +222,42 @@ int hfm_op_jacobi(const hfm_operator *op, const float *phi, const float *rhs, fl
   return HFM_OK;
 }
 
+int hfm_op_jacobi_typed(const hfm_operator *op, int dtype, const void *phi, const void *rhs,
+                        void *out, int B, int Z, int Y, int X, float omega, unsigned flags,
+                        hfm_stream_t stream) {
+  int st;
+  if ((st = check_grid(B, Z, Y, X))) return st;
+  if (!op || !rhs || !out || (!phi && !(flags & HFM_FLAG_ZERO_GUESS)))
+    return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: NULL argument");
+  if (dtype != HFM_F32 && dtype != HFM_BF16 && dtype != HFM_F16)
+    return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: dtype must be F32, BF16 or F16");
+  if (op->kind == HFM_OP_SIGMA7 || op->kind == HFM_OP_DIR7) {
+    if (op->coef_dtype != dtype) return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: coef_dtype must equal dtype");
+    for (int i = 0; i < (op->kind == HFM_OP_SIGMA7 ? 3 : 7); ++i)
+      if (!op->coef[i]) return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: missing coefficient array");
+  } else if (op->kind != HFM_OP_CONST7 && op->kind != HFM_OP_K27) {
+    return fail(HFM_ERR_BAD_ARG, "unknown operator kind");
+  }
+  if (phi == out) return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: phi aliases out");
+  const int64_t n = (int64_t)Z * Y * X;
+  DevOp d = make_devop(*op, n);
+  const void *base = (flags & HFM_FLAG_ZERO_GUESS) ? nullptr : phi;
+#define HFM_TYPED(T)                                                                         \
+  {                                                                                          \
+    PhiSrc<T> p;                                                                             \
+    memset(&p, 0, sizeof(p));                                                                \
+    p.base = (const T *)base;                                                                \
+    p.base_stride = n;                                                                       \
+    p.zero_xend = (flags & HFM_FLAG_ZERO_XEND) ? 1 : 0;                                      \
+    return launch_smooth<T>(op->kind, d, p, (const T *)rhs, n, (T *)out, n, B, Grid3{Z, Y, X}, \
+                            omega, flags, nullptr, (cudaStream_t)stream);                    \
+  }
+  if (dtype == HFM_F32) HFM_TYPED(float)
+  if (dtype == HFM_BF16) HFM_TYPED(__nv_bfloat16)
+  HFM_TYPED(__half)
+#undef HFM_TYPED
+}
+
 int hfm_residual_restrict(const hfm_operator *op, const float *phi, const float *b,
                           float *r_fine, float *r_coarse, int B, int Z, int Y, int X,
                           unsigned flags, hfm_stream_t stream) {

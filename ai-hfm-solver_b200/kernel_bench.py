@@ -33,6 +33,8 @@ def main():
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--dtype", default="f32", choices=["f32", "bf16", "f16"],
+                    help="storage of fields and conductivities (smooth only)")
     a = ap.parse_args()
     import torch
     import __graft_entry__ as ge
@@ -58,7 +60,20 @@ def main():
     L = hfm._lib
     P = lambda t: C.c_void_p(t.data_ptr() if t is not None else 0)
 
-    if a.kernel == "smooth":
+    tdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[a.dtype]
+    if a.kernel == "smooth" and a.dtype != "f32":
+        xt, bt, ot = x.to(tdt), b.to(tdt), out.to(tdt)
+        keep = []
+        if a.form == "sigma7":
+            keep = [s[k].to(tdt).contiguous() for k in range(3)]
+            for k in range(3):
+                st.coef[k] = keep[k].data_ptr()
+        st.coef_dtype = {"bf16": L.BF16, "f16": L.F16}[a.dtype]
+        dcode = st.coef_dtype
+        fn = lambda: L.call("hfm_op_jacobi_typed", C.byref(st), dcode, P(xt), P(bt), P(ot), B, Z, Y,
+                            X, 2.0 / 3.0, 0, stream)
+        BYTES[("smooth", a.form)] = BYTES[("smooth", a.form)] * (2 / 4)
+    elif a.kernel == "smooth":
         fn = lambda: L.call("hfm_op_jacobi", C.byref(st), P(x), P(b), P(out), P(None), B, Z, Y, X,
                             2.0 / 3.0, 1, 0, stream)
     elif a.kernel == "resid":

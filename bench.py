@@ -1,25 +1,30 @@
-"""Benchmark: multigrid solves/s at 1e-6 relative residual on one B200 (per rank).
+"""Benchmark: served multigrid solves/s and p99 latency at 1e-6 relative residual, 1 B200.
 
-Workload (``--workload batch64``, default): 64 independent anisotropic potential problems
--div(sigma grad phi) = f on 64^3 cell-centred grids (seeded log-normal sigma per axis, log-std
-1, 5^3 box-filtered; +1/-1 point dipole), each solved to ||b - A phi|| / ||b|| < 1e-6 by
-conjugate gradients preconditioned with one V(2,2) weighted-Jacobi (omega = 2/3) cycle
-(2x2x2 averaging restriction, nearest prolongation, coarsest 4^3), float32.  One step =
-install the 64 operators (coefficient hierarchies), load, iterate to tolerance, fetch.
+Default workload (``--workload serve``): a stream of 1024 anisotropic forward-solve requests
+-div(sigma grad phi) = f, cubic edge uniform over {32, 48, 64, 96, 128}, each with its own
+seeded log-normal sigma per axis (log-std uniform in [0.5, 2], 5^3 box-filtered) and a
++1/-1 dipole, Poisson arrivals at 2000 requests/s, HBM admission budget 120 GB, target
+||b - A phi|| / ||b|| < 1e-6 measured in float64.  Solver: float64 iterative refinement
+around conjugate gradients preconditioned by one V(2,2) weighted-Jacobi (omega 2/3) cycle
+with 2x2x2 averaging restriction and nearest prolongation; the inner cycles store fields and
+conductivities in bf16 (served path).  One step = serving the whole stream.
 
-``value``  whole-job solves/s with inputs resident in HBM;
-``e2e``    the same through the public API from pinned host buffers (sigma, f in; phi out);
-``plain_solves_per_s``  the one-request-at-a-time float32 path (one slot, host polls);
-``roofline``  the fine-level smoother kernel (dominant kernel), CUDA-event timed;
+``value``  whole-job served solves/s, request inputs resident in HBM, arrivals in real time;
+``e2e``    the same stream with inputs in pinned host memory (host->device per request at
+           admission) and every float64 solution copied back to the host;
+``plain_solves_per_s``  the one-request-at-a-time float32 path (single-slot handle, host
+           polls), on a bounded sample of the same stream;
+``roofline``  the served path's dominant kernel, the bf16 fine-level smoother, on the 128^3
+           bucket's shape (64 slots), CUDA-event timed;
 ``cpu_baseline``  the multi-threaded CPU port of the same algorithm on a bounded sample.
 
-``--impl reference`` times the CPU port (the stand-in for the reference's TensorFlow CPU
-path, which cannot be installed here) on the same workload, rank 0 only.
-
-Multi-GPU (torchrun): every rank solves its own 64 problems (replicas, no collective);
-``value`` = all ranks' solves / max-over-ranks time.
+``--workload batch64``: 64 independent 64^3 problems (log-std 1) solved together.
+``--impl reference`` times the CPU port (stand-in for the reference's TensorFlow CPU path,
+which cannot be installed here) on the same stream, rank 0 only.
+Multi-GPU (torchrun): every rank serves its own stream (replicas, no collective).
 """
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -32,41 +37,30 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "MG solves/s @1e-6 rel resid (64^3 anisotropic, batch of 64 per GPU)"
+METRIC = "MG solves/s & p99 latency @1e-6 rel resid: served vs plain, 1 B200; HBM GB/s"
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="batch64")
-    p.add_argument("--n", type=int, default=64)
-    p.add_argument("--batch", type=int, default=64)
+    p.add_argument("--workload", default="serve", choices=["serve", "batch64"])
+    p.add_argument("--requests", type=int, default=1024)
+    p.add_argument("--rate", type=float, default=2000.0)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--no-e2e", action="store_true")
     return p.parse_args()
 
 
-def dist_init(args):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
-
-
-def make_inputs(pkg, n, batch, seed0):
-    sig = np.empty((3, batch, n, n, n), np.float32)
-    f = np.empty((batch, n, n, n), np.float32)
-    for i in range(batch):
-        s = pkg.problems.anisotropic_sigma((n, n, n), seed=seed0 + i, log_std=1.0)
-        sig[:, i] = s
-        f[i] = pkg.problems.dipole((n, n, n), seed=seed0 + i)
-    return sig, f
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
 
     def __init__(self, index):
         self.index = index
@@ -82,7 +76,7 @@ class Clocks:
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
                  "clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -116,62 +110,241 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_sample(pkg, sig, f, n, budget_s=20.0):
-    """The CPU port on as many of the batch's problems as fit in ``budget_s``."""
+def peak_hbm():
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        return float(json.load(open(pk))["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    return 6650.0, "fallback 6650 GB/s"
+
+
+def smoother_roofline(pkg, torch, dtype, slots, n, reps=20):
+    """CUDA-event time of one fine-level smoother sweep (sigma form) on a (slots, n^3) batch."""
+    L, ops = pkg._lib, pkg.ops
+    g = torch.Generator(device="cuda").manual_seed(1)
+    tdt = {"f32": torch.float32, "bf16": torch.bfloat16}[dtype]
+    code = {"f32": L.F32, "bf16": L.BF16}[dtype]
+    x = torch.randn((slots, n, n, n), device="cuda", generator=g).to(tdt)
+    b = torch.randn((slots, n, n, n), device="cuda", generator=g).to(tdt)
+    y = torch.empty_like(x)
+    s = [torch.exp(torch.randn((slots, n, n, n), device="cuda", generator=g)).to(tdt) for _ in range(3)]
+    st = L.HfmOperator()
+    st.kind, st.coef_dtype, st.scale = L.OP_SIGMA7, code, 1.0
+    for i in range(3):
+        st.c[i] = 1.0
+        st.coef[i] = s[i].data_ptr()
+    stream = ops._stream()
+    fn = lambda: L.call("hfm_op_jacobi_typed", C.byref(st), code, C.c_void_p(x.data_ptr()),
+                        C.c_void_p(b.data_ptr()), C.c_void_p(y.data_ptr()), slots, n, n, n,
+                        2.0 / 3.0, 0, stream)
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    es = 2 if dtype == "bf16" else 4
+    bytes_alg = 6 * es * slots * n ** 3  # read phi, f, sx, sy, sz; write phi'
+    peak, src = peak_hbm()
+    achieved = bytes_alg / (ms / 1e3) / 1e9
+    del x, b, y, s
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None,
+            "kernel": "k_tma<SIGMA7,%s,SMOOTH> fine-level weighted Jacobi (%d x %d^3)" % (dtype, slots, n),
+            "bytes_per_launch": bytes_alg, "ms_per_launch": round(ms, 4), "peak_source": src}
+
+
+def cpu_sample_stream(reqs, budget_s=20.0):
+    """The CPU port on the stream's first requests until ``budget_s`` is spent."""
     from oracle import cpu_port, mg as omg
     cores = cpu_port.threads()
-    nl = len(omg.level_shapes((n, n, n)))
-    done, t0 = 0, time.perf_counter()
-    iters = []
-    while done < f.shape[0]:
-        ops = cpu_port.hierarchy(sig[:, done], nl)
-        _, it = cpu_port.pcg_solve(ops, f[done], tol=1e-6)
-        iters.append(it)
+    done, t0, its, sizes = 0, time.perf_counter(), [], []
+    for r in reqs:
+        sig = r.sigma.cpu().numpy()
+        f = r.rhs.cpu().numpy()
+        ops = cpu_port.hierarchy(sig, len(omg.level_shapes((r.n,) * 3)))
+        _, it = cpu_port.pcg_solve(ops, f, tol=1e-6, max_iter=600)
+        its.append(it)
+        sizes.append(r.n)
         done += 1
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
     return {"value": done / dt, "unit": "solves/s", "cores": cores, "kind": "port",
-            "sample": "%d of the %d 64^3 problems (PCG-V(2,2), mean %.1f iterations), torch CPU "
-                      "port of the oracle" % (done, f.shape[0], float(np.mean(iters)))}
+            "sample": "first %d requests of the stream (edges %s), PCG-V(2,2) float32, torch CPU "
+                      "port of the oracle" % (done, sorted(set(sizes)))}
 
 
 def run_reference(args):
-    rank, world, _ = dist_init(args)
+    rank, world, _ = dist_env()
     if rank != 0:
         return 0
+    import torch
     import __graft_entry__ as ge
     pkg = ge.load_package()
-    n, batch = args.n, args.batch
-    per_step = 4  # problems per step: a bounded sample of the workload
-    sig, f = make_inputs(pkg, n, max(per_step, 1), 1000)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    reqs = pkg.serving.make_stream(count=64, rate=args.rate, seed=1, device=dev) \
+        if dev == "cuda" else None
     from oracle import cpu_port, mg as omg
     cores = cpu_port.threads()
-    nl = len(omg.level_shapes((n, n, n)))
+    per_step = 4
+
+    def step(k):
+        for r in reqs[k * per_step:(k + 1) * per_step]:
+            ops = cpu_port.hierarchy(r.sigma.cpu().numpy(), len(omg.level_shapes((r.n,) * 3)))
+            cpu_port.pcg_solve(ops, r.rhs.cpu().numpy(), tol=1e-6, max_iter=600)
+
+    for k in range(args.warmup):
+        step(k % 8)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        step(k % 8)
+    dt = time.perf_counter() - t0
+    v = per_step * args.steps / dt
+    print(json.dumps({
+        "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "serving stream, edges 32-128, log-std 0.5-2, 1e-6", "sample_per_step": per_step},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": "%d stream requests per step, PCG-V(2,2), torch CPU port" % per_step},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
+def run_serve(args, pkg, torch, rank, world, local):
+    sv, M, L = pkg.serving, pkg.multigrid, pkg._lib
+    dev = torch.device("cuda", local)
+    reqs = sv.make_stream(count=args.requests, rate=args.rate, seed=1 + 7919 * rank, device=dev)
+    cfg = M.SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6, max_cycles=600)
+    server = sv.SolveServer(cfg=cfg, slots=64, budget_bytes=120e9, cycles_per_tick=4)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        server.serve(reqs, realtime=True)
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = L.lib().hfm_kernel_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    all_res = []
+    for _ in range(args.steps):
+        all_res.extend(server.serve(reqs, realtime=True))
+    e1.record()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = (L.lib().hfm_kernel_launch_count() - l0) // max(args.steps, 1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    bad = [r for r in all_res if r.status != 0]
+    lat = sv.latency_stats(all_res)
+    value = len(reqs) * world / (ms / 1e3)
+
+    e2e = None
+    if not args.no_e2e:
+        host = [sv.SolveRequest(r.rid, r.n, r.arrival, r.sigma.cpu().pin_memory(),
+                                r.rhs.cpu().pin_memory(), r.log_std) for r in reqs]
+        server.serve(host, realtime=True, host_out=True)  # warm the staging path
+        barrier()
+        t0 = time.perf_counter()
+        res_e2e = server.serve(host, realtime=True, host_out=True)
+        barrier()
+        dt = time.perf_counter() - t0
+        h2d = sum(r.sigma.numel() * 4 + r.rhs.numel() * 4 for r in host)
+        d2h = sum(r.n ** 3 * 8 for r in host)
+        e2e = {"value": round(len(host) * world / dt, 3), "unit": "solves/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "p50_ms": round(sv.latency_stats(res_e2e)["p50_ms"], 3),
+               "p99_ms": round(sv.latency_stats(res_e2e)["p99_ms"], 3)}
+        del host
+    server.close()
+
+    # plain path: one request at a time, float32 storage, bounded sample of the same stream
+    pcfg = M.SolverConfig(cycle="V", accel="ir", storage="f32", tol=1e-6, max_cycles=600)
+    sv.solve_one_at_a_time(reqs[:10], cfg=pcfg)  # warm-up (graph capture per edge)
+    plain, pdt = sv.solve_one_at_a_time(reqs, cfg=pcfg, time_budget_s=8.0)
+    plain_sps = len(plain) / pdt
+    roof = smoother_roofline(pkg, torch, "bf16", 64, 128)
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+        "data": "synthetic",
+        "config": {"workload": "serving stream: %d requests, edges {32,48,64,96,128}, log-std U[0.5,2], "
+                               "Poisson %.0f req/s, HBM budget 120 GB" % (len(reqs), args.rate),
+                   "solver": "float64 iterative refinement around PCG + V(2,2) Jacobi omega=2/3 "
+                             "(avg restriction, nearest prolongation, coarsest 4^3 / 3^3), "
+                             "bf16 inner storage, float32 accumulation",
+                   "tol": 1e-6, "slots_per_edge": {str(n): b.slots for n, b in server.buckets.items()},
+                   "l2": "inputs larger than L2 (stream inputs %.1f GB resident)" %
+                         (sum(r.sigma.numel() * 4 + r.rhs.numel() * 4 for r in reqs) / 1e9),
+                   "parallelism": "replicas x%d" % world},
+        "p50_ms": round(lat["p50_ms"], 3), "p99_ms": round(lat["p99_ms"], 3),
+        "failed": len(bad),
+        "iterations_mean": round(float(np.mean([r.cycles for r in all_res])), 2),
+        "plain_solves_per_s": round(plain_sps, 3),
+        "plain_sample": "%d requests one at a time (float32 storage), %.2f s" % (len(plain), pdt),
+        "plain_p50_ms": round(sv.latency_stats(plain)["p50_ms"], 3),
+        "plain_p99_ms": round(sv.latency_stats(plain)["p99_ms"], 3),
+        "served_over_plain": round(value / world / plain_sps, 3),
+        "e2e": e2e, "roofline": roof, "gpu_launches": int(launches), "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_sample_stream(reqs)
+    else:
+        out["cpu_baseline"] = None
+    return out
+
+
+def run_batch64(args, pkg, torch, rank, world, local):
+    L, M, ops = pkg._lib, pkg.multigrid, pkg.ops
+    n, batch = 64, 64
+    dev = torch.device("cuda", local)
+    sig = np.empty((3, batch, n, n, n), np.float32)
+    f = np.empty((batch, n, n, n), np.float32)
+    for i in range(batch):
+        sig[:, i] = pkg.problems.anisotropic_sigma((n, n, n), seed=1000 + i, log_std=1.0)
+        f[i] = pkg.problems.dipole((n, n, n), seed=1000 + i)
+    sig_d = torch.from_numpy(sig).to(dev)
+    f_d = torch.from_numpy(f).to(dev)
+    phi_d = torch.empty_like(f_d)
+    cfg = M.SolverConfig(cycle="V", accel="cg", tol=1e-6, max_cycles=200)
+    h = M.Multigrid((n, n, n), L.OP_SIGMA7, cfg, slots=batch)
 
     def step():
-        for i in range(per_step):
-            ops = cpu_port.hierarchy(sig[:, i], nl)
-            cpu_port.pcg_solve(ops, f[i], tol=1e-6)
+        h.set_operator(ops.Sigma7(sig_d[0], sig_d[1], sig_d[2]))
+        L.lib().hfm_mg_solve(h._h, C.c_void_p(f_d.data_ptr()), C.c_void_p(phi_d.data_ptr()),
+                             h._stats, ops._stream())
 
     for _ in range(args.warmup):
         step()
-    t0 = time.perf_counter()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
     for _ in range(args.steps):
         step()
-    dt = time.perf_counter() - t0
-    v = per_step * args.steps / dt
-    out = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-           "data": "synthetic", "impl": "reference",
-           "config": {"workload": "64^3 anisotropic PCG-V(2,2) to 1e-6", "n": n,
-                      "sample_per_step": per_step},
-           "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                            "sample": "%d problems per step" % per_step},
-           "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(out))
-    return 0
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    h.close()
+    return {"metric": "MG solves/s @1e-6 (64 x 64^3, log-std 1, PCG-V(2,2), float32)",
+            "value": round(batch * world / (ms / 1e3), 3), "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": "batch64"},
+            "roofline": smoother_roofline(pkg, torch, "f32", 64, 64)}
 
 
 def main():
@@ -180,139 +353,17 @@ def main():
         return run_reference(args)
     import torch
     import __graft_entry__ as ge
-    rank, world, local = dist_init(args)
+    rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
         import torch.distributed as dist
         dist.init_process_group("nccl", device_id=torch.device("cuda", local))
     pkg = ge.load_package()
-    L, M, ops = pkg._lib, pkg.multigrid, pkg.ops
-    n, batch = args.n, args.batch
-    dev = torch.device("cuda", local)
-    sig_h, f_h = make_inputs(pkg, n, batch, 1000 + 100000 * rank)
-    sig_pin = torch.from_numpy(sig_h).pin_memory()
-    f_pin = torch.from_numpy(f_h).pin_memory()
-    out_pin = torch.empty((batch, n, n, n), dtype=torch.float32).pin_memory()
-    sig_d = sig_pin.to(dev)
-    f_d = f_pin.to(dev)
-    phi_d = torch.empty_like(f_d)
-    cfg = M.SolverConfig(cycle="V", accel="cg", tol=1e-6, max_cycles=200, cycles_per_launch=4)
-    h = M.Multigrid((n, n, n), L.OP_SIGMA7, cfg, slots=batch)
-    stats_box = {}
-
-    def solve_resident():
-        h.set_operator(ops.Sigma7(sig_d[0], sig_d[1], sig_d[2]))
-        st = L.lib().hfm_mg_solve(h._h, __import__("ctypes").c_void_p(f_d.data_ptr()),
-                                  __import__("ctypes").c_void_p(phi_d.data_ptr()), h._stats,
-                                  ops._stream())
-        stats_box["st"] = st
-
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
-    def timed(fn, steps):
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(steps):
-            fn()
-        e1.record()
-        barrier()
-        ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
-
-    for _ in range(args.warmup):
-        solve_resident()
-    torch.cuda.synchronize()
-    clocks = Clocks(local)
-    clocks.start()
-    l0 = L.lib().hfm_kernel_launch_count()
-    ms = timed(solve_resident, args.steps)
-    launches = (L.lib().hfm_kernel_launch_count() - l0) // max(args.steps, 1)
-    clk = clocks.stop()
-    st = [dict(status=s.status, cycles=s.cycles, rel=s.rel_resid) for s in h._stats]
-    assert all(s["status"] == 0 for s in st), st
-    value = batch * world / (ms / 1000.0)
-
-    # end to end: pinned host sigma and f in, phi out, through the public API
-    def solve_e2e():
-        sig_d.copy_(sig_pin, non_blocking=True)
-        f_d.copy_(f_pin, non_blocking=True)
-        solve_resident()
-        out_pin.copy_(phi_d, non_blocking=True)
-    for _ in range(2):
-        solve_e2e()
-    ms_e2e = timed(solve_e2e, max(2, args.steps // 2))
-    e2e = {"value": batch * world / (ms_e2e / 1000.0), "unit": "solves/s",
-           "h2d_bytes_per_step": int(sig_pin.numel() * 4 + f_pin.numel() * 4),
-           "d2h_bytes_per_step": int(out_pin.numel() * 4)}
-
-    # plain path: one request at a time, one slot, float32
-    hp = M.Multigrid((n, n, n), L.OP_SIGMA7, cfg, slots=1)
-    n_plain = min(8, batch)
-
-    def plain():
-        for i in range(n_plain):
-            hp.set_operator(ops.Sigma7(sig_d[0, i], sig_d[1, i], sig_d[2, i]))
-            hp.solve(f_d[i:i + 1])
-    plain()
-    ms_plain = timed(plain, 1)
-    plain_sps = n_plain / (ms_plain / 1000.0)
-    hp.close()
-
-    # roofline: the smoother on the batch's fine level (Sigma7 Jacobi, 24 B/cell), CUDA events
-    op = ops.Sigma7(sig_d[0], sig_d[1], sig_d[2])
-    x = torch.randn_like(f_d)
-    y = torch.empty_like(f_d)
-    s = op.struct()
-    import ctypes as C
-    stream = ops._stream()
-
-    def sweep():
-        L.call("hfm_op_jacobi", C.byref(s), C.c_void_p(x.data_ptr()), C.c_void_p(f_d.data_ptr()),
-               C.c_void_p(y.data_ptr()), C.c_void_p(0), batch, n, n, n, 2.0 / 3.0, 1, 0, stream)
-    for _ in range(5):
-        sweep()
-    reps = 20
-    ms_sweep = timed(sweep, reps)
-    cells = batch * n ** 3
-    bytes_alg = 24 * cells
-    achieved = bytes_alg / (ms_sweep / 1000.0) / 1e9
-    peaks = {}
-    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(pk):
-        peaks = json.load(open(pk))
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
-                "kernel": "k_smooth<SIGMA7,float> (fine-level weighted Jacobi)",
-                "bytes_per_launch": bytes_alg, "ms_per_launch": ms_sweep,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650"}
-    h.close()
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(pkg, sig_h, f_h, n)
+    if args.workload == "serve":
+        out = run_serve(args, pkg, torch, rank, world, local)
+    else:
+        out = run_batch64(args, pkg, torch, rank, world, local)
     if rank == 0:
-        out = {"metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
-               "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
-               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-               "data": "synthetic",
-               "config": {"workload": "batch of %d anisotropic %d^3 solves per GPU (log-std 1, dipole)" % (batch, n),
-                          "solver": "PCG + V(2,2) Jacobi omega=2/3, avg restriction, nearest prolongation, coarsest 4^3",
-                          "tol": 1e-6, "l2": "inputs larger than L2 (%.0f MB per GPU)" % (batch * n ** 3 * 40 / 1e6),
-                          "parallelism": "replicas x%d" % world},
-               "plain_solves_per_s": round(plain_sps, 3),
-               "iterations": {"mean": float(np.mean([s["cycles"] for s in st])),
-                              "max": int(max(s["cycles"] for s in st))},
-               "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
-               "clocks": clk}
         print(json.dumps(out))
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -122,6 +122,13 @@ int hfm_op_jacobi(const hfm_operator *op, const float *phi, const float *rhs, fl
                   float *tmp, int B, int Z, int Y, int X, float omega, int sweeps,
                   unsigned flags, hfm_stream_t stream);
 
+/* One weighted-Jacobi sweep with fields and conductivities stored as `dtype` (HFM_F32,
+ * HFM_BF16 or HFM_F16; arithmetic in float32): the smoother of the reduced-precision inner
+ * cycles, exposed for direct use and measurement.  op->coef_dtype must equal dtype. */
+int hfm_op_jacobi_typed(const hfm_operator *op, int dtype, const void *phi, const void *rhs,
+                        void *out, int B, int Z, int Y, int X, float omega, unsigned flags,
+                        hfm_stream_t stream);
+
 /* Fused residual + restriction: r_coarse = R (A phi - b) on the even grid (Z, Y, X), and
  * r_fine = A phi - b when r_fine is not NULL (7point.ipynb:409-419). */
 int hfm_residual_restrict(const hfm_operator *op, const float *phi, const float *b,
