@@ -99,6 +99,7 @@ SIGNATURES = {
     "hfm_mg_load": (I, [P, I, P, P, P]),
     "hfm_mg_run": (I, [P, I, P]),
     "hfm_mg_query": (I, [P, C.POINTER(HfmSlotStats), P]),
+    "hfm_mg_query_async": (I, [P, P, P]),
     "hfm_mg_fetch": (I, [P, I, P, P]),
     "hfm_mg_cancel": (I, [P, I, P]),
     "hfm_mg_solve": (I, [P, P, P, C.POINTER(HfmSlotStats), P]),

@@ -185,43 +185,68 @@ __global__ void k_check_outer(const double *__restrict__ partials, int nblk, Slo
   }
 }
 
+// float64 outer residual r = b - A x (sigma / kernel read as float32), partial sums of r^2.
+// Work items of the vector kernels: (slot, chunk) pairs.  A block takes items blockIdx.x,
+// blockIdx.x + gridDim.x, ...; chunk c of a slot covers elements [n c / CH, n (c+1) / CH).
+// Items of inactive slots are skipped, so however few slots are active the whole grid works
+// on them; reductions produce one partial per (slot, chunk), independent of which block
+// handled the item, so the summation order is fixed.
+struct Items {
+  int B, CH;
+  int64_t n;
+};
+
+__device__ __forceinline__ double block_reduce_sum(double v) {
+  __shared__ double sh[32];
+  __syncthreads();  // sh is reused across items
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+  return t;
+}
+
+#define HFM_FOR_ITEMS(it, MASK)                                                   \
+  for (int w_ = blockIdx.x; w_ < (it).B * (it).CH; w_ += gridDim.x) {            \
+    const int slot = w_ / (it).CH, ch = w_ - slot * (it).CH;                     \
+    if (!(MASK)) continue;                                                        \
+    const int64_t lo = (it).n * ch / (it).CH, hi = (it).n * (ch + 1) / (it).CH;   \
+    const int64_t base = (int64_t)slot * (it).n;                                  \
+    (void)base;
+#define HFM_END_ITEMS }
+
 // x64 += x_in for slots whose outer step is due (not before the first inner solve).
-__global__ void k_ir_update(double *__restrict__ x64, const float *__restrict__ xin, int64_t n,
+__global__ void k_ir_update(double *__restrict__ x64, const float *__restrict__ xin, Items it,
                             const SlotState *st, const int *outer_mask) {
-  const int64_t inst = blockIdx.y;
-  if (!outer_mask[inst] || st[inst].first) return;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    x64[inst * n + i] += (double)xin[inst * n + i];
+  HFM_FOR_ITEMS(it, outer_mask[slot] && !st[slot].first)
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) x64[base + i] += (double)xin[base + i];
+  HFM_END_ITEMS
 }
 
 // A new inner solve starts from x_in = 0.
-__global__ void k_ir_start_inner(float *__restrict__ xin, int64_t n, const SlotState *st,
+__global__ void k_ir_start_inner(float *__restrict__ xin, Items it, const SlotState *st,
                                  const int *active) {
-  const int64_t inst = blockIdx.y;
-  if (!active[inst] || st[inst].inner_cycles != 0) return;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    xin[inst * n + i] = 0.f;
+  HFM_FOR_ITEMS(it, active[slot] && st[slot].inner_cycles == 0)
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) xin[base + i] = 0.f;
+  HFM_END_ITEMS
 }
 
-// float64 outer residual r = b - A x (sigma / kernel read as float32), partial sums of r^2.
+// float64 outer residual r = b - A x (sigma / kernel read as float32), written as the float32
+// right-hand side of the next inner solve, with partial sums of r^2.
 template <int KIND>
 __global__ void k_residual64(DevOp op, const double *__restrict__ x, const double *__restrict__ b,
-                             float *__restrict__ rout, int Z, int Y, int X,
+                             float *__restrict__ rout, int Z, int Y, int X, Items it,
                              const int *__restrict__ mask, double *__restrict__ partials) {
-  __shared__ double sh[32];
-  const int64_t inst = blockIdx.y;
-  if (!mask[inst]) return;
-  const int64_t n = (int64_t)Z * Y * X;
-  const double *xi = x + inst * n;
+  HFM_FOR_ITEMS(it, mask[slot])
+  const double *xi = x + base;
   auto P = [&](int zz, int yy, int xx) -> double {
     if (zz < 0 || zz >= Z || yy < 0 || yy >= Y || xx < 0 || xx >= X) return 0.0;
     return xi[((int64_t)zz * Y + yy) * X + xx];
   };
   double acc = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     const int xx = (int)(i % X);
     const int64_t t = i / X;
     const int yy = (int)(t % Y), zz = (int)(t / Y);
@@ -231,17 +256,17 @@ __global__ void k_residual64(DevOp op, const double *__restrict__ x, const doubl
       for (int a = 0; a < 3; ++a)
         for (int bb = 0; bb < 3; ++bb)
           for (int c = 0; c < 3; ++c) {
-            const float w = op.k[9 * a + 3 * bb + c];
-            if (w != 0.f) ax += (double)w * P(zz + a - 1, yy + bb - 1, xx + c - 1);
+            const float wgt = op.k[9 * a + 3 * bb + c];
+            if (wgt != 0.f) ax += (double)wgt * P(zz + a - 1, yy + bb - 1, xx + c - 1);
           }
     } else if (KIND == HFM_OP_CONST7) {
       const double kz = op.k[0], ky = op.k[1], kx = op.k[2];
       ax = 2.0 * (kz + ky + kx) * P(zz, yy, xx) - kz * (P(zz - 1, yy, xx) + P(zz + 1, yy, xx)) -
            ky * (P(zz, yy - 1, xx) + P(zz, yy + 1, xx)) - kx * (P(zz, yy, xx - 1) + P(zz, yy, xx + 1));
     } else {
-      const float *sx = (const float *)op.coef[0] + inst * op.coef_stride;
-      const float *sy = (const float *)op.coef[1] + inst * op.coef_stride;
-      const float *sz = (const float *)op.coef[2] + inst * op.coef_stride;
+      const float *sx = (const float *)op.coef[0] + (int64_t)slot * op.coef_stride;
+      const float *sy = (const float *)op.coef[1] + (int64_t)slot * op.coef_stride;
+      const float *sz = (const float *)op.coef[2] + (int64_t)slot * op.coef_stride;
       const double sc = op.scale;
       const double cz = op.c[0] * sc, cy = op.c[1] * sc, cx = op.c[2] * sc;
       const double vx = sx[i], vy = sy[i], vz = sz[i];
@@ -257,18 +282,13 @@ __global__ void k_residual64(DevOp op, const double *__restrict__ x, const doubl
            aym * (pc - P(zz, yy - 1, xx)) + ayp * (pc - P(zz, yy + 1, xx)) +
            azm * (pc - P(zz - 1, yy, xx)) + azp * (pc - P(zz + 1, yy, xx));
     }
-    const double r = b[inst * n + i] - ax;
-    rout[inst * n + i] = (float)r;
+    const double r = b[base + i] - ax;
+    rout[base + i] = (float)r;
     acc += r * r;
   }
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
-    partials[inst * gridDim.x + blockIdx.x] = t;
-  }
+  const double t = block_reduce_sum(acc);
+  if (threadIdx.x == 0) partials[(int64_t)slot * it.CH + ch] = t;
+  HFM_END_ITEMS
 }
 
 template <class T>
@@ -314,6 +334,21 @@ __global__ void k_sumsq64(const double *__restrict__ x, int64_t n, double *__res
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
     partials[inst * gridDim.x + blockIdx.x] = t;
   }
+}
+
+// Pack the public per-slot statistics (for the asynchronous query).
+__global__ void k_pack_stats(const SlotState *st, const int *active, const int *outer, int B,
+                             hfm_slot_stats *out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= B) return;
+  hfm_slot_stats o;
+  o.active = active[i] | (outer ? outer[i] : 0);
+  o.status = st[i].status;
+  o.cycles = st[i].cycles;
+  o.outer = st[i].outer;
+  o.norm_b = st[i].norm_b;
+  o.rel_resid = st[i].rel;
+  out[i] = o;
 }
 
 // Initial state of every slot from its ||b||^2 (batched load).
@@ -371,26 +406,17 @@ __device__ __forceinline__ float pc_scale(const SlotState &s, int64_t n, int sca
 }
 
 template <class TZ>
-__global__ void k_dot_partials(const float *__restrict__ a, const TZ *__restrict__ b,
-                               int64_t n, int64_t sa, int64_t sb, double *partials,
-                               const int *active, const SlotState *st, int scaled) {
-  __shared__ double sh[32];
-  const int64_t inst = blockIdx.y;
-  if (!active[inst]) return;
-  const double zs = st ? pc_scale(st[inst], n, scaled) : 1.0;
+__global__ void k_dot_partials(const float *__restrict__ a, const TZ *__restrict__ b, Items it,
+                               double *partials, const int *active, const SlotState *st,
+                               int scaled) {
+  HFM_FOR_ITEMS(it, active[slot])
+  const double zs = st ? pc_scale(st[slot], it.n, scaled) : 1.0;
   double acc = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    acc += (double)a[inst * sa + i] * (double)St<TZ>::ld(b + inst * sb + i);
-  acc *= zs;
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
-    partials[inst * gridDim.x + blockIdx.x] = t;
-  }
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
+    acc += (double)a[base + i] * (double)St<TZ>::ld(b + base + i);
+  const double t = block_reduce_sum(acc * zs);
+  if (threadIdx.x == 0) partials[(int64_t)slot * it.CH + ch] = t;
+  HFM_END_ITEMS
 }
 
 // which: 0 -> rz (new), 1 -> pq
@@ -414,21 +440,18 @@ __global__ void k_scalar_sum(const double *__restrict__ partials, int nblk, Slot
 
 // p = z + beta p (beta = rz_new / rz; first iteration p = z); rz <- rz_new.
 template <class TZ>
-__global__ void k_cg_p(const TZ *__restrict__ z, float *__restrict__ p, int64_t n, int64_t sz,
-                       int64_t sp, SlotState *st, const double *rz_new, const int *active,
-                       int scaled) {
-  const int64_t inst = blockIdx.y;
-  if (!active[inst]) return;
-  const SlotState s = st[inst];
-  const double rzn = rz_new[inst];
+__global__ void k_cg_p(const TZ *__restrict__ z, float *__restrict__ p, Items it, SlotState *st,
+                       const double *rz_new, const int *active, int scaled) {
+  HFM_FOR_ITEMS(it, active[slot])
+  const SlotState s = st[slot];
   const bool first = s.inner_cycles == 0 || s.rz == 0.0;
-  const float beta = first ? 0.f : (float)(rzn / s.rz);
-  const float zs = pc_scale(s, n, scaled);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const float zv = zs * St<TZ>::ld(z + inst * sz + i);
-    p[inst * sp + i] = first ? zv : zv + beta * p[inst * sp + i];
+  const float beta = first ? 0.f : (float)(rz_new[slot] / s.rz);
+  const float zs = pc_scale(s, it.n, scaled);
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const float zv = zs * St<TZ>::ld(z + base + i);
+    p[base + i] = first ? zv : zv + beta * p[base + i];
   }
+  HFM_END_ITEMS
 }
 
 __global__ void k_cg_commit_rz(SlotState *st, const double *rz_new, const int *active, int B) {
@@ -438,30 +461,22 @@ __global__ void k_cg_commit_rz(SlotState *st, const double *rz_new, const int *a
 
 // x += alpha p, r -= alpha q, partial sums of r^2.
 __global__ void k_cg_xr(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
-                        const float *__restrict__ q, int64_t n, int64_t stride,
-                        const SlotState *st, double *partials, const int *active) {
-  __shared__ double sh[32];
-  const int64_t inst = blockIdx.y;
-  if (!active[inst]) return;
-  const SlotState s = st[inst];
+                        const float *__restrict__ q, Items it, const SlotState *st,
+                        double *partials, const int *active) {
+  HFM_FOR_ITEMS(it, active[slot])
+  const SlotState s = st[slot];
   const float alpha = (s.pq != 0.0) ? (float)(s.rz / s.pq) : 0.f;
   double acc = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t k = inst * stride + i;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const int64_t k = base + i;
     x[k] += alpha * p[k];
-    float rv = r[k] - alpha * q[k];
+    const float rv = r[k] - alpha * q[k];
     r[k] = rv;
     acc += (double)rv * rv;
   }
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
-    partials[inst * gridDim.x + blockIdx.x] = t;
-  }
+  const double t = block_reduce_sum(acc);
+  if (threadIdx.x == 0) partials[(int64_t)slot * it.CH + ch] = t;
+  HFM_END_ITEMS
 }
 
 // r = b - A x computed as -(A x - b): negate in place.
@@ -472,15 +487,23 @@ __global__ void k_negate(float *__restrict__ v, int64_t n) {
 }
 
 template <class T>
-__global__ void k_to_storage(const float *__restrict__ a, T *__restrict__ b, int64_t n,
-                             const int *active, int64_t stride, const SlotState *st,
-                             int scaled) {
-  const int64_t inst = blockIdx.y;
-  if (!active[inst]) return;
-  const float inv = 1.f / pc_scale(st[inst], n, scaled);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    b[inst * stride + i] = St<T>::from(a[inst * stride + i] * inv);
+__global__ void k_to_storage(const float *__restrict__ a, T *__restrict__ b, Items it,
+                             const int *active, const SlotState *st, int scaled) {
+  HFM_FOR_ITEMS(it, active[slot])
+  const float inv = 1.f / pc_scale(st[slot], it.n, scaled);
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
+    b[base + i] = St<T>::from(a[base + i] * inv);
+  HFM_END_ITEMS
+}
+
+// Chunks per slot for the vector kernels (about 4096 elements each) and their grid.
+int item_chunks(int64_t n) {
+  int64_t c = (n + 4095) / 4096;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(c, 4096));
+}
+int item_blocks(int B, int CH) {
+  int64_t want = (int64_t)sm_count() * 8;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)B * CH));
 }
 
 int vec_blocks(int64_t n, int B) {
@@ -531,6 +554,7 @@ struct hfm_mg {
   double *x64 = nullptr;    // refinement: float64 solution and right-hand side
   double *b64 = nullptr;
   hfm::SlotState *state = nullptr;
+  hfm_slot_stats *stats_dev = nullptr;  // packed per-slot statistics for asynchronous queries
   double *partials = nullptr;
   int64_t partials_per_slot = 0;
   double *scal = nullptr;  // per-slot scratch scalars (rz_new), and ||b||^2 at load
@@ -702,31 +726,29 @@ class Engine : public EngineBase {
   int outer_step(cudaStream_t s) {
     const int B = m_->slots;
     const int64_t nf = n(0);
-    const int vb = vec_blocks(nf, B);
-    k_ir_update<<<dim3(vb, B), 256, 0, s>>>(m_->x64, m_->cg[0], nf, m_->state, m_->outer);
+    const Items it{B, item_chunks(nf), nf};
+    const int vb = it.CH, ib = item_blocks(B, it.CH);
+    k_ir_update<<<ib, 256, 0, s>>>(m_->x64, m_->cg[0], it, m_->state, m_->outer);
     HFM_CHECK_LAUNCH("k_ir_update");
     DevOp d = fine32_;
     switch (kind()) {
       case HFM_OP_SIGMA7:
-        k_residual64<HFM_OP_SIGMA7><<<dim3(vb, B), 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1],
-                                                                g(0).Z, g(0).Y, g(0).X, m_->outer,
-                                                                m_->partials);
+        k_residual64<HFM_OP_SIGMA7><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], g(0).Z,
+                                                        g(0).Y, g(0).X, it, m_->outer, m_->partials);
         break;
       case HFM_OP_CONST7:
-        k_residual64<HFM_OP_CONST7><<<dim3(vb, B), 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1],
-                                                                g(0).Z, g(0).Y, g(0).X, m_->outer,
-                                                                m_->partials);
+        k_residual64<HFM_OP_CONST7><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], g(0).Z,
+                                                        g(0).Y, g(0).X, it, m_->outer, m_->partials);
         break;
       default:
-        k_residual64<HFM_OP_K27><<<dim3(vb, B), 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1],
-                                                             g(0).Z, g(0).Y, g(0).X, m_->outer,
-                                                             m_->partials);
+        k_residual64<HFM_OP_K27><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], g(0).Z,
+                                                     g(0).Y, g(0).X, it, m_->outer, m_->partials);
     }
     HFM_CHECK_LAUNCH("k_residual64");
     k_check_outer<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
                                     m_->cfg.tol, m_->cfg.max_cycles);
     HFM_CHECK_LAUNCH("k_check_outer");
-    k_ir_start_inner<<<dim3(vb, B), 256, 0, s>>>(m_->cg[0], nf, m_->state, m_->active);
+    k_ir_start_inner<<<ib, 256, 0, s>>>(m_->cg[0], it, m_->state, m_->active);
     HFM_CHECK_LAUNCH("k_ir_start_inner");
     return HFM_OK;
   }
@@ -735,22 +757,22 @@ class Engine : public EngineBase {
     const int B = m_->slots;
     const int64_t nf = n(0);
     float *x = m_->cg[0], *r = m_->cg[1], *p = m_->cg[2], *q = m_->cg[3];
-    const int vb = vec_blocks(nf, B);
+    const Items it{B, item_chunks(nf), nf};
+    const int vb = it.CH, ib = item_blocks(B, it.CH);
     const int scaled = std::is_same<T, float>::value ? 0 : 1;
     int st;
     // z = M r  (rhs(0) holds r / s in the storage type; float32 storage reads r in place)
     if (!std::is_same<T, float>::value) {
-      k_to_storage<T><<<dim3(vb, B), 256, 0, s>>>(r, rhs(0), nf, m_->active, nf, m_->state, scaled);
+      k_to_storage<T><<<ib, 256, 0, s>>>(r, rhs(0), it, m_->active, m_->state, scaled);
       HFM_CHECK_LAUNCH("k_to_storage");
     }
     if ((st = vcycle(0, true, m_->cfg.cycle == HFM_CYCLE_F, 0, s))) return st;
     const T *z = buf(0, cur_[0]);
     // rz_new = r . z ; p = z + beta p
-    k_dot_partials<T><<<dim3(vb, B), 256, 0, s>>>(r, z, nf, nf, nf, m_->partials, m_->active,
-                                                  m_->state, scaled);
+    k_dot_partials<T><<<ib, 256, 0, s>>>(r, z, it, m_->partials, m_->active, m_->state, scaled);
     HFM_CHECK_LAUNCH("k_dot_partials");
     k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 0, m_->scal);
-    k_cg_p<T><<<dim3(vb, B), 256, 0, s>>>(z, p, nf, nf, nf, m_->state, m_->scal, m_->active, scaled);
+    k_cg_p<T><<<ib, 256, 0, s>>>(z, p, it, m_->state, m_->scal, m_->active, scaled);
     k_cg_commit_rz<<<(B + 127) / 128, 128, 0, s>>>(m_->state, m_->scal, m_->active, B);
     HFM_CHECK_LAUNCH("k_cg_p");
     // q = A p ; pq = p . q   (FP32 operator on the fine level)
@@ -759,11 +781,10 @@ class Engine : public EngineBase {
     pp.base = p;
     pp.base_stride = nf;
     if ((st = launch_apply<float>(kind(), fine32_, pp, q, nf, B, g(0), m_->active, s))) return st;
-    k_dot_partials<float><<<dim3(vb, B), 256, 0, s>>>(p, q, nf, nf, nf, m_->partials, m_->active,
-                                                      nullptr, 0);
+    k_dot_partials<float><<<ib, 256, 0, s>>>(p, q, it, m_->partials, m_->active, nullptr, 0);
     k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 1, m_->scal);
     // x += alpha p ; r -= alpha q ; ||r||
-    k_cg_xr<<<dim3(vb, B), 256, 0, s>>>(x, r, p, q, nf, nf, m_->state, m_->partials, m_->active);
+    k_cg_xr<<<ib, 256, 0, s>>>(x, r, p, q, it, m_->state, m_->partials, m_->active);
     HFM_CHECK_LAUNCH("k_cg_xr");
     if (!ir) return check(vb, 0, s);
     k_check_inner<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
@@ -1144,10 +1165,12 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
     m->saw[0] = dalloc(m.get(), nf * es, &st);
     m->saw[1] = dalloc(m.get(), nf * es, &st);
   }
-  m->partials_per_slot = std::max<int64_t>(4096, max_partial_blocks(lv[0], slots));
+  m->partials_per_slot = std::max<int64_t>(std::max<int64_t>(4096, max_partial_blocks(lv[0], slots)),
+                                          item_chunks(lv[0].n()));
   m->partials = (double *)dalloc(m.get(), (size_t)slots * m->partials_per_slot * 8, &st);
   m->active = (int *)dalloc(m.get(), (size_t)slots * 4, &st);
   m->state = (SlotState *)dalloc(m.get(), (size_t)slots * sizeof(SlotState), &st);
+  m->stats_dev = (hfm_slot_stats *)dalloc(m.get(), (size_t)slots * sizeof(hfm_slot_stats), &st);
   m->scal = (double *)dalloc(m.get(), (size_t)(slots + 1) * 8, &st);
   if (!st) {
     if (cudaMemset(m->active, 0, (size_t)slots * 4) != cudaSuccess ||
@@ -1273,6 +1296,17 @@ int hfm_mg_query(hfm_mg *m, hfm_slot_stats *out, hfm_stream_t stream) {
     out[i].norm_b = st[i].norm_b;
     out[i].rel_resid = st[i].rel;
   }
+  return HFM_OK;
+}
+
+int hfm_mg_query_async(hfm_mg *m, hfm_slot_stats *stats_host, hfm_stream_t stream) {
+  if (!m || !stats_host) return fail(HFM_ERR_BAD_ARG, "hfm_mg_query_async: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  k_pack_stats<<<(m->slots + 127) / 128, 128, 0, s>>>(m->state, m->active, m->outer, m->slots,
+                                                      m->stats_dev);
+  HFM_CHECK_LAUNCH("k_pack_stats");
+  HFM_CUDA(cudaMemcpyAsync(stats_host, m->stats_dev, m->slots * sizeof(hfm_slot_stats),
+                           cudaMemcpyDeviceToHost, s));
   return HFM_OK;
 }
 

@@ -1,6 +1,7 @@
 // TMA-pipelined plane-marching stencil kernels for the large levels (X >= 64).
 //
-// A block owns a TY x TX (8 x 64) tile of the (y, x) plane and marches through a chunk of z
+// A block owns a TY x TX tile of the (y, x) plane (8 x 64 for float32, 16 x 64 for 16-bit
+// storage) and marches through a chunk of z
 // planes.  For every plane one thread issues `cp.async.bulk.tensor.4d` loads of the plane's
 // tiles into a shared-memory stage - phi with a one-row / HX-column halo, the three
 // conductivities (sx with x halo, sy with y halo, sz), the right-hand side and, for the fused
@@ -27,7 +28,7 @@ static __device__ int g_tma_timeouts;
 
 namespace {
 
-constexpr int TX = 64, TY = 8, NS = 5, kT = 128;
+constexpr int TX = 64, NS = 5;
 constexpr int kMaxSpin = 1 << 20;
 
 enum { M_SMOOTH = FAST_SMOOTH, M_RESID = FAST_RESID, M_RESTRICT = FAST_RESTRICT };
@@ -35,10 +36,14 @@ enum { M_SMOOTH = FAST_SMOOTH, M_RESID = FAST_RESID, M_RESTRICT = FAST_RESTRICT 
 // Stage layout for storage T; SIG: the stage carries the three conductivity tiles, CC: the
 // coarse correction tile (stages of the other kernels are smaller, so more blocks fit).
 template <class T, bool SIG = true, bool CC = true> struct Geo {
+  // 8 rows x 64 columns per block for float32, 16 rows for 16-bit storage (same bytes per
+  // stage); 16 threads per row, 4 consecutive x per thread
+  static constexpr int TY = sizeof(T) == 4 ? 8 : 16;
+  static constexpr int THREADS = 16 * TY;
   static constexpr int HX = 16 / (int)sizeof(T);
   static constexpr int PW = TX + 2 * HX;           // phi / sx tile width
   static constexpr int CW = TX / 2 + 2 * HX;       // coarse tile width
-  static constexpr int PHI = (TY + 2) * PW;
+  static constexpr int PHI = (TY + 2) * PW;  // with the one-row y halo
   static constexpr int SXN = TY * PW;
   static constexpr int SYN = (TY + 2) * TX;
   static constexpr int SZN = TY * TX;
@@ -107,25 +112,49 @@ __device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap *map, i
 
 template <class T> __device__ __forceinline__ float sld(const T *p) { return St<T>::to(*p); }
 
-template <class T> struct V4 {
-  static __device__ __forceinline__ void get(const T *p, float (&v)[4]) {
-    if (sizeof(T) == 4) {
-      float4 a = *reinterpret_cast<const float4 *>(p);
-      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-    } else {
-#pragma unroll
-      for (int e = 0; e < 4; ++e) v[e] = St<T>::to(p[e]);
-    }
+// Four consecutive values from shared memory (16-byte float32 / 8-byte 16-bit load; every
+// call site is aligned to four elements).
+template <class T> struct V4;
+template <> struct V4<float> {
+  static __device__ __forceinline__ void get(const float *p, float (&v)[4]) {
+    float4 a = *reinterpret_cast<const float4 *>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+};
+template <> struct V4<__nv_bfloat16> {
+  static __device__ __forceinline__ void get(const __nv_bfloat16 *p, float (&v)[4]) {
+    uint2 u = *reinterpret_cast<const uint2 *>(p);
+    float2 a = __bfloat1622float2(*reinterpret_cast<__nv_bfloat162 *>(&u.x));
+    float2 b = __bfloat1622float2(*reinterpret_cast<__nv_bfloat162 *>(&u.y));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+};
+template <> struct V4<__half> {
+  static __device__ __forceinline__ void get(const __half *p, float (&v)[4]) {
+    uint2 u = *reinterpret_cast<const uint2 *>(p);
+    float2 a = __half22float2(*reinterpret_cast<__half2 *>(&u.x));
+    float2 b = __half22float2(*reinterpret_cast<__half2 *>(&u.y));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
   }
 };
 
-template <class T> __device__ __forceinline__ void gst4(T *p, const float (&v)[4]) {
-  if (sizeof(T) == 4) {
-    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
-  } else {
-#pragma unroll
-    for (int e = 0; e < 4; ++e) p[e] = St<T>::from(v[e]);
-  }
+template <class T> __device__ __forceinline__ void gst4(T *p, const float (&v)[4]);
+template <> __device__ __forceinline__ void gst4<float>(float *p, const float (&v)[4]) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+template <> __device__ __forceinline__ void gst4<__nv_bfloat16>(__nv_bfloat16 *p, const float (&v)[4]) {
+  __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), b = __floats2bfloat162_rn(v[2], v[3]);
+  uint2 u;
+  u.x = *reinterpret_cast<unsigned *>(&a);
+  u.y = *reinterpret_cast<unsigned *>(&b);
+  *reinterpret_cast<uint2 *>(p) = u;
+}
+template <> __device__ __forceinline__ void gst4<__half>(__half *p, const float (&v)[4]) {
+  __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
+  uint2 u;
+  u.x = *reinterpret_cast<unsigned *>(&a);
+  u.y = *reinterpret_cast<unsigned *>(&b);
+  *reinterpret_cast<uint2 *>(p) = u;
 }
 
 // Issue the loads of plane p (may lie outside [0, Z): the TMA unit zero-fills) into `stage`.
@@ -133,6 +162,8 @@ template <class T, int CORR, bool SIG>
 __device__ __forceinline__ void issue_plane(const TmaArgs<T> &a, char *stage, uint32_t bar, int p,
                                             int x0, int y0, int b) {
   using G = Geo<T, SIG, CORR != 0>;
+  constexpr int TY = G::TY;
+  (void)TY;
   mbar_expect(bar, a.stage_bytes);
   if (a.has_phi) tma_load(smem_u32(stage + G::O_PHI), &a.m_phi, x0 - G::HX, y0 - 1, p, b, bar);
   if (SIG) {
@@ -144,21 +175,23 @@ __device__ __forceinline__ void issue_plane(const TmaArgs<T> &a, char *stage, ui
   if (CORR) tma_load(smem_u32(stage + G::O_CC), &a.m_cc, (x0 >> 1) - G::HX, (y0 >> 1) - 1, p >> 1, b, bar);
 }
 
-__device__ __forceinline__ double block_sum128(double v) {
-  __shared__ double sh[kT / 32];
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[32];
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
   __syncthreads();
   double t = 0.0;
   if (threadIdx.x == 0)
-    for (int w = 0; w < kT / 32; ++w) t += sh[w];
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
   return t;
 }
 
 template <int KIND, class T, int MODE, int CORR>
-__global__ void __launch_bounds__(kT, 3) k_tma(const __grid_constant__ TmaArgs<T> a) {
+__global__ void __launch_bounds__(Geo<T>::THREADS, sizeof(T) == 4 ? 3 : 2)
+    k_tma(const __grid_constant__ TmaArgs<T> a) {
   constexpr bool SIG = KIND == HFM_OP_SIGMA7;
   using G = Geo<T, SIG, CORR != 0>;
+  constexpr int TY = G::TY;
   extern __shared__ __align__(128) char smem[];
   __shared__ __align__(8) uint64_t bars[NS];
   const int64_t inst = blockIdx.z;
@@ -380,7 +413,7 @@ __global__ void __launch_bounds__(kT, 3) k_tma(const __grid_constant__ TmaArgs<T
     return;
   }
   if (MODE != M_SMOOTH && a.partials) {
-    double t = block_sum128(acc);
+    double t = block_sum(acc);
     if (tid == 0) a.partials[inst * (gridDim.x * gridDim.y) + blockIdx.y * gridDim.x + blockIdx.x] = t;
   }
 }
@@ -437,7 +470,7 @@ int go(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   });
   if (attr_err != cudaSuccess) return cuda_status(attr_err, "cudaFuncSetAttribute(k_tma)");
-  k_tma<KIND, T, MODE, CORR><<<grid, kT, smem, s>>>(a);
+  k_tma<KIND, T, MODE, CORR><<<grid, G::THREADS, smem, s>>>(a);
   HFM_CHECK_LAUNCH("k_tma");
   return HFM_OK;
 }
@@ -446,7 +479,7 @@ int go(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
 
 bool tma_eligible(int kind, Grid3 g, int mode, const void *corr, int corr_coarse, int es) {
   if (kind != HFM_OP_CONST7 && kind != HFM_OP_SIGMA7 && kind != HFM_OP_K27) return false;
-  if (g.X < TX || g.Y < TY) return false;
+  if (g.X < TX || g.Y < (es == 4 ? 8 : 16)) return false;
   if ((g.X * es) % 16) return false;  // tensor-map strides are multiples of 16 bytes
   if (corr && !corr_coarse) return false;
   if (corr && ((g.X / 2) * es) % 16) return false;
@@ -462,6 +495,7 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
                unsigned flags, const int *active, double *partials, int *nblk_out,
                cudaStream_t s) {
   using G = Geo<T>;  // tile extents (identical for every stage layout)
+  constexpr int TY = G::TY;
   TmaArgs<T> a;
   memset(&a, 0, sizeof(a));
   int st;

@@ -151,6 +151,17 @@ class Multigrid:
         return [dict(active=s.active, status=s.status, cycles=s.cycles, outer=s.outer,
                      norm_b=s.norm_b, rel_resid=s.rel_resid) for s in self._stats]
 
+    def query_async(self, host_buf):
+        """Enqueue a copy of all slots' statistics into ``host_buf`` (pinned uint8 tensor of
+        ``slots * sizeof(HfmSlotStats)`` bytes); decode with ``decode_stats`` once the stream
+        has passed this point."""
+        L.call("hfm_mg_query_async", self._h, C.c_void_p(host_buf.data_ptr()), _stream())
+
+    def decode_stats(self, host_buf):
+        arr = (L.HfmSlotStats * self.slots).from_address(host_buf.data_ptr())
+        return [dict(active=s.active, status=s.status, cycles=s.cycles, outer=s.outer,
+                     norm_b=s.norm_b, rel_resid=s.rel_resid) for s in arr]
+
     def fetch(self, slot, out=None):
         out = torch.empty(self.shape, dtype=torch.float32, device="cuda") if out is None else out
         L.call("hfm_mg_fetch", self._h, int(slot), C.c_void_p(out.data_ptr()), _stream())

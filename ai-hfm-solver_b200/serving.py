@@ -12,8 +12,10 @@ hierarchies live in HBM, sized so the buckets fit an HBM budget (admission by fo
    each bucket on its own stream so the buckets overlap on the GPU); inside the graph every
    slot runs on its own: a slot that converges, fails or hits its cycle cap switches itself
    off and the remaining kernels skip it;
-3. polls the buckets, retires finished slots (solution copied out, latency recorded) and
-   frees them for the next arrivals.
+3. as soon as a bucket's own launch has completed (non-blocking event check on an
+   asynchronous copy of the per-slot statistics), retires its finished slots (solution copied
+   out, latency recorded), admits waiting requests into the freed slots and launches the
+   bucket again; buckets of different sizes never wait for one another.
 
 A request that arrives while others are on the GPU therefore joins the next launch of its
 bucket: iteration-level continuous batching, not a queue that waits for a batch to drain.
@@ -24,7 +26,7 @@ The plain baseline (``solve_one_at_a_time``) is the same solver with one slot pe
 one request at a time, float32 storage.
 """
 import collections
-import math
+import ctypes as C
 import time
 from dataclasses import dataclass, field
 
@@ -105,15 +107,27 @@ def make_stream(count=1024, rate=2000.0, edges=EDGES, log_std=(0.5, 2.0), seed=0
 
 
 class _Bucket:
+    """One edge size: a resident handle with ``slots`` slots on its own CUDA stream.  Launches
+    are asynchronous: after each graph launch the per-slot statistics are copied into pinned
+    host memory and an event is recorded; the server harvests the bucket when the event has
+    completed, so buckets of different sizes never wait for one another."""
+
     def __init__(self, n, cfg, slots, keep_solutions):
         self.n = n
         self.slots = slots
         self.mg = Multigrid((n, n, n), L.OP_SIGMA7, cfg, slots=slots)
         self.stream = torch.cuda.Stream()
         self.free = list(range(slots - 1, -1, -1))
-        self.busy = {}  # slot -> (request, admitted time)
+        self.busy = {}  # slot -> (request, admitted time, staging tensors)
         self.keep = keep_solutions
-        self.dev_in = None
+        self.stats_buf = torch.empty(slots * C.sizeof(L.HfmSlotStats), dtype=torch.uint8,
+                                     pin_memory=True)
+        self.event = torch.cuda.Event()
+        self.inflight = False
+        self.launched = ()
+
+    def ready(self):
+        return not self.inflight or self.event.query()
 
     def admit(self, req, now):
         slot = self.free.pop()
@@ -124,37 +138,42 @@ class _Bucket:
                 rhs = rhs.to("cuda", non_blocking=True)
             self.mg.set_operator(Sigma7(sig[0], sig[1], sig[2]), slot=slot)
             self.mg.load(slot, rhs)
-            if not req.sigma.is_cuda:
-                # keep the staging tensors alive until the stream has consumed them
-                self.busy[slot] = (req, now, (sig, rhs))
-                return
-        self.busy[slot] = (req, now, None)
+        # the staging tensors stay referenced until the slot retires
+        self.busy[slot] = (req, now, (sig, rhs))
 
     def launch(self, cycles):
-        if self.busy:
-            with torch.cuda.stream(self.stream):
-                self.mg.run(cycles)
-
-    def poll(self, clock, t0, host_out):
         if not self.busy:
-            return []
+            return
         with torch.cuda.stream(self.stream):
-            stats = self.mg.query()  # synchronises this bucket's stream
-            done = []
-            for slot, (req, adm, _) in list(self.busy.items()):
-                s = stats[slot]
-                if s["active"]:
-                    continue
-                phi = None
-                if self.keep or host_out:
+            self.mg.run(cycles)
+            self.mg.query_async(self.stats_buf)
+            self.event.record(self.stream)
+        self.inflight = True
+        self.launched = tuple(self.busy.keys())
+
+    def harvest(self, clock, t0, host_out):
+        """Retire the slots of the completed launch that have finished (call when ready())."""
+        if not self.inflight:
+            return []
+        self.inflight = False
+        stats = self.mg.decode_stats(self.stats_buf)
+        done = []
+        now = clock() - t0
+        for slot in self.launched:
+            s = stats[slot]
+            if s["active"]:
+                continue
+            req, adm, _ = self.busy.pop(slot)
+            phi = None
+            if self.keep or host_out:
+                with torch.cuda.stream(self.stream):
                     phi = self.mg.fetch_f64(slot) if self.mg.cfg.accel == "ir" else self.mg.fetch(slot)
                     if host_out:
-                        phi = phi.to("cpu", non_blocking=False)
-                now = clock() - t0
-                done.append(SolveResult(req.rid, req.n, s["status"], s["cycles"], s["outer"],
-                                        s["rel_resid"], adm, now, now - req.arrival, phi))
-                del self.busy[slot]
-                self.free.append(slot)
+                        phi = phi.to("cpu")
+                        now = clock() - t0
+            done.append(SolveResult(req.rid, req.n, s["status"], s["cycles"], s["outer"],
+                                    s["rel_resid"], adm, now, now - req.arrival, phi))
+            self.free.append(slot)
         return done
 
 
@@ -191,23 +210,29 @@ class SolveServer:
         torch.cuda.synchronize()
         t0 = clock()
         total = len(pending)
+        buckets = list(self.buckets.values())
         while len(results) < total:
             now = clock() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 r = pending.popleft()
                 queued[r.n].append(r)
-            for n, q in queued.items():
-                b = self.buckets[n]
+            idle = True
+            for b in buckets:
+                if not b.ready():
+                    idle = False
+                    continue
+                results.extend(b.harvest(clock, t0, host_out))
+                q = queued[b.n]
                 while q and b.free:
                     b.admit(q.popleft(), clock() - t0)
-            for b in self.buckets.values():
                 b.launch(self.cycles_per_tick)
-            for b in self.buckets.values():
-                results.extend(b.poll(clock, t0, host_out))
-            if realtime and not any(b.busy for b in self.buckets.values()) and pending:
+                if b.inflight:
+                    idle = False
+            if idle and pending:
                 wait = pending[0].arrival - (clock() - t0)
                 if wait > 0:
-                    time.sleep(min(wait, 1e-3))
+                    time.sleep(min(wait, 2e-4))
+        torch.cuda.synchronize()
         return results
 
 

@@ -258,6 +258,10 @@ int hfm_mg_load(hfm_mg *mg, int slot, const float *rhs, const float *phi0, hfm_s
 int hfm_mg_run(hfm_mg *mg, int cycles, hfm_stream_t stream);
 /* Copy per-slot statistics to host memory (synchronises `stream`). */
 int hfm_mg_query(hfm_mg *mg, hfm_slot_stats *stats_host, hfm_stream_t stream);
+/* Enqueue a copy of every slot's statistics into stats_host (pinned host memory, `slots`
+ * entries) on `stream` without synchronising; read it after the stream reaches this point
+ * (e.g. a CUDA event recorded after the call). */
+int hfm_mg_query_async(hfm_mg *mg, hfm_slot_stats *stats_host, hfm_stream_t stream);
 /* Copy a slot's current solution into phi_out (device, [Z][Y][X] float32). */
 int hfm_mg_fetch(hfm_mg *mg, int slot, float *phi_out, hfm_stream_t stream);
 /* Stop a slot (request cancelled); its memory can be reloaded at once. */
