@@ -89,6 +89,7 @@ SIGNATURES = {
     "hfm_norm2_f64": (I, [P, I64, I, P, P, P]),
     "hfm_max_abs": (I, [P, I64, I, P, P, P]),
     "hfm_norm2_f64_noalloc": (I, [P, I64, I, P, P]),
+    "hfm_sigma7_grad_logsigma": (I, [P, P, P, P, P, I, I, I, I, F, F, F, P, P, P, I, P]),
     "hfm_mg_config_default": (None, [C.POINTER(HfmMgConfig)]),
     "hfm_mg_footprint_bytes": (C.c_size_t, [C.POINTER(HfmMgConfig), I, I, I, I]),
     "hfm_mg_create": (I, [C.POINTER(HfmMgConfig), I, I, I, I, C.POINTER(P)]),

@@ -200,6 +200,19 @@ int hfm_max_abs(const float *x, int64_t n, int B, float *out, void *scratch,
 #define HFM_NORM2_NOALLOC_SCRATCH_BYTES (512u * 1024u)
 int hfm_norm2_f64_noalloc(const float *x, int64_t n, int B, double *out, hfm_stream_t stream);
 
+/* --------------------------------------------------------------- resistivity tomography */
+/* Gradient of the misfit J = 1/2 sum_s |P u_s - d_s|^2 with respect to per-cell log sx, sy,
+ * sz for the SIGMA7 operator (face means, wall faces c_d s_c), given the forward fields u_s
+ * and adjoint fields lam_s (A lam_s = P^T (P u_s - d_s)), S fields each of [Z][Y][X] float64:
+ *   g_d(c) = - s_d(c) sum_s dA/ds_d(c)[lam_s, u_s].
+ * accumulate != 0 adds into g (source groups), else overwrites.  No counterpart layer in the
+ * reference, whose resistivity notebooks stop at the forward solve; the operator follows
+ * Anisotropic Resistivity Tomography/README:14-26. */
+int hfm_sigma7_grad_logsigma(const float *sx, const float *sy, const float *sz, const double *u,
+                             const double *lam, int S, int Z, int Y, int X, float cz, float cy,
+                             float cx, double *gx, double *gy, double *gz, int accumulate,
+                             hfm_stream_t stream);
+
 /* ------------------------------------------------------------------ multigrid handle */
 typedef enum { HFM_CYCLE_SAWTOOTH = 0, HFM_CYCLE_V = 1, HFM_CYCLE_F = 2 } hfm_cycle;
 /* NONE: stationary cycles; CG: the cycle preconditions conjugate gradients; IR: float64

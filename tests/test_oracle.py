@@ -153,3 +153,35 @@ def test_vcycle_converges_and_pcg_faster(pkg):
     _, h = mg.solve(ops, f, mg.CycleConfig(), "V", 1e-6, 400)
     assert h[-1] < 1e-6
     assert all(b < a for a, b in zip(h, h[1:]))
+
+
+def test_tomography_oracle_gradient_matches_finite_differences():
+    """The float64 adjoint gradient of the oracle equals central differences of J."""
+    from oracle import tomography as tomo
+    rng = np.random.default_rng(5)
+    n = 6
+    logs = rng.normal(0, 0.5, (3, n, n, n))
+    q = np.zeros((2, n, n, n))
+    q[0, 2, 2, 2], q[0, 3, 4, 1] = 1, -1
+    q[1, 4, 1, 3], q[1, 1, 3, 3] = 1, -1
+    rec = np.array([1, 5, 9, 14, 20, 27, 33])
+    d_obs = rng.normal(0, 0.01, (2, len(rec)))
+    J, g, _ = tomo.misfit(np.exp(logs), q, rec, d_obs)
+    eps = 1e-4  # the config's step; truncation error ~eps^2, roundoff ~1e-16 J / eps
+    for (k, z, y, x) in [(0, 2, 2, 2), (1, 0, 3, 5), (2, 5, 0, 0), (0, 3, 4, 1), (2, 2, 2, 3)]:
+        lp, lm = logs.copy(), logs.copy()
+        lp[k, z, y, x] += eps
+        lm[k, z, y, x] -= eps
+        fd = (tomo.misfit(np.exp(lp), q, rec, d_obs, want_grad=False)[0]
+              - tomo.misfit(np.exp(lm), q, rec, d_obs, want_grad=False)[0]) / (2 * eps)
+        assert fd == pytest.approx(g[k, z, y, x], rel=1e-6, abs=1e-12 * abs(J))
+
+
+def test_tomography_matrix_matches_operator():
+    from oracle import tomography as tomo
+    rng = np.random.default_rng(6)
+    s = np.exp(rng.normal(0, 1, (3, 4, 5, 6)))
+    x = rng.normal(0, 1, (4, 5, 6))
+    A = tomo.assemble(s)
+    ref = mg.Sigma7(s[0], s[1], s[2], dtype=np.float64).apply(x)
+    np.testing.assert_allclose(A @ x.ravel(), ref.ravel(), rtol=1e-12, atol=1e-12)
