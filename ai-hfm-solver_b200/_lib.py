@@ -89,6 +89,13 @@ SIGNATURES = {
     "hfm_norm2_f64": (I, [P, I64, I, P, P, P]),
     "hfm_max_abs": (I, [P, I64, I, P, P, P]),
     "hfm_norm2_f64_noalloc": (I, [P, I64, I, P, P]),
+    "hfm_ns_momentum": (I, [P, P, P, P, P, P, P, P, P, I, I, I, P, P, P, P, F, P]),
+    "hfm_ns_pressure_gradient": (I, [P, P, P, P, I, I, I, P, P, P, P]),
+    "hfm_ns_divergence": (I, [P, P, P, P, I, I, I, P, P, P, I, P]),
+    "hfm_ns_immersed_body": (I, [P, P, P, P, I, I, I, F, P]),
+    "hfm_ns_bc_scratch_bytes": (C.c_size_t, [I, I, I]),
+    "hfm_ns_bc_velocity": (I, [P, P, P, I, I, I, F, P, P]),
+    "hfm_ns_bc_pressure": (I, [P, I, I, I, P, P]),
     "hfm_sigma7_grad_logsigma": (I, [P, P, P, P, P, I, I, I, I, F, F, F, P, P, P, I, P]),
     "hfm_mg_config_default": (None, [C.POINTER(HfmMgConfig)]),
     "hfm_mg_footprint_bytes": (C.c_size_t, [C.POINTER(HfmMgConfig), I, I, I, I]),

@@ -351,6 +351,16 @@ __global__ void k_pack_stats(const SlotState *st, const int *active, const int *
   out[i] = o;
 }
 
+template <class T>
+__global__ void k_copy_active(const T *__restrict__ src, T *__restrict__ dst, int64_t n,
+                              const int *active) {
+  const int64_t inst = blockIdx.y;
+  if (!active[inst]) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dst[inst * n + i] = src[inst * n + i];
+}
+
 // Initial state of every slot from its ||b||^2 (batched load).
 __global__ void k_init_states(SlotState *st, int *active, int B, const double *sumsq_b,
                               int *outer_mask) {
@@ -806,8 +816,14 @@ class Engine : public EngineBase {
       else st = vcycle(0, false, c.cycle == HFM_CYCLE_F, 1, s);
       if (st) return st;
     }
-    if (m_->cfg.accel == HFM_ACCEL_NONE && cur_[0] != 0)
-      return fail(HFM_ERR_BAD_ARG, "internal: odd number of fine-level sweeps in a launch");
+    if (m_->cfg.accel == HFM_ACCEL_NONE && cur_[0] != 0) {
+      // an odd number of fine-level sweeps: bring the iterate back to the canonical buffer
+      // (slots switched off inside this launch keep their solution where the check saw it)
+      k_copy_active<T><<<dim3(vec_blocks(n(0), m_->slots), m_->slots), 256, 0, s>>>(
+          buf(0, 1), buf(0, 0), n(0), m_->active);
+      HFM_CHECK_LAUNCH("k_copy_active");
+      cur_[0] = 0;
+    }
     return HFM_OK;
   }
 
@@ -1241,7 +1257,6 @@ int hfm_mg_load(hfm_mg *m, int slot, const float *rhs, const float *phi0, hfm_st
 
 int hfm_mg_run(hfm_mg *m, int cycles, hfm_stream_t stream) {
   if (!m || cycles < 1) return fail(HFM_ERR_BAD_ARG, "hfm_mg_run: bad argument");
-  if (m->eng->cycle_flips_parity() && (cycles & 1)) cycles += 1;
   cudaGraphExec_t exec = nullptr;
   auto it = m->graphs.find(cycles);
   if (it != m->graphs.end()) {

@@ -171,3 +171,40 @@ def observe(sigma, survey, solver):
 def misfit_value(log_sigma, survey, d_obs, solver):
     sigma = torch.exp(log_sigma).float().contiguous()
     return _misfit_fields(sigma, survey, d_obs, solver)[0]
+
+
+def config4_check(n=96, n_src=32, n_rec=64, n_fd=20, eps=1e-4, seed=0, group=32):
+    """The differentiation workload: misfit at a homogeneous start against data from the
+    three-ellipsoid model, adjoint gradient, and central finite differences on ``n_fd``
+    random cells.  Returns a dict of timings and agreement figures."""
+    import time
+    survey = make_survey(n=n, n_src=n_src, n_rec=n_rec, seed=seed)
+    solver = ForwardSolver(n, group=group, tol=1e-10)
+    try:
+        d_obs = observe(true_sigma(n, seed=seed), survey, solver)
+        logs = torch.zeros((3, n, n, n), dtype=torch.float64, device="cuda", requires_grad=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        J = misfit(logs, survey, d_obs, solver)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        J.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        g = logs.grad.cpu().numpy()
+        rng = np.random.default_rng(seed + 1)
+        base = logs.detach()
+        errs = []
+        for _ in range(n_fd):
+            k, z, y, x = (int(rng.integers(0, 3)),) + tuple(int(v) for v in rng.integers(0, n, 3))
+            lp, lm = base.clone(), base.clone()
+            lp[k, z, y, x] += eps
+            lm[k, z, y, x] -= eps
+            fd = (misfit_value(lp, survey, d_obs, solver) - misfit_value(lm, survey, d_obs, solver)) / (2 * eps)
+            errs.append(abs(fd - g[k, z, y, x]) / max(abs(g).max(), 1e-300))
+        return {"n": n, "sources": n_src, "receivers": n_rec, "J": float(J.detach()),
+                "grad_max": float(np.abs(g).max()), "forward_s": t1 - t0, "backward_s": t2 - t1,
+                "fd_cells": n_fd, "fd_max_err_rel_to_gmax": float(max(errs)),
+                "fd_median_err_rel_to_gmax": float(np.median(errs))}
+    finally:
+        solver.close()

@@ -200,6 +200,39 @@ int hfm_max_abs(const float *x, int64_t n, int B, float *out, void *scratch,
 #define HFM_NORM2_NOALLOC_SCRATCH_BYTES (512u * 1024u)
 int hfm_norm2_f64_noalloc(const float *x, int64_t n, int B, double *out, hfm_stream_t stream);
 
+/* ---------------------------------------------------------------- NS time-stepper operators */
+/* Operators of scripts/naiver_stokes_3D.py (and Urban Modelling/AI_HFM_v3.ipynb cell 19) on
+ * single (Z, Y, X) float32 fields; x is the flow direction (inflow x = 0, outflow X-1),
+ * extents >= 3.  Kernel arguments are 27 host weights (dz, dy, dx), e.g. w1 (diffusion),
+ * w2-w4 (smoothed central differences, naiver_stokes_3D.py:36-94), w6-w8 (divergence). */
+/* out_f = base_f + coef (Dif(a_f) - a_u Dx(a_f) - a_v Dy(a_f) - a_w Dz(a_f)) for f = u, v, w:
+ * stage 1 of the momentum update with a = base = u^n, coef 0.5; stage 2 with a = b, base = u^n,
+ * coef 1 (naiver_stokes_3D.py:580-622).  Outputs must not alias the advected fields. */
+int hfm_ns_momentum(const float *adv_u, const float *adv_v, const float *adv_w,
+                    const float *base_u, const float *base_v, const float *base_w, float *out_u,
+                    float *out_v, float *out_w, int Z, int Y, int X, const float *w_dif,
+                    const float *w_dx, const float *w_dy, const float *w_dz, float coef,
+                    hfm_stream_t stream);
+/* u -= conv(p, w_px), v -= conv(p, w_py), w -= conv(p, w_pz) (CNN3D_pu/pv/pw, :631-633). */
+int hfm_ns_pressure_gradient(const float *p, float *u, float *v, float *w, int Z, int Y, int X,
+                             const float *w_px, const float *w_py, const float *w_pz,
+                             hfm_stream_t stream);
+/* b = -(Su(u) + Sv(v) + Sw(w)) (:641); bc_source != 0 applies boundary_condition_source
+ * (plane x = 0 takes plane x = 1, :467-473). */
+int hfm_ns_divergence(const float *u, const float *v, const float *w, float *b, int Z, int Y,
+                      int X, const float *w_su, const float *w_sv, const float *w_sw,
+                      int bc_source, hfm_stream_t stream);
+/* bluff_body: u, v, w /= (1 + dt sigma) (:478-483). */
+int hfm_ns_immersed_body(float *u, float *v, float *w, const float *sigma, int Z, int Y, int X,
+                         float dt, hfm_stream_t stream);
+/* boundary_condition_velocity / _pressure (:420-462) in place, with the reference's
+ * assignment order and copies read from the input; scratch: caller device memory of
+ * hfm_ns_bc_scratch_bytes(Z, Y, X) bytes. */
+size_t hfm_ns_bc_scratch_bytes(int Z, int Y, int X);
+int hfm_ns_bc_velocity(float *u, float *v, float *w, int Z, int Y, int X, float ub,
+                       void *scratch, hfm_stream_t stream);
+int hfm_ns_bc_pressure(float *p, int Z, int Y, int X, void *scratch, hfm_stream_t stream);
+
 /* --------------------------------------------------------------- resistivity tomography */
 /* Gradient of the misfit J = 1/2 sum_s |P u_s - d_s|^2 with respect to per-cell log sx, sy,
  * sz for the SIGMA7 operator (face means, wall faces c_d s_c), given the forward fields u_s

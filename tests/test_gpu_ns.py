@@ -1,0 +1,98 @@
+"""NS time-stepper operators (rows B1-B7) on the GPU against the oracle, and a full
+reference time step."""
+import numpy as np
+import pytest
+
+from oracle import ns as ons, weights as OW
+
+pytestmark = pytest.mark.gpu
+SHAPE = (10, 12, 14)
+
+
+def close(got, ref, rtol=1e-5):
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    err = np.abs(got - ref).max() / max(np.abs(ref).max(), 1e-30)
+    assert err <= rtol, "max rel err %.3e > %.1e" % (err, rtol)
+
+
+@pytest.fixture(scope="module")
+def env(hfm):
+    import torch
+    rng = np.random.default_rng(31)
+    f = {k: rng.standard_normal(SHAPE).astype(np.float32) for k in ("u", "v", "w", "p", "b")}
+    return hfm, torch, f
+
+
+def D(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def test_boundary_conditions(env):
+    hfm, torch, f = env
+    ns = hfm.ns
+    u, v, w = D(torch, f["u"]), D(torch, f["v"]), D(torch, f["w"])
+    ns.boundary_condition_velocity(u, v, w, 1.5)
+    ru, rv, rw = ons.bc_velocity(f["u"], f["v"], f["w"], 1.5)
+    np.testing.assert_array_equal(u.cpu().numpy(), ru)
+    np.testing.assert_array_equal(v.cpu().numpy(), rv)
+    np.testing.assert_array_equal(w.cpu().numpy(), rw)
+    p = D(torch, f["p"])
+    ns.boundary_condition_pressure(p)
+    np.testing.assert_array_equal(p.cpu().numpy(), ons.bc_pressure(f["p"]))
+
+
+def test_momentum_gradient_divergence_ibm(env):
+    hfm, torch, f = env
+    ns, W = hfm.ns, hfm.weights
+    dt = 0.1
+    Kd = W.diffusion27(dt, 0.25)
+    Kx, Ky, Kz = W.advection(dt)
+    u, v, w = (D(torch, f[k]) for k in "uvw")
+    ou, ov, ow = (torch.empty_like(u) for _ in range(3))
+    ns.momentum_stage((u, v, w), (u, v, w), (ou, ov, ow), Kd, Kx, Ky, Kz, 0.5)
+    for got, name in zip((ou, ov, ow), "uvw"):
+        ref = 0.5 * ons.momentum_rhs(f[name], f["u"], f["v"], f["w"], Kd, Kx, Ky, Kz) + f[name]
+        close(got.cpu(), ref)
+    p = D(torch, f["p"])
+    u2, v2, w2 = (D(torch, f[k]) for k in "uvw")
+    ns.pressure_gradient(p, u2, v2, w2, Kx, Ky, Kz)
+    for got, ref in zip((u2, v2, w2), ons.pressure_gradient(f["p"], f["u"], f["v"], f["w"], Kx, Ky, Kz)):
+        close(got.cpu(), ref)
+    Su, Sv, Sw = W.divergence(dt)
+    b = torch.empty_like(u)
+    ns.divergence(u, v, w, b, Su, Sv, Sw, bc_source=True)
+    close(b.cpu(), ons.divergence_rhs(f["u"], f["v"], f["w"], Su, Sv, Sw))
+    sig = np.where(np.random.default_rng(2).random(SHAPE) < 0.2, 1e5, 0).astype(np.float32)
+    u3, v3, w3 = (D(torch, f[k]) for k in "uvw")
+    ns.bluff_body(u3, v3, w3, D(torch, sig), dt)
+    for got, ref in zip((u3, v3, w3), ons.bluff_body(f["u"], f["v"], f["w"], sig, dt)):
+        np.testing.assert_allclose(got.cpu().numpy(), ref, rtol=1e-6, atol=1e-12)
+
+
+@pytest.mark.parametrize("multi_itr", [2, 5])
+def test_reference_step(env, multi_itr):
+    """Two reference time steps (naiver_stokes_3D.py:571-727) on 16^3 with an obstacle."""
+    hfm, torch, f = env
+    ns = hfm.ns
+    n = 16
+    cfg = ns.NSConfig(dt=0.1, Re=0.25, ub=1.0, pressure="reference", multi_itr=multi_itr)
+    sig = ns.obstacle_mask((n, n, n), n_boxes=2, footprint=(2, 4), height=(3, 6), seed=1)
+    st = ns.NSStepper((n, n, n), cfg, sigma=sig)
+    W = hfm.weights
+    Kd = W.diffusion27(cfg.dt, cfg.Re)
+    Kx, Ky, Kz = W.advection(cfg.dt)
+    Su, Sv, Sw = W.divergence(cfg.dt)
+    Kp = W.pressure27()
+    z = np.zeros((n, n, n), np.float32)
+    ru, rv, rw, rp = z, z, z, z
+    signp = sig.cpu().numpy()
+    try:
+        for _ in range(2):
+            st.step()
+            ru, rv, rw, rp = ons.step(ru, rv, rw, rp, signp, cfg.dt, cfg.ub, Kd, Kx, Ky, Kz, Su, Sv,
+                                      Sw, Kp, 4, multi_itr)
+        for got, ref in zip((st.u, st.v, st.w, st.p), (ru, rv, rw, rp)):
+            close(got.cpu(), ref, rtol=1e-4)
+    finally:
+        st.close()
