@@ -53,7 +53,10 @@ template <> struct St<__nv_bfloat16> {
 };
 template <> struct St<__half> {
   static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
-  static __device__ __forceinline__ __half from(float v) { return __float2half(v); }
+  // saturating: a transient value beyond the fp16 range is stored as +-65504, not inf
+  static __device__ __forceinline__ __half from(float v) {
+    return __float2half(fminf(fmaxf(v, -65504.f), 65504.f));
+  }
   static __device__ __forceinline__ float to(__half v) { return __half2float(v); }
 };
 

@@ -351,6 +351,41 @@ __global__ void k_pack_stats(const SlotState *st, const int *active, const int *
   out[i] = o;
 }
 
+// Geometric mean of a slot's three conductivity arrays (one block per slot).
+__global__ void k_log_mean(const void *sx, const void *sy, const void *sz, int dt, int64_t n,
+                           int slot0, double *gscale) {
+  __shared__ double sh[32];
+  const int64_t sl = blockIdx.x;
+  const void *arr[3] = {sx, sy, sz};
+  double acc = 0.0;
+  for (int a = 0; a < 3; ++a)
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+      const int64_t k = sl * n + i;
+      const double v = dt == HFM_F64 ? ((const double *)arr[a])[k] : (double)((const float *)arr[a])[k];
+      acc += log(v);
+    }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    gscale[slot0 + sl] = exp(t / (3.0 * (double)n));
+  }
+}
+
+template <class T>
+__global__ void k_convert_scaled(const void *__restrict__ src, int dt, T *__restrict__ dst,
+                                 int64_t n, int count, int slot0, const double *gscale) {
+  const int64_t tot = n * count;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < tot;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double g = gscale[slot0 + i / n];
+    const double v = dt == HFM_F64 ? ((const double *)src)[i] : (double)((const float *)src)[i];
+    dst[i] = St<T>::from((float)(v / g));
+  }
+}
+
 template <class T>
 __global__ void k_copy_active(const T *__restrict__ src, T *__restrict__ dst, int64_t n,
                               const int *active) {
@@ -411,16 +446,25 @@ __global__ void k_fetch_all(const T *__restrict__ b0, const T *__restrict__ b1,
 // ----------------------------------------------------------------- CG vector kernels
 // Scale of the preconditioner input for 16-bit storage: the cycle solves for r / s with
 // s = RMS(r), so its fields stay O(1) in bf16 / fp16 whatever the residual's size; z = s M(r/s).
-__device__ __forceinline__ float pc_scale(const SlotState &s, int64_t n, int scaled) {
-  return (scaled && s.rr > 0.0) ? (float)sqrt(s.rr / (double)n) : 1.f;
+// scaled = 0: none (float32 / bf16: the exponent range of float32); 2: fp16 - the cycle
+// solves for r / |r|_2 (entries <= 1) with conductivities divided by their geometric mean
+// g, so z = (|r|_2 / g) M'(r / |r|_2).  pc_in is the divisor of the input, pc_out the factor
+// of the output.
+__device__ __forceinline__ float pc_in(const SlotState &s, int64_t n, int scaled) {
+  (void)n;
+  return (scaled == 2 && s.rr > 0.0) ? (float)sqrt(s.rr) : 1.f;
+}
+__device__ __forceinline__ float pc_out(const SlotState &s, int64_t n, int scaled,
+                                        const double *gscale, int64_t slot) {
+  return scaled == 2 ? (float)(pc_in(s, n, scaled) / gscale[slot]) : 1.f;
 }
 
 template <class TZ>
 __global__ void k_dot_partials(const float *__restrict__ a, const TZ *__restrict__ b, Items it,
                                double *partials, const int *active, const SlotState *st,
-                               int scaled) {
+                               int scaled, const double *gscale) {
   HFM_FOR_ITEMS(it, active[slot])
-  const double zs = st ? pc_scale(st[slot], it.n, scaled) : 1.0;
+  const double zs = st ? pc_out(st[slot], it.n, scaled, gscale, slot) : 1.0;
   double acc = 0.0;
   for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
     acc += (double)a[base + i] * (double)St<TZ>::ld(b + base + i);
@@ -451,12 +495,13 @@ __global__ void k_scalar_sum(const double *__restrict__ partials, int nblk, Slot
 // p = z + beta p (beta = rz_new / rz; first iteration p = z); rz <- rz_new.
 template <class TZ>
 __global__ void k_cg_p(const TZ *__restrict__ z, float *__restrict__ p, Items it, SlotState *st,
-                       const double *rz_new, const int *active, int scaled) {
+                       const double *rz_new, const int *active, int scaled,
+                       const double *gscale) {
   HFM_FOR_ITEMS(it, active[slot])
   const SlotState s = st[slot];
   const bool first = s.inner_cycles == 0 || s.rz == 0.0;
   const float beta = first ? 0.f : (float)(rz_new[slot] / s.rz);
-  const float zs = pc_scale(s, it.n, scaled);
+  const float zs = pc_out(s, it.n, scaled, gscale, slot);
   for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     const float zv = zs * St<TZ>::ld(z + base + i);
     p[base + i] = first ? zv : zv + beta * p[base + i];
@@ -500,7 +545,7 @@ template <class T>
 __global__ void k_to_storage(const float *__restrict__ a, T *__restrict__ b, Items it,
                              const int *active, const SlotState *st, int scaled) {
   HFM_FOR_ITEMS(it, active[slot])
-  const float inv = 1.f / pc_scale(st[slot], it.n, scaled);
+  const float inv = 1.f / pc_in(st[slot], it.n, scaled);
   for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
     b[base + i] = St<T>::from(a[base + i] * inv);
   HFM_END_ITEMS
@@ -568,6 +613,7 @@ struct hfm_mg {
   double *partials = nullptr;
   int64_t partials_per_slot = 0;
   double *scal = nullptr;  // per-slot scratch scalars (rz_new), and ||b||^2 at load
+  double *gscale = nullptr;  // fp16 storage: geometric mean of each slot's conductivities
   hfm_operator fine_desc;
   cudaStream_t cap = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
@@ -769,7 +815,7 @@ class Engine : public EngineBase {
     float *x = m_->cg[0], *r = m_->cg[1], *p = m_->cg[2], *q = m_->cg[3];
     const Items it{B, item_chunks(nf), nf};
     const int vb = it.CH, ib = item_blocks(B, it.CH);
-    const int scaled = std::is_same<T, float>::value ? 0 : 1;
+    const int scaled = std::is_same<T, __half>::value ? 2 : 0;
     int st;
     // z = M r  (rhs(0) holds r / s in the storage type; float32 storage reads r in place)
     if (!std::is_same<T, float>::value) {
@@ -779,10 +825,11 @@ class Engine : public EngineBase {
     if ((st = vcycle(0, true, m_->cfg.cycle == HFM_CYCLE_F, 0, s))) return st;
     const T *z = buf(0, cur_[0]);
     // rz_new = r . z ; p = z + beta p
-    k_dot_partials<T><<<ib, 256, 0, s>>>(r, z, it, m_->partials, m_->active, m_->state, scaled);
+    k_dot_partials<T><<<ib, 256, 0, s>>>(r, z, it, m_->partials, m_->active, m_->state, scaled,
+                                         m_->gscale);
     HFM_CHECK_LAUNCH("k_dot_partials");
     k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 0, m_->scal);
-    k_cg_p<T><<<ib, 256, 0, s>>>(z, p, it, m_->state, m_->scal, m_->active, scaled);
+    k_cg_p<T><<<ib, 256, 0, s>>>(z, p, it, m_->state, m_->scal, m_->active, scaled, m_->gscale);
     k_cg_commit_rz<<<(B + 127) / 128, 128, 0, s>>>(m_->state, m_->scal, m_->active, B);
     HFM_CHECK_LAUNCH("k_cg_p");
     // q = A p ; pq = p . q   (FP32 operator on the fine level)
@@ -791,7 +838,8 @@ class Engine : public EngineBase {
     pp.base = p;
     pp.base_stride = nf;
     if ((st = launch_apply<float>(kind(), fine32_, pp, q, nf, B, g(0), m_->active, s))) return st;
-    k_dot_partials<float><<<ib, 256, 0, s>>>(p, q, it, m_->partials, m_->active, nullptr, 0);
+    k_dot_partials<float><<<ib, 256, 0, s>>>(p, q, it, m_->partials, m_->active, nullptr, 0,
+                                             nullptr);
     k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 1, m_->scal);
     // x += alpha p ; r -= alpha q ; ||r||
     k_cg_xr<<<ib, 256, 0, s>>>(x, r, p, q, it, m_->state, m_->partials, m_->active);
@@ -848,10 +896,26 @@ class Engine : public EngineBase {
       return fail(HFM_ERR_BAD_ARG, "coefficients must be float32 or float64");
     // slot < 0: every slot at once (the arrays hold all slots), one launch per level
     const int lo = slot < 0 ? 0 : slot, cnt = slot < 0 ? m_->slots : 1;
-    for (int a = 0; a < 3; ++a) {
+    // fp16 cycles used as a preconditioner store sigma / g (their output is rescaled by 1/g);
+    // stationary fp16 cycles keep sigma itself, their iterate is the solution
+    const bool normalize = std::is_same<T, __half>::value && m_->cfg.accel != HFM_ACCEL_NONE;
+    for (int a = 0; a < 3; ++a)
       if (!op.coef[a]) return fail(HFM_ERR_BAD_ARG, "SIGMA7 needs sx, sy, sz");
-      int st = launch_convert<T>(op.coef[a], op.coef_dtype, (T *)m_->lv[0].coef[a] + lo * n(0),
-                                 n(0) * cnt, s);
+    if (normalize) {
+      k_log_mean<<<cnt, 256, 0, s>>>(op.coef[0], op.coef[1], op.coef[2], op.coef_dtype, n(0), lo,
+                                     m_->gscale);
+      HFM_CHECK_LAUNCH("k_log_mean");
+    }
+    for (int a = 0; a < 3; ++a) {
+      int st = HFM_OK;
+      if (normalize) {
+        k_convert_scaled<T><<<vec_blocks(n(0) * cnt, 1), 256, 0, s>>>(
+            op.coef[a], op.coef_dtype, (T *)m_->lv[0].coef[a] + lo * n(0), n(0), cnt, lo, m_->gscale);
+        HFM_CHECK_LAUNCH("k_convert_scaled");
+      } else {
+        st = launch_convert<T>(op.coef[a], op.coef_dtype, (T *)m_->lv[0].coef[a] + lo * n(0),
+                               n(0) * cnt, s);
+      }
       if (st) return st;
       if (fine32_coef_[a] && (st = launch_convert<float>(op.coef[a], op.coef_dtype,
                                                          fine32_coef_[a] + lo * n(0), n(0) * cnt, s)))
@@ -1188,6 +1252,7 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
   m->state = (SlotState *)dalloc(m.get(), (size_t)slots * sizeof(SlotState), &st);
   m->stats_dev = (hfm_slot_stats *)dalloc(m.get(), (size_t)slots * sizeof(hfm_slot_stats), &st);
   m->scal = (double *)dalloc(m.get(), (size_t)(slots + 1) * 8, &st);
+  m->gscale = (double *)dalloc(m.get(), (size_t)slots * 8, &st);
   if (!st) {
     if (cudaMemset(m->active, 0, (size_t)slots * 4) != cudaSuccess ||
         cudaMemset(m->outer, 0, (size_t)slots * 4) != cudaSuccess ||

@@ -70,8 +70,8 @@ template <> __device__ __forceinline__ void st4<__nv_bfloat16>(__nv_bfloat16 *p,
   *reinterpret_cast<uint2 *>(p) = u;
 }
 template <> __device__ __forceinline__ void st4<__half>(__half *p, const F4 &v) {
-  __half2 a = __floats2half2_rn(v.v[0], v.v[1]);
-  __half2 b = __floats2half2_rn(v.v[2], v.v[3]);
+  __half2 a = __floats2half2_rn(fminf(fmaxf(v.v[0], -65504.f), 65504.f), fminf(fmaxf(v.v[1], -65504.f), 65504.f));
+  __half2 b = __floats2half2_rn(fminf(fmaxf(v.v[2], -65504.f), 65504.f), fminf(fmaxf(v.v[3], -65504.f), 65504.f));
   uint2 u;
   u.x = *reinterpret_cast<unsigned *>(&a);
   u.y = *reinterpret_cast<unsigned *>(&b);

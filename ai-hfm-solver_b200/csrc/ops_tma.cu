@@ -150,7 +150,9 @@ template <> __device__ __forceinline__ void gst4<__nv_bfloat16>(__nv_bfloat16 *p
   *reinterpret_cast<uint2 *>(p) = u;
 }
 template <> __device__ __forceinline__ void gst4<__half>(__half *p, const float (&v)[4]) {
-  __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
+  const float c0 = fminf(fmaxf(v[0], -65504.f), 65504.f), c1 = fminf(fmaxf(v[1], -65504.f), 65504.f);
+  const float c2 = fminf(fmaxf(v[2], -65504.f), 65504.f), c3 = fminf(fmaxf(v[3], -65504.f), 65504.f);
+  __half2 a = __floats2half2_rn(c0, c1), b = __floats2half2_rn(c2, c3);
   uint2 u;
   u.x = *reinterpret_cast<unsigned *>(&a);
   u.y = *reinterpret_cast<unsigned *>(&b);

@@ -202,3 +202,46 @@ class Multigrid:
         stats = [dict(active=s.active, status=s.status, cycles=s.cycles, outer=s.outer,
                       norm_b=s.norm_b, rel_resid=s.rel_resid) for s in self._stats]
         return phi, stats
+
+
+def precision_check(n=256, log_std=2.0, seed=0, tol=1e-10, storages=("bf16", "f16", "f32"),
+                    oracle_error=False):
+    """The precision workload: the anisotropic operator at ``n``^3 with sigma log-std
+    ``log_std`` solved by float64 iterative refinement around CG preconditioned by V(2,2)
+    cycles stored in each of ``storages``.  Reports per storage the cycles, refinement steps,
+    float64 relative residual, time and - with ``oracle_error`` - the error against a float64
+    solve of the same system (float64 refinement driven to 1e-13 with float32 inner cycles)."""
+    import time
+    from . import problems, ops
+    sig = problems.anisotropic_sigma((n, n, n), seed=seed, log_std=log_std)
+    f = problems.dipole((n, n, n), seed=seed)
+    sd = torch.from_numpy(sig).cuda()
+    fd = torch.from_numpy(f.astype(np.float64)).cuda()
+    op = ops.Sigma7(sd[0], sd[1], sd[2])
+
+    def run(storage, t):
+        cfg = SolverConfig(cycle="V", accel="ir", storage=storage, tol=t, max_cycles=2000)
+        with Multigrid((n, n, n), L.OP_SIGMA7, cfg, slots=1) as h:
+            h.set_operator(op)
+            h.load_f64(0, fd)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            while True:
+                h.run(8)
+                st = h.query()[0]
+                if not st["active"]:
+                    break
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            return h.fetch_f64(0), st, dt
+
+    ref = run("f32", 1e-13)[0] if oracle_error else None
+    out = {}
+    for s in storages:
+        x, st, dt = run(s, tol)
+        d = {"status": st["status"], "cycles": st["cycles"], "outer": st["outer"],
+             "rel_resid": st["rel_resid"], "seconds": dt}
+        if ref is not None:
+            d["error_vs_f64"] = float((x - ref).norm() / ref.norm())
+        out[s] = d
+    return out
