@@ -697,8 +697,12 @@ class Engine : public EngineBase {
     int st;
     if (l == m_->L - 1) return coarse_solve(l, s);
     if (zero) cur_[l] = 0;
+    // NS outflow rule on the fine level (as the reference cycle applies it): the iterate is
+    // read as zero on x = X-1 and the residual is zero there
+    const int xend = (l == 0 && (c.flags & HFM_FLAG_ZERO_XEND)) ? 1 : 0;
     for (int k = 0; k < c.nu_pre; ++k) {
       PhiSrc<T> p = src((zero && k == 0) ? nullptr : buf(l, cur_[l]), n(l));
+      p.zero_xend = xend;
       if ((st = smooth(l, p, rhs(l), buf(l, cur_[l] ^ 1), c.omega, 0u, s))) return st;
       cur_[l] ^= 1;
     }
@@ -706,9 +710,19 @@ class Engine : public EngineBase {
     int nblk = 0;
     const bool chk = (l == 0 && check_level0);
     PhiSrc<T> p = src(still_zero ? nullptr : buf(l, cur_[l]), n(l));
-    if ((st = launch_residual_restrict<T>(kind(), m_->lv[l].op, p, rhs(l), n(l), nullptr, 0,
-                                          rhs(l + 1), n(l + 1), m_->slots, g(l), 0u,
-                                          m_->active, chk ? m_->partials : nullptr, &nblk, s)))
+    if (xend) {
+      // residual of the iterate with its x = X-1 plane read as zero, zero there, restricted
+      T *rf = (T *)m_->saw[0];
+      p.zero_xend = 1;
+      if ((st = launch_residual<T>(kind(), m_->lv[l].op, p, rhs(l), n(l), rf, n(l), m_->slots,
+                                   g(l), HFM_FLAG_ZERO_XEND, m_->active,
+                                   chk ? m_->partials : nullptr, &nblk, s)))
+        return st;
+      if ((st = launch_restrict<T>(rf, n(l), rhs(l + 1), n(l + 1), m_->slots, g(l), m_->active, s)))
+        return st;
+    } else if ((st = launch_residual_restrict<T>(kind(), m_->lv[l].op, p, rhs(l), n(l), nullptr, 0,
+                                                 rhs(l + 1), n(l + 1), m_->slots, g(l), 0u,
+                                                 m_->active, chk ? m_->partials : nullptr, &nblk, s)))
       return st;
     if (chk && (st = check(nblk, cur_[0], s))) return st;
     if (fcycle) {
@@ -722,6 +736,7 @@ class Engine : public EngineBase {
     for (int k = 0; k < post; ++k) {
       PhiSrc<T> q = src(still_zero && k == 0 ? nullptr : buf(l, cur_[l]), n(l));
       if (k == 0) q = with_coarse(q, l + 1, buf(l + 1, cur_[l + 1]), -1.f);
+      q.zero_xend = xend;
       float om = c.nu_post == 0 ? 0.f : c.omega;
       if ((st = smooth(l, q, rhs(l), buf(l, cur_[l] ^ 1), om, 0u, s))) return st;
       cur_[l] ^= 1;
@@ -1136,6 +1151,10 @@ int validate_cfg(const hfm_mg_config &c, int Z, int Y, int X, int slots) {
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: bad cycle / accel");
   if (c.cycle == HFM_CYCLE_SAWTOOTH && c.accel != HFM_ACCEL_NONE)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: the sawtooth cycle is not symmetric; use V or F with CG");
+  if (c.accel != HFM_ACCEL_NONE && (c.flags & HFM_FLAG_ZERO_XEND))
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: the x-end rule is for stationary cycles only");
+  if (c.accel != HFM_ACCEL_NONE && c.cycle == HFM_CYCLE_F)
+    return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: the F-cycle is not symmetric and cannot precondition CG; use V");
   if (c.accel != HFM_ACCEL_NONE && c.nu_pre != c.nu_post)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: CG needs a symmetric cycle (nu_pre == nu_post)");
   if (c.nu_pre < 0 || c.nu_post < 0 || c.coarse_sweeps < 1 || c.max_cycles < 1)
@@ -1187,7 +1206,7 @@ size_t hfm_mg_footprint_bytes(const hfm_mg_config *c, int Z, int Y, int X, int s
     tot += nf * 5 * 4;  // x r p q b
     if (c->accel == HFM_ACCEL_IR) tot += nf * 2 * 8;  // float64 x, b
     if (c->op_kind == HFM_OP_SIGMA7 && c->storage != HFM_F32) tot += nf * 3 * 4;
-  } else if (c->cycle == HFM_CYCLE_SAWTOOTH) {
+  } else if (c->cycle == HFM_CYCLE_SAWTOOTH || (c->flags & HFM_FLAG_ZERO_XEND)) {
     tot += nf * 2 * es;
   }
   tot *= (size_t)slots;
@@ -1241,7 +1260,7 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
     for (int i = 0; i < 4; ++i) m->cg[i] = (float *)dalloc(m.get(), nf * 4, &st);
     m->fine_b = dalloc(m.get(), nf * 4, &st);
     if (cfg->storage == HFM_F32) m->lv[0].rhs = m->cg[1];
-  } else if (cfg->cycle == HFM_CYCLE_SAWTOOTH) {
+  } else if (cfg->cycle == HFM_CYCLE_SAWTOOTH || (cfg->flags & HFM_FLAG_ZERO_XEND)) {
     m->saw[0] = dalloc(m.get(), nf * es, &st);
     m->saw[1] = dalloc(m.get(), nf * es, &st);
   }

@@ -250,12 +250,15 @@ def sawtooth_cycle(ops, phi, b, fine_smooth=True, zero_xend=False, top_copy=Fals
 # --------------------------------------------------------------------------------------
 class CycleConfig:
     def __init__(self, nu_pre=2, nu_post=2, omega=2.0 / 3.0, coarse_sweeps=32,
-                 coarse_omega=None):
+                 coarse_omega=None, zero_xend=False):
         self.nu_pre = nu_pre
         self.nu_post = nu_post
         self.omega = omega
         self.coarse_sweeps = coarse_sweeps
         self.coarse_omega = omega if coarse_omega is None else coarse_omega
+        # NS outflow rule on the fine level: iterate read as zero on x = X-1, residual zero
+        # there (the reference applies it in its pressure cycle, naiver_stokes_3D.py:650-701)
+        self.zero_xend = zero_xend
 
 
 def _coarse_solve(op, f, cfg):
@@ -265,18 +268,34 @@ def _coarse_solve(op, f, cfg):
     return w
 
 
+def _xz(phi, on):
+    if not on:
+        return phi
+    phi = np.array(phi, copy=True)
+    phi[..., -1] = 0
+    return phi
+
+
+def _fine_residual(op, phi, f, on):
+    r = residual(op, _xz(phi, on), f)
+    if on:
+        r[..., -1] = 0
+    return r
+
+
 def vcycle(ops, l, phi, f, cfg):
     """V(nu_pre, nu_post) cycle on level ``l`` for ``A_l phi = f``."""
     op = ops[l]
     if l == len(ops) - 1:
         return _coarse_solve(op, f, cfg)
+    xe = l == 0 and getattr(cfg, "zero_xend", False)
     for _ in range(cfg.nu_pre):
-        phi = jacobi(op, phi, f, cfg.omega)
-    fc = tfops.restrict_avg(residual(op, phi, f), op.dtype)
+        phi = jacobi(op, _xz(phi, xe), f, cfg.omega)
+    fc = tfops.restrict_avg(_fine_residual(op, phi, f, xe), op.dtype)
     wc = vcycle(ops, l + 1, np.zeros_like(fc), fc, cfg)
     phi = phi - tfops.prolong_nearest(wc, op.dtype)
     for _ in range(cfg.nu_post):
-        phi = jacobi(op, phi, f, cfg.omega)
+        phi = jacobi(op, _xz(phi, xe), f, cfg.omega)
     return phi
 
 
@@ -286,14 +305,15 @@ def fcycle(ops, l, phi, f, cfg):
     op = ops[l]
     if l == len(ops) - 1:
         return _coarse_solve(op, f, cfg)
+    xe = l == 0 and getattr(cfg, "zero_xend", False)
     for _ in range(cfg.nu_pre):
-        phi = jacobi(op, phi, f, cfg.omega)
-    fc = tfops.restrict_avg(residual(op, phi, f), op.dtype)
+        phi = jacobi(op, _xz(phi, xe), f, cfg.omega)
+    fc = tfops.restrict_avg(_fine_residual(op, phi, f, xe), op.dtype)
     wc = fcycle(ops, l + 1, np.zeros_like(fc), fc, cfg)
     wc = vcycle(ops, l + 1, wc, fc, cfg)
     phi = phi - tfops.prolong_nearest(wc, op.dtype)
     for _ in range(cfg.nu_post):
-        phi = jacobi(op, phi, f, cfg.omega)
+        phi = jacobi(op, _xz(phi, xe), f, cfg.omega)
     return phi
 
 

@@ -69,3 +69,7 @@ def test_bad_arguments_fail_without_gpu(lib, pkg):
     h = C.c_void_p()
     assert lib.hfm_mg_create(C.byref(cfg), 8, 8, 8, 1, C.byref(h)) == L.ERR_BAD_ARG
     assert b"symmetric" in lib.hfm_last_error()
+    cfg.nu_post = 2
+    cfg.cycle = L.CYCLE_F
+    assert lib.hfm_mg_create(C.byref(cfg), 8, 8, 8, 1, C.byref(h)) == L.ERR_BAD_ARG
+    assert b"F-cycle" in lib.hfm_last_error()
