@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--rate", type=float, default=2000.0)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--quick", action="store_true",
+                   help="served leg only (no plain / e2e / roofline / CPU legs), for profiling")
     return p.parse_args()
 
 
@@ -253,6 +255,12 @@ def run_serve(args, pkg, torch, rank, world, local):
     value = len(reqs) * world / (ms / 1e3)
 
     e2e = None
+    if args.quick:
+        server.close()
+        return {"metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+                "p50_ms": round(lat["p50_ms"], 3), "p99_ms": round(lat["p99_ms"], 3),
+                "failed": len(bad), "gpu_launches": int(launches), "quick": True}
     if not args.no_e2e:
         host = [sv.SolveRequest(r.rid, r.n, r.arrival, r.sigma.cpu().pin_memory(),
                                 r.rhs.cpu().pin_memory(), r.log_std) for r in reqs]
