@@ -209,6 +209,25 @@ int fast_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const
                 int *nblk_out, cudaStream_t s);
 // TMA-pipelined kernels (ops_tma.cu) for X >= 64: same modes as fast_launch.
 bool tma_eligible(int kind, Grid3 g, int mode, const void *corr, int corr_coarse, int es);
+// Vector access alignment: every pointer the plane-marching kernels load or store in vectors
+// is aligned to `bytes` (16 for the TMA kernels, whose tensor maps also need it; 4 elements
+// for the register-queue kernels) and so are the per-instance strides.  Callers whose
+// pointers violate this take the generic one-cell-per-thread kernels.
+template <class T>
+bool vec_aligned(int kind, const DevOp &op, const PhiSrc<T> &phi, const void *rhs,
+                 const void *out, const void *coarse, int64_t stride, int64_t bytes) {
+  auto al = [bytes](const void *p) { return ((uintptr_t)p % (uintptr_t)bytes) == 0; };
+  const int64_t es = (int64_t)sizeof(T);
+  if (!al(phi.base) || !al(phi.corr) || !al(rhs) || !al(out) || !al(coarse)) return false;
+  if ((stride * es) % bytes) return false;
+  if (phi.corr && (phi.corr_stride * es) % bytes) return false;
+  if (kind == HFM_OP_SIGMA7) {
+    for (int k = 0; k < 3; ++k)
+      if (!al(op.coef[k])) return false;
+    if ((op.coef_stride * es) % bytes) return false;
+  }
+  return true;
+}
 template <class T>
 int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const T *rhs, T *out,
                T *coarse, int64_t stride, int64_t coarse_stride, int B, Grid3 g, float omega,

@@ -243,11 +243,13 @@ int launch_smooth(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
                   unsigned flags, const int *active, cudaStream_t s) {
   if ((!phi.base || phi.base_stride == out_stride) && (phi.base || phi.corr || rhs) &&
       (!rhs || rhs_stride == out_stride) &&
-      tma_eligible(kind, g, FAST_SMOOTH, phi.corr, phi.corr_coarse, (int)sizeof(T)))
+      tma_eligible(kind, g, FAST_SMOOTH, phi.corr, phi.corr_coarse, (int)sizeof(T)) &&
+      vec_aligned<T>(kind, op, phi, rhs, out, nullptr, out_stride, 16))
     return tma_launch<T>(kind, FAST_SMOOTH, op, phi, rhs, out, nullptr, out_stride, 0, B, g,
                          omega, flags, active, nullptr, nullptr, s);
   if (fast_eligible(kind, g, false) && (!rhs || rhs_stride == out_stride) &&
-      (!phi.base || phi.base_stride == out_stride) && (!phi.corr || phi.corr_coarse || phi.corr_stride == out_stride))
+      (!phi.base || phi.base_stride == out_stride) && (!phi.corr || phi.corr_coarse || phi.corr_stride == out_stride) &&
+      vec_aligned<T>(kind, op, phi, rhs, out, nullptr, out_stride, 4 * (int64_t)sizeof(T)))
     return fast_launch<T>(kind, FAST_SMOOTH, op, phi, rhs, out, nullptr, out_stride, 0, B, g,
                           omega, flags, active, nullptr, nullptr, s);
   dim3 grid(blocks_for(g.n(), B), B);
@@ -263,11 +265,13 @@ int launch_residual(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *b,
                     int64_t b_stride, T *r, int64_t r_stride, int B, Grid3 g, unsigned flags,
                     const int *active, double *partials, int *nblk_out, cudaStream_t s) {
   if (phi.base && !phi.corr && !phi.zero_xend && r && phi.base_stride == r_stride &&
-      (!b || b_stride == r_stride) && tma_eligible(kind, g, FAST_RESID, nullptr, 0, (int)sizeof(T)))
+      (!b || b_stride == r_stride) && tma_eligible(kind, g, FAST_RESID, nullptr, 0, (int)sizeof(T)) &&
+      vec_aligned<T>(kind, op, phi, b, r, nullptr, r_stride, 16))
     return tma_launch<T>(kind, FAST_RESID, op, phi, b, r, nullptr, r_stride, 0, B, g, 0.f,
                          flags, active, partials, nblk_out, s);
   if (fast_eligible(kind, g, false) && !phi.corr && !phi.zero_xend && r &&
-      (!b || b_stride == r_stride) && (!phi.base || phi.base_stride == r_stride))
+      (!b || b_stride == r_stride) && (!phi.base || phi.base_stride == r_stride) &&
+      vec_aligned<T>(kind, op, phi, b, r, nullptr, r_stride, 4 * (int64_t)sizeof(T)))
     return fast_launch<T>(kind, FAST_RESID, op, phi, b, r, nullptr, r_stride, 0, B, g, 0.f,
                           flags, active, partials, nblk_out, s);
   int nb = blocks_for(g.n(), B);
@@ -296,12 +300,14 @@ int launch_residual_restrict(int kind, const DevOp &op, const PhiSrc<T> &phi, co
   if ((g.Z | g.Y | g.X) & 1) return fail(HFM_ERR_BAD_ARG, "residual_restrict needs even extents");
   if (phi.base && !phi.corr && !phi.zero_xend && b && phi.base_stride == b_stride &&
       (!r_fine || rf_stride == b_stride) && rc_stride == b_stride / 8 &&
-      tma_eligible(kind, g, FAST_RESTRICT, nullptr, 0, (int)sizeof(T)))
+      tma_eligible(kind, g, FAST_RESTRICT, nullptr, 0, (int)sizeof(T)) &&
+      vec_aligned<T>(kind, op, phi, b, r_fine, nullptr, b_stride, 16))
     return tma_launch<T>(kind, FAST_RESTRICT, op, phi, b, r_fine, r_coarse, b_stride, rc_stride,
                          B, g, 0.f, flags, active, partials, nblk_out, s);
   if (fast_eligible(kind, g, true) && !phi.corr && !phi.zero_xend && b &&
       (!r_fine || rf_stride == b_stride) && (!phi.base || phi.base_stride == b_stride) &&
-      rc_stride == b_stride / 8)
+      rc_stride == b_stride / 8 &&
+      vec_aligned<T>(kind, op, phi, b, r_fine, r_coarse, b_stride, 4 * (int64_t)sizeof(T)))
     return fast_launch<T>(kind, FAST_RESTRICT, op, phi, b, r_fine, r_coarse, b_stride, rc_stride,
                           B, g, 0.f, flags, active, partials, nblk_out, s);
   int64_t nc = g.n() / 8;

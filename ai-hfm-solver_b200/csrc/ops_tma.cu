@@ -6,7 +6,9 @@
 // tiles into a shared-memory stage - phi with a one-row / HX-column halo, the three
 // conductivities (sx with x halo, sy with y halo, sz), the right-hand side and, for the fused
 // correction, the coarse correction tile - and one mbarrier per stage counts the bytes in.
-// NS = 5 stages: planes z-1, z, z+1 are read while z+2, z+3 are in flight.  Tiles that reach
+// NS = 5 stages for float32 (planes z-1, z, z+1 are read while z+2, z+3 are in flight) and 4
+// for 16-bit storage, whose kernels are issue-bound rather than bandwidth-bound: the smaller
+// ring lets four blocks share an SM instead of three.  Tiles that reach
 // past the grid (walls, the planes before 0 and after Z-1) are zero-filled by the TMA unit,
 // which is exactly the SAME zero padding of the reference's Conv3D layers; the kernels then
 // apply the wall rule for conductivities (ghost sigma = interior sigma) from the global
@@ -28,7 +30,7 @@ static __device__ int g_tma_timeouts;
 
 namespace {
 
-constexpr int TX = 64, NS = 5;
+constexpr int TX = 64;
 constexpr int kMaxSpin = 1 << 20;
 
 enum { M_SMOOTH = FAST_SMOOTH, M_RESID = FAST_RESID, M_RESTRICT = FAST_RESTRICT };
@@ -37,9 +39,14 @@ enum { M_SMOOTH = FAST_SMOOTH, M_RESID = FAST_RESID, M_RESTRICT = FAST_RESTRICT 
 // coarse correction tile (stages of the other kernels are smaller, so more blocks fit).
 template <class T, bool SIG = true, bool CC = true> struct Geo {
   // 8 rows x 64 columns per block for float32, 16 rows for 16-bit storage (same bytes per
-  // stage); 16 threads per row, 4 consecutive x per thread
+  // stage); a thread owns 16 bytes of x: 4 float32 / 8 16-bit values, so 16 / 8 threads per
+  // row and 128 threads per block either way
   static constexpr int TY = sizeof(T) == 4 ? 8 : 16;
-  static constexpr int THREADS = 16 * TY;
+  static constexpr int VEC = 16 / (int)sizeof(T);
+  static constexpr int TPR = TX / VEC;
+  static constexpr int THREADS = TPR * TY;
+  static constexpr int NS = sizeof(T) == 4 ? 5 : 4;    // pipeline stages
+  static constexpr int MINB = sizeof(T) == 4 ? 3 : 4;  // resident blocks per SM
   static constexpr int HX = 16 / (int)sizeof(T);
   static constexpr int PW = TX + 2 * HX;           // phi / sx tile width
   static constexpr int CW = TX / 2 + 2 * HX;       // coarse tile width
@@ -112,51 +119,63 @@ __device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap *map, i
 
 template <class T> __device__ __forceinline__ float sld(const T *p) { return St<T>::to(*p); }
 
-// Four consecutive values from shared memory (16-byte float32 / 8-byte 16-bit load; every
-// call site is aligned to four elements).
-template <class T> struct V4;
-template <> struct V4<float> {
-  static __device__ __forceinline__ void get(const float *p, float (&v)[4]) {
-    float4 a = *reinterpret_cast<const float4 *>(p);
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-  }
-};
-template <> struct V4<__nv_bfloat16> {
-  static __device__ __forceinline__ void get(const __nv_bfloat16 *p, float (&v)[4]) {
-    uint2 u = *reinterpret_cast<const uint2 *>(p);
-    float2 a = __bfloat1622float2(*reinterpret_cast<__nv_bfloat162 *>(&u.x));
-    float2 b = __bfloat1622float2(*reinterpret_cast<__nv_bfloat162 *>(&u.y));
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-  }
-};
-template <> struct V4<__half> {
-  static __device__ __forceinline__ void get(const __half *p, float (&v)[4]) {
-    uint2 u = *reinterpret_cast<const uint2 *>(p);
-    float2 a = __half22float2(*reinterpret_cast<__half2 *>(&u.x));
-    float2 b = __half22float2(*reinterpret_cast<__half2 *>(&u.y));
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-  }
-};
+// Two 16-bit values packed in 32 bits <-> float2.
+template <class T> __device__ __forceinline__ float2 cvt2(unsigned u);
+template <> __device__ __forceinline__ float2 cvt2<__nv_bfloat16>(unsigned u) {
+  return __bfloat1622float2(*reinterpret_cast<__nv_bfloat162 *>(&u));
+}
+template <> __device__ __forceinline__ float2 cvt2<__half>(unsigned u) {
+  return __half22float2(*reinterpret_cast<__half2 *>(&u));
+}
+template <class T> __device__ __forceinline__ unsigned pack2(float x, float y);
+template <> __device__ __forceinline__ unsigned pack2<__nv_bfloat16>(float x, float y) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(x, y);
+  return *reinterpret_cast<unsigned *>(&h);
+}
+template <> __device__ __forceinline__ unsigned pack2<__half>(float x, float y) {
+  // saturating, as St<__half>::from
+  __half2 h = __floats2half2_rn(fminf(fmaxf(x, -65504.f), 65504.f), fminf(fmaxf(y, -65504.f), 65504.f));
+  return *reinterpret_cast<unsigned *>(&h);
+}
 
-template <class T> __device__ __forceinline__ void gst4(T *p, const float (&v)[4]);
-template <> __device__ __forceinline__ void gst4<float>(float *p, const float (&v)[4]) {
-  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+// N consecutive values from shared memory as float (one 16-, 8- or 4-byte load; every call
+// site is aligned to N elements).
+template <class T, int N> __device__ __forceinline__ void vld(const T *p, float (&v)[N]) {
+  if constexpr (sizeof(T) == 4) {
+    if constexpr (N == 4) {
+      const float4 a = *reinterpret_cast<const float4 *>(p);
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    } else {
+      static_assert(N == 2, "float32 vectors are 2 or 4 wide");
+      const float2 a = *reinterpret_cast<const float2 *>(p);
+      v[0] = a.x; v[1] = a.y;
+    }
+  } else if constexpr (N == 8) {
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    const float2 a = cvt2<T>(u.x), b = cvt2<T>(u.y), c = cvt2<T>(u.z), d = cvt2<T>(u.w);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
+  } else {
+    static_assert(N == 4, "16-bit vectors are 4 or 8 wide");
+    const uint2 u = *reinterpret_cast<const uint2 *>(p);
+    const float2 a = cvt2<T>(u.x), b = cvt2<T>(u.y);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
 }
-template <> __device__ __forceinline__ void gst4<__nv_bfloat16>(__nv_bfloat16 *p, const float (&v)[4]) {
-  __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), b = __floats2bfloat162_rn(v[2], v[3]);
-  uint2 u;
-  u.x = *reinterpret_cast<unsigned *>(&a);
-  u.y = *reinterpret_cast<unsigned *>(&b);
-  *reinterpret_cast<uint2 *>(p) = u;
-}
-template <> __device__ __forceinline__ void gst4<__half>(__half *p, const float (&v)[4]) {
-  const float c0 = fminf(fmaxf(v[0], -65504.f), 65504.f), c1 = fminf(fmaxf(v[1], -65504.f), 65504.f);
-  const float c2 = fminf(fmaxf(v[2], -65504.f), 65504.f), c3 = fminf(fmaxf(v[3], -65504.f), 65504.f);
-  __half2 a = __floats2half2_rn(c0, c1), b = __floats2half2_rn(c2, c3);
-  uint2 u;
-  u.x = *reinterpret_cast<unsigned *>(&a);
-  u.y = *reinterpret_cast<unsigned *>(&b);
-  *reinterpret_cast<uint2 *>(p) = u;
+
+// N consecutive values to global memory (16-byte store; 16-byte aligned, see tma_eligible).
+template <class T, int N> __device__ __forceinline__ void vst(T *p, const float (&v)[N]) {
+  if constexpr (sizeof(T) == 4) {
+    static_assert(N == 4, "float32 stores are 4 wide");
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    static_assert(N == 8, "16-bit stores are 8 wide");
+    uint4 u;
+    u.x = pack2<T>(v[0], v[1]);
+    u.y = pack2<T>(v[2], v[3]);
+    u.z = pack2<T>(v[4], v[5]);
+    u.w = pack2<T>(v[6], v[7]);
+    *reinterpret_cast<uint4 *>(p) = u;
+  }
 }
 
 // Issue the loads of plane p (may lie outside [0, Z): the TMA unit zero-fills) into `stage`.
@@ -189,11 +208,10 @@ __device__ __forceinline__ double block_sum(double v) {
 }
 
 template <int KIND, class T, int MODE, int CORR>
-__global__ void __launch_bounds__(Geo<T>::THREADS, sizeof(T) == 4 ? 3 : 2)
-    k_tma(const __grid_constant__ TmaArgs<T> a) {
+__global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __grid_constant__ TmaArgs<T> a) {
   constexpr bool SIG = KIND == HFM_OP_SIGMA7;
   using G = Geo<T, SIG, CORR != 0>;
-  constexpr int TY = G::TY;
+  constexpr int TY = G::TY, V = G::VEC, NS = G::NS;
   extern __shared__ __align__(128) char smem[];
   __shared__ __align__(8) uint64_t bars[NS];
   const int64_t inst = blockIdx.z;
@@ -203,8 +221,9 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, sizeof(T) == 4 ? 3 : 2)
   const int x0 = tx * TX, y0 = ty * TY;
   const int z0 = blockIdx.y * a.zc, z1 = min(Z, z0 + a.zc);
   const int tid = threadIdx.x;
-  const int r = tid >> 4, c = tid & 15;
-  const int gx = x0 + 4 * c, gy = y0 + r;
+  const int r = tid / G::TPR, c = tid % G::TPR;
+  const int gx = x0 + V * c, gy = y0 + r;
+  // X is a multiple of V (16-byte rows), so a thread's vector is wholly inside or outside
   const bool valid = gx < X && gy < Y;
   const int b = (int)inst;
 
@@ -239,6 +258,7 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, sizeof(T) == 4 ? 3 : 2)
 
   const float s = a.op.scale;
   const float cz = a.op.c[0] * s, cy = a.op.c[1] * s, cx = a.op.c[2] * s;
+  const float hz = cz * 0.5f, hy = cy * 0.5f, hx = cx * 0.5f;
   const float kz = a.op.k[0], ky = a.op.k[1], kx = a.op.k[2];
   const float dconst = 2.f * (kz + ky + kx);
 
@@ -255,29 +275,41 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, sizeof(T) == 4 ? 3 : 2)
     if (a.zero_xend && x0 - G::HX + rx == X - 1) v = 0.f;
     return v;
   };
-  auto phi4 = [&](const char *st, int ry, float (&v)[4]) {
-    const int rx = G::HX + 4 * c;
-    if (!a.has_phi && !CORR) {
-      v[0] = v[1] = v[2] = v[3] = 0.f;
-    } else if (!CORR && !a.zero_xend) {
-      V4<T>::get(reinterpret_cast<const T *>(st + G::O_PHI) + ry * G::PW + rx, v);
+  // the thread's V values of phi' on tile row ry
+  auto phiV = [&](const char *st, int ry, float (&v)[V]) {
+    const int rx = G::HX + V * c;
+    if (a.has_phi) {
+      vld<T, V>(reinterpret_cast<const T *>(st + G::O_PHI) + ry * G::PW + rx, v);
     } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e) v[e] = phiv(st, ry, rx + e);
+      for (int e = 0; e < V; ++e) v[e] = 0.f;
     }
+    if (CORR) {
+      // coarse cells of x pairs: tile column (gx >> 1) - ((x0 >> 1) - HX) = V/2 c + HX
+      const int cyy = ((y0 - 1 + ry) >> 1) - ((y0 >> 1) - 1);
+      float cv[V / 2];
+      vld<T, V / 2>(reinterpret_cast<const T *>(st + G::O_CC) + cyy * G::CW + (V / 2) * c + G::HX, cv);
+#pragma unroll
+      for (int e = 0; e < V; ++e) v[e] += a.corr_sign * cv[e >> 1];
+    }
+    if (a.zero_xend && gx + V == X) v[V - 1] = 0.f;
   };
 
   // z-face coefficient below plane z0 (SIGMA7)
-  float azlo[4] = {0.f, 0.f, 0.f, 0.f};
-  if (KIND == HFM_OP_SIGMA7 && ok) {
-    float szc[4], szm[4];
-    V4<T>::get(reinterpret_cast<const T *>(stage_of(z0) + G::O_SZ) + r * TX + 4 * c, szc);
-    V4<T>::get(reinterpret_cast<const T *>(stage_of(z0 - 1) + G::O_SZ) + r * TX + 4 * c, szm);
+  float azlo[V];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) azlo[e] = z0 > 0 ? cz * 0.5f * (szc[e] + szm[e]) : cz * szc[e];
+  for (int e = 0; e < V; ++e) azlo[e] = 0.f;
+  if (KIND == HFM_OP_SIGMA7 && ok) {
+    float szc[V], szm[V];
+    vld<T, V>(reinterpret_cast<const T *>(stage_of(z0) + G::O_SZ) + r * TX + V * c, szc);
+    vld<T, V>(reinterpret_cast<const T *>(stage_of(z0 - 1) + G::O_SZ) + r * TX + V * c, szm);
+#pragma unroll
+    for (int e = 0; e < V; ++e) azlo[e] = z0 > 0 ? hz * (szc[e] + szm[e]) : cz * szc[e];
   }
   double acc = 0.0;
-  float cpart[2] = {0.f, 0.f};
+  float cpart[V / 2];
+#pragma unroll
+  for (int e = 0; e < V / 2; ++e) cpart[e] = 0.f;
 
   for (int z = z0; z < z1 && ok; ++z) {
     const bool w = wait_plane(z + 1);
@@ -288,114 +320,143 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, sizeof(T) == 4 ? 3 : 2)
     const char *sm_ = stage_of(z - 1);
     const char *sc = stage_of(z);
     const char *sp = stage_of(z + 1);
-    float res[4];
-    float Ax[4], dg[4];
-    float pc[4];
-    phi4(sc, r + 1, pc);
+    float res[V];
+    float Ax[V], dg[V];
+    float pc[V];
+    phiV(sc, r + 1, pc);
     if (KIND == HFM_OP_K27) {
       const float *K = a.op.k;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) Ax[e] = 0.f;
+      for (int e = 0; e < V; ++e) Ax[e] = 0.f;
       const char *pl3[3] = {sm_, sc, sp};
 #pragma unroll
       for (int aa = 0; aa < 3; ++aa) {
 #pragma unroll
         for (int bb = 0; bb < 3; ++bb) {
-          float row[6];
-          row[0] = phiv(pl3[aa], r + bb, G::HX + 4 * c - 1);
-          float m4[4];
-          phi4(pl3[aa], r + bb, m4);
-          row[1] = m4[0]; row[2] = m4[1]; row[3] = m4[2]; row[4] = m4[3];
-          row[5] = phiv(pl3[aa], r + bb, G::HX + 4 * c + 4);
+          float row[V + 2], mid[V];
+          row[0] = phiv(pl3[aa], r + bb, G::HX + V * c - 1);
+          phiV(pl3[aa], r + bb, mid);
+#pragma unroll
+          for (int e = 0; e < V; ++e) row[e + 1] = mid[e];
+          row[V + 1] = phiv(pl3[aa], r + bb, G::HX + V * c + V);
           const float k0 = K[9 * aa + 3 * bb], k1 = K[9 * aa + 3 * bb + 1], k2 = K[9 * aa + 3 * bb + 2];
 #pragma unroll
-          for (int e = 0; e < 4; ++e) Ax[e] += k0 * row[e] + k1 * row[e + 1] + k2 * row[e + 2];
+          for (int e = 0; e < V; ++e) Ax[e] += k0 * row[e] + k1 * row[e + 1] + k2 * row[e + 2];
         }
       }
 #pragma unroll
-      for (int e = 0; e < 4; ++e) dg[e] = K[13];
+      for (int e = 0; e < V; ++e) dg[e] = K[13];
     } else {
-      float pym[4], pyp[4], pzm[4], pzp[4];
-      phi4(sc, r, pym);
-      phi4(sc, r + 2, pyp);
-      phi4(sm_, r + 1, pzm);
-      phi4(sp, r + 1, pzp);
-      const float pl = phiv(sc, r + 1, G::HX + 4 * c - 1);
-      const float pr = phiv(sc, r + 1, G::HX + 4 * c + 4);
+      float pym[V], pyp[V], pzm[V], pzp[V];
+      phiV(sc, r, pym);
+      phiV(sc, r + 2, pyp);
+      phiV(sm_, r + 1, pzm);
+      phiV(sp, r + 1, pzp);
+      const float pl = phiv(sc, r + 1, G::HX + V * c - 1);
+      const float pr = phiv(sc, r + 1, G::HX + V * c + V);
       if (KIND == HFM_OP_CONST7) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
+        for (int e = 0; e < V; ++e) {
           const float xm = e == 0 ? pl : pc[e - 1];
-          const float xp = e == 3 ? pr : pc[e + 1];
+          const float xp = e == V - 1 ? pr : pc[e + 1];
           Ax[e] = dconst * pc[e] - kz * (pzm[e] + pzp[e]) - ky * (pym[e] + pyp[e]) - kx * (xm + xp);
           dg[e] = dconst;
         }
       } else {
-        const T *SX = reinterpret_cast<const T *>(sc + G::O_SX) + r * G::PW + G::HX + 4 * c;
-        const T *SY = reinterpret_cast<const T *>(sc + G::O_SY) + (r + 1) * TX + 4 * c;
-        float sxc[4], syc[4], sym[4], syp[4], szc[4], szp[4];
-        V4<T>::get(SX, sxc);
-        V4<T>::get(SY, syc);
-        V4<T>::get(SY - TX, sym);
-        V4<T>::get(SY + TX, syp);
-        V4<T>::get(reinterpret_cast<const T *>(sc + G::O_SZ) + r * TX + 4 * c, szc);
-        V4<T>::get(reinterpret_cast<const T *>(sp + G::O_SZ) + r * TX + 4 * c, szp);
-        const float sxl = gx > 0 ? sld<T>(SX - 1) : sxc[0];
-        const float sxr = gx + 4 < X ? sld<T>(SX + 4) : sxc[3];
+        const T *SX = reinterpret_cast<const T *>(sc + G::O_SX) + r * G::PW + G::HX + V * c;
+        const T *SY = reinterpret_cast<const T *>(sc + G::O_SY) + (r + 1) * TX + V * c;
+        const T *SZ = reinterpret_cast<const T *>(sc + G::O_SZ) + r * TX + V * c;
+        // at a wall the ghost conductivity is the cell's own: read the cell's row instead,
+        // (s + s) / 2 = s exactly
         const bool ylo = gy > 0, yhi = gy + 1 < Y, zhi = z + 1 < Z;
+        float sxc[V], syc[V], sym[V], syp[V], szc[V], szp[V];
+        vld<T, V>(SX, sxc);
+        vld<T, V>(SY, syc);
+        vld<T, V>(ylo ? SY - TX : SY, sym);
+        vld<T, V>(yhi ? SY + TX : SY, syp);
+        vld<T, V>(SZ, szc);
+        vld<T, V>(zhi ? reinterpret_cast<const T *>(sp + G::O_SZ) + r * TX + V * c : SZ, szp);
+        // the V + 1 x faces of the thread's cells (wall faces: c_x sigma of the cell)
+        float ax[V + 1];
+        ax[0] = gx > 0 ? hx * (sxc[0] + sld<T>(SX - 1)) : cx * sxc[0];
+        ax[V] = gx + V < X ? hx * (sxc[V - 1] + sld<T>(SX + V)) : cx * sxc[V - 1];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const float sxm = e == 0 ? sxl : sxc[e - 1];
-          const float sxp = e == 3 ? sxr : sxc[e + 1];
-          const float axm = cx * 0.5f * (sxc[e] + sxm);
-          const float axp = cx * 0.5f * (sxc[e] + sxp);
-          const float aym = cy * 0.5f * (syc[e] + (ylo ? sym[e] : syc[e]));
-          const float ayp = cy * 0.5f * (syc[e] + (yhi ? syp[e] : syc[e]));
-          const float azhi = cz * 0.5f * (szc[e] + (zhi ? szp[e] : szc[e]));
-          const float xm = e == 0 ? pl : pc[e - 1];
-          const float xp = e == 3 ? pr : pc[e + 1];
-          const float p = pc[e];
-          Ax[e] = axm * (p - xm) + axp * (p - xp) + aym * (p - pym[e]) + ayp * (p - pyp[e]) +
-                  azlo[e] * (p - pzm[e]) + azhi * (p - pzp[e]);
-          dg[e] = axm + axp + aym + ayp + azlo[e] + azhi;
-          azlo[e] = azhi;
+        for (int e = 1; e < V; ++e) ax[e] = hx * (sxc[e] + sxc[e - 1]);
+        // cells in pairs on the packed float32 pipe (fma / add / mul .f32x2); p - q is
+        // formed as fma(q, -1, p), which is exact up to the one rounding of the subtraction
+        const float2 m1 = make_float2(-1.f, -1.f), hy2 = make_float2(hy, hy), hz2 = make_float2(hz, hz);
+#pragma unroll
+        for (int e = 0; e < V; e += 2) {
+          const float2 p = make_float2(pc[e], pc[e + 1]);
+          const float2 aym = __fmul2_rn(hy2, __fadd2_rn(make_float2(syc[e], syc[e + 1]), make_float2(sym[e], sym[e + 1])));
+          const float2 ayp = __fmul2_rn(hy2, __fadd2_rn(make_float2(syc[e], syc[e + 1]), make_float2(syp[e], syp[e + 1])));
+          const float2 azh = __fmul2_rn(hz2, __fadd2_rn(make_float2(szc[e], szc[e + 1]), make_float2(szp[e], szp[e + 1])));
+          const float2 azl = make_float2(azlo[e], azlo[e + 1]);
+          const float2 axm = make_float2(ax[e], ax[e + 1]), axp = make_float2(ax[e + 1], ax[e + 2]);
+          const float2 xm = make_float2(e == 0 ? pl : pc[e - 1], pc[e]);
+          const float2 xp = make_float2(pc[e + 1], e + 2 == V ? pr : pc[e + 2]);
+          float2 A = __fmul2_rn(axm, __ffma2_rn(xm, m1, p));
+          A = __ffma2_rn(axp, __ffma2_rn(xp, m1, p), A);
+          A = __ffma2_rn(aym, __ffma2_rn(make_float2(pym[e], pym[e + 1]), m1, p), A);
+          A = __ffma2_rn(ayp, __ffma2_rn(make_float2(pyp[e], pyp[e + 1]), m1, p), A);
+          A = __ffma2_rn(azl, __ffma2_rn(make_float2(pzm[e], pzm[e + 1]), m1, p), A);
+          A = __ffma2_rn(azh, __ffma2_rn(make_float2(pzp[e], pzp[e + 1]), m1, p), A);
+          const float2 d = __fadd2_rn(__fadd2_rn(__fadd2_rn(axm, axp), __fadd2_rn(aym, ayp)),
+                                      __fadd2_rn(azl, azh));
+          Ax[e] = A.x; Ax[e + 1] = A.y;
+          dg[e] = d.x; dg[e + 1] = d.y;
+          azlo[e] = azh.x; azlo[e + 1] = azh.y;
         }
       }
     }
-    float f[4] = {0.f, 0.f, 0.f, 0.f};
-    if (a.has_f) V4<T>::get(reinterpret_cast<const T *>(sc + G::O_F) + r * TX + 4 * c, f);
-    if (MODE == M_SMOOTH) {
-#pragma unroll
-      for (int e = 0; e < 4; ++e) res[e] = pc[e] + a.omega * __fdividef(f[e] - Ax[e], dg[e]);
+    float f[V];
+    if (a.has_f) {
+      vld<T, V>(reinterpret_cast<const T *>(sc + G::O_F) + r * TX + V * c, f);
     } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e) res[e] = Ax[e] - f[e];
-      if (a.zero_xend_out && gx + 4 == X) res[3] = 0.f;
+      for (int e = 0; e < V; ++e) f[e] = 0.f;
+    }
+    if (MODE == M_SMOOTH) {
+      const float2 om = make_float2(a.omega, a.omega), m1 = make_float2(-1.f, -1.f);
+#pragma unroll
+      for (int e = 0; e < V; e += 2) {
+        const float2 num = __ffma2_rn(make_float2(Ax[e], Ax[e + 1]), m1, make_float2(f[e], f[e + 1]));
+        const float2 rd = make_float2(__fdividef(1.f, dg[e]), __fdividef(1.f, dg[e + 1]));
+        const float2 v = __ffma2_rn(om, __fmul2_rn(num, rd), make_float2(pc[e], pc[e + 1]));
+        res[e] = v.x;
+        res[e + 1] = v.y;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < V; ++e) res[e] = Ax[e] - f[e];
+      if (a.zero_xend_out && gx + V == X) res[V - 1] = 0.f;
       if (valid) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc += (double)res[e] * res[e];
+        for (int e = 0; e < V; ++e) acc += (double)res[e] * res[e];
       }
     }
     const int64_t off = inst * a.stride + ((int64_t)z * Y + gy) * X + gx;
     if (valid && a.out) {
-      if (MODE == M_SMOOTH && a.top_copy && z == 1) gst4<T>(a.out + inst * a.stride + (int64_t)gy * X + gx, res);
-      if (!(MODE == M_SMOOTH && a.top_copy && z == 0 && Z > 1)) gst4<T>(a.out + off, res);
+      if (MODE == M_SMOOTH && a.top_copy && z == 1) vst<T, V>(a.out + inst * a.stride + (int64_t)gy * X + gx, res);
+      if (!(MODE == M_SMOOTH && a.top_copy && z == 0 && Z > 1)) vst<T, V>(a.out + off, res);
     }
     if (MODE == M_RESTRICT) {
-      // x pairs in the vector, y pairs with the lane 16 above (row r + 1), z pairs over planes
-      float p0 = res[0] + res[1], p1 = res[2] + res[3];
-      p0 += __shfl_down_sync(0xffffffffu, p0, 16);
-      p1 += __shfl_down_sync(0xffffffffu, p1, 16);
-      cpart[0] += 0.125f * p0;
-      cpart[1] += 0.125f * p1;
+      // x pairs in the vector, y pairs with the lane TPR above (row r + 1), z pairs over planes
+#pragma unroll
+      for (int k = 0; k < V / 2; ++k) {
+        float pk = res[2 * k] + res[2 * k + 1];
+        pk += __shfl_down_sync(0xffffffffu, pk, G::TPR);
+        cpart[k] += 0.125f * pk;
+      }
       if (z & 1) {
         if (valid && !(r & 1)) {
           T *cp = a.coarse + inst * a.coarse_stride +
                   ((int64_t)(z >> 1) * (Y >> 1) + (gy >> 1)) * (X >> 1) + (gx >> 1);
-          cp[0] = St<T>::from(cpart[0]);
-          cp[1] = St<T>::from(cpart[1]);
+#pragma unroll
+          for (int k = 0; k < V / 2; ++k) cp[k] = St<T>::from(cpart[k]);
         }
-        cpart[0] = cpart[1] = 0.f;
+#pragma unroll
+        for (int k = 0; k < V / 2; ++k) cpart[k] = 0.f;
       }
     }
     __syncthreads();  // every thread is done with plane z-1's stage
@@ -466,7 +527,7 @@ int go(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
   using G = Geo<T, KIND == HFM_OP_SIGMA7, CORR != 0>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
-  const int smem = NS * G::STAGE;
+  const int smem = G::NS * G::STAGE;
   std::call_once(once, [&] {
     attr_err = cudaFuncSetAttribute(k_tma<KIND, T, MODE, CORR>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
