@@ -311,12 +311,23 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
 #pragma unroll
   for (int e = 0; e < V / 2; ++e) cpart[e] = 0.f;
 
+  bool mine = true;  // this thread's latest plane wait completed
   for (int z = z0; z < z1 && ok; ++z) {
-    const bool w = wait_plane(z + 1);
-    if (__syncthreads_or(!w)) {
+    // One barrier per plane.  It certifies that every thread is done with plane z-2, whose
+    // stage thread 0 then refills before anyone waits for plane z+1 (so two planes stay in
+    // flight), and it publishes the outcome of the previous waits: a thread whose wait ran
+    // out computed one plane from an incomplete stage, and the whole block stops here.
+    if (__syncthreads_or(!mine)) {
       ok = false;
       break;
     }
+    if (tid == 0 && z > z0 && p_next <= p_last) {
+      const int q = p_next - p_first;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue_plane<T, CORR, SIG>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
+      ++p_next;
+    }
+    mine = wait_plane(z + 1);
     const char *sm_ = stage_of(z - 1);
     const char *sc = stage_of(z);
     const char *sp = stage_of(z + 1);
@@ -459,14 +470,8 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
         for (int k = 0; k < V / 2; ++k) cpart[k] = 0.f;
       }
     }
-    __syncthreads();  // every thread is done with plane z-1's stage
-    if (tid == 0 && p_next <= p_last) {
-      const int q = p_next - p_first;
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_plane<T, CORR, SIG>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
-      ++p_next;
-    }
   }
+  if (ok && __syncthreads_or(!mine)) ok = false;  // the last plane's wait
   if (!ok) {
     if (tid == 0) atomicAdd(&g_tma_timeouts, 1);
     // drain: wait (bounded) for the planes whose loads are still in flight, so that no
