@@ -125,6 +125,7 @@ class _Bucket:
         self.event = torch.cuda.Event()
         self.inflight = False
         self.launched = ()
+        self.copies = []  # solutions on their way to host memory: (event, result, host, dev)
 
     def ready(self):
         return not self.inflight or self.event.query()
@@ -152,7 +153,11 @@ class _Bucket:
         self.launched = tuple(self.busy.keys())
 
     def harvest(self, clock, t0, host_out):
-        """Retire the slots of the completed launch that have finished (call when ready())."""
+        """Retire the slots of the completed launch that have finished (call when ready()).
+        With ``host_out`` a finished solution is copied into pinned host memory
+        asynchronously on the bucket's stream; its result is reported by ``poll_copies``
+        once that copy has completed, and the slot is free for the next request at once
+        (later work on the slot is ordered after the copy by the stream)."""
         if not self.inflight:
             return []
         self.inflight = False
@@ -164,17 +169,37 @@ class _Bucket:
             if s["active"]:
                 continue
             req, adm, _ = self.busy.pop(slot)
+            self.free.append(slot)
             phi = None
             if self.keep or host_out:
                 with torch.cuda.stream(self.stream):
                     phi = self.mg.fetch_f64(slot) if self.mg.cfg.accel == "ir" else self.mg.fetch(slot)
                     if host_out:
-                        phi = phi.to("cpu")
-                        now = clock() - t0
+                        host = torch.empty(phi.shape, dtype=phi.dtype, pin_memory=True)
+                        host.copy_(phi, non_blocking=True)
+                        ev = torch.cuda.Event()
+                        ev.record(self.stream)
+                        res = SolveResult(req.rid, req.n, s["status"], s["cycles"], s["outer"],
+                                          s["rel_resid"], adm, 0.0, 0.0, host)
+                        self.copies.append((ev, res, host, phi, req))
+                        continue
             done.append(SolveResult(req.rid, req.n, s["status"], s["cycles"], s["outer"],
                                     s["rel_resid"], adm, now, now - req.arrival, phi))
-            self.free.append(slot)
         return done
+
+    def poll_copies(self, clock, t0):
+        """Results whose solution has arrived in host memory (non-blocking)."""
+        out, keep = [], []
+        for item in self.copies:
+            ev, res, _, _, req = item
+            if ev.query():
+                now = clock() - t0
+                res.done, res.latency = now, now - req.arrival
+                out.append(res)
+            else:
+                keep.append(item)
+        self.copies = keep
+        return out
 
 
 class SolveServer:
@@ -218,6 +243,9 @@ class SolveServer:
                 queued[r.n].append(r)
             idle = True
             for b in buckets:
+                if b.copies:
+                    results.extend(b.poll_copies(clock, t0))
+                    idle = False
                 if not b.ready():
                     idle = False
                     continue

@@ -56,6 +56,20 @@ def parse():
     return p.parse_args()
 
 
+def stream_seed(rank):
+    """Seed of a replica's request stream: every rank serves its own stream."""
+    return 1 + 7919 * rank
+
+
+def max_over_ranks(torch, ms, device):
+    """Whole-job time of a step: the slowest rank's device-timed milliseconds."""
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return ms
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -153,8 +167,12 @@ def smoother_roofline(pkg, torch, dtype, slots, n, reps=20):
     peak, src = peak_hbm()
     achieved = bytes_alg / (ms / 1e3) / 1e9
     del x, b, y, s
+    # DRAM bytes of one launch of this kernel on this shape, read + write, from the ncu
+    # capture summarised in profiles/k_tma_smooth_sigma7_bf16.md (bf16, 64 x 128^3)
+    traffic = 1.364133e9 + 0.257936e9 if (dtype, slots, n) == ("bf16", 64, 128) else None
     return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": None,
+            "frac": round(achieved / peak, 4), "traffic": traffic,
+            "traffic_note": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
             "kernel": "k_tma<SIGMA7,%s,SMOOTH> fine-level weighted Jacobi (%d x %d^3)" % (dtype, slots, n),
             "bytes_per_launch": bytes_alg, "ms_per_launch": round(ms, 4), "peak_source": src}
 
@@ -221,7 +239,7 @@ def run_reference(args):
 def run_serve(args, pkg, torch, rank, world, local):
     sv, M, L = pkg.serving, pkg.multigrid, pkg._lib
     dev = torch.device("cuda", local)
-    reqs = sv.make_stream(count=args.requests, rate=args.rate, seed=1 + 7919 * rank, device=dev)
+    reqs = sv.make_stream(count=args.requests, rate=args.rate, seed=stream_seed(rank), device=dev)
     cfg = M.SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6, max_cycles=600)
     server = sv.SolveServer(cfg=cfg, slots=64, budget_bytes=120e9, cycles_per_tick=4)
 
@@ -239,17 +257,16 @@ def run_serve(args, pkg, torch, rank, world, local):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     all_res = []
+    torch.cuda.nvtx.range_push("served")  # lets a profiler select the timed region
     for _ in range(args.steps):
         all_res.extend(server.serve(reqs, realtime=True))
+    torch.cuda.nvtx.range_pop()
     e1.record()
     barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
     launches = (L.lib().hfm_kernel_launch_count() - l0) // max(args.steps, 1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(torch, ms, dev)
     bad = [r for r in all_res if r.status != 0]
     lat = sv.latency_stats(all_res)
     value = len(reqs) * world / (ms / 1e3)
@@ -345,7 +362,7 @@ def run_batch64(args, pkg, torch, rank, world, local):
         step()
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(torch, e0.elapsed_time(e1) / args.steps, dev)
     h.close()
     return {"metric": "MG solves/s @1e-6 (64 x 64^3, log-std 1, PCG-V(2,2), float32)",
             "value": round(batch * world / (ms / 1e3), 3), "unit": "solves/s", "n_gpus": world,
