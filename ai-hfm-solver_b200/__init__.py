@@ -15,7 +15,7 @@ __all__ = ["_lib", "weights", "problems", "ops", "multigrid"]
 
 def __getattr__(name):
     # ops / multigrid import torch; keep the package importable for the build step.
-    if name in ("ops", "multigrid", "serving", "precision", "tomography", "ns"):
+    if name in ("ops", "multigrid", "serving", "precision", "tomography", "ns", "kolmogorov"):
         import importlib
         return importlib.import_module("." + name, __name__)
     raise AttributeError(name)

@@ -16,7 +16,7 @@ F32, BF16, F16, F64 = range(4)
 # hfm_op_kind
 OP_CONST7, OP_SIGMA7, OP_DIR7, OP_K27 = range(4)
 # flags
-FLAG_ZERO_XEND, FLAG_TOP_COPY, FLAG_ZERO_GUESS = 1, 2, 4
+FLAG_ZERO_XEND, FLAG_TOP_COPY, FLAG_ZERO_GUESS, FLAG_PERIODIC, FLAG_SAME_LEVEL_CORR = 1, 2, 4, 8, 16
 # hfm_cycle / hfm_accel
 CYCLE_SAWTOOTH, CYCLE_V, CYCLE_F = range(3)
 ACCEL_NONE, ACCEL_CG, ACCEL_IR = range(3)
@@ -97,6 +97,20 @@ SIGNATURES = {
     "hfm_ns_bc_velocity": (I, [P, P, P, I, I, I, F, P, P]),
     "hfm_ns_bc_pressure": (I, [P, I, I, I, P, P]),
     "hfm_sigma7_grad_logsigma": (I, [P, P, P, P, P, I, I, I, I, F, F, F, P, P, P, I, P]),
+    # 2D operators and the Kolmogorov-flow stepper
+    "hfm_conv2d_k3": (I, [P, P, I, I, I, P, U, P]),
+    "hfm_restrict_avg2d": (I, [I, P, P, I, I, I, P]),
+    "hfm_prolong_nearest2d": (I, [I, P, P, I, I, I, P]),
+    "hfm_jacobi2d": (I, [I, P, P, P, F, P, P, I, I, I, F, U, P]),
+    "hfm_residual2d": (I, [I, P, P, P, P, I, I, I, U, P]),
+    "hfm_residual_restrict2d": (I, [I, P, P, P, P, I, I, I, U, P]),
+    "hfm_outer_residual2d": (I, [P, P, P, I, P, I, I, I, U, P, P, P]),
+    "hfm_update2d": (I, [P, I, P, F, I64, P]),
+    "hfm_coarse_jacobi2d": (I, [I, P, P, P, I, I, I, F, I, U, P]),
+    "hfm_mean_subtract2d": (I, [P, I, I64, P]),
+    "hfm_kolmogorov_stage": (I, [P, P, P, P, P, P, I, I, F, F, F, F, F, F, P]),
+    "hfm_kolmogorov_divergence": (I, [P, P, P, I, I, F, F, P]),
+    "hfm_kolmogorov_project": (I, [P, P, P, I, I, F, F, P]),
     "hfm_mg_config_default": (None, [C.POINTER(HfmMgConfig)]),
     "hfm_mg_footprint_bytes": (C.c_size_t, [C.POINTER(HfmMgConfig), I, I, I, I]),
     "hfm_mg_create": (I, [C.POINTER(HfmMgConfig), I, I, I, I, C.POINTER(P)]),

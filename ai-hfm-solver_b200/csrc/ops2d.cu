@@ -1,0 +1,518 @@
+// Two-dimensional operators: the reference's Conv2D form of the multigrid
+// (Unstructured Mesh/Multigrid_2D.ipynb: 3x3 SAME convolution #c7, 2x2 VALID averaging
+// restriction with weight 0.25 #c9, UpSampling2D #c11, sawtooth cycle #c18) with zero or
+// periodic padding, in float32 or bf16 storage with float32 arithmetic, and the kernels of the
+// doubly periodic Kolmogorov-flow stepper (two-stage momentum with sin(k y) forcing,
+// divergence, pressure-gradient projection).
+//
+// Layout: (B, Y, X) float32 / bf16, x fastest.  The fields of this path are small (512^2 cells,
+// 1 MB per float32 field) and stay in L2 across the kernels of a step, so these kernels map one
+// thread to one output cell and are launched from captured CUDA graphs.
+#include "hfm_internal.cuh"
+
+namespace hfm {
+
+namespace {
+
+constexpr int kT2 = 256;
+
+struct W9 {
+  float w[9];  // w[3a + b]: weight of phi[y + a - 1][x + b - 1]
+};
+
+// phi' = base + sign * coarse[y/2][x/2] at (y, x) of instance b, or 0 outside a zero-padded grid
+template <class T> struct Src2 {
+  const T *base;
+  const T *coarse;
+  float sign;
+  int64_t stride, cstride;
+  int Y, X, Xc;
+  int periodic;
+  int cshift;  // 1: coarse is the next coarser level (nearest upsampling); 0: same level
+  __device__ __forceinline__ float operator()(int64_t b, int y, int x) const {
+    if (periodic) {
+      y = y < 0 ? y + Y : (y >= Y ? y - Y : y);
+      x = x < 0 ? x + X : (x >= X ? x - X : x);
+    } else if (y < 0 || y >= Y || x < 0 || x >= X) {
+      return 0.f;
+    }
+    float v = base ? St<T>::ld(base + b * stride + (int64_t)y * X + x) : 0.f;
+    if (coarse) v += sign * St<T>::ld(coarse + b * cstride + (int64_t)(y >> cshift) * Xc + (x >> cshift));
+    return v;
+  }
+};
+
+template <class T>
+__device__ __forceinline__ float conv9(const W9 &w, const Src2<T> &s, int64_t b, int y, int x,
+                                       float *centre) {
+  float acc = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float v = s(b, y + a - 1, x + c - 1);
+      if (a == 1 && c == 1) *centre = v;
+      acc += w.w[3 * a + c] * v;
+    }
+  return acc;
+}
+
+// MODE 0: out = A phi; 1: out = A phi - f; 2: out = phi + omega (f - A phi) / w[4]
+template <class T, int MODE>
+__global__ void __launch_bounds__(kT2) k2_stencil(W9 w, Src2<T> s, const T *__restrict__ f,
+                                                  T *__restrict__ out, float omega) {
+  const int64_t b = blockIdx.y;
+  const int64_t n = (int64_t)s.Y * s.X;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / s.X), x = (int)(i % s.X);
+    float pc;
+    const float ax = conv9<T>(w, s, b, y, x, &pc);
+    const float fv = f ? St<T>::ld(f + b * s.stride + i) : 0.f;
+    float r;
+    if (MODE == 0) r = ax;
+    else if (MODE == 1) r = ax - fv;
+    else r = pc + omega * (fv - ax) / w.w[4];
+    out[b * s.stride + i] = St<T>::from(r);
+  }
+}
+
+// Coarse cell (yc, xc) = 0.25 * sum over its 2x2 fine cells of (A phi - f); float32 phi and f
+// may be read while the coarse output is stored in T (TI = input storage).
+template <class TI, class TO>
+__global__ void __launch_bounds__(kT2) k2_resid_restrict(W9 w, Src2<TI> s, const TI *__restrict__ f,
+                                                         TO *__restrict__ rc, int64_t cstride) {
+  const int64_t b = blockIdx.y;
+  const int Yc = s.Y >> 1, Xc = s.X >> 1;
+  const int64_t nc = (int64_t)Yc * Xc;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nc;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const int yc = (int)(j / Xc), xc = (int)(j % Xc);
+    float sum = 0.f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int y = 2 * yc + a, x = 2 * xc + c;
+        float pc;
+        float v = conv9<TI>(w, s, b, y, x, &pc);
+        if (f) v -= St<TI>::ld(f + b * s.stride + (int64_t)y * s.X + x);
+        sum += v;
+      }
+    rc[b * cstride + j] = St<TO>::from(0.25f * sum);
+  }
+}
+
+// Residual A phi - f of float32 phi / f stored in T (the outer defect of a mixed-precision
+// solve), with per-block partial sums of its square (float64) when `partials` is given.
+template <class TO>
+__global__ void __launch_bounds__(kT2) k2_outer_resid(W9 w, Src2<float> s, const float *__restrict__ f,
+                                                      TO *__restrict__ r, double *partials) {
+  __shared__ double sh[kT2 / 32];
+  const int64_t b = blockIdx.y;
+  const int64_t n = (int64_t)s.Y * s.X;
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / s.X), x = (int)(i % s.X);
+    float pc;
+    const float v = conv9<float>(w, s, b, y, x, &pc) - f[b * s.stride + i];
+    r[b * s.stride + i] = St<TO>::from(v);
+    acc += (double)v * v;
+  }
+  if (!partials) return;
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < kT2 / 32; ++k) t += sh[k];
+    partials[b * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kT2) k2_restrict(const T *__restrict__ fine, T *__restrict__ coarse,
+                                                   int Y, int X) {
+  const int64_t b = blockIdx.y;
+  const int Yc = Y >> 1, Xc = X >> 1;
+  const int64_t nc = (int64_t)Yc * Xc, nf = (int64_t)Y * X;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nc;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const int yc = (int)(j / Xc), xc = (int)(j % Xc);
+    const T *p = fine + b * nf + (int64_t)(2 * yc) * X + 2 * xc;
+    const float s = (St<T>::to(p[0]) + St<T>::to(p[1])) + (St<T>::to(p[X]) + St<T>::to(p[X + 1]));
+    coarse[b * nc + j] = St<T>::from(0.25f * s);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kT2) k2_prolong(const T *__restrict__ coarse, T *__restrict__ fine,
+                                                  int Yc, int Xc) {
+  const int64_t b = blockIdx.y;
+  const int Y = 2 * Yc, X = 2 * Xc;
+  const int64_t nf = (int64_t)Y * X, nc = (int64_t)Yc * Xc;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nf;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / X), x = (int)(i % X);
+    fine[b * nf + i] = coarse[b * nc + (int64_t)(y >> 1) * Xc + (x >> 1)];
+  }
+}
+
+// p += sign * w (float32 p, w in T)
+template <class T>
+__global__ void __launch_bounds__(kT2) k2_update(float *__restrict__ p, const T *__restrict__ w,
+                                                 float sign, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] += sign * St<T>::to(w[i]);
+}
+
+// `sweeps` Jacobi sweeps from phi = 0 on a small grid held in shared memory, one block per
+// instance (the coarsest level of a cycle).
+template <class T>
+__global__ void __launch_bounds__(kT2) k2_coarse_jacobi(W9 w, const T *__restrict__ f, T *__restrict__ out,
+                                                        int Y, int X, float omega, int sweeps,
+                                                        int periodic) {
+  extern __shared__ float sm2[];
+  const int n = Y * X;
+  float *a = sm2, *c = sm2 + n, *ff = sm2 + 2 * n;
+  const int64_t b = blockIdx.x;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    a[i] = 0.f;
+    ff[i] = St<T>::to(f[b * n + i]);
+  }
+  __syncthreads();
+  for (int s = 0; s < sweeps; ++s) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int y = i / X, x = i % X;
+      float acc = 0.f;
+      for (int aa = 0; aa < 3; ++aa)
+        for (int cc = 0; cc < 3; ++cc) {
+          int yy = y + aa - 1, xx = x + cc - 1;
+          float v;
+          if (periodic) {
+            yy = (yy + Y) % Y;
+            xx = (xx + X) % X;
+            v = a[yy * X + xx];
+          } else {
+            v = (yy < 0 || yy >= Y || xx < 0 || xx >= X) ? 0.f : a[yy * X + xx];
+          }
+          acc += w.w[3 * aa + cc] * v;
+        }
+      c[i] = a[i] + omega * (ff[i] - acc) / w.w[4];
+    }
+    __syncthreads();
+    float *t = a;
+    a = c;
+    c = t;
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) out[b * n + i] = St<T>::from(a[i]);
+}
+
+// Subtract each instance's mean (the constant null space of a periodic operator).
+__global__ void __launch_bounds__(1024) k2_mean_subtract(float *p, int64_t n) {
+  __shared__ double sh[32];
+  __shared__ float mean;
+  float *q = p + (int64_t)blockIdx.x * n;
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) acc += q[i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+    mean = (float)(t / (double)n);
+  }
+  __syncthreads();
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) q[i] -= mean;
+}
+
+// ------------------------------------------------------------------ Kolmogorov stepper
+__device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// out = base + c dt (nu L phi - U d/dx phi - V d/dy phi + F) for both velocity components,
+// with (U, V) = (phi_u, phi_v), L the 5-point Laplacian, d/dx the central difference and
+// F = (famp sin(fk y h), 0); doubly periodic grid of spacing h.
+__global__ void __launch_bounds__(kT2) k2_ns_stage(const float *__restrict__ pu, const float *__restrict__ pv,
+                                                   const float *__restrict__ bu, const float *__restrict__ bv,
+                                                   float *__restrict__ ou, float *__restrict__ ov, int Y,
+                                                   int X, float c, float dt, float nu, float h,
+                                                   float famp, float fk) {
+  const int64_t n = (int64_t)Y * X;
+  const float ih = 1.f / h, ih2 = ih * ih, i2h = 0.5f * ih;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / X), x = (int)(i % X);
+    const int64_t l = (int64_t)y * X + wrap(x - 1, X), r = (int64_t)y * X + wrap(x + 1, X);
+    const int64_t d = (int64_t)wrap(y - 1, Y) * X + x, u = (int64_t)wrap(y + 1, Y) * X + x;
+    const float U = pu[i], V = pv[i];
+    const float lap_u = (pu[l] + pu[r] + pu[d] + pu[u] - 4.f * U) * ih2;
+    const float lap_v = (pv[l] + pv[r] + pv[d] + pv[u] - 4.f * V) * ih2;
+    const float ux = (pu[r] - pu[l]) * i2h, uy = (pu[u] - pu[d]) * i2h;
+    const float vx = (pv[r] - pv[l]) * i2h, vy = (pv[u] - pv[d]) * i2h;
+    const float force = famp * sinf(fk * (float)y * h);
+    ou[i] = bu[i] + c * dt * (nu * lap_u - U * ux - V * uy + force);
+    ov[i] = bv[i] + c * dt * (nu * lap_v - U * vx - V * vy);
+  }
+}
+
+// f = -(du/dx + dv/dy) / dt  (right-hand side of -L p = f; central differences)
+__global__ void __launch_bounds__(kT2) k2_ns_divergence(const float *__restrict__ u, const float *__restrict__ v,
+                                                        float *__restrict__ f, int Y, int X, float h,
+                                                        float dt) {
+  const int64_t n = (int64_t)Y * X;
+  const float i2h = 0.5f / h;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / X), x = (int)(i % X);
+    const float div = (u[(int64_t)y * X + wrap(x + 1, X)] - u[(int64_t)y * X + wrap(x - 1, X)]) * i2h +
+                      (v[(int64_t)wrap(y + 1, Y) * X + x] - v[(int64_t)wrap(y - 1, Y) * X + x]) * i2h;
+    f[i] = -div / dt;
+  }
+}
+
+// u -= dt dp/dx, v -= dt dp/dy (central differences)
+__global__ void __launch_bounds__(kT2) k2_ns_project(float *__restrict__ u, float *__restrict__ v,
+                                                     const float *__restrict__ p, int Y, int X, float h,
+                                                     float dt) {
+  const int64_t n = (int64_t)Y * X;
+  const float i2h = 0.5f / h;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / X), x = (int)(i % X);
+    u[i] -= dt * (p[(int64_t)y * X + wrap(x + 1, X)] - p[(int64_t)y * X + wrap(x - 1, X)]) * i2h;
+    v[i] -= dt * (p[(int64_t)wrap(y + 1, Y) * X + x] - p[(int64_t)wrap(y - 1, Y) * X + x]) * i2h;
+  }
+}
+
+int blocks2(int64_t n, int B) {
+  int64_t want = (int64_t)sm_count() * 8 / (B > 0 ? B : 1);
+  if (want < 1) want = 1;
+  int64_t need = (n + kT2 - 1) / kT2;
+  int64_t b = need < want ? need : want;
+  return (int)(b < 1 ? 1 : (b > 65535 ? 65535 : b));
+}
+
+int check2(int B, int Y, int X) {
+  if (B < 1 || Y < 1 || X < 1) return fail(HFM_ERR_BAD_ARG, "2D: extents must be >= 1");
+  if (B > 65535) return fail(HFM_ERR_BAD_ARG, "2D: at most 65535 instances");
+  return HFM_OK;
+}
+
+int check_dtype2(int dtype) {
+  if (dtype != HFM_F32 && dtype != HFM_BF16) return fail(HFM_ERR_BAD_ARG, "2D: dtype must be F32 or BF16");
+  return HFM_OK;
+}
+
+W9 w9_of(const float *w) {
+  W9 k;
+  for (int i = 0; i < 9; ++i) k.w[i] = w[i];
+  return k;
+}
+
+template <class T>
+Src2<T> src2(const void *base, const void *coarse, float sign, int Y, int X, unsigned flags) {
+  Src2<T> s;
+  s.base = (const T *)base;
+  s.coarse = (const T *)coarse;
+  s.sign = sign;
+  s.cshift = (flags & HFM_FLAG_SAME_LEVEL_CORR) ? 0 : 1;
+  s.stride = (int64_t)Y * X;
+  s.cstride = (int64_t)(Y >> s.cshift) * (X >> s.cshift);
+  s.Y = Y;
+  s.X = X;
+  s.Xc = X >> s.cshift;
+  s.periodic = (flags & HFM_FLAG_PERIODIC) ? 1 : 0;
+  return s;
+}
+
+}  // namespace
+}  // namespace hfm
+
+using namespace hfm;
+
+#define HFM2_DT(dtype, ...)                                  \
+  if ((dtype) == HFM_F32) {                                  \
+    using T = float;                                         \
+    __VA_ARGS__;                                             \
+  } else {                                                   \
+    using T = __nv_bfloat16;                                 \
+    __VA_ARGS__;                                             \
+  }
+
+extern "C" {
+
+int hfm_conv2d_k3(const float *x, float *y, int B, int Y, int X, const float *w9_host,
+                  unsigned flags, hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Y, X))) return st;
+  if (!x || !y || !w9_host) return fail(HFM_ERR_BAD_ARG, "hfm_conv2d_k3: NULL argument");
+  if (x == y) return fail(HFM_ERR_BAD_ARG, "hfm_conv2d_k3: in-place call");
+  const int64_t n = (int64_t)Y * X;
+  k2_stencil<float, 0><<<dim3(blocks2(n, B), B), kT2, 0, (cudaStream_t)stream>>>(
+      w9_of(w9_host), src2<float>(x, nullptr, 0.f, Y, X, flags), nullptr, y, 0.f);
+  HFM_CHECK_LAUNCH("k2_stencil");
+  return HFM_OK;
+}
+
+int hfm_restrict_avg2d(int dtype, const void *fine, void *coarse, int B, int Y, int X,
+                       hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Y, X)) || (st = check_dtype2(dtype))) return st;
+  if (!fine || !coarse) return fail(HFM_ERR_BAD_ARG, "hfm_restrict_avg2d: NULL argument");
+  if (Y < 2 || X < 2) return fail(HFM_ERR_BAD_ARG, "hfm_restrict_avg2d: extents must be >= 2");
+  const int64_t nc = (int64_t)(Y / 2) * (X / 2);
+  HFM2_DT(dtype, (k2_restrict<T><<<dim3(blocks2(nc, B), B), kT2, 0, (cudaStream_t)stream>>>(
+                     (const T *)fine, (T *)coarse, Y, X)));
+  HFM_CHECK_LAUNCH("k2_restrict");
+  return HFM_OK;
+}
+
+int hfm_prolong_nearest2d(int dtype, const void *coarse, void *fine, int B, int Yc, int Xc,
+                          hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Yc, Xc)) || (st = check_dtype2(dtype))) return st;
+  if (!fine || !coarse) return fail(HFM_ERR_BAD_ARG, "hfm_prolong_nearest2d: NULL argument");
+  const int64_t nf = (int64_t)4 * Yc * Xc;
+  HFM2_DT(dtype, (k2_prolong<T><<<dim3(blocks2(nf, B), B), kT2, 0, (cudaStream_t)stream>>>(
+                     (const T *)coarse, (T *)fine, Yc, Xc)));
+  HFM_CHECK_LAUNCH("k2_prolong");
+  return HFM_OK;
+}
+
+int hfm_jacobi2d(int dtype, const float *w9_host, const void *base, const void *coarse,
+                 float coarse_sign, const void *rhs, void *out, int B, int Y, int X, float omega,
+                 unsigned flags, hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Y, X)) || (st = check_dtype2(dtype))) return st;
+  if (!w9_host || !out) return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: NULL argument");
+  if (w9_host[4] == 0.f) return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: zero diagonal weight");
+  if ((base && base == out) || (coarse && coarse == out))
+    return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: out aliases an input");
+  if (coarse && !(flags & HFM_FLAG_SAME_LEVEL_CORR) && ((Y | X) & 1))
+    return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: coarse correction needs even extents");
+  const int64_t n = (int64_t)Y * X;
+  HFM2_DT(dtype, (k2_stencil<T, 2><<<dim3(blocks2(n, B), B), kT2, 0, (cudaStream_t)stream>>>(
+                     w9_of(w9_host), src2<T>(base, coarse, coarse_sign, Y, X, flags),
+                     (const T *)rhs, (T *)out, omega)));
+  HFM_CHECK_LAUNCH("k2_stencil");
+  return HFM_OK;
+}
+
+int hfm_residual2d(int dtype, const float *w9_host, const void *phi, const void *rhs, void *r,
+                   int B, int Y, int X, unsigned flags, hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Y, X)) || (st = check_dtype2(dtype))) return st;
+  if (!w9_host || !phi || !r) return fail(HFM_ERR_BAD_ARG, "hfm_residual2d: NULL argument");
+  if (phi == r) return fail(HFM_ERR_BAD_ARG, "hfm_residual2d: in-place call");
+  const int64_t n = (int64_t)Y * X;
+  HFM2_DT(dtype, (k2_stencil<T, 1><<<dim3(blocks2(n, B), B), kT2, 0, (cudaStream_t)stream>>>(
+                     w9_of(w9_host), src2<T>(phi, nullptr, 0.f, Y, X, flags), (const T *)rhs,
+                     (T *)r, 0.f)));
+  HFM_CHECK_LAUNCH("k2_stencil");
+  return HFM_OK;
+}
+
+int hfm_residual_restrict2d(int dtype, const float *w9_host, const void *phi, const void *rhs,
+                            void *r_coarse, int B, int Y, int X, unsigned flags,
+                            hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Y, X)) || (st = check_dtype2(dtype))) return st;
+  if (!w9_host || !r_coarse) return fail(HFM_ERR_BAD_ARG, "hfm_residual_restrict2d: NULL argument");
+  if ((Y | X) & 1) return fail(HFM_ERR_BAD_ARG, "hfm_residual_restrict2d: extents must be even");
+  const int64_t nc = (int64_t)(Y / 2) * (X / 2);
+  HFM2_DT(dtype, (k2_resid_restrict<T, T><<<dim3(blocks2(nc, B), B), kT2, 0, (cudaStream_t)stream>>>(
+                     w9_of(w9_host), src2<T>(phi, nullptr, 0.f, Y, X, flags), (const T *)rhs,
+                     (T *)r_coarse, nc)));
+  HFM_CHECK_LAUNCH("k2_resid_restrict");
+  return HFM_OK;
+}
+
+int hfm_outer_residual2d(const float *w9_host, const float *phi, const float *rhs, int out_dtype,
+                         void *r, int B, int Y, int X, unsigned flags, double *partials,
+                         int *nblk_out, hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Y, X)) || (st = check_dtype2(out_dtype))) return st;
+  if (!w9_host || !phi || !rhs || !r) return fail(HFM_ERR_BAD_ARG, "hfm_outer_residual2d: NULL argument");
+  const int64_t n = (int64_t)Y * X;
+  const int nb = blocks2(n, B);
+  if (nblk_out) *nblk_out = nb;
+  HFM2_DT(out_dtype, (k2_outer_resid<T><<<dim3(nb, B), kT2, 0, (cudaStream_t)stream>>>(
+                         w9_of(w9_host), src2<float>(phi, nullptr, 0.f, Y, X, flags), rhs, (T *)r,
+                         partials)));
+  HFM_CHECK_LAUNCH("k2_outer_resid");
+  return HFM_OK;
+}
+
+int hfm_update2d(float *p, int dtype, const void *w, float sign, int64_t n, hfm_stream_t stream) {
+  int st;
+  if ((st = check_dtype2(dtype))) return st;
+  if (!p || !w || n < 1) return fail(HFM_ERR_BAD_ARG, "hfm_update2d: bad argument");
+  HFM2_DT(dtype, (k2_update<T><<<blocks2(n, 1), kT2, 0, (cudaStream_t)stream>>>(p, (const T *)w, sign, n)));
+  HFM_CHECK_LAUNCH("k2_update");
+  return HFM_OK;
+}
+
+int hfm_coarse_jacobi2d(int dtype, const float *w9_host, const void *rhs, void *out, int B, int Y,
+                        int X, float omega, int sweeps, unsigned flags, hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Y, X)) || (st = check_dtype2(dtype))) return st;
+  if (!w9_host || !rhs || !out || sweeps < 0) return fail(HFM_ERR_BAD_ARG, "hfm_coarse_jacobi2d: bad argument");
+  if ((int64_t)Y * X > 4096) return fail(HFM_ERR_BAD_ARG, "hfm_coarse_jacobi2d: at most 4096 cells");
+  if (w9_host[4] == 0.f) return fail(HFM_ERR_BAD_ARG, "hfm_coarse_jacobi2d: zero diagonal weight");
+  const size_t smem = (size_t)3 * Y * X * sizeof(float);
+  HFM2_DT(dtype, (k2_coarse_jacobi<T><<<B, kT2, smem, (cudaStream_t)stream>>>(
+                     w9_of(w9_host), (const T *)rhs, (T *)out, Y, X, omega, sweeps,
+                     (flags & HFM_FLAG_PERIODIC) ? 1 : 0)));
+  HFM_CHECK_LAUNCH("k2_coarse_jacobi");
+  return HFM_OK;
+}
+
+int hfm_mean_subtract2d(float *p, int B, int64_t n, hfm_stream_t stream) {
+  if (!p || B < 1 || n < 1) return fail(HFM_ERR_BAD_ARG, "hfm_mean_subtract2d: bad argument");
+  k2_mean_subtract<<<B, 1024, 0, (cudaStream_t)stream>>>(p, n);
+  HFM_CHECK_LAUNCH("k2_mean_subtract");
+  return HFM_OK;
+}
+
+int hfm_kolmogorov_stage(const float *phi_u, const float *phi_v, const float *base_u,
+                         const float *base_v, float *out_u, float *out_v, int Y, int X, float c,
+                         float dt, float nu, float h, float famp, float fk, hfm_stream_t stream) {
+  int st;
+  if ((st = check2(1, Y, X))) return st;
+  if (!phi_u || !phi_v || !base_u || !base_v || !out_u || !out_v)
+    return fail(HFM_ERR_BAD_ARG, "hfm_kolmogorov_stage: NULL argument");
+  if (out_u == phi_u || out_v == phi_v || out_u == phi_v || out_v == phi_u)
+    return fail(HFM_ERR_BAD_ARG, "hfm_kolmogorov_stage: outputs alias the differentiated fields");
+  const int64_t n = (int64_t)Y * X;
+  k2_ns_stage<<<blocks2(n, 1), kT2, 0, (cudaStream_t)stream>>>(phi_u, phi_v, base_u, base_v, out_u,
+                                                               out_v, Y, X, c, dt, nu, h, famp, fk);
+  HFM_CHECK_LAUNCH("k2_ns_stage");
+  return HFM_OK;
+}
+
+int hfm_kolmogorov_divergence(const float *u, const float *v, float *f, int Y, int X, float h,
+                              float dt, hfm_stream_t stream) {
+  int st;
+  if ((st = check2(1, Y, X))) return st;
+  if (!u || !v || !f) return fail(HFM_ERR_BAD_ARG, "hfm_kolmogorov_divergence: NULL argument");
+  const int64_t n = (int64_t)Y * X;
+  k2_ns_divergence<<<blocks2(n, 1), kT2, 0, (cudaStream_t)stream>>>(u, v, f, Y, X, h, dt);
+  HFM_CHECK_LAUNCH("k2_ns_divergence");
+  return HFM_OK;
+}
+
+int hfm_kolmogorov_project(float *u, float *v, const float *p, int Y, int X, float h, float dt,
+                           hfm_stream_t stream) {
+  int st;
+  if ((st = check2(1, Y, X))) return st;
+  if (!u || !v || !p) return fail(HFM_ERR_BAD_ARG, "hfm_kolmogorov_project: NULL argument");
+  const int64_t n = (int64_t)Y * X;
+  k2_ns_project<<<blocks2(n, 1), kT2, 0, (cudaStream_t)stream>>>(u, v, p, Y, X, h, dt);
+  HFM_CHECK_LAUNCH("k2_ns_project");
+  return HFM_OK;
+}
+
+}  // extern "C"

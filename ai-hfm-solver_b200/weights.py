@@ -56,3 +56,12 @@ def divergence(dt, dx=1.0, factor=1.0):
     kx, ky, kz = advection(1.0, 1.0, 1.0)
     s = factor / (dx * dt)
     return (kx * s).astype(np.float32), (ky * s).astype(np.float32), (kz * s).astype(np.float32)
+
+
+def advection_diffusion_2d(dt=10.0, dx=1.0, dy=1.0, Dx=0.1, Dy=0.1, ub=1.0):
+    """3x3 implicit advection-diffusion operator of ``Unstructured Mesh/Multigrid_2D.ipynb``
+    cell 3 (``w2[0][a][b][0]`` as ``[a, b]``), for the 2D reference cycle."""
+    cx, cy, cu = Dx * dt / dx ** 2, Dy * dt / dy ** 2, ub * dt / dx
+    return np.array([[0.0, -cy, 0.0],
+                     [-cx - cu, 1.0 + 2.0 * (cx + cy) + 2.0 * cu, -cx],
+                     [0.0, -cy - cu, 0.0]])

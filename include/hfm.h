@@ -54,6 +54,8 @@ typedef enum {
 #define HFM_FLAG_ZERO_XEND 1u  /* NS pressure form: residual / corrected phi zero on plane x = X-1 */
 #define HFM_FLAG_TOP_COPY 2u   /* after smoothing copy plane z = 1 onto z = 0 (boundary_condition_top) */
 #define HFM_FLAG_ZERO_GUESS 4u /* the input phi is identically zero (not read) */
+#define HFM_FLAG_PERIODIC 8u   /* 2D operators: wrap around instead of zero padding */
+#define HFM_FLAG_SAME_LEVEL_CORR 16u /* hfm_jacobi2d: `coarse` is on the same grid (no upsampling) */
 
 /* Operator descriptor (plain data, copied by value into each launch).
  *   CONST7: k[0..2] = (kz, ky, kx) = (Dz/dz^2, Dy/dy^2, Dx/dx^2); diagonal 2(kz+ky+kx).
@@ -245,6 +247,72 @@ int hfm_sigma7_grad_logsigma(const float *sx, const float *sy, const float *sz, 
                              const double *lam, int S, int Z, int Y, int X, float cz, float cy,
                              float cx, double *gx, double *gy, double *gz, int accumulate,
                              hfm_stream_t stream);
+
+/* ---------------------------------------------------------------- 2D operators
+ * The reference's two-dimensional multigrid (Unstructured Mesh/Multigrid_2D.ipynb) on
+ * (B, Y, X) fields, x fastest, float32 or bf16 storage (dtype HFM_F32 / HFM_BF16) with
+ * float32 arithmetic.  w9 is a host array of 9 weights, w9[3a + b] multiplying
+ * phi[y + a - 1][x + b - 1] (cross-correlation, the Conv2D kernel w2[0][a][b][0] of cell 3).
+ * Padding is zero (Conv2D 'SAME') unless flags has HFM_FLAG_PERIODIC. */
+/* y = conv(x, w9): CNN3D_A_<n> Conv2D(1, 3, 'SAME') layers, Multigrid_2D.ipynb#c7. */
+int hfm_conv2d_k3(const float *x, float *y, int B, int Y, int X, const float *w9_host,
+                  unsigned flags, hfm_stream_t stream);
+/* 2x2 VALID average, weight 0.25 (odd extents floored): CNN3D_res_<n>, Multigrid_2D.ipynb#c9. */
+int hfm_restrict_avg2d(int dtype, const void *fine, void *coarse, int B, int Y, int X,
+                       hfm_stream_t stream);
+/* UpSampling2D(2): CNN3D_prol_<n>, Multigrid_2D.ipynb#c11. */
+int hfm_prolong_nearest2d(int dtype, const void *coarse, void *fine, int B, int Yc, int Xc,
+                          hfm_stream_t stream);
+/* One Jacobi sweep out = phi + omega (rhs - A phi) / w9[4] with phi = base + coarse_sign *
+ * P(coarse) (either may be NULL = 0; P = nearest upsampling, even extents, or the identity
+ * with HFM_FLAG_SAME_LEVEL_CORR), rhs NULL = 0:
+ * the per-level update `w - A(w)/d + r/d` of Multigrid_2D.ipynb#c18 (omega = 1), fused with
+ * the prolongation that precedes it. */
+int hfm_jacobi2d(int dtype, const float *w9_host, const void *base, const void *coarse,
+                 float coarse_sign, const void *rhs, void *out, int B, int Y, int X, float omega,
+                 unsigned flags, hfm_stream_t stream);
+/* r = A phi - rhs (rhs NULL = 0): Multigrid_2D.ipynb#c18 `CNN3D_A_128(values) - b`. */
+int hfm_residual2d(int dtype, const float *w9_host, const void *phi, const void *rhs, void *r,
+                   int B, int Y, int X, unsigned flags, hfm_stream_t stream);
+/* r_coarse = R(A phi - rhs) in one pass (phi NULL = 0, even extents). */
+int hfm_residual_restrict2d(int dtype, const float *w9_host, const void *phi, const void *rhs,
+                            void *r_coarse, int B, int Y, int X, unsigned flags,
+                            hfm_stream_t stream);
+/* Outer defect of a mixed-precision solve: r (out_dtype) = A phi - rhs from float32 phi and
+ * rhs, with per-block float64 partial sums of r^2 in partials[b * nblk + k] when partials is
+ * not NULL; nblk (returned in *nblk_out) is at most 8 x the SM count (hfm_device_sm_count).
+ * No reference counterpart (the reference runs float32 only). */
+int hfm_outer_residual2d(const float *w9_host, const float *phi, const float *rhs, int out_dtype,
+                         void *r, int B, int Y, int X, unsigned flags, double *partials,
+                         int *nblk_out, hfm_stream_t stream);
+/* p += sign * w over n values (float32 p, w in dtype): the correction `values - w_128`. */
+int hfm_update2d(float *p, int dtype, const void *w, float sign, int64_t n, hfm_stream_t stream);
+/* `sweeps` Jacobi sweeps from zero on a grid of at most 4096 cells, one block per instance in
+ * shared memory (the coarsest level of a cycle). */
+int hfm_coarse_jacobi2d(int dtype, const float *w9_host, const void *rhs, void *out, int B, int Y,
+                        int X, float omega, int sweeps, unsigned flags, hfm_stream_t stream);
+/* Subtract each instance's mean from p (B instances of n values): the constant null space of
+ * a periodic pressure operator. */
+int hfm_mean_subtract2d(float *p, int B, int64_t n, hfm_stream_t stream);
+
+/* ---------------------------------------------------------------- 2D Kolmogorov flow
+ * Doubly periodic incompressible flow on a Y x X grid of spacing h forced by
+ * famp sin(fk y h) in x.  The reference has no Kolmogorov-flow code (its "2D Kolmogorov
+ * Flow" folder holds empty placeholders); the stage follows the two-stage momentum update of
+ * Anisotropic Resistivity Tomography/scripts/naiver_stokes_3D.py:580-622 in two dimensions with
+ * central differences and a 5-point Laplacian, and the projection its pressure-gradient step
+ * (:631-633). */
+/* out = base + c dt (nu L phi - phi_u d/dx phi - phi_v d/dy phi + F), both components. */
+int hfm_kolmogorov_stage(const float *phi_u, const float *phi_v, const float *base_u,
+                         const float *base_v, float *out_u, float *out_v, int Y, int X, float c,
+                         float dt, float nu, float h, float famp, float fk, hfm_stream_t stream);
+/* f = -(du/dx + dv/dy) / dt (right-hand side of -L p = f). */
+int hfm_kolmogorov_divergence(const float *u, const float *v, float *f, int Y, int X, float h,
+                              float dt, hfm_stream_t stream);
+/* u -= dt dp/dx, v -= dt dp/dy. */
+int hfm_kolmogorov_project(float *u, float *v, const float *p, int Y, int X, float h, float dt,
+                           hfm_stream_t stream);
+
 
 /* ------------------------------------------------------------------ multigrid handle */
 typedef enum { HFM_CYCLE_SAWTOOTH = 0, HFM_CYCLE_V = 1, HFM_CYCLE_F = 2 } hfm_cycle;

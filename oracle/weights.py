@@ -98,3 +98,17 @@ def directional_kernels():
         k[tuple(idx)] = -1.0
         ks.append(k)
     return ks
+
+
+def w2_2d_advection_diffusion(dt=10.0, dx=1.0, dy=1.0, Dx=0.1, Dy=0.1, ub=1.0):
+    """The 3x3 operator of ``Unstructured Mesh/Multigrid_2D.ipynb`` cell 3 (implicit
+    advection-diffusion, upwind in both directions), as ``w2[0][a][b][0]`` -> ``[a, b]``:
+    north / south ``-Dy dt/dy^2`` (south also ``-ub dt/dx``), west ``-Dx dt/dx^2 - ub dt/dx``,
+    east ``-Dx dt/dx^2``, centre ``1 + 2(Dx dt/dx^2 + Dy dt/dy^2) + 2 ub dt/dx``."""
+    w = np.zeros((3, 3))
+    w[0, 1] = -Dy * dt / dy ** 2
+    w[1, 0] = -Dx * dt / dx ** 2 - ub * dt / dx
+    w[1, 1] = 1 + 2 * (Dx * dt / dx ** 2 + Dy * dt / dy ** 2) + 2 * ub * dt / dx
+    w[1, 2] = -Dx * dt / dx ** 2
+    w[2, 1] = -Dy * dt / dy ** 2 - ub * dt / dx
+    return w

@@ -41,6 +41,10 @@ def test_product_weights_match_oracle(pkg):
     for a, b in zip(w.divergence(0.1), W.divergence_kernels(0.1)):
         np.testing.assert_allclose(a, b, rtol=1e-6)
     assert w.pressure27()[1, 1, 1] == pytest.approx(88 / 26, rel=1e-6)
+    np.testing.assert_allclose(w.advection_diffusion_2d(), W.w2_2d_advection_diffusion(), rtol=1e-12)
+    # the 2D reference prints 'Sum up the weights of filter' = 1 (cell 3): the upwind and
+    # diffusion terms cancel, the identity remains
+    assert W.w2_2d_advection_diffusion().sum() == pytest.approx(1.0)
 
 
 def test_param_counts(pins, pkg):
@@ -185,3 +189,47 @@ def test_tomography_matrix_matches_operator():
     A = tomo.assemble(s)
     ref = mg.Sigma7(s[0], s[1], s[2], dtype=np.float64).apply(x)
     np.testing.assert_allclose(A @ x.ravel(), ref.ravel(), rtol=1e-12, atol=1e-12)
+
+
+# ------------------------------------------------------------------------------ 2D path
+def test_conv2d_matches_torch_zero_and_periodic():
+    import torch
+    from oracle import kolmogorov as K2
+    rng = np.random.default_rng(21)
+    x = rng.standard_normal((9, 14)).astype(np.float32)
+    w = rng.standard_normal((3, 3)).astype(np.float32)
+    t = torch.from_numpy(x)[None, None]
+    k = torch.from_numpy(w)[None, None]
+    zero = torch.nn.functional.conv2d(t, k, padding=1)[0, 0].numpy()
+    wrap = torch.nn.functional.conv2d(torch.nn.functional.pad(t, (1, 1, 1, 1), mode="circular"), k)[0, 0].numpy()
+    np.testing.assert_allclose(K2.conv2d(x, w), zero, rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(K2.conv2d(x, w, periodic=True), wrap, rtol=1e-5, atol=1e-5)
+
+
+def test_2d_reference_cycle_converges():
+    """Multigrid_2D.ipynb#c18 on its own problem (128^2, box source of 40 x 40 ones at
+    (43, 43)): the residual falls cycle after cycle."""
+    from oracle import kolmogorov as K2
+    w = W.w2_2d_advection_diffusion()
+    b = np.zeros((128, 128), np.float32)
+    b[43:83, 43:83] = 1.0
+    v = b.copy()
+    res = []
+    for _ in range(5):
+        v = K2.sawtooth2d(w, v, b, len(K2.level_shapes((128, 128), 1)))
+        res.append(np.linalg.norm(K2.conv2d(v, w) - b))
+    assert all(r1 < r0 for r0, r1 in zip(res, res[1:]))
+
+
+def test_periodic_vcycle_contracts():
+    from oracle import kolmogorov as K2
+    n = 64
+    rng = np.random.default_rng(3)
+    f = rng.standard_normal((n, n))
+    f -= f.mean()
+    mg = K2.VCycle2D(K2.laplace5(2 * np.pi / n), (n, n))
+    p = np.zeros((n, n))
+    r0 = mg.rel_residual(p, f)
+    p = mg.solve(p, f, 4)
+    assert mg.rel_residual(p, f) < 1e-3 * r0
+    assert abs(p.mean()) < 1e-12
