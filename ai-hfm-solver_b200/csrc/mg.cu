@@ -576,7 +576,7 @@ struct Level {
   int Z, Y, X;
   int64_t n;
   void *phi = nullptr, *tmp = nullptr, *rhs = nullptr;
-  void *coef[3] = {nullptr, nullptr, nullptr};
+  void *coef[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   DevOp op;
 };
 
@@ -906,7 +906,8 @@ class Engine : public EngineBase {
       fine32_ = m_->lv[0].op;
       return HFM_OK;
     }
-    if (k != HFM_OP_SIGMA7) return fail(HFM_ERR_UNSUPPORTED, "handle supports CONST7, SIGMA7, K27");
+    if (k == HFM_OP_DIR7) return set_directional(slot, op, s);
+    if (k != HFM_OP_SIGMA7) return fail(HFM_ERR_UNSUPPORTED, "unknown operator kind");
     if (op.coef_dtype != HFM_F32 && op.coef_dtype != HFM_F64)
       return fail(HFM_ERR_BAD_ARG, "coefficients must be float32 or float64");
     // slot < 0: every slot at once (the arrays hold all slots), one launch per level
@@ -952,6 +953,39 @@ class Engine : public EngineBase {
     fine32_ = m_->lv[0].op;
     if (fine32_coef_[0])
       for (int a = 0; a < 3; ++a) fine32_.coef[a] = fine32_coef_[a];
+    return HFM_OK;
+  }
+
+  // The directional form of BGS_multigrid_v1.ipynb cells 38-40: six per-cell face
+  // coefficient arrays (x-, x+, y-, y+, z-, z+) and their sum (the diagonal A_MAT_TOT); coarse
+  // levels restrict all seven with the averaging restriction, without rescaling (cell 38,
+  // lines 16-33); coarse_scale^l multiplies level l as for the other forms.
+  int set_directional(int slot, const hfm_operator &op, cudaStream_t s) {
+    if (op.coef_dtype != HFM_F32 && op.coef_dtype != HFM_F64)
+      return fail(HFM_ERR_BAD_ARG, "coefficients must be float32 or float64");
+    for (int a = 0; a < 7; ++a)
+      if (!op.coef[a]) return fail(HFM_ERR_BAD_ARG, "DIR7 needs seven coefficient arrays");
+    const int lo = slot < 0 ? 0 : slot, cnt = slot < 0 ? m_->slots : 1;
+    for (int a = 0; a < 7; ++a) {
+      int st = launch_convert<T>(op.coef[a], op.coef_dtype, (T *)m_->lv[0].coef[a] + lo * n(0),
+                                 n(0) * cnt, s);
+      if (st) return st;
+      for (int l = 1; l < m_->L; ++l)
+        if ((st = launch_restrict<T>((T *)m_->lv[l - 1].coef[a] + lo * n(l - 1), n(l - 1),
+                                     (T *)m_->lv[l].coef[a] + lo * n(l), n(l), cnt, g(l - 1),
+                                     nullptr, s)))
+          return st;
+    }
+    float sc = 1.f;
+    for (int l = 0; l < m_->L; ++l) {
+      hfm_operator o = op;
+      o.scale = (op.scale == 0.f ? 1.f : op.scale) * sc;
+      o.coef_dtype = HFM_F32;
+      for (int a = 0; a < 7; ++a) o.coef[a] = m_->lv[l].coef[a];
+      m_->lv[l].op = make_devop(o, n(l));
+      sc *= m_->cfg.coarse_scale;
+    }
+    fine32_ = m_->lv[0].op;
     return HFM_OK;
   }
 
@@ -1001,7 +1035,7 @@ class Engine : public EngineBase {
       if (phi0) {
         HFM_CUDA(cudaMemcpyAsync(x, phi0, nf * 4, cudaMemcpyDeviceToDevice, s));
         DevOp d = fine32_;
-        for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 7; ++a)
           if (d.coef[a]) d.coef[a] = (const char *)d.coef[a] + (size_t)slot * nf * 4;
         PhiSrc<float> p;
         memset(&p, 0, sizeof(p));
@@ -1143,8 +1177,11 @@ std::vector<Grid3> plan_levels(const hfm_mg_config &c, int Z, int Y, int X) {
 int validate_cfg(const hfm_mg_config &c, int Z, int Y, int X, int slots) {
   if (Z <= 0 || Y <= 0 || X <= 0 || slots <= 0 || slots > 65535)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: bad extents or slot count");
-  if (c.op_kind != HFM_OP_CONST7 && c.op_kind != HFM_OP_SIGMA7 && c.op_kind != HFM_OP_K27)
-    return fail(HFM_ERR_UNSUPPORTED, "hfm_mg_create: operator kind must be CONST7, SIGMA7 or K27");
+  if (c.op_kind != HFM_OP_CONST7 && c.op_kind != HFM_OP_SIGMA7 && c.op_kind != HFM_OP_K27 &&
+      c.op_kind != HFM_OP_DIR7)
+    return fail(HFM_ERR_UNSUPPORTED, "hfm_mg_create: unknown operator kind");
+  if (c.op_kind == HFM_OP_DIR7 && (c.storage != HFM_F32 || c.accel == HFM_ACCEL_IR))
+    return fail(HFM_ERR_UNSUPPORTED, "hfm_mg_create: the directional form runs in float32 storage without refinement");
   if (c.storage != HFM_F32 && c.storage != HFM_BF16 && c.storage != HFM_F16)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: storage must be F32, BF16 or F16");
   if (c.cycle < 0 || c.cycle > 2 || c.accel < 0 || c.accel > 2)
@@ -1198,7 +1235,7 @@ size_t hfm_mg_footprint_bytes(const hfm_mg_config *c, int Z, int Y, int X, int s
   size_t tot = 0;
   for (size_t l = 0; l < lv.size(); ++l) {
     size_t nl = (size_t)lv[l].n();
-    size_t fields = 3 + (c->op_kind == HFM_OP_SIGMA7 ? 3 : 0);
+    size_t fields = 3 + (c->op_kind == HFM_OP_SIGMA7 ? 3 : 0) + (c->op_kind == HFM_OP_DIR7 ? 7 : 0);
     tot += nl * fields * es;
   }
   const size_t nf = (size_t)Z * Y * X;
@@ -1249,6 +1286,8 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
       L.rhs = dalloc(m.get(), b, &st);
     if (cfg->op_kind == HFM_OP_SIGMA7)
       for (int a = 0; a < 3; ++a) L.coef[a] = dalloc(m.get(), b, &st);
+    if (cfg->op_kind == HFM_OP_DIR7)
+      for (int a = 0; a < 7; ++a) L.coef[a] = dalloc(m.get(), b, &st);
   }
   const size_t nf = (size_t)Z * Y * X * slots;
   if (cfg->accel == HFM_ACCEL_IR) {

@@ -152,6 +152,48 @@ class Dir7(Operator):
         return s
 
 
+def bgs_mesh(shape, ax=0.02, ay=0.4, az=0.02):
+    """Non-uniform cell sizes of ``BGS_multigrid_v1.ipynb`` cell 34 on a (Z, Y, X) grid:
+    dx = 1 + ax k and dy = 1 + ay k with k the distance in cells from the centre plane (the
+    same on both halves), dz = 1 + az z.  Returns (mesh_x, mesh_y, mesh_z) float64 arrays of
+    the grid's shape."""
+    Z, Y, X = shape
+
+    def sym(n, a):
+        i = np.arange(n)
+        return 1.0 + a * np.where(i >= n // 2, i - n // 2, n // 2 - 1 - i)
+
+    mx = np.broadcast_to(sym(X, ax)[None, None, :], shape).copy()
+    my = np.broadcast_to(sym(Y, ay)[None, :, None], shape).copy()
+    mz = np.broadcast_to((1.0 + az * np.arange(Z))[:, None, None], shape).copy()
+    return mx, my, mz
+
+
+def bgs_mesh_p1(mesh, axis):
+    """The shifted sizes of ``BGS_multigrid_v1.ipynb`` cell 36: interior cells take the size
+    of the next cell along ``axis`` (axis 0 = z, 1 = y, 2 = x); the two boundary cells keep
+    their own."""
+    out = np.array(mesh, copy=True)
+    sl = lambda a, b: tuple(slice(a, b) if d == axis else slice(None) for d in range(3))
+    out[sl(1, -1)] = mesh[sl(2, None)]
+    return out
+
+
+def dir7_from_mesh(D, mesh_x, mesh_y, mesh_z, device="cuda"):
+    """``Dir7`` coefficients of ``BGS_multigrid_v1.ipynb`` cell 38: A_{x-} = D / mesh_x^2,
+    A_{x+} = D / mesh_x_p1^2 (likewise y, z), A_TOT their sum in the cell's order; computed in
+    float64 on the host as the reference does with NumPy, stored float32 on the device.
+    ``D`` is a scalar or an array of the grid's shape."""
+    p1 = [bgs_mesh_p1(m, ax) for m, ax in ((mesh_x, 2), (mesh_y, 1), (mesh_z, 0))]
+    D = np.asarray(D, np.float64)
+    a = {"xm": D / mesh_x ** 2, "ym": D / mesh_y ** 2, "zm": D / mesh_z ** 2,
+         "xp": D / p1[0] ** 2, "yp": D / p1[1] ** 2, "zp": D / p1[2] ** 2}
+    a["tot"] = a["xm"] + a["ym"] + a["zm"] + a["xp"] + a["yp"] + a["zp"]
+    shape = np.broadcast_shapes(np.shape(mesh_x), np.shape(D))
+    return Dir7({k: torch.from_numpy(np.ascontiguousarray(np.broadcast_to(v, shape), np.float32)).to(device)
+                 for k, v in a.items()})
+
+
 # ---------------------------------------------------------------------------- functions
 def conv3d_same(x, K, out=None):
     """``Conv3D(1, kernel_size=3, strides=1, padding='SAME')`` with frozen kernel ``K``."""

@@ -321,7 +321,8 @@ typedef enum { HFM_CYCLE_SAWTOOTH = 0, HFM_CYCLE_V = 1, HFM_CYCLE_F = 2 } hfm_cy
 typedef enum { HFM_ACCEL_NONE = 0, HFM_ACCEL_CG = 1, HFM_ACCEL_IR = 2 } hfm_accel;
 
 typedef struct {
-  int op_kind;            /* hfm_op_kind: CONST7, SIGMA7, K27 (DIR7 via stateless calls) */
+  int op_kind;            /* hfm_op_kind: CONST7, SIGMA7, K27; DIR7 with float32 storage
+                             and accel NONE or CG (BGS_multigrid_v1.ipynb cells 38-42) */
   int cycle;              /* hfm_cycle */
   int accel;              /* hfm_accel: NONE = stationary cycles, CG = cycle preconditions CG */
   int n_levels;           /* 0 = automatic (halve while extents even and min > min_coarse_edge) */

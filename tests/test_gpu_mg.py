@@ -274,3 +274,53 @@ def test_fcycle_with_outflow_rule_matches_oracle(hfm, T, n):
             h.run(1)
             got = h.fetch(0).cpu().numpy()
             close(got[..., :-1], ref[..., :-1])
+
+
+def test_sawtooth_directional_nonuniform_mesh(hfm, T):
+    """BGS_multigrid_v1.ipynb: the six-array directional operator on the stretched mesh of
+    cells 34-38 (sizes grow from the centre in x and y and along z), coefficient hierarchy by
+    restriction (cell 38), reference sawtooth cycle (cell 42), against the oracle."""
+    ops = hfm.ops
+    shape = (40, 32, 32)
+    mx, my, mz = ops.bgs_mesh(shape)
+    gop = ops.dir7_from_mesh(100.0, mx, my, mz)
+    arrs = {k: v.cpu().numpy() for k, v in zip(gop.ORDER, gop.A)}
+    oop = mg.Dir7({k: v for k, v in arrs.items() if k != "tot"}, arrs["tot"], np.float32)
+    # the product's coefficients are the oracle's cell-38 formula
+    ref = mg.bgs_coefficients(100.0, mx, my, mz, ops.bgs_mesh_p1(mx, 2), ops.bgs_mesh_p1(my, 1),
+                              ops.bgs_mesh_p1(mz, 0))
+    for k in mg.Dir7.ORDER:
+        np.testing.assert_allclose(arrs[k], ref[k], rtol=1e-6)
+    b = np.zeros(shape, np.float32)
+    b[10:20, 12:20, 12:20] = 1.0
+    n_levels = 4  # 40x32x32 .. 5x4x4, exact halvings as in the reference's 640x128x128 case
+    hier = mg.hierarchy(oop, n_levels)
+    refv = b.copy()
+    for _ in range(4):
+        refv = mg.sawtooth_cycle(hier, refv, b)
+    M = hfm.multigrid
+    cfg = M.SolverConfig.reference(n_levels=n_levels, cycles=10)
+    with M.Multigrid(shape, hfm._lib.OP_DIR7, cfg, slots=1) as h:
+        h.set_operator(gop)
+        h.load(0, dev(T, b), dev(T, b))
+        h.run(2)
+        h.run(2)
+        close(h.fetch(0).cpu(), refv)
+
+
+def test_directional_cg_solve(hfm, T):
+    """The directional form in a config-mode solve: PCG with V(2,2) on the stretched mesh
+    reaches 1e-6 measured by the float64 oracle."""
+    ops = hfm.ops
+    shape = (32, 32, 32)
+    gop = ops.dir7_from_mesh(100.0, *ops.bgs_mesh(shape))
+    f = hfm.problems.dipole(shape, seed=9)
+    M = hfm.multigrid
+    cfg = M.SolverConfig(cycle="V", accel="cg", tol=1e-6, max_cycles=500)
+    with M.Multigrid(shape, hfm._lib.OP_DIR7, cfg, slots=1) as h:
+        h.set_operator(gop)
+        phi, st = h.solve(dev(T, f[None]))
+    assert st[0]["status"] == 0, st
+    arrs = {k: v.double().cpu().numpy() for k, v in zip(gop.ORDER, gop.A)}
+    oop = mg.Dir7({k: v for k, v in arrs.items() if k != "tot"}, arrs["tot"], np.float64)
+    assert mg.rel_residual(oop, phi[0].double().cpu().numpy(), f) < 1.5e-6
