@@ -64,6 +64,10 @@ template <> struct St<__half> {
 // Resolved operator for one level: `coef` point at instance 0, instance i is at
 // coef + i * coef_stride.  `k` already includes `scale` (coefficients for CONST7/K27),
 // and `scale` is kept for the array forms (SIGMA7 / DIR7) whose coefficients are in memory.
+// Internal launch flag (never set by callers): residual kernels accumulate sum(res * phi)
+// instead of sum(res^2) in their partials, i.e. p . (A p) for CG when b is absent.
+constexpr unsigned HFM_INT_DOT_PHI = 1u << 30;
+
 struct DevOp {
   float k[27];
   float c[3];  // cz, cy, cx

@@ -234,11 +234,12 @@ __global__ void k_ir_start_inner(float *__restrict__ xin, Items it, const SlotSt
 }
 
 // float64 outer residual r = b - A x (sigma / kernel read as float32), written as the float32
-// right-hand side of the next inner solve, with partial sums of r^2.
-template <int KIND>
+// right-hand side of the next inner solve (and, when `rstore` is given, as the 16-bit copy the
+// inner cycle reads), with partial sums of r^2.
+template <int KIND, class T>
 __global__ void k_residual64(DevOp op, const double *__restrict__ x, const double *__restrict__ b,
-                             float *__restrict__ rout, int Z, int Y, int X, Items it,
-                             const int *__restrict__ mask, double *__restrict__ partials) {
+                             float *__restrict__ rout, T *__restrict__ rstore, int Z, int Y, int X,
+                             Items it, const int *__restrict__ mask, double *__restrict__ partials) {
   HFM_FOR_ITEMS(it, mask[slot])
   const double *xi = x + base;
   auto P = [&](int zz, int yy, int xx) -> double {
@@ -284,6 +285,7 @@ __global__ void k_residual64(DevOp op, const double *__restrict__ x, const doubl
     }
     const double r = b[base + i] - ax;
     rout[base + i] = (float)r;
+    if (rstore) rstore[base + i] = St<T>::from((float)r);
     acc += r * r;
   }
   const double t = block_reduce_sum(acc);
@@ -487,8 +489,12 @@ __global__ void k_scalar_sum(const double *__restrict__ partials, int nblk, Slot
   if (threadIdx.x == 0) {
     double t = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
-    if (which == 0) rz_new[inst] = t;
-    else st[inst].pq = t;
+    if (which == 0) {
+      rz_new[inst] = t;
+    } else {  // p.q of this iteration; rz_new becomes the current r.z (beta used the old one)
+      st[inst].pq = t;
+      st[inst].rz = rz_new[inst];
+    }
   }
 }
 
@@ -509,15 +515,12 @@ __global__ void k_cg_p(const TZ *__restrict__ z, float *__restrict__ p, Items it
   HFM_END_ITEMS
 }
 
-__global__ void k_cg_commit_rz(SlotState *st, const double *rz_new, const int *active, int B) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < B && active[i]) st[i].rz = rz_new[i];
-}
-
-// x += alpha p, r -= alpha q, partial sums of r^2.
+// x += alpha p, r -= alpha q, partial sums of r^2; with `rstore` also the storage-type copy of
+// the new r that the next iteration's cycle reads (bf16 refinement: no separate conversion).
+template <class T>
 __global__ void k_cg_xr(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
-                        const float *__restrict__ q, Items it, const SlotState *st,
-                        double *partials, const int *active) {
+                        const float *__restrict__ q, T *__restrict__ rstore, Items it,
+                        const SlotState *st, double *partials, const int *active) {
   HFM_FOR_ITEMS(it, active[slot])
   const SlotState s = st[slot];
   const float alpha = (s.pq != 0.0) ? (float)(s.rz / s.pq) : 0.f;
@@ -527,6 +530,7 @@ __global__ void k_cg_xr(float *__restrict__ x, float *__restrict__ r, const floa
     x[k] += alpha * p[k];
     const float rv = r[k] - alpha * q[k];
     r[k] = rv;
+    if (rstore) rstore[k] = St<T>::from(rv);
     acc += (double)rv * rv;
   }
   const double t = block_reduce_sum(acc);
@@ -643,6 +647,11 @@ class Engine : public EngineBase {
   Grid3 g(int l) { return Grid3{m_->lv[l].Z, m_->lv[l].Y, m_->lv[l].X}; }
   int64_t n(int l) { return m_->lv[l].n; }
   int kind() { return m_->cfg.op_kind; }
+  // bf16 refinement: the storage-type copy of the CG residual is written by the kernels that
+  // produce r (outer residual, k_cg_xr) instead of a separate conversion pass
+  bool fused_rhs() const {
+    return std::is_same<T, __nv_bfloat16>::value && m_->cfg.accel == HFM_ACCEL_IR;
+  }
 
   PhiSrc<T> src(const T *base, int64_t stride) {
     PhiSrc<T> p;
@@ -802,18 +811,19 @@ class Engine : public EngineBase {
     k_ir_update<<<ib, 256, 0, s>>>(m_->x64, m_->cg[0], it, m_->state, m_->outer);
     HFM_CHECK_LAUNCH("k_ir_update");
     DevOp d = fine32_;
+    T *rs = fused_rhs() ? rhs(0) : nullptr;
     switch (kind()) {
       case HFM_OP_SIGMA7:
-        k_residual64<HFM_OP_SIGMA7><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], g(0).Z,
-                                                        g(0).Y, g(0).X, it, m_->outer, m_->partials);
+        k_residual64<HFM_OP_SIGMA7, T><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], rs, g(0).Z,
+                                                           g(0).Y, g(0).X, it, m_->outer, m_->partials);
         break;
       case HFM_OP_CONST7:
-        k_residual64<HFM_OP_CONST7><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], g(0).Z,
-                                                        g(0).Y, g(0).X, it, m_->outer, m_->partials);
+        k_residual64<HFM_OP_CONST7, T><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], rs, g(0).Z,
+                                                           g(0).Y, g(0).X, it, m_->outer, m_->partials);
         break;
       default:
-        k_residual64<HFM_OP_K27><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], g(0).Z,
-                                                     g(0).Y, g(0).X, it, m_->outer, m_->partials);
+        k_residual64<HFM_OP_K27, T><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], rs, g(0).Z,
+                                                        g(0).Y, g(0).X, it, m_->outer, m_->partials);
     }
     HFM_CHECK_LAUNCH("k_residual64");
     k_check_outer<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
@@ -832,8 +842,9 @@ class Engine : public EngineBase {
     const int vb = it.CH, ib = item_blocks(B, it.CH);
     const int scaled = std::is_same<T, __half>::value ? 2 : 0;
     int st;
-    // z = M r  (rhs(0) holds r / s in the storage type; float32 storage reads r in place)
-    if (!std::is_same<T, float>::value) {
+    // z = M r  (rhs(0) holds r / s in the storage type; float32 storage reads r in place; the
+    // bf16 refinement path has it written already by the outer residual or the last k_cg_xr)
+    if (!std::is_same<T, float>::value && !fused_rhs()) {
       k_to_storage<T><<<ib, 256, 0, s>>>(r, rhs(0), it, m_->active, m_->state, scaled);
       HFM_CHECK_LAUNCH("k_to_storage");
     }
@@ -845,19 +856,22 @@ class Engine : public EngineBase {
     HFM_CHECK_LAUNCH("k_dot_partials");
     k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 0, m_->scal);
     k_cg_p<T><<<ib, 256, 0, s>>>(z, p, it, m_->state, m_->scal, m_->active, scaled, m_->gscale);
-    k_cg_commit_rz<<<(B + 127) / 128, 128, 0, s>>>(m_->state, m_->scal, m_->active, B);
     HFM_CHECK_LAUNCH("k_cg_p");
-    // q = A p ; pq = p . q   (FP32 operator on the fine level)
+    // q = A p with the partial sums of p . q in the same pass (float32 operator on the fine
+    // level); the p.q reduction also makes rz_new the current r.z
     PhiSrc<float> pp;
     memset(&pp, 0, sizeof(pp));
     pp.base = p;
     pp.base_stride = nf;
-    if ((st = launch_apply<float>(kind(), fine32_, pp, q, nf, B, g(0), m_->active, s))) return st;
-    k_dot_partials<float><<<ib, 256, 0, s>>>(p, q, it, m_->partials, m_->active, nullptr, 0,
-                                             nullptr);
-    k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 1, m_->scal);
+    int nblk_pq = 0;
+    if ((st = launch_residual<float>(kind(), fine32_, pp, nullptr, 0, q, nf, B, g(0), HFM_INT_DOT_PHI,
+                                     m_->active, m_->partials, &nblk_pq, s)))
+      return st;
+    k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, nblk_pq, m_->state, m_->active, 1, m_->scal);
+    HFM_CHECK_LAUNCH("k_scalar_sum");
     // x += alpha p ; r -= alpha q ; ||r||
-    k_cg_xr<<<ib, 256, 0, s>>>(x, r, p, q, it, m_->state, m_->partials, m_->active);
+    k_cg_xr<T><<<ib, 256, 0, s>>>(x, r, p, q, fused_rhs() ? rhs(0) : nullptr, it, m_->state,
+                                  m_->partials, m_->active);
     HFM_CHECK_LAUNCH("k_cg_xr");
     if (!ir) return check(vb, 0, s);
     k_check_inner<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,

@@ -93,6 +93,7 @@ template <class T> struct FastArgs {
   int zero_xend;      // input: phi' = 0 on x = X-1 (NS correction before the sweep)
   int zero_xend_out;  // output: residual = 0 on x = X-1 (NS residual)
   int top_copy;
+  int dot_phi;        // partials of res * phi instead of res^2 (RESID)
 };
 
 template <class T, int CORR>
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(kFastThreads)
         if (a.zero_xend_out && x0 + 4 == X) res[r].v[3] = 0.f;
         if (in) {
 #pragma unroll
-          for (int e = 0; e < 4; ++e) acc += (double)res[r].v[e] * res[r].v[e];
+          for (int e = 0; e < 4; ++e) acc += (double)res[r].v[e] * (a.dot_phi ? pc[r].v[e] : res[r].v[e]);
         }
       }
       if (in && a.out) {
@@ -413,7 +414,7 @@ __global__ void __launch_bounds__(kFastThreads)
       if (a.zero_xend_out && x0 + 4 == X) res.v[3] = 0.f;
       if (valid) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc2 += (double)res.v[e] * res.v[e];
+        for (int e = 0; e < 4; ++e) acc2 += (double)res.v[e] * (a.dot_phi ? cen_cur.v[e] : res.v[e]);
       }
     }
     if (valid && a.out) {
@@ -487,6 +488,7 @@ int fast_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const
   a.zero_xend = phi.zero_xend ? 1 : 0;
   a.zero_xend_out = (mode != M_SMOOTH && (flags & HFM_FLAG_ZERO_XEND)) ? 1 : 0;
   a.top_copy = (mode == M_SMOOTH && (flags & HFM_FLAG_TOP_COPY)) ? 1 : 0;
+  a.dot_phi = (mode == M_RESID && (flags & HFM_INT_DOT_PHI)) ? 1 : 0;
   a.zc = 0;
   if (phi.base && phi.base_stride != stride) return fail(HFM_ERR_BAD_ARG, "fast path: stride mismatch");
   const int corr = phi.corr ? (phi.corr_coarse ? C_COARSE : C_SAME) : C_NONE;

@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kThreads)
     if (b) v -= St<T>::ld(b + inst * b_stride + i);
     if ((flags & HFM_FLAG_ZERO_XEND) && x == X - 1) v = 0.f;
     if (r) r[inst * r_stride + i] = St<T>::from(v);
-    acc += (double)v * (double)v;
+    acc += (double)v * (double)((flags & HFM_INT_DOT_PHI) ? phi(inst, z, y, x, Y, X) : v);
   }
   if (partials) {
     acc = block_sum(acc, sh);

@@ -77,7 +77,7 @@ template <class T> struct TmaArgs {
   int64_t stride, coarse_stride;
   int Z, Y, X, zc, tiles_x;
   float omega, corr_sign;
-  int has_phi, has_f, has_sigma, zero_xend, zero_xend_out, top_copy;
+  int has_phi, has_f, has_sigma, zero_xend, zero_xend_out, top_copy, dot_phi;
   unsigned stage_bytes;
 };
 
@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
       if (a.zero_xend_out && gx + V == X) res[V - 1] = 0.f;
       if (valid) {
 #pragma unroll
-        for (int e = 0; e < V; ++e) acc += (double)res[e] * res[e];
+        for (int e = 0; e < V; ++e) acc += (double)res[e] * (a.dot_phi ? pc[e] : res[e]);
       }
     }
     const int64_t off = inst * a.stride + ((int64_t)z * Y + gy) * X + gx;
@@ -606,6 +606,7 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
   a.zero_xend = phi.zero_xend ? 1 : 0;
   a.zero_xend_out = (mode != M_SMOOTH && (flags & HFM_FLAG_ZERO_XEND)) ? 1 : 0;
   a.top_copy = (mode == M_SMOOTH && (flags & HFM_FLAG_TOP_COPY)) ? 1 : 0;
+  a.dot_phi = (mode == M_RESID && (flags & HFM_INT_DOT_PHI)) ? 1 : 0;
   a.tiles_x = (g.X + TX - 1) / TX;
   const int tiles = a.tiles_x * ((g.Y + TY - 1) / TY);
   // z chunks: about 3 resident blocks per SM and four waves; chunks of at least 2 planes
