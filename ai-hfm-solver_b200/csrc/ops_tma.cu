@@ -547,7 +547,10 @@ int go(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
 
 bool tma_eligible(int kind, Grid3 g, int mode, const void *corr, int corr_coarse, int es) {
   if (kind != HFM_OP_CONST7 && kind != HFM_OP_SIGMA7 && kind != HFM_OP_K27) return false;
-  if (g.X < TX || g.Y < (es == 4 ? 8 : 16)) return false;
+  // grids narrower than a tile (48 <= X < 64) use the same boxes: the columns past X are
+  // zero-filled, not read.  Below X = 48 the register-queue kernels are as fast or faster
+  // (measured: 32^3 and 24^3 levels of 64 instances).
+  if (g.X < 48 || g.Y < (es == 4 ? 8 : 16)) return false;
   if ((g.X * es) % 16) return false;  // tensor-map strides are multiples of 16 bytes
   if (corr && !corr_coarse) return false;
   if (corr && ((g.X / 2) * es) % 16) return false;
