@@ -20,6 +20,7 @@ FLAG_ZERO_XEND, FLAG_TOP_COPY, FLAG_ZERO_GUESS, FLAG_PERIODIC, FLAG_SAME_LEVEL_C
 # hfm_cycle / hfm_accel
 CYCLE_SAWTOOTH, CYCLE_V, CYCLE_F = range(3)
 ACCEL_NONE, ACCEL_CG, ACCEL_IR = range(3)
+OPT_NO_FUSED_COARSE = 1
 
 
 class HfmOperator(C.Structure):
@@ -34,7 +35,7 @@ class HfmMgConfig(C.Structure):
                 ("coarse_omega", C.c_float), ("coarse_scale", C.c_float),
                 ("sawtooth_fine_smooth", C.c_int), ("flags", C.c_uint), ("storage", C.c_int),
                 ("tol", C.c_double), ("max_cycles", C.c_int), ("cycles_per_launch", C.c_int),
-                ("inner_tol", C.c_double), ("inner_max_cycles", C.c_int), ("reserved_cfg", C.c_int)]
+                ("inner_tol", C.c_double), ("inner_max_cycles", C.c_int), ("options", C.c_int)]
 
 
 class HfmSlotStats(C.Structure):

@@ -237,6 +237,30 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
                T *coarse, int64_t stride, int64_t coarse_stride, int B, Grid3 g, float omega,
                unsigned flags, const int *active, double *partials, int *nblk_out,
                cudaStream_t s);
+// The coarse end of a V-cycle in one kernel (subcycle.cu): levels l0 .. coarsest of a SIGMA7
+// hierarchy, one block per instance, all fields in shared memory.
+constexpr int kMaxSubLevels = 8;
+constexpr size_t kSubcycleMaxSmem = 200 * 1024;
+template <class T> struct SubLevel {
+  int Z, Y, X, n;
+  float cz, cy, cx;          // face multipliers of this level (c_d times the level's scale)
+  const T *sx, *sy, *sz;     // the level's conductivities, instance stride n
+  int o_phi, o_tmp, o_rhs;   // float offsets of the level's fields in shared memory
+  int o_sig;                 // element offset of its conductivities in the T region
+};
+template <class T> struct SubArgs {
+  SubLevel<T> lv[kMaxSubLevels];
+  int nlev;
+  const T *rhs;  // right-hand side of level l0, instance stride lv[0].n
+  T *out;        // its approximate solution
+  const int *active;
+  float omega, coarse_omega;
+  int nu_pre, nu_post, coarse_sweeps;
+  int sig_byte_offset;
+};
+size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size);
+template <class T> int launch_subcycle(SubArgs<T> a, int B, cudaStream_t s);
+
 // Upper bound of blocks per instance of any residual launch on grid g (partials sizing).
 int64_t max_partial_blocks(Grid3 g, int B);
 

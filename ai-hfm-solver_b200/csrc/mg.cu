@@ -701,10 +701,57 @@ class Engine : public EngineBase {
   }
 
   // Approximately solve A_l phi = rhs(l); `zero` says the current iterate is zero.
+  // First level of the fused coarse V-cycle (subcycle.cu), or -1: the deepest levels of at
+  // most 4096 cells of a SIGMA7 hierarchy, at least two of them, below the fine level.
+  int fused_first_level() {
+    const hfm_mg_config &c = m_->cfg;
+    if (kind() != HFM_OP_SIGMA7 || (c.options & HFM_OPT_NO_FUSED_COARSE)) return -1;
+    if (n(m_->L - 1) > coarse_smem_limit()) return -1;
+    int l0 = m_->L - 1;
+    while (l0 - 1 >= 1 && n(l0 - 1) <= 4096 && m_->L - (l0 - 1) <= kMaxSubLevels) --l0;
+    if (l0 >= m_->L - 1) return -1;
+    int ns[kMaxSubLevels];
+    for (int l = l0; l < m_->L; ++l) ns[l - l0] = (int)n(l);
+    if (subcycle_smem_bytes(ns, m_->L - l0, (int)sizeof(T)) > kSubcycleMaxSmem) return -1;
+    return l0;
+  }
+
+  int fused_vcycle(int l0, cudaStream_t s) {
+    const hfm_mg_config &c = m_->cfg;
+    SubArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    a.nlev = m_->L - l0;
+    for (int l = l0; l < m_->L; ++l) {
+      SubLevel<T> &q = a.lv[l - l0];
+      const DevOp &op = m_->lv[l].op;
+      q.Z = m_->lv[l].Z;
+      q.Y = m_->lv[l].Y;
+      q.X = m_->lv[l].X;
+      q.n = (int)n(l);
+      q.cz = op.c[0] * op.scale;
+      q.cy = op.c[1] * op.scale;
+      q.cx = op.c[2] * op.scale;
+      q.sx = (const T *)op.coef[0];
+      q.sy = (const T *)op.coef[1];
+      q.sz = (const T *)op.coef[2];
+    }
+    a.rhs = rhs(l0);
+    a.out = buf(l0, 0);
+    a.active = m_->active;
+    a.omega = c.omega;
+    a.coarse_omega = c.coarse_omega;
+    a.nu_pre = c.nu_pre;
+    a.nu_post = c.nu_post;
+    a.coarse_sweeps = c.coarse_sweeps;
+    cur_[l0] = 0;
+    return launch_subcycle<T>(a, m_->slots, s);
+  }
+
   int vcycle(int l, bool zero, bool fcycle, int check_level0, cudaStream_t s) {
     const hfm_mg_config &c = m_->cfg;
     int st;
     if (l == m_->L - 1) return coarse_solve(l, s);
+    if (zero && !fcycle && l > 0 && l == fused_l0_) return fused_vcycle(l, s);
     if (zero) cur_[l] = 0;
     // NS outflow rule on the fine level (as the reference cycle applies it): the iterate is
     // read as zero on x = X-1 and the residual is zero there
@@ -883,6 +930,7 @@ class Engine : public EngineBase {
   int emit_cycles(int cycles, cudaStream_t s) override {
     int st;
     for (int k = 0; k < kMaxLevels; ++k) cur_[k] = 0;
+    fused_l0_ = fused_first_level();
     for (int i = 0; i < cycles; ++i) {
       const hfm_mg_config &c = m_->cfg;
       if (c.accel == HFM_ACCEL_IR) {
@@ -1149,6 +1197,7 @@ class Engine : public EngineBase {
  private:
   hfm_mg *m_;
   int cur_[kMaxLevels] = {0};
+  int fused_l0_ = -1;  // first level of the fused coarse V-cycle, -1: none
 };
 
 }  // namespace hfm

@@ -1,0 +1,204 @@
+// The coarse end of a V-cycle in one kernel: one thread block per instance runs the V-cycle
+// of every level from l0 (at most 4096 cells) down to the coarsest and back, with all fields
+// of those levels in shared memory.
+//
+// On the deep levels the stencil kernels are a few microseconds of work behind a launch and a
+// dependency each (the 16^3, 8^3, 4^3 levels of 64 instances make ~15 launches per cycle);
+// this kernel replaces them with one launch whose sweeps are separated by __syncthreads().
+// The sequence is the one the multi-kernel V-cycle runs (nu_pre sweeps from zero, residual +
+// 2x2x2 averaging restriction, recursion, coarsest level `coarse_sweeps` sweeps from zero with
+// coarse_omega, nearest prolongation + correction fused with the first post-sweep, the
+// remaining post-sweeps); iterates stay in float32 between sweeps (the multi-kernel path
+// rounds them to the storage type).  SIGMA7 operator: face coefficient c_d (s_i + s_j) / 2,
+// wall face c_d s_i, ghost phi = 0.
+#include "hfm_internal.cuh"
+
+namespace hfm {
+
+namespace {
+
+constexpr int kSubThreads = 512;
+
+template <class T>
+__device__ __forceinline__ float sub_apply(const SubLevel<T> &L, const float *ph, const float *cor,
+                                           const SubLevel<T> *Lc, const T *S, int z, int y, int x,
+                                           float *diag) {
+  const int X = L.X, Y = L.Y, Z = L.Z;
+  auto P = [&](int zz, int yy, int xx) -> float {
+    if (zz < 0 || zz >= Z || yy < 0 || yy >= Y || xx < 0 || xx >= X) return 0.f;
+    float v = ph ? ph[(zz * Y + yy) * X + xx] : 0.f;
+    if (cor) v -= cor[((zz >> 1) * Lc->Y + (yy >> 1)) * Lc->X + (xx >> 1)];
+    return v;
+  };
+  const T *sx = S + L.o_sig, *sy = sx + L.n, *sz = sy + L.n;
+  const int i = (z * Y + y) * X + x;
+  const float vx = St<T>::to(sx[i]), vy = St<T>::to(sy[i]), vz = St<T>::to(sz[i]);
+  const float axm = L.cx * (x > 0 ? 0.5f * (vx + St<T>::to(sx[i - 1])) : vx);
+  const float axp = L.cx * (x < X - 1 ? 0.5f * (vx + St<T>::to(sx[i + 1])) : vx);
+  const float aym = L.cy * (y > 0 ? 0.5f * (vy + St<T>::to(sy[i - X])) : vy);
+  const float ayp = L.cy * (y < Y - 1 ? 0.5f * (vy + St<T>::to(sy[i + X])) : vy);
+  const float azm = L.cz * (z > 0 ? 0.5f * (vz + St<T>::to(sz[i - X * Y])) : vz);
+  const float azp = L.cz * (z < Z - 1 ? 0.5f * (vz + St<T>::to(sz[i + X * Y])) : vz);
+  const float pc = P(z, y, x);
+  *diag = axm + axp + aym + ayp + azm + azp;
+  return axm * (pc - P(z, y, x - 1)) + axp * (pc - P(z, y, x + 1)) + aym * (pc - P(z, y - 1, x)) +
+         ayp * (pc - P(z, y + 1, x)) + azm * (pc - P(z - 1, y, x)) + azp * (pc - P(z + 1, y, x));
+}
+
+// out = phi' + om (f - A phi') / diag with phi' = in - P(cor) (in / cor may be null)
+template <class T>
+__device__ void sub_sweep(const SubLevel<T> &L, const float *in, const float *cor,
+                          const SubLevel<T> *Lc, const float *f, float *out, float om,
+                          const T *S) {
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+    const int x = i % L.X, t = i / L.X, y = t % L.Y, z = t / L.Y;
+    float dg;
+    const float ax = sub_apply<T>(L, in, cor, Lc, S, z, y, x, &dg);
+    float pc = in ? in[i] : 0.f;
+    if (cor) pc -= cor[((z >> 1) * Lc->Y + (y >> 1)) * Lc->X + (x >> 1)];
+    out[i] = pc + om * __fdividef(f[i] - ax, dg);
+  }
+  __syncthreads();
+}
+
+// fc = R(A phi - f): 0.125 times the sum over each coarse cell's eight fine residuals
+template <class T>
+__device__ void sub_resid_restrict(const SubLevel<T> &L, const float *ph, const float *f,
+                                   const SubLevel<T> &Lc, float *fc, const T *S) {
+  for (int j = threadIdx.x; j < Lc.n; j += blockDim.x) {
+    const int xc = j % Lc.X, t = j / Lc.X, yc = t % Lc.Y, zc = t / Lc.Y;
+    float sum = 0.f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int z = 2 * zc + a, y = 2 * yc + b, x = 2 * xc + c;
+          float dg;
+          sum += sub_apply<T>(L, ph, nullptr, nullptr, S, z, y, x, &dg) - f[(z * L.Y + y) * L.X + x];
+        }
+    fc[j] = 0.125f * sum;
+  }
+  __syncthreads();
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant__ SubArgs<T> a) {
+  const int64_t inst = blockIdx.x;
+  if (a.active && !a.active[inst]) return;
+  extern __shared__ __align__(16) unsigned char sub_smem[];
+  float *F = reinterpret_cast<float *>(sub_smem);
+  T *S = reinterpret_cast<T *>(sub_smem + a.sig_byte_offset);
+  const int nl = a.nlev;
+  for (int l = 0; l < nl; ++l) {
+    const SubLevel<T> &L = a.lv[l];
+    const int64_t g = inst * (int64_t)L.n;
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+      S[L.o_sig + i] = L.sx[g + i];
+      S[L.o_sig + L.n + i] = L.sy[g + i];
+      S[L.o_sig + 2 * L.n + i] = L.sz[g + i];
+    }
+  }
+  for (int i = threadIdx.x; i < a.lv[0].n; i += blockDim.x)
+    F[a.lv[0].o_rhs + i] = St<T>::to(a.rhs[inst * (int64_t)a.lv[0].n + i]);
+  __syncthreads();
+
+  int cur[kMaxSubLevels];    // 0: iterate in phi, 1: in tmp
+  bool zero[kMaxSubLevels];  // iterate still identically zero (nu_pre == 0)
+  // down: pre-smoothing from zero, residual, restriction
+  for (int l = 0; l < nl - 1; ++l) {
+    const SubLevel<T> &L = a.lv[l];
+    float *buf[2] = {F + L.o_phi, F + L.o_tmp};
+    const float *f = F + L.o_rhs;
+    int c = 0;
+    for (int k = 0; k < a.nu_pre; ++k) {
+      sub_sweep<T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, f, buf[c ^ 1], a.omega, S);
+      c ^= 1;
+    }
+    cur[l] = c;
+    zero[l] = a.nu_pre == 0;
+    sub_resid_restrict<T>(L, zero[l] ? nullptr : buf[c], f, a.lv[l + 1], F + a.lv[l + 1].o_rhs, S);
+  }
+  // coarsest: coarse_sweeps sweeps from zero
+  {
+    const SubLevel<T> &L = a.lv[nl - 1];
+    float *buf[2] = {F + L.o_phi, F + L.o_tmp};
+    int c = 0;
+    for (int k = 0; k < a.coarse_sweeps; ++k) {
+      sub_sweep<T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1],
+                   a.coarse_omega, S);
+      c ^= 1;
+    }
+    if (a.coarse_sweeps == 0) {
+      for (int i = threadIdx.x; i < L.n; i += blockDim.x) buf[0][i] = 0.f;
+      __syncthreads();
+    }
+    cur[nl - 1] = c;
+  }
+  // up: prolongation + correction with the first post-sweep, then the other post-sweeps
+  const int post = a.nu_post > 0 ? a.nu_post : 1;
+  for (int l = nl - 2; l >= 0; --l) {
+    const SubLevel<T> &L = a.lv[l];
+    const SubLevel<T> &Lc = a.lv[l + 1];
+    float *buf[2] = {F + L.o_phi, F + L.o_tmp};
+    const float *coarse = F + (cur[l + 1] ? Lc.o_tmp : Lc.o_phi);
+    int c = cur[l];
+    for (int k = 0; k < post; ++k) {
+      const float om = a.nu_post == 0 ? 0.f : a.omega;
+      if (k == 0) sub_sweep<T>(L, zero[l] ? nullptr : buf[c], coarse, &Lc, F + L.o_rhs, buf[c ^ 1], om, S);
+      else sub_sweep<T>(L, buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1], om, S);
+      c ^= 1;
+    }
+    cur[l] = c;
+  }
+  const float *res = F + (cur[0] ? a.lv[0].o_tmp : a.lv[0].o_phi);
+  for (int i = threadIdx.x; i < a.lv[0].n; i += blockDim.x)
+    a.out[inst * (int64_t)a.lv[0].n + i] = St<T>::from(res[i]);
+}
+
+}  // namespace
+
+size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size) {
+  size_t f = 0, sg = 0;
+  for (int l = 0; l < nlev; ++l) {
+    f += (size_t)3 * n[l];
+    sg += (size_t)3 * n[l];
+  }
+  const size_t fbytes = ((f * 4 + 15) / 16) * 16;
+  return fbytes + sg * (size_t)elem_size;
+}
+
+template <class T>
+int launch_subcycle(SubArgs<T> a, int B, cudaStream_t s) {
+  int n[kMaxSubLevels];
+  for (int l = 0; l < a.nlev; ++l) n[l] = a.lv[l].n;
+  // shared-memory layout: float fields of every level, then the conductivities (type T)
+  int off = 0;
+  for (int l = 0; l < a.nlev; ++l) {
+    a.lv[l].o_phi = off;
+    a.lv[l].o_tmp = off + n[l];
+    a.lv[l].o_rhs = off + 2 * n[l];
+    off += 3 * n[l];
+  }
+  a.sig_byte_offset = ((off * 4 + 15) / 16) * 16;
+  int soff = 0;
+  for (int l = 0; l < a.nlev; ++l) {
+    a.lv[l].o_sig = soff;
+    soff += 3 * n[l];
+  }
+  const size_t smem = subcycle_smem_bytes(n, a.nlev, (int)sizeof(T));
+  static cudaError_t attr = cudaFuncSetAttribute(k_subcycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)kSubcycleMaxSmem);
+  if (attr != cudaSuccess) return cuda_status(attr, "cudaFuncSetAttribute(k_subcycle)");
+  if (smem > kSubcycleMaxSmem) return fail(HFM_ERR_BAD_ARG, "subcycle: levels exceed shared memory");
+  k_subcycle<T><<<B, kSubThreads, smem, s>>>(a);
+  HFM_CHECK_LAUNCH("k_subcycle");
+  return HFM_OK;
+}
+
+template int launch_subcycle<float>(SubArgs<float>, int, cudaStream_t);
+template int launch_subcycle<__nv_bfloat16>(SubArgs<__nv_bfloat16>, int, cudaStream_t);
+template int launch_subcycle<__half>(SubArgs<__half>, int, cudaStream_t);
+
+}  // namespace hfm

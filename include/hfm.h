@@ -340,8 +340,13 @@ typedef struct {
   int cycles_per_launch;  /* cycles captured in one CUDA graph between host checks (default 4) */
   double inner_tol;       /* IR: an inner CG solve stops at max(inner_tol ||r0||, 0.3 tol ||b||) */
   int inner_max_cycles;   /* IR: iteration cap of one inner solve (default 200) */
-  int reserved_cfg;
+  int options;             /* HFM_OPT_* bits (default 0) */
 } hfm_mg_config;
+
+/* options: run every level of the V-cycle as separate kernel launches, including the deep
+ * levels that otherwise run as one fused kernel (one block per instance, fields in shared
+ * memory, for SIGMA7 levels of at most 4096 cells) */
+#define HFM_OPT_NO_FUSED_COARSE 1
 
 typedef struct {
   int active;       /* 1 while the slot is still iterating */

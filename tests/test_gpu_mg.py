@@ -324,3 +324,25 @@ def test_directional_cg_solve(hfm, T):
     arrs = {k: v.double().cpu().numpy() for k, v in zip(gop.ORDER, gop.A)}
     oop = mg.Dir7({k: v for k, v in arrs.items() if k != "tot"}, arrs["tot"], np.float64)
     assert mg.rel_residual(oop, phi[0].double().cpu().numpy(), f) < 1.5e-6
+
+
+@pytest.mark.parametrize("cycle,storage", [("V", "f32"), ("F", "f32"), ("V", "bf16")])
+def test_fused_coarse_cycle_matches_separate_kernels(hfm, T, cycle, storage):
+    """The deep levels (<= 4096 cells) run as one fused kernel by default; the same cycles
+    with every level launched separately (HFM_OPT_NO_FUSED_COARSE) give the same iterate to
+    float32 rounding (float32 storage) or to the storage rounding the separate kernels add
+    between sweeps (bf16)."""
+    sig, f = _problem(hfm, 32, 8)
+    M = hfm.multigrid
+    outs = []
+    for fused in (True, False):
+        cfg = M.SolverConfig(cycle=cycle, storage=storage, tol=1e-300, max_cycles=10,
+                             cycles_per_launch=1, fused_coarse=fused)
+        with M.Multigrid((32, 32, 32), hfm._lib.OP_SIGMA7, cfg, slots=2) as h:
+            for s in range(2):
+                h.set_operator(hfm.ops.Sigma7(*(dev(T, sig[k]) for k in range(3))), slot=s)
+                h.load(s, dev(T, f))
+            h.run(3)
+            outs.append([h.fetch(s).cpu().numpy() for s in range(2)])
+    close(outs[0][0], outs[1][0], rtol=1e-5 if storage == "f32" else 2e-2)
+    np.testing.assert_array_equal(outs[0][0], outs[0][1])
