@@ -67,6 +67,9 @@ template <> struct St<__half> {
 // Internal launch flag (never set by callers): residual kernels accumulate sum(res * phi)
 // instead of sum(res^2) in their partials, i.e. p . (A p) for CG when b is absent.
 constexpr unsigned HFM_INT_DOT_PHI = 1u << 30;
+// Internal launch flag: smoothing kernels write block partial sums of out * rhs (z . r for a
+// CG preconditioner whose right-hand side is r) when given a partials buffer.
+constexpr unsigned HFM_INT_DOT_RHS = 1u << 29;
 
 struct DevOp {
   float k[27];
@@ -174,7 +177,8 @@ struct Grid3 {
 template <class T>
 int launch_smooth(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
                   int64_t rhs_stride, T *out, int64_t out_stride, int B, Grid3 g, float omega,
-                  unsigned flags, const int *active, cudaStream_t s);
+                  unsigned flags, const int *active, cudaStream_t s, double *partials = nullptr,
+                  int *nblk_out = nullptr);
 template <class T>
 int launch_residual(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *b,
                     int64_t b_stride, T *r, int64_t r_stride, int B, Grid3 g, unsigned flags,

@@ -671,9 +671,9 @@ class Engine : public EngineBase {
   }
 
   int smooth(int l, const PhiSrc<T> &p, const T *f, T *out, float omega, unsigned flags,
-             cudaStream_t s) {
+             cudaStream_t s, double *partials = nullptr, int *nblk = nullptr) {
     return launch_smooth<T>(kind(), m_->lv[l].op, p, f, n(l), out, n(l), m_->slots, g(l),
-                            omega, flags, m_->active, s);
+                            omega, flags, m_->active, s, partials, nblk);
   }
 
   int check(int nblk, int which, cudaStream_t s) {
@@ -794,7 +794,11 @@ class Engine : public EngineBase {
       if (k == 0) q = with_coarse(q, l + 1, buf(l + 1, cur_[l + 1]), -1.f);
       q.zero_xend = xend;
       float om = c.nu_post == 0 ? 0.f : c.omega;
-      if ((st = smooth(l, q, rhs(l), buf(l, cur_[l] ^ 1), om, 0u, s))) return st;
+      // a CG preconditioner's last fine-level sweep also sums z . r (r is its right-hand side)
+      const bool dot = want_rz_ && l == 0 && k == post - 1;
+      if ((st = smooth(l, q, rhs(l), buf(l, cur_[l] ^ 1), om, dot ? HFM_INT_DOT_RHS : 0u, s,
+                       dot ? m_->partials : nullptr, dot ? &nblk_rz_ : nullptr)))
+        return st;
       cur_[l] ^= 1;
     }
     return HFM_OK;
@@ -895,13 +899,22 @@ class Engine : public EngineBase {
       k_to_storage<T><<<ib, 256, 0, s>>>(r, rhs(0), it, m_->active, m_->state, scaled);
       HFM_CHECK_LAUNCH("k_to_storage");
     }
-    if ((st = vcycle(0, true, m_->cfg.cycle == HFM_CYCLE_F, 0, s))) return st;
+    // bf16 refinement: r . z comes from the cycle's last sweep (z . the bf16 copy of r)
+    want_rz_ = fused_rhs();
+    nblk_rz_ = 0;
+    st = vcycle(0, true, m_->cfg.cycle == HFM_CYCLE_F, 0, s);
+    want_rz_ = false;
+    if (st) return st;
     const T *z = buf(0, cur_[0]);
     // rz_new = r . z ; p = z + beta p
-    k_dot_partials<T><<<ib, 256, 0, s>>>(r, z, it, m_->partials, m_->active, m_->state, scaled,
-                                         m_->gscale);
-    HFM_CHECK_LAUNCH("k_dot_partials");
-    k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 0, m_->scal);
+    if (nblk_rz_ > 0) {
+      k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, nblk_rz_, m_->state, m_->active, 0, m_->scal);
+    } else {
+      k_dot_partials<T><<<ib, 256, 0, s>>>(r, z, it, m_->partials, m_->active, m_->state, scaled,
+                                           m_->gscale);
+      HFM_CHECK_LAUNCH("k_dot_partials");
+      k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 0, m_->scal);
+    }
     k_cg_p<T><<<ib, 256, 0, s>>>(z, p, it, m_->state, m_->scal, m_->active, scaled, m_->gscale);
     HFM_CHECK_LAUNCH("k_cg_p");
     // q = A p with the partial sums of p . q in the same pass (float32 operator on the fine
@@ -1198,6 +1211,8 @@ class Engine : public EngineBase {
   hfm_mg *m_;
   int cur_[kMaxLevels] = {0};
   int fused_l0_ = -1;  // first level of the fused coarse V-cycle, -1: none
+  bool want_rz_ = false;  // the next fine-level post-sweep sums z . r into the partials
+  int nblk_rz_ = 0;       // partials per slot it wrote (0: none)
 };
 
 }  // namespace hfm

@@ -94,6 +94,7 @@ template <class T> struct FastArgs {
   int zero_xend_out;  // output: residual = 0 on x = X-1 (NS residual)
   int top_copy;
   int dot_phi;        // partials of res * phi instead of res^2 (RESID)
+  int dot_rhs;        // partials of out * rhs (SMOOTH)
 };
 
 template <class T, int CORR>
@@ -293,6 +294,10 @@ __global__ void __launch_bounds__(kFastThreads)
       if (MODE == M_SMOOTH) {
 #pragma unroll
         for (int e = 0; e < 4; ++e) res[r].v[e] = pc[r].v[e] + a.omega * __fdividef(f.v[e] - Ax.v[e], dg.v[e]);
+        if (a.dot_rhs && in) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) acc += (double)res[r].v[e] * f.v[e];
+        }
       } else {
 #pragma unroll
         for (int e = 0; e < 4; ++e) res[r].v[e] = Ax.v[e] - f.v[e];
@@ -328,7 +333,7 @@ __global__ void __launch_bounds__(kFastThreads)
       }
     }
   }
-  if (MODE != M_SMOOTH && a.partials) {
+  if ((MODE != M_SMOOTH || a.dot_rhs) && a.partials) {
     double t = block_reduce(acc);
     if (threadIdx.x == 0) a.partials[inst * (gridDim.x * gridDim.y) + blockIdx.y * gridDim.x + blockIdx.x] = t;
   }
@@ -408,6 +413,10 @@ __global__ void __launch_bounds__(kFastThreads)
     if (MODE == M_SMOOTH) {
 #pragma unroll
       for (int e = 0; e < 4; ++e) res.v[e] = cen_cur.v[e] + a.omega * __fdividef(f.v[e] - Ax.v[e], diag);
+      if (a.dot_rhs && valid) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc2 += (double)res.v[e] * f.v[e];
+      }
     } else {
 #pragma unroll
       for (int e = 0; e < 4; ++e) res.v[e] = Ax.v[e] - f.v[e];
@@ -428,7 +437,7 @@ __global__ void __launch_bounds__(kFastThreads)
     }
     cen_cur = cen_next;
   }
-  if (MODE != M_SMOOTH && a.partials) {
+  if ((MODE != M_SMOOTH || a.dot_rhs) && a.partials) {
     double t = block_reduce(acc2);
     if (threadIdx.x == 0) a.partials[inst * (gridDim.x * gridDim.y) + blockIdx.y * gridDim.x + blockIdx.x] = t;
   }
@@ -489,6 +498,7 @@ int fast_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const
   a.zero_xend_out = (mode != M_SMOOTH && (flags & HFM_FLAG_ZERO_XEND)) ? 1 : 0;
   a.top_copy = (mode == M_SMOOTH && (flags & HFM_FLAG_TOP_COPY)) ? 1 : 0;
   a.dot_phi = (mode == M_RESID && (flags & HFM_INT_DOT_PHI)) ? 1 : 0;
+  a.dot_rhs = (mode == M_SMOOTH && (flags & HFM_INT_DOT_RHS) && partials) ? 1 : 0;
   a.zc = 0;
   if (phi.base && phi.base_stride != stride) return fail(HFM_ERR_BAD_ARG, "fast path: stride mismatch");
   const int corr = phi.corr ? (phi.corr_coarse ? C_COARSE : C_SAME) : C_NONE;

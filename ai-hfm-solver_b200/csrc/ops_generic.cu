@@ -38,10 +38,12 @@ template <int KIND, class T>
 __global__ void __launch_bounds__(kThreads)
     k_smooth(DevOp op, PhiSrc<T> phi, const T *__restrict__ rhs, int64_t rhs_stride,
              T *__restrict__ out, int64_t out_stride, int Z, int Y, int X, float omega,
-             unsigned flags, const int *__restrict__ active) {
+             unsigned flags, const int *__restrict__ active, double *__restrict__ partials) {
+  __shared__ double sh[32];
   const int64_t inst = blockIdx.y;
   if (active && !active[inst]) return;
   const int64_t n = (int64_t)Z * Y * X;
+  double acc = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     int x = (int)(i % X);
@@ -54,7 +56,13 @@ __global__ void __launch_bounds__(kThreads)
     float ax = op_apply_at<KIND, T>(op, phi, inst, z, y, x, Z, Y, X, &diag);
     float pc = phi(inst, z, y, x, Y, X);
     float f = rhs ? St<T>::ld(rhs + inst * rhs_stride + ((int64_t)z * Y + y) * X + x) : 0.f;
-    out[inst * out_stride + i] = St<T>::from(pc + omega * (f - ax) / diag);
+    const float v = pc + omega * (f - ax) / diag;
+    out[inst * out_stride + i] = St<T>::from(v);
+    acc += (double)v * f;
+  }
+  if (partials) {
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) partials[inst * gridDim.x + blockIdx.x] = acc;
   }
 }
 
@@ -240,22 +248,26 @@ int64_t max_partial_blocks(Grid3 g, int B) {
 template <class T>
 int launch_smooth(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
                   int64_t rhs_stride, T *out, int64_t out_stride, int B, Grid3 g, float omega,
-                  unsigned flags, const int *active, cudaStream_t s) {
+                  unsigned flags, const int *active, cudaStream_t s, double *partials,
+                  int *nblk_out) {
+  if (!(flags & HFM_INT_DOT_RHS)) partials = nullptr;
   if ((!phi.base || phi.base_stride == out_stride) && (phi.base || phi.corr || rhs) &&
       (!rhs || rhs_stride == out_stride) &&
       tma_eligible(kind, g, FAST_SMOOTH, phi.corr, phi.corr_coarse, (int)sizeof(T)) &&
       vec_aligned<T>(kind, op, phi, rhs, out, nullptr, out_stride, 16))
     return tma_launch<T>(kind, FAST_SMOOTH, op, phi, rhs, out, nullptr, out_stride, 0, B, g,
-                         omega, flags, active, nullptr, nullptr, s);
+                         omega, flags, active, partials, nblk_out, s);
   if (fast_eligible(kind, g, false) && (!rhs || rhs_stride == out_stride) &&
       (!phi.base || phi.base_stride == out_stride) && (!phi.corr || phi.corr_coarse || phi.corr_stride == out_stride) &&
       vec_aligned<T>(kind, op, phi, rhs, out, nullptr, out_stride, 4 * (int64_t)sizeof(T)))
     return fast_launch<T>(kind, FAST_SMOOTH, op, phi, rhs, out, nullptr, out_stride, 0, B, g,
-                          omega, flags, active, nullptr, nullptr, s);
-  dim3 grid(blocks_for(g.n(), B), B);
+                          omega, flags, active, partials, nblk_out, s);
+  const int nb = blocks_for(g.n(), B);
+  if (nblk_out) *nblk_out = nb;
+  dim3 grid(nb, B);
   HFM_DISPATCH_KIND(kind, (k_smooth<K_, T><<<grid, kThreads, 0, s>>>(
                               op, phi, rhs, rhs_stride, out, out_stride, g.Z, g.Y, g.X, omega,
-                              flags, active)));
+                              flags, active, partials)));
   HFM_CHECK_LAUNCH("k_smooth");
   return HFM_OK;
 }
@@ -361,7 +373,7 @@ int launch_coarse_jacobi(int kind, const DevOp &op, const T *rhs, int64_t rhs_st
 #define HFM_INST(T)                                                                         \
   template int launch_smooth<T>(int, const DevOp &, const PhiSrc<T> &, const T *, int64_t,  \
                                 T *, int64_t, int, Grid3, float, unsigned, const int *,     \
-                                cudaStream_t);                                              \
+                                cudaStream_t, double *, int *);                             \
   template int launch_residual<T>(int, const DevOp &, const PhiSrc<T> &, const T *,         \
                                   int64_t, T *, int64_t, int, Grid3, unsigned, const int *, \
                                   double *, int *, cudaStream_t);                           \

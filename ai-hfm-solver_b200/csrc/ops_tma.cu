@@ -77,7 +77,7 @@ template <class T> struct TmaArgs {
   int64_t stride, coarse_stride;
   int Z, Y, X, zc, tiles_x;
   float omega, corr_sign;
-  int has_phi, has_f, has_sigma, zero_xend, zero_xend_out, top_copy, dot_phi;
+  int has_phi, has_f, has_sigma, zero_xend, zero_xend_out, top_copy, dot_phi, dot_rhs;
   unsigned stage_bytes;
 };
 
@@ -437,6 +437,10 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
         res[e] = v.x;
         res[e + 1] = v.y;
       }
+      if (a.dot_rhs && valid) {
+#pragma unroll
+        for (int e = 0; e < V; ++e) acc += (double)res[e] * f[e];
+      }
     } else {
 #pragma unroll
       for (int e = 0; e < V; ++e) res[e] = Ax[e] - f[e];
@@ -480,7 +484,7 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
       for (int p = p_waited + 1; p < p_next; ++p) wait_plane(p);
     return;
   }
-  if (MODE != M_SMOOTH && a.partials) {
+  if ((MODE != M_SMOOTH || a.dot_rhs) && a.partials) {
     double t = block_sum(acc);
     if (tid == 0) a.partials[inst * (gridDim.x * gridDim.y) + blockIdx.y * gridDim.x + blockIdx.x] = t;
   }
@@ -610,6 +614,7 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
   a.zero_xend_out = (mode != M_SMOOTH && (flags & HFM_FLAG_ZERO_XEND)) ? 1 : 0;
   a.top_copy = (mode == M_SMOOTH && (flags & HFM_FLAG_TOP_COPY)) ? 1 : 0;
   a.dot_phi = (mode == M_RESID && (flags & HFM_INT_DOT_PHI)) ? 1 : 0;
+  a.dot_rhs = (mode == M_SMOOTH && (flags & HFM_INT_DOT_RHS) && partials) ? 1 : 0;
   a.tiles_x = (g.X + TX - 1) / TX;
   const int tiles = a.tiles_x * ((g.Y + TY - 1) / TY);
   // z chunks: about 3 resident blocks per SM and four waves; chunks of at least 2 planes
