@@ -446,15 +446,15 @@ __global__ void k_fetch_all(const T *__restrict__ b0, const T *__restrict__ b1,
 }
 
 // ----------------------------------------------------------------- CG vector kernels
-// Scale of the preconditioner input for 16-bit storage: the cycle solves for r / s with
-// s = RMS(r), so its fields stay O(1) in bf16 / fp16 whatever the residual's size; z = s M(r/s).
-// scaled = 0: none (float32 / bf16: the exponent range of float32); 2: fp16 - the cycle
-// solves for r / |r|_2 (entries <= 1) with conductivities divided by their geometric mean
-// g, so z = (|r|_2 / g) M'(r / |r|_2).  pc_in is the divisor of the input, pc_out the factor
-// of the output.
+// Scale of the preconditioner input for fp16 storage.  scaled = 0: none (float32 / bf16 have
+// the exponent range of float32); 2: fp16 - the cycle solves for r / s with s = RMS(r) =
+// |r|_2 / sqrt(n), with conductivities divided by their geometric mean g, so
+// z = (s / g) M'(r / s).  Entries of r / s are O(1) and at most sqrt(n) (a single spike), well
+// inside fp16's range on both sides: normalising by |r|_2 instead pushed typical entries of a
+// 256^3 residual (~1 / sqrt(n)) into fp16's subnormal range, and the refinement stalled near
+// 1e-9.  pc_in is the divisor of the input, pc_out the factor of the output.
 __device__ __forceinline__ float pc_in(const SlotState &s, int64_t n, int scaled) {
-  (void)n;
-  return (scaled == 2 && s.rr > 0.0) ? (float)sqrt(s.rr) : 1.f;
+  return (scaled == 2 && s.rr > 0.0) ? (float)sqrt(s.rr / (double)n) : 1.f;
 }
 __device__ __forceinline__ float pc_out(const SlotState &s, int64_t n, int scaled,
                                         const double *gscale, int64_t slot) {
