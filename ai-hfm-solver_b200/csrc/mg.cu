@@ -512,8 +512,15 @@ __global__ void k_dot_partials(const float *__restrict__ a, const TZ *__restrict
   HFM_FOR_ITEMS(it, active[slot])
   const double zs = st ? pc_out(st[slot], it.n, scaled, gscale, slot) : 1.0;
   double acc = 0.0;
-  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
-    acc += (double)a[base + i] * (double)St<TZ>::ld(b + base + i);
+  if (v4) {
+    for (int64_t i = lo + 4 * threadIdx.x; i < hi; i += 4 * blockDim.x) {
+      const float4 av = ld4v<float>(a + base + i), bv = ld4v<TZ>(b + base + i);
+      acc += (double)av.x * bv.x + (double)av.y * bv.y + (double)av.z * bv.z + (double)av.w * bv.w;
+    }
+  } else {
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
+      acc += (double)a[base + i] * (double)St<TZ>::ld(b + base + i);
+  }
   const double t = block_reduce_sum(acc * zs);
   if (threadIdx.x == 0) partials[(int64_t)slot * it.CH + ch] = t;
   HFM_END_ITEMS
@@ -623,8 +630,15 @@ __global__ void k_to_storage(const float *__restrict__ a, T *__restrict__ b, Ite
                              const int *active, const SlotState *st, int scaled) {
   HFM_FOR_ITEMS(it, active[slot])
   const float inv = 1.f / pc_in(st[slot], it.n, scaled);
-  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
-    b[base + i] = St<T>::from(a[base + i] * inv);
+  if (v4) {
+    for (int64_t i = lo + 4 * threadIdx.x; i < hi; i += 4 * blockDim.x) {
+      const float4 v = ld4v<float>(a + base + i);
+      st4v<T>(b + base + i, make_float4(v.x * inv, v.y * inv, v.z * inv, v.w * inv));
+    }
+  } else {
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
+      b[base + i] = St<T>::from(a[base + i] * inv);
+  }
   HFM_END_ITEMS
 }
 
@@ -972,8 +986,9 @@ class Engine : public EngineBase {
       k_to_storage<T><<<ib, 256, 0, s>>>(r, rhs(0), it, m_->active, m_->state, scaled);
       HFM_CHECK_LAUNCH("k_to_storage");
     }
-    // bf16 refinement: r . z comes from the cycle's last sweep (z . the bf16 copy of r)
-    want_rz_ = fused_rhs();
+    // r . z comes from the cycle's last fine-level sweep, whose right-hand side is r itself
+    // (float32 storage: rhs(0) is the CG residual) or its bf16 copy (bf16 refinement)
+    want_rz_ = fused_rhs() || std::is_same<T, float>::value;
     nblk_rz_ = 0;
     st = vcycle(0, true, m_->cfg.cycle == HFM_CYCLE_F, 0, s);
     want_rz_ = false;
