@@ -265,6 +265,12 @@ template <class T> struct SubArgs {
 size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size);
 template <class T> int launch_subcycle(SubArgs<T> a, int B, cudaStream_t s);
 
+// The first two Jacobi sweeps from a zero iterate in one pass (SIGMA7, TMA-eligible grids):
+// out = J(phi1) with phi1 = omega f * invd, invd = 1 / diag of the level.
+template <class T>
+int tma_launch_pre2(const DevOp &op, const T *f, const T *invd, T *out, int64_t stride, int B,
+                    Grid3 g, float omega, const int *active, cudaStream_t s);
+
 // Upper bound of blocks per instance of any residual launch on grid g (partials sizing).
 int64_t max_partial_blocks(Grid3 g, int B);
 

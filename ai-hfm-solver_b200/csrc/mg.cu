@@ -489,6 +489,32 @@ __global__ void k_fetch_all(const T *__restrict__ b0, const T *__restrict__ b1,
     out[o + i] = bx ? bx[o + i] : St<T>::to(which ? b1[o + i] : b0[o + i]);
 }
 
+// 1 / diagonal of a SIGMA7 level (faces c_d (s_i + s_j) / 2, wall faces c_d s_i), for cells
+// [0, total) of consecutive instances of n = Z Y X cells each.
+template <class T>
+__global__ void k_invdiag(const T *__restrict__ sx, const T *__restrict__ sy,
+                          const T *__restrict__ sz, float cz, float cy, float cx, int Z, int Y,
+                          int X, int64_t total, T *__restrict__ out) {
+  const int64_t n = (int64_t)Z * Y * X;
+  const float hz = 0.5f * cz, hy = 0.5f * cy, hx = 0.5f * cx;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = k % n;
+    const int x = (int)(i % X);
+    const int64_t t = i / X;
+    const int y = (int)(t % Y), z = (int)(t / Y);
+    const float vx = St<T>::to(sx[k]), vy = St<T>::to(sy[k]), vz = St<T>::to(sz[k]);
+    const float axm = x > 0 ? hx * (vx + St<T>::to(sx[k - 1])) : cx * vx;
+    const float axp = x < X - 1 ? hx * (vx + St<T>::to(sx[k + 1])) : cx * vx;
+    const float aym = y > 0 ? hy * (vy + St<T>::to(sy[k - X])) : cy * vy;
+    const float ayp = y < Y - 1 ? hy * (vy + St<T>::to(sy[k + X])) : cy * vy;
+    const int64_t P = (int64_t)X * Y;
+    const float azm = z > 0 ? hz * (vz + St<T>::to(sz[k - P])) : cz * vz;
+    const float azp = z < Z - 1 ? hz * (vz + St<T>::to(sz[k + P])) : cz * vz;
+    out[k] = St<T>::from(1.f / (((axm + axp) + (aym + ayp)) + (azm + azp)));
+  }
+}
+
 // ----------------------------------------------------------------- CG vector kernels
 // Scale of the preconditioner input for fp16 storage.  scaled = 0: none (float32 / bf16 have
 // the exponent range of float32); 2: fp16 - the cycle solves for r / s with s = RMS(r) =
@@ -668,6 +694,7 @@ struct Level {
   int64_t n;
   void *phi = nullptr, *tmp = nullptr, *rhs = nullptr;
   void *coef[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void *invd = nullptr;  // SIGMA7: 1 / diagonal of the level's operator (two-sweep pass)
   DevOp op;
 };
 
@@ -788,6 +815,18 @@ class Engine : public EngineBase {
   }
 
   // Approximately solve A_l phi = rhs(l); `zero` says the current iterate is zero.
+  // The fused first two sweeps run on the TMA path: SIGMA7 levels the TMA kernels take.
+  bool pre2_ok(int l) {
+    if (kind() != HFM_OP_SIGMA7 || !m_->lv[l].invd || (m_->cfg.options & HFM_OPT_NO_FUSED_PRE))
+      return false;
+    if (!tma_eligible(HFM_OP_SIGMA7, g(l), FAST_SMOOTH, nullptr, 0, (int)sizeof(T))) return false;
+    PhiSrc<T> p = src(rhs(l), n(l));
+    return vec_aligned<T>(HFM_OP_SIGMA7, m_->lv[l].op, p, m_->lv[l].invd, buf(l, 0), nullptr,
+                          n(l), 16) &&
+           vec_aligned<T>(HFM_OP_SIGMA7, m_->lv[l].op, p, m_->lv[l].invd, buf(l, 1), nullptr,
+                          n(l), 16);
+  }
+
   // First level of the fused coarse V-cycle (subcycle.cu), or -1: the deepest levels of at
   // most 4096 cells of a SIGMA7 hierarchy, at least two of them, below the fine level.
   int fused_first_level() {
@@ -843,7 +882,17 @@ class Engine : public EngineBase {
     // NS outflow rule on the fine level (as the reference cycle applies it): the iterate is
     // read as zero on x = X-1 and the residual is zero there
     const int xend = (l == 0 && (c.flags & HFM_FLAG_ZERO_XEND)) ? 1 : 0;
-    for (int k = 0; k < c.nu_pre; ++k) {
+    int k0 = 0;
+    if (zero && c.nu_pre >= 2 && !xend && pre2_ok(l)) {
+      // the first two sweeps from zero in one pass (phi1 = omega f / diag is pointwise)
+      if ((st = tma_launch_pre2<T>(m_->lv[l].op, rhs(l), (const T *)m_->lv[l].invd,
+                                   buf(l, cur_[l] ^ 1), n(l), m_->slots, g(l), c.omega,
+                                   m_->active, s)))
+        return st;
+      cur_[l] ^= 1;
+      k0 = 2;
+    }
+    for (int k = k0; k < c.nu_pre; ++k) {
       PhiSrc<T> p = src((zero && k == 0) ? nullptr : buf(l, cur_[l]), n(l));
       p.zero_xend = xend;
       if ((st = smooth(l, p, rhs(l), buf(l, cur_[l] ^ 1), c.omega, 0u, s))) return st;
@@ -1116,6 +1165,16 @@ class Engine : public EngineBase {
     fine32_ = m_->lv[0].op;
     if (fine32_coef_[0])
       for (int a = 0; a < 3; ++a) fine32_.coef[a] = fine32_coef_[a];
+    // 1 / diagonal per level, for the fused first two sweeps of a cycle
+    for (int l = 0; l < m_->L; ++l) {
+      const DevOp &op = m_->lv[l].op;
+      const int64_t nl = n(l);
+      k_invdiag<T><<<vec_blocks(nl * cnt, 1), 256, 0, s>>>(
+          (const T *)op.coef[0] + lo * nl, (const T *)op.coef[1] + lo * nl,
+          (const T *)op.coef[2] + lo * nl, op.c[0] * op.scale, op.c[1] * op.scale,
+          op.c[2] * op.scale, g(l).Z, g(l).Y, g(l).X, nl * cnt, (T *)m_->lv[l].invd + lo * nl);
+      HFM_CHECK_LAUNCH("k_invdiag");
+    }
     return HFM_OK;
   }
 
@@ -1401,7 +1460,7 @@ size_t hfm_mg_footprint_bytes(const hfm_mg_config *c, int Z, int Y, int X, int s
   size_t tot = 0;
   for (size_t l = 0; l < lv.size(); ++l) {
     size_t nl = (size_t)lv[l].n();
-    size_t fields = 3 + (c->op_kind == HFM_OP_SIGMA7 ? 3 : 0) + (c->op_kind == HFM_OP_DIR7 ? 7 : 0);
+    size_t fields = 3 + (c->op_kind == HFM_OP_SIGMA7 ? 4 : 0) + (c->op_kind == HFM_OP_DIR7 ? 7 : 0);
     tot += nl * fields * es;
   }
   const size_t nf = (size_t)Z * Y * X;
@@ -1450,8 +1509,10 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
     // float32 CG: the fine-level cycle reads the CG residual in place (set below)
     if (!(l == 0 && cfg->accel != HFM_ACCEL_NONE && cfg->storage == HFM_F32))
       L.rhs = dalloc(m.get(), b, &st);
-    if (cfg->op_kind == HFM_OP_SIGMA7)
+    if (cfg->op_kind == HFM_OP_SIGMA7) {
       for (int a = 0; a < 3; ++a) L.coef[a] = dalloc(m.get(), b, &st);
+      L.invd = dalloc(m.get(), b, &st);
+    }
     if (cfg->op_kind == HFM_OP_DIR7)
       for (int a = 0; a < 7; ++a) L.coef[a] = dalloc(m.get(), b, &st);
   }

@@ -33,11 +33,14 @@ namespace {
 constexpr int TX = 64;
 constexpr int kMaxSpin = 1 << 20;
 
-enum { M_SMOOTH = FAST_SMOOTH, M_RESID = FAST_RESID, M_RESTRICT = FAST_RESTRICT };
+// M_PRE2: the first two Jacobi sweeps from a zero iterate in one pass.  The first sweep is
+// pointwise, phi1 = omega f / diag, so the kernel loads f and 1/diag with the phi halos and
+// forms phi1 on the fly where the second sweep reads phi.
+enum { M_SMOOTH = FAST_SMOOTH, M_RESID = FAST_RESID, M_RESTRICT = FAST_RESTRICT, M_PRE2 = 3 };
 
 // Stage layout for storage T; SIG: the stage carries the three conductivity tiles, CC: the
 // coarse correction tile (stages of the other kernels are smaller, so more blocks fit).
-template <class T, bool SIG = true, bool CC = true> struct Geo {
+template <class T, bool SIG = true, bool CC = true, bool DS = false> struct Geo {
   // 8 rows x 64 columns per block for float32, 16 rows for 16-bit storage (same bytes per
   // stage); a thread owns 16 bytes of x: 4 float32 / 8 16-bit values, so 16 / 8 threads per
   // row and 128 threads per block either way
@@ -64,11 +67,12 @@ template <class T, bool SIG = true, bool CC = true> struct Geo {
   static constexpr int O_SZ = O_SY + (SIG ? al(SYN) : 0);
   static constexpr int O_F = O_SZ + (SIG ? al(SZN) : 0);
   static constexpr int O_CC = O_F + al(FN);
-  static constexpr int STAGE = O_CC + (CC ? al(CCN) : 0);
+  static constexpr int O_DS = O_CC + (CC ? al(CCN) : 0);  // 1 / diag with the phi halos (M_PRE2)
+  static constexpr int STAGE = O_DS + (DS ? al(PHI) : 0);
 };
 
 template <class T> struct TmaArgs {
-  CUtensorMap m_phi, m_sx, m_sy, m_sz, m_f, m_cc;
+  CUtensorMap m_phi, m_sx, m_sy, m_sz, m_f, m_cc, m_ds;
   DevOp op;
   T *out;
   T *coarse;
@@ -179,10 +183,10 @@ template <class T, int N> __device__ __forceinline__ void vst(T *p, const float 
 }
 
 // Issue the loads of plane p (may lie outside [0, Z): the TMA unit zero-fills) into `stage`.
-template <class T, int CORR, bool SIG>
+template <class T, int CORR, bool SIG, bool DS = false>
 __device__ __forceinline__ void issue_plane(const TmaArgs<T> &a, char *stage, uint32_t bar, int p,
                                             int x0, int y0, int b) {
-  using G = Geo<T, SIG, CORR != 0>;
+  using G = Geo<T, SIG, CORR != 0, DS>;
   constexpr int TY = G::TY;
   (void)TY;
   mbar_expect(bar, a.stage_bytes);
@@ -194,6 +198,7 @@ __device__ __forceinline__ void issue_plane(const TmaArgs<T> &a, char *stage, ui
   }
   if (a.has_f) tma_load(smem_u32(stage + G::O_F), &a.m_f, x0, y0, p, b, bar);
   if (CORR) tma_load(smem_u32(stage + G::O_CC), &a.m_cc, (x0 >> 1) - G::HX, (y0 >> 1) - 1, p >> 1, b, bar);
+  if (DS) tma_load(smem_u32(stage + G::O_DS), &a.m_ds, x0 - G::HX, y0 - 1, p, b, bar);
 }
 
 __device__ __forceinline__ double block_sum(double v) {
@@ -210,7 +215,8 @@ __device__ __forceinline__ double block_sum(double v) {
 template <int KIND, class T, int MODE, int CORR>
 __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __grid_constant__ TmaArgs<T> a) {
   constexpr bool SIG = KIND == HFM_OP_SIGMA7;
-  using G = Geo<T, SIG, CORR != 0>;
+  constexpr bool PRE2 = MODE == M_PRE2;
+  using G = Geo<T, SIG, CORR != 0, PRE2>;
   constexpr int TY = G::TY, V = G::VEC, NS = G::NS;
   extern __shared__ __align__(128) char smem[];
   __shared__ __align__(8) uint64_t bars[NS];
@@ -240,7 +246,7 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
   if (tid == 0) {
     for (; p_next <= p_last && p_next < p_first + NS; ++p_next) {
       const int q = p_next - p_first;
-      issue_plane<T, CORR, SIG>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
+      issue_plane<T, CORR, SIG, PRE2>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
     }
   }
   int p_waited = p_first - 1;  // last plane whose loads completed
@@ -265,6 +271,9 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
   // phi' at tile coordinates (ry, rx) of plane stage st (global y0-1+ry, x0-HX+rx)
   auto phiv = [&](const char *st, int ry, int rx) -> float {
     const T *ph = reinterpret_cast<const T *>(st + G::O_PHI);
+    if (PRE2)  // phi1 = omega f / diag
+      return a.omega * sld<T>(ph + ry * G::PW + rx) *
+             sld<T>(reinterpret_cast<const T *>(st + G::O_DS) + ry * G::PW + rx);
     float v = a.has_phi ? sld<T>(ph + ry * G::PW + rx) : 0.f;
     if (CORR) {
       const int yy = y0 - 1 + ry, xx = x0 - G::HX + rx;
@@ -278,6 +287,14 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
   // the thread's V values of phi' on tile row ry
   auto phiV = [&](const char *st, int ry, float (&v)[V]) {
     const int rx = G::HX + V * c;
+    if (PRE2) {
+      float d[V];
+      vld<T, V>(reinterpret_cast<const T *>(st + G::O_PHI) + ry * G::PW + rx, v);
+      vld<T, V>(reinterpret_cast<const T *>(st + G::O_DS) + ry * G::PW + rx, d);
+#pragma unroll
+      for (int e = 0; e < V; ++e) v[e] = a.omega * v[e] * d[e];
+      return;
+    }
     if (a.has_phi) {
       vld<T, V>(reinterpret_cast<const T *>(st + G::O_PHI) + ry * G::PW + rx, v);
     } else {
@@ -324,7 +341,7 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
     if (tid == 0 && z > z0 && p_next <= p_last) {
       const int q = p_next - p_first;
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_plane<T, CORR, SIG>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
+      issue_plane<T, CORR, SIG, PRE2>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
       ++p_next;
     }
     mine = wait_plane(z + 1);
@@ -421,13 +438,15 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
       }
     }
     float f[V];
-    if (a.has_f) {
+    if (PRE2) {  // f is the phi tile's centre row
+      vld<T, V>(reinterpret_cast<const T *>(sc + G::O_PHI) + (r + 1) * G::PW + G::HX + V * c, f);
+    } else if (a.has_f) {
       vld<T, V>(reinterpret_cast<const T *>(sc + G::O_F) + r * TX + V * c, f);
     } else {
 #pragma unroll
       for (int e = 0; e < V; ++e) f[e] = 0.f;
     }
-    if (MODE == M_SMOOTH) {
+    if (MODE == M_SMOOTH || PRE2) {
       const float2 om = make_float2(a.omega, a.omega), m1 = make_float2(-1.f, -1.f);
 #pragma unroll
       for (int e = 0; e < V; e += 2) {
@@ -533,7 +552,7 @@ int make_map(CUtensorMap *m, const void *ptr, int X, int Y, int Z, int B, int64_
 
 template <int KIND, class T, int MODE, int CORR>
 int go(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
-  using G = Geo<T, KIND == HFM_OP_SIGMA7, CORR != 0>;
+  using G = Geo<T, KIND == HFM_OP_SIGMA7, CORR != 0, MODE == M_PRE2>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   const int smem = G::NS * G::STAGE;
@@ -545,6 +564,23 @@ int go(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
   k_tma<KIND, T, MODE, CORR><<<grid, G::THREADS, smem, s>>>(a);
   HFM_CHECK_LAUNCH("k_tma");
   return HFM_OK;
+}
+
+// Grid (plane tiles, z chunks, instances): z chunks sized for about 3 resident blocks per SM
+// and four waves, at least 2 planes each.
+template <class T>
+dim3 tma_grid(TmaArgs<T> &a, Grid3 g, int B) {
+  constexpr int TY = Geo<T>::TY;
+  a.tiles_x = (g.X + TX - 1) / TX;
+  const int tiles = a.tiles_x * ((g.Y + TY - 1) / TY);
+  const int64_t slots = (int64_t)sm_count() * 3 * 4;
+  int64_t chunks = (slots + (int64_t)tiles * B - 1) / ((int64_t)tiles * B);
+  int zc = (int)((g.Z + chunks - 1) / chunks);
+  if (zc < 2) zc = 2;
+  if (zc & 1) ++zc;
+  if (zc > g.Z) zc = g.Z;
+  a.zc = zc;
+  return dim3(tiles, (g.Z + zc - 1) / zc, B);
 }
 
 }  // namespace
@@ -615,17 +651,7 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
   a.top_copy = (mode == M_SMOOTH && (flags & HFM_FLAG_TOP_COPY)) ? 1 : 0;
   a.dot_phi = (mode == M_RESID && (flags & HFM_INT_DOT_PHI)) ? 1 : 0;
   a.dot_rhs = (mode == M_SMOOTH && (flags & HFM_INT_DOT_RHS) && partials) ? 1 : 0;
-  a.tiles_x = (g.X + TX - 1) / TX;
-  const int tiles = a.tiles_x * ((g.Y + TY - 1) / TY);
-  // z chunks: about 3 resident blocks per SM and four waves; chunks of at least 2 planes
-  const int64_t slots = (int64_t)sm_count() * 3 * 4;
-  int64_t chunks = (slots + (int64_t)tiles * B - 1) / ((int64_t)tiles * B);
-  int zc = (int)((g.Z + chunks - 1) / chunks);
-  if (zc < 2) zc = 2;
-  if (zc & 1) ++zc;
-  if (zc > g.Z) zc = g.Z;
-  a.zc = zc;
-  dim3 grid(tiles, (g.Z + zc - 1) / zc, B);
+  dim3 grid = tma_grid(a, g, B);
   if (nblk_out) *nblk_out = grid.x * grid.y;
 #define HFM_TMA_GO(KIND, MODE, CORR) return go<KIND, T, MODE, CORR>(a, grid, s)
 #define HFM_TMA_MODES(KIND)                                              \
@@ -649,6 +675,34 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
   return fail(HFM_ERR_UNSUPPORTED, "tma path: unsupported combination");
 }
 
+template <class T>
+int tma_launch_pre2(const DevOp &op, const T *f, const T *invd, T *out, int64_t stride, int B,
+                    Grid3 g, float omega, const int *active, cudaStream_t s) {
+  using G = Geo<T, true, false, true>;
+  constexpr int TY = G::TY;
+  TmaArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  int st;
+  if ((st = make_map<T>(&a.m_phi, f, g.X, g.Y, g.Z, B, stride, G::PW, TY + 2))) return st;
+  if ((st = make_map<T>(&a.m_ds, invd, g.X, g.Y, g.Z, B, stride, G::PW, TY + 2))) return st;
+  if ((st = make_map<T>(&a.m_sx, op.coef[0], g.X, g.Y, g.Z, B, op.coef_stride, G::PW, TY))) return st;
+  if ((st = make_map<T>(&a.m_sy, op.coef[1], g.X, g.Y, g.Z, B, op.coef_stride, TX, TY + 2))) return st;
+  if ((st = make_map<T>(&a.m_sz, op.coef[2], g.X, g.Y, g.Z, B, op.coef_stride, TX, TY))) return st;
+  a.has_phi = 1;
+  a.has_sigma = 1;
+  a.stage_bytes = (unsigned)((2 * G::PHI + G::SXN + G::SYN + G::SZN) * sizeof(T));
+  a.op = op;
+  a.out = out;
+  a.active = active;
+  a.stride = stride;
+  a.Z = g.Z;
+  a.Y = g.Y;
+  a.X = g.X;
+  a.omega = omega;
+  dim3 grid = tma_grid(a, g, B);
+  return go<HFM_OP_SIGMA7, T, M_PRE2, 0>(a, grid, s);
+}
+
 #define HFM_TMA_INST(T)                                                                       \
   template int tma_launch<T>(int, int, const DevOp &, const PhiSrc<T> &, const T *, T *, T *, \
                              int64_t, int64_t, int, Grid3, float, unsigned, const int *,      \
@@ -656,6 +710,13 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
 HFM_TMA_INST(float)
 HFM_TMA_INST(__nv_bfloat16)
 HFM_TMA_INST(__half)
+template int tma_launch_pre2<float>(const DevOp &, const float *, const float *, float *, int64_t,
+                                    int, Grid3, float, const int *, cudaStream_t);
+template int tma_launch_pre2<__nv_bfloat16>(const DevOp &, const __nv_bfloat16 *,
+                                            const __nv_bfloat16 *, __nv_bfloat16 *, int64_t, int,
+                                            Grid3, float, const int *, cudaStream_t);
+template int tma_launch_pre2<__half>(const DevOp &, const __half *, const __half *, __half *,
+                                     int64_t, int, Grid3, float, const int *, cudaStream_t);
 
 }  // namespace hfm
 

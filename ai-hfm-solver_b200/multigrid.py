@@ -44,6 +44,7 @@ class SolverConfig:
     inner_tol: float = 1e-6     # "ir": inner CG stops at max(inner_tol ||r0||, 0.3 tol ||b||)
     inner_max_cycles: int = 200
     fused_coarse: bool = True   # deep V-cycle levels (<= 4096 cells) in one fused kernel
+    fused_pre: bool = True      # first two pre-sweeps from zero in one pass (SIGMA7, TMA levels)
 
     @staticmethod
     def reference(n_levels, fine_smooth=True, top_copy=False, zero_xend=False, cycles=1000):
@@ -75,7 +76,8 @@ class SolverConfig:
         c.cycles_per_launch = self.cycles_per_launch
         c.inner_tol = self.inner_tol
         c.inner_max_cycles = self.inner_max_cycles
-        c.options = 0 if self.fused_coarse else L.OPT_NO_FUSED_COARSE
+        c.options = (0 if self.fused_coarse else L.OPT_NO_FUSED_COARSE) | \
+            (0 if self.fused_pre else L.OPT_NO_FUSED_PRE)
         return c
 
 

@@ -347,6 +347,9 @@ typedef struct {
  * levels that otherwise run as one fused kernel (one block per instance, fields in shared
  * memory, for SIGMA7 levels of at most 4096 cells) */
 #define HFM_OPT_NO_FUSED_COARSE 1
+/* options: run the first two pre-smoothing sweeps from zero as two passes instead of one
+ * (by default the pointwise first sweep phi1 = omega f / diag is formed inside the second) */
+#define HFM_OPT_NO_FUSED_PRE 2
 
 typedef struct {
   int active;       /* 1 while the slot is still iterating */

@@ -346,3 +346,25 @@ def test_fused_coarse_cycle_matches_separate_kernels(hfm, T, cycle, storage):
             outs.append([h.fetch(s).cpu().numpy() for s in range(2)])
     close(outs[0][0], outs[1][0], rtol=1e-5 if storage == "f32" else 2e-2)
     np.testing.assert_array_equal(outs[0][0], outs[0][1])
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16", "f16"])
+def test_fused_presmoothing_matches_two_sweeps(hfm, T, storage):
+    """The first two pre-sweeps from zero run as one pass on TMA levels (phi1 = omega f / diag
+    formed where the second sweep reads phi); against two separate sweeps
+    (HFM_OPT_NO_FUSED_PRE) the iterate agrees to float32 rounding (float32 storage) or to the
+    rounding of phi1 that the two-pass path stores (16-bit)."""
+    shape = (32, 48, 64)
+    sig = hfm.problems.anisotropic_sigma(shape, seed=11, log_std=1.0)
+    f = hfm.problems.dipole(shape, seed=11)
+    M = hfm.multigrid
+    outs = []
+    for fused in (True, False):
+        cfg = M.SolverConfig(cycle="V", storage=storage, tol=1e-300, max_cycles=10,
+                             cycles_per_launch=1, fused_pre=fused)
+        with M.Multigrid(shape, hfm._lib.OP_SIGMA7, cfg, slots=1) as h:
+            h.set_operator(hfm.ops.Sigma7(*(dev(T, sig[k]) for k in range(3))))
+            h.load(0, dev(T, f))
+            h.run(2)
+            outs.append(h.fetch(0).cpu().numpy())
+    close(outs[0], outs[1], rtol={"f32": 1e-5, "bf16": 2e-2, "f16": 3e-3}[storage])
