@@ -98,6 +98,9 @@ SIGNATURES = {
     "hfm_ns_bc_velocity": (I, [P, P, P, I, I, I, F, P, P]),
     "hfm_ns_bc_pressure": (I, [P, I, I, I, P, P]),
     "hfm_sigma7_grad_logsigma": (I, [P, P, P, P, P, I, I, I, I, F, F, F, P, P, P, I, P]),
+    "hfm_ns_momentum_pg": (I, [P, P, P, P, P, P, P, P, P, P, P, P, I, I, I, P, P, P, F, P]),
+    "hfm_ns_pg_scratch_bytes": (C.c_size_t, [I, I, I]),
+    "hfm_ns_pg_dissipation": (I, [P, P, P, P, P, P, P, I, I, I, P, P, P, P, F, F, P, P]),
     # 2D operators and the Kolmogorov-flow stepper
     "hfm_conv2d_k3": (I, [P, P, I, I, I, P, U, P]),
     "hfm_restrict_avg2d": (I, [I, P, P, I, I, I, P]),

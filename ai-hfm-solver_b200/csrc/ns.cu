@@ -26,13 +26,15 @@ __device__ __forceinline__ float at(const float *f, int z, int y, int x, int Z, 
 
 // out_f = base_f + coef * (Dif(a_f) - a_u Dx(a_f) - a_v Dy(a_f) - a_w Dz(a_f)), f in {u, v, w}
 // (naiver_stokes_3D.py:580-622: stage 1 with a = base = u^n, coef 1/2; stage 2 with a = b,
-// base = u^n, coef 1).
+// base = u^n, coef 1).  With ex / ey / ez (and a zero diffusion kernel) the diffusion term is
+// the given field instead: the Petrov-Galerkin form of INHALE_demo.ipynb cell 24.
 __global__ void __launch_bounds__(256)
     k_momentum(const float *__restrict__ au, const float *__restrict__ av,
                const float *__restrict__ aw, const float *__restrict__ bu,
                const float *__restrict__ bv, const float *__restrict__ bw, float *__restrict__ ou,
                float *__restrict__ ov, float *__restrict__ ow, int Z, int Y, int X, K4 K,
-               float coef) {
+               float coef, const float *__restrict__ ex, const float *__restrict__ ey,
+               const float *__restrict__ ez) {
   const int64_t n = (int64_t)Z * Y * X;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -57,8 +59,95 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int q = 0; q < 4; ++q) d[q] += K.k[q][j] * v;
           }
-      const float acc = ((d[0] - uc * d[1]) - vc * d[2]) - wc * d[3];
+      const float *es[3] = {ex, ey, ez};
+      const float d0 = es[f] ? __ldg(es[f] + i) : d[0];
+      const float acc = ((d0 - uc * d[1]) - vc * d[2]) - wc * d[3];
       os[f][i] = coef * acc + __ldg(bs[f] + i);
+    }
+  }
+}
+
+// Petrov-Galerkin dissipation (INHALE_demo.ipynb cell 20), on the velocities damped by the
+// immersed body, u_d = u / (1 + dt sigma).  Pass 1, per component f:
+//   k_f = min(2 |(|u_d| + |v_d| + |w_d|) / 3 * Dif(f_d)| /
+//             (eps + (|Dx f_d| + |Dy f_d| + |Dz f_d|) / 3), 0.5) / (1 + dt sigma)
+__device__ __forceinline__ float damped(const float *f, const float *sg, float dt, int z, int y,
+                                        int x, int Z, int Y, int X) {
+  if (z < 0 || z >= Z || y < 0 || y >= Y || x < 0 || x >= X) return 0.f;
+  const int64_t i = ((int64_t)z * Y + y) * X + x;
+  return __ldg(f + i) / (1.f + dt * __ldg(sg + i));
+}
+
+__global__ void __launch_bounds__(256)
+    k_pg_coef(const float *__restrict__ u, const float *__restrict__ v, const float *__restrict__ w,
+              const float *__restrict__ sg, float *__restrict__ ku, float *__restrict__ kv,
+              float *__restrict__ kw, int Z, int Y, int X, K4 K, float dt, float eps) {
+  const int64_t n = (int64_t)Z * Y * X;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % X);
+    const int64_t t = i / X;
+    const int y = (int)(t % Y), z = (int)(t / Y);
+    const float den = 1.f + dt * __ldg(sg + i);
+    const float speed = (fabsf(__ldg(u + i) / den) + fabsf(__ldg(v + i) / den)) + fabsf(__ldg(w + i) / den);
+    const float *fs[3] = {u, v, w};
+    float *ks[3] = {ku, kv, kw};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int j = 9 * a + 3 * b + c;
+            const float val = damped(fs[f], sg, dt, z + a - 1, y + b - 1, x + c - 1, Z, Y, X);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) d[q] += K.k[q][j] * val;
+          }
+      const float num = 2.f * fabsf(speed / 3.f * d[0]);
+      const float k = num / (eps + ((fabsf(d[1]) + fabsf(d[2])) + fabsf(d[3])) / 3.f);
+      ks[f][i] = fminf(k, 0.5f) / den;
+    }
+  }
+}
+
+// Pass 2: out_f = 1.5 (k_f Dif(f_d) + Dif(f_d k_f) - f_d Dif(k_f)).
+__global__ void __launch_bounds__(256)
+    k_pg_flux(const float *__restrict__ u, const float *__restrict__ v, const float *__restrict__ w,
+              const float *__restrict__ sg, const float *__restrict__ ku,
+              const float *__restrict__ kv, const float *__restrict__ kw, float *__restrict__ ox,
+              float *__restrict__ oy, float *__restrict__ oz, int Z, int Y, int X, K4 K,
+              float dt) {
+  const int64_t n = (int64_t)Z * Y * X;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % X);
+    const int64_t t = i / X;
+    const int y = (int)(t % Y), z = (int)(t / Y);
+    const float *fs[3] = {u, v, w};
+    const float *ks[3] = {ku, kv, kw};
+    float *os[3] = {ox, oy, oz};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      float df = 0.f, dfk = 0.f, dk = 0.f;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const float wgt = K.k[0][9 * a + 3 * b + c];
+            const int zz = z + a - 1, yy = y + b - 1, xx = x + c - 1;
+            const float fv = damped(fs[f], sg, dt, zz, yy, xx, Z, Y, X);
+            const float kv_ = at(ks[f], zz, yy, xx, Z, Y, X);
+            df += wgt * fv;
+            dfk += wgt * (fv * kv_);
+            dk += wgt * kv_;
+          }
+      const float fc = __ldg(fs[f] + i) / (1.f + dt * __ldg(sg + i));
+      os[f][i] = 1.5f * ((__ldg(ks[f] + i) * df + dfk) - fc * dk);
     }
   }
 }
@@ -285,8 +374,64 @@ int hfm_ns_momentum(const float *adv_u, const float *adv_v, const float *adv_w,
   const int64_t n = (int64_t)Z * Y * X;
   k_momentum<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(adv_u, adv_v, adv_w, base_u, base_v,
                                                              base_w, out_u, out_v, out_w, Z, Y, X,
-                                                             K, coef);
+                                                             K, coef, nullptr, nullptr, nullptr);
   HFM_CHECK_LAUNCH("k_momentum");
+  return HFM_OK;
+}
+
+int hfm_ns_momentum_pg(const float *adv_u, const float *adv_v, const float *adv_w,
+                       const float *base_u, const float *base_v, const float *base_w,
+                       float *out_u, float *out_v, float *out_w, const float *k_x,
+                       const float *k_y, const float *k_z, int Z, int Y, int X, const float *w_dx,
+                       const float *w_dy, const float *w_dz, float coef, hfm_stream_t stream) {
+  int st;
+  if ((st = check_ns(Z, Y, X))) return st;
+  if (!adv_u || !adv_v || !adv_w || !base_u || !base_v || !base_w || !out_u || !out_v || !out_w ||
+      !k_x || !k_y || !k_z || !w_dx || !w_dy || !w_dz)
+    return fail(HFM_ERR_BAD_ARG, "hfm_ns_momentum_pg: NULL");
+  if (out_u == adv_u || out_v == adv_v || out_w == adv_w || out_u == adv_v || out_u == adv_w ||
+      out_v == adv_u || out_v == adv_w || out_w == adv_u || out_w == adv_v)
+    return fail(HFM_ERR_BAD_ARG, "hfm_ns_momentum_pg: outputs must not alias the advected fields");
+  K4 K;
+  memset(K.k[0], 0, 27 * 4);
+  memcpy(K.k[1], w_dx, 27 * 4);
+  memcpy(K.k[2], w_dy, 27 * 4);
+  memcpy(K.k[3], w_dz, 27 * 4);
+  const int64_t n = (int64_t)Z * Y * X;
+  k_momentum<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(adv_u, adv_v, adv_w, base_u, base_v,
+                                                             base_w, out_u, out_v, out_w, Z, Y, X,
+                                                             K, coef, k_x, k_y, k_z);
+  HFM_CHECK_LAUNCH("k_momentum");
+  return HFM_OK;
+}
+
+size_t hfm_ns_pg_scratch_bytes(int Z, int Y, int X) {
+  if (Z <= 0 || Y <= 0 || X <= 0) return 0;
+  return (size_t)3 * Z * Y * X * sizeof(float);
+}
+
+int hfm_ns_pg_dissipation(const float *u, const float *v, const float *w, const float *sigma,
+                          float *k_x, float *k_y, float *k_z, int Z, int Y, int X,
+                          const float *w_dif, const float *w_dx, const float *w_dy,
+                          const float *w_dz, float dt, float eps_k, void *scratch,
+                          hfm_stream_t stream) {
+  int st;
+  if ((st = check_ns(Z, Y, X))) return st;
+  if (!u || !v || !w || !sigma || !k_x || !k_y || !k_z || !w_dif || !w_dx || !w_dy || !w_dz || !scratch)
+    return fail(HFM_ERR_BAD_ARG, "hfm_ns_pg_dissipation: NULL");
+  K4 K;
+  memcpy(K.k[0], w_dif, 27 * 4);
+  memcpy(K.k[1], w_dx, 27 * 4);
+  memcpy(K.k[2], w_dy, 27 * 4);
+  memcpy(K.k[3], w_dz, 27 * 4);
+  const int64_t n = (int64_t)Z * Y * X;
+  float *ku = (float *)scratch, *kv = ku + n, *kw = kv + n;
+  k_pg_coef<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(u, v, w, sigma, ku, kv, kw, Z, Y, X, K,
+                                                            dt, eps_k);
+  HFM_CHECK_LAUNCH("k_pg_coef");
+  k_pg_flux<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(u, v, w, sigma, ku, kv, kw, k_x, k_y, k_z,
+                                                            Z, Y, X, K, dt);
+  HFM_CHECK_LAUNCH("k_pg_flux");
   return HFM_OK;
 }
 

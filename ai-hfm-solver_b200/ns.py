@@ -51,6 +51,13 @@ class _Scratch:
             cls.cache[key] = torch.empty(max(nb, 16), dtype=torch.uint8, device=device)
         return cls.cache[key]
 
+    @classmethod
+    def get_bytes(cls, nbytes, device):
+        key = ("bytes", int(nbytes), str(device))
+        if key not in cls.cache:
+            cls.cache[key] = torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=device)
+        return cls.cache[key]
+
 
 def boundary_condition_velocity(u, v, w, ub):
     """In place (naiver_stokes_3D.py:420-447)."""
@@ -79,6 +86,28 @@ def momentum_stage(adv, base, out, Kdif, Kx, Ky, Kz, coef):
     keep = [_w(K) for K in (Kdif, Kx, Ky, Kz)]
     L.call("hfm_ns_momentum", *(_p(t) for t in adv), *(_p(t) for t in base), *(_p(t) for t in out),
            Z, Y, X, *(k[1] for k in keep), float(coef), _stream())
+    return out
+
+
+def momentum_stage_pg(adv, base, out, k, Kx, Ky, Kz, coef):
+    """out = base + coef (k - adv . grad adv_f): the stage of INHALE_demo.ipynb cell 24 with
+    the Petrov-Galerkin terms k = (k_x, k_y, k_z) in place of the diffusion stencil."""
+    Z, Y, X = _shape(adv[0])
+    keep = [_w(K) for K in (Kx, Ky, Kz)]
+    L.call("hfm_ns_momentum_pg", *(_p(t) for t in adv), *(_p(t) for t in base),
+           *(_p(t) for t in out), *(_p(t) for t in k), Z, Y, X, *(kk[1] for kk in keep),
+           float(coef), _stream())
+    return out
+
+
+def pg_dissipation(u, v, w, sigma, out, Kdif, Kx, Ky, Kz, dt, eps_k=1e-3):
+    """Petrov-Galerkin dissipation (INHALE_demo.ipynb cell 20) of u, v, w into out = (k_x, k_y,
+    k_z); eps_k = 1e-3 as the notebook sets it (INH:867)."""
+    Z, Y, X = _shape(u)
+    keep = [_w(K) for K in (Kdif, Kx, Ky, Kz)]
+    scratch = _Scratch.get_bytes(L.lib().hfm_ns_pg_scratch_bytes(Z, Y, X), u.device)
+    L.call("hfm_ns_pg_dissipation", _p(u), _p(v), _p(w), _p(sigma), *(_p(t) for t in out), Z, Y, X,
+           *(kk[1] for kk in keep), float(dt), float(eps_k), _p(scratch), _stream())
     return out
 
 
@@ -115,6 +144,25 @@ def obstacle_mask(shape, n_boxes=24, footprint=(4, 16), height=(8, 40), sigma=1e
     return torch.from_numpy(m).to(device)
 
 
+def mask_from_mesh(mesh, shape, sigma=1e5, offset=16, device="cuda"):
+    """Sigma mask from the reference's geometry array (``naiver_stokes_3D.py:527,560-564``):
+    ``mesh`` has shape (1, X + 2 offset, Y + 2 offset, Z', 1) indexed [0][x + offset]
+    [y + offset][z][0]; an interior cell (1 <= x, y, z <= extent - 2) whose mesh value is 0 is
+    solid and gets ``sigma``, every other cell 0.  Returns a (Z, Y, X) float32 tensor."""
+    Z, Y, X = shape
+    m = np.asarray(mesh)[0, offset:offset + X, offset:offset + Y, :Z, 0]  # (X, Y, Z)
+    solid = np.transpose(m == 0, (2, 1, 0))                               # (Z, Y, X)
+    out = np.zeros(shape, np.float32)
+    inner = (slice(1, Z - 1), slice(1, Y - 1), slice(1, X - 1))
+    out[inner] = np.where(solid[inner], np.float32(sigma), np.float32(0))
+    return torch.from_numpy(out).to(device)
+
+
+def load_mesh_mask(path, shape, sigma=1e5, offset=16, device="cuda"):
+    """``np.load`` of a reference mesh file (e.g. ``mesh_64_sk.npy``) and ``mask_from_mesh``."""
+    return mask_from_mesh(np.load(path), shape, sigma, offset, device)
+
+
 @dataclass
 class NSConfig:
     dt: float = 0.1
@@ -127,6 +175,8 @@ class NSConfig:
     multi_itr: int = 10
     p_tol: float = 1e-5
     n_levels: int = 0           # 0: down to 2^3 (reference form)
+    pg: bool = False            # Petrov-Galerkin dissipation instead of the diffusion stencil
+    eps_k: float = 1e-3         #   (INHALE_demo.ipynb cells 20, 24; eps as INH:867)
 
 
 def laplacian7(scale):
@@ -149,6 +199,7 @@ class NSStepper:
         self.bu, self.bv, self.bw = z(), z(), z()
         self.nu, self.nv, self.nw = z(), z(), z()
         self.rhs = z()
+        self.kx, self.ky, self.kz = (z(), z(), z()) if self.cfg.pg else (None, None, None)
         self.sigma = sigma if sigma is not None else z()
         self.Kdif = (W.diffusion27(c.dt, c.Re, c.dx) if c.diffusion == "27"
                      else laplacian7(c.dt * c.Re / c.dx ** 2))
@@ -196,11 +247,18 @@ class NSStepper:
         u, v, w, p = self.u, self.v, self.w, self.p
         boundary_condition_velocity(u, v, w, c.ub)
         boundary_condition_pressure(p)
-        momentum_stage((u, v, w), (u, v, w), (self.bu, self.bv, self.bw),
-                       self.Kdif, self.Kx, self.Ky, self.Kz, 0.5)
-        boundary_condition_velocity(self.bu, self.bv, self.bw, c.ub)
-        momentum_stage((self.bu, self.bv, self.bw), (u, v, w), (self.nu, self.nv, self.nw),
-                       self.Kdif, self.Kx, self.Ky, self.Kz, 1.0)
+        b, n = (self.bu, self.bv, self.bw), (self.nu, self.nv, self.nw)
+        if c.pg:  # INHALE_demo.ipynb cell 24
+            k = (self.kx, self.ky, self.kz)
+            pg_dissipation(u, v, w, self.sigma, k, self.Kdif, self.Kx, self.Ky, self.Kz, c.dt, c.eps_k)
+            momentum_stage_pg((u, v, w), (u, v, w), b, k, self.Kx, self.Ky, self.Kz, 0.5)
+            boundary_condition_velocity(*b, c.ub)
+            pg_dissipation(*b, self.sigma, k, self.Kdif, self.Kx, self.Ky, self.Kz, c.dt, c.eps_k)
+            momentum_stage_pg(b, (u, v, w), n, k, self.Kx, self.Ky, self.Kz, 1.0)
+        else:
+            momentum_stage((u, v, w), (u, v, w), b, self.Kdif, self.Kx, self.Ky, self.Kz, 0.5)
+            boundary_condition_velocity(*b, c.ub)
+            momentum_stage(b, (u, v, w), n, self.Kdif, self.Kx, self.Ky, self.Kz, 1.0)
         self.u, self.nu = self.nu, self.u
         self.v, self.nv = self.nv, self.v
         self.w, self.nw = self.nw, self.w

@@ -215,6 +215,24 @@ int hfm_ns_momentum(const float *adv_u, const float *adv_v, const float *adv_w,
                     float *out_v, float *out_w, int Z, int Y, int X, const float *w_dif,
                     const float *w_dx, const float *w_dy, const float *w_dz, float coef,
                     hfm_stream_t stream);
+/* The momentum stage of Urban Modelling/INHALE_demo.ipynb cell 24, where the Petrov-Galerkin
+ * dissipation k_f replaces the diffusion stencil: out_f = base_f + coef (k_f - a_u Dx(a_f) -
+ * a_v Dy(a_f) - a_w Dz(a_f)). */
+int hfm_ns_momentum_pg(const float *adv_u, const float *adv_v, const float *adv_w,
+                       const float *base_u, const float *base_v, const float *base_w,
+                       float *out_u, float *out_v, float *out_w, const float *k_x,
+                       const float *k_y, const float *k_z, int Z, int Y, int X, const float *w_dx,
+                       const float *w_dy, const float *w_dz, float coef, hfm_stream_t stream);
+/* Petrov_Galerkin_dissipation of INHALE_demo.ipynb cell 20 on the velocities damped by the
+ * immersed body (u / (1 + dt sigma)): per component k_f = min(2 |(|u|+|v|+|w|)/3 Dif(f)| /
+ * (eps_k + (|Dx f| + |Dy f| + |Dz f|)/3), 0.5) / (1 + dt sigma), then
+ * out_f = 1.5 (k_f Dif(f) + Dif(f k_f) - f Dif(k_f)).  scratch: hfm_ns_pg_scratch_bytes. */
+size_t hfm_ns_pg_scratch_bytes(int Z, int Y, int X);
+int hfm_ns_pg_dissipation(const float *u, const float *v, const float *w, const float *sigma,
+                          float *k_x, float *k_y, float *k_z, int Z, int Y, int X,
+                          const float *w_dif, const float *w_dx, const float *w_dy,
+                          const float *w_dz, float dt, float eps_k, void *scratch,
+                          hfm_stream_t stream);
 /* u -= conv(p, w_px), v -= conv(p, w_py), w -= conv(p, w_pz) (CNN3D_pu/pv/pw, :631-633). */
 int hfm_ns_pressure_gradient(const float *p, float *u, float *v, float *w, int Z, int Y, int X,
                              const float *w_px, const float *w_py, const float *w_pz,

@@ -113,3 +113,35 @@ def step(u, v, w, p, sigma, dt, ub, Kdif, Kx, Ky, Kz, Su, Sv, Sw, Kp, n_levels, 
     u, v, w = bc_velocity(u, v, w, ub)
     u, v, w = bluff_body(u, v, w, sigma, dt)
     return u, v, w, p
+
+
+def pg_dissipation(u, v, w, sigma, dt, eps_k, Kdif, Kx, Ky, Kz):
+    """``Petrov_Galerkin_dissipation`` (``Urban Modelling/INHALE_demo.ipynb`` cell 20), float32
+    in the cell's order: velocities damped by (1 + dt sigma), coefficients k_f clipped at 0.5,
+    then 1.5 (k_f D(f) + D(f k_f) - f D(k_f)) with D the diffusion stencil."""
+    f32 = np.float32
+    c = lambda a, K: tfops.conv3d_same(a, K)
+    den = (f32(1) + f32(dt) * np.asarray(sigma, f32)).astype(f32)
+    u, v, w = (np.asarray(a, f32) / den for a in (u, v, w))
+    speed = (np.abs(u) + np.abs(v)) + np.abs(w)
+    out = []
+    for f in (u, v, w):
+        k = f32(2) * np.abs(speed / f32(3) * c(f, Kdif)) / (
+            f32(eps_k) + ((np.abs(c(f, Kx)) + np.abs(c(f, Ky))) + np.abs(c(f, Kz))) / f32(3))
+        k = np.minimum(k, f32(0.5)) / den
+        out.append(f32(1.5) * ((k * c(f, Kdif) + c(f * k, Kdif)) - f * c(k, Kdif)))
+    return out
+
+
+def momentum_pg(u, v, w, ub, sigma, dt, eps_k, Kdif, Kx, Ky, Kz):
+    """The two-stage momentum update of ``INHALE_demo.ipynb`` cell 24 with Petrov-Galerkin
+    dissipation in place of the diffusion stencil: a = k - u Dx - v Dy - w Dz (stage 1 on u^n,
+    b = u + a / 2, BC(b); stage 2 with k and the advecting velocity from b, u += a(b))."""
+    c = lambda a, K: tfops.conv3d_same(a, K)
+    k = pg_dissipation(u, v, w, sigma, dt, eps_k, Kdif, Kx, Ky, Kz)
+    b = [(0.5 * (((kf - u * c(f, Kx)) - v * c(f, Ky)) - w * c(f, Kz)) + f)
+         for kf, f in zip(k, (u, v, w))]
+    bu, bv, bw = bc_velocity(*b, ub)
+    kb = pg_dissipation(bu, bv, bw, sigma, dt, eps_k, Kdif, Kx, Ky, Kz)
+    return tuple(f + (((kf - bu * c(g, Kx)) - bv * c(g, Ky)) - bw * c(g, Kz))
+                 for kf, f, g in zip(kb, (u, v, w), (bu, bv, bw)))

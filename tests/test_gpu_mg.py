@@ -368,3 +368,20 @@ def test_fused_presmoothing_matches_two_sweeps(hfm, T, storage):
             h.run(2)
             outs.append(h.fetch(0).cpu().numpy())
     close(outs[0], outs[1], rtol={"f32": 1e-5, "bf16": 2e-2, "f16": 3e-3}[storage])
+
+
+def test_sawtooth_aspect_ratio_coarsest(hfm, T):
+    """INHALE_demo.ipynb: flat domains (nz << nx, ny) coarsen to a 1 x r x r coarsest level
+    (INH:13419); here 16 x 64 x 64 -> 1 x 4 x 4 with the NS pressure cycle (27-point w5, no
+    fine-level Jacobi on w, x = X-1 rule), against the oracle."""
+    b = np.zeros((16, 64, 64), np.float32)
+    b[4:12, 20:40, 24:44] = 1.0
+    b -= b.mean()
+    ops = mg.hierarchy(mg.Stencil27(W.w5_pressure27()), 5)
+    ref = np.zeros_like(b)
+    for _ in range(2):
+        ref = mg.sawtooth_cycle(ops, ref, b, fine_smooth=False, zero_xend=True)
+    outs, levels = run_sawtooth(hfm, T, W.w5_pressure27(), b, np.zeros_like(b), 5, 2,
+                                fine_smooth=False, zero_xend=True)
+    assert levels[-1] == (1, 4, 4)
+    close(outs[-1], ref)

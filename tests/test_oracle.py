@@ -233,3 +233,21 @@ def test_periodic_vcycle_contracts():
     p = mg.solve(p, f, 4)
     assert mg.rel_residual(p, f) < 1e-3 * r0
     assert abs(p.mean()) < 1e-12
+
+
+def test_mesh_mask_follows_reference_loop(pkg):
+    """ns.mask_from_mesh against the reference's loop (naiver_stokes_3D.py:560-564) on a
+    synthetic mesh array."""
+    pytest.importorskip("torch")
+    ns = pkg.ns
+    nx, ny, nz = 12, 10, 8
+    rng = np.random.default_rng(4)
+    mesh = (rng.random((1, nx + 32, ny + 32, nz, 1)) > 0.3).astype(np.float64)
+    ref = np.zeros((1, nz, ny, nx, 1))
+    for i in range(1, nx - 1):
+        for j in range(1, ny - 1):
+            for k in range(1, nz - 1):
+                if mesh[0][i + 16][j + 16][k][0] == 0:
+                    ref[0][k][j][i][0] = 100000
+    got = ns.mask_from_mesh(mesh, (nz, ny, nx), device="cpu").numpy()
+    np.testing.assert_array_equal(got, ref[0, ..., 0])
