@@ -1,4 +1,4 @@
-// Operators of the NS time stepper (rows B1-B7 of the hot path): fused two-stage momentum
+// Operators of the NS time stepper: fused two-stage momentum
 // update, pressure-gradient correction, divergence right-hand side with the source boundary
 // rule, sigma-mask immersed body, and the velocity / pressure boundary rules.
 //

@@ -30,6 +30,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -81,7 +82,7 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % os.getpid())
+        self.path = os.path.join(tempfile.gettempdir(), "hfm_bench_clocks_%d.csv" % os.getpid())
 
     def start(self):
         try:
@@ -385,7 +386,10 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         import torch.distributed as dist
-        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+        import datetime
+        # a short timeout: a rank that dies ends the others' next collective with an error
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=datetime.timedelta(seconds=300))
     pkg = ge.load_package()
     if args.workload == "serve":
         out = run_serve(args, pkg, torch, rank, world, local)

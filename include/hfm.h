@@ -42,7 +42,8 @@ typedef enum {
 
 typedef enum { HFM_F32 = 0, HFM_BF16 = 1, HFM_F16 = 2, HFM_F64 = 3 } hfm_dtype;
 
-/* Operator kinds. */
+/* Operator kinds: the reference's constant-coefficient 7-point, per-cell conductivity and
+ * directional forms, and any frozen 3x3x3 kernel. */
 typedef enum {
   HFM_OP_CONST7 = 0, /* anisotropic 7-point, constant coefficients kz, ky, kx (7point.ipynb w2) */
   HFM_OP_SIGMA7 = 1, /* 7-point from per-cell conductivities sx, sy, sz (face means) */
@@ -145,8 +146,8 @@ int hfm_prolong_correct_smooth(const hfm_operator *op, const float *phi,
                                int Z, int Y, int X, float omega, unsigned flags,
                                hfm_stream_t stream);
 
-/* Named wrappers: constant-coefficient 7-point (A1), per-cell sigma 7-point
- * (A2) and 27-point (B1-B4) forms of apply / residual / jacobi. */
+/* Named wrappers: constant-coefficient 7-point, per-cell sigma 7-point
+ * and 27-point forms of apply / residual / jacobi. */
 int hfm_stencil7_const_apply(const float *phi, float *out, int B, int Z, int Y, int X,
                              float kz, float ky, float kx, hfm_stream_t stream);
 int hfm_stencil7_const_residual(const float *phi, const float *b, float *r, int B, int Z,

@@ -1,4 +1,4 @@
-"""Multi-threaded CPU port of the anisotropic multigrid solve (TEST / BASELINE ONLY).
+"""Multi-threaded CPU port of the anisotropic multigrid solve (test and CPU-baseline infrastructure only).
 
 The same discrete operators and the same PCG + V(2,2) weighted-Jacobi algorithm as
 ``oracle.mg`` (whose numpy arithmetic restates the reference's TensorFlow layers), written

@@ -1,4 +1,4 @@
-"""Oracle for the two-dimensional path (TEST / BASELINE ONLY): the reference's Conv2D
+"""Oracle for the two-dimensional path (test and CPU-baseline infrastructure only): the reference's Conv2D
 multigrid and the doubly periodic Kolmogorov-flow stepper built on it.
 
 2D multigrid semantics follow ``Unstructured Mesh/Multigrid_2D.ipynb``: the 3x3 operator is a

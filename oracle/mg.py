@@ -193,7 +193,7 @@ def residual(op, phi, b):
 
 
 # --------------------------------------------------------------------------------------
-# Reference sawtooth cycle (8(a) A8)
+# Reference sawtooth cycle
 # --------------------------------------------------------------------------------------
 def sawtooth_cycle(ops, phi, b, fine_smooth=True, zero_xend=False, top_copy=False,
                    coarse_zero_shape=None, keep=None):
@@ -246,7 +246,7 @@ def sawtooth_cycle(ops, phi, b, fine_smooth=True, zero_xend=False, top_copy=Fals
 
 
 # --------------------------------------------------------------------------------------
-# Textbook cycles used by the solver configurations (8(a) A9)
+# Textbook cycles used by the solver configurations
 # --------------------------------------------------------------------------------------
 class CycleConfig:
     def __init__(self, nu_pre=2, nu_post=2, omega=2.0 / 3.0, coarse_sweeps=32,

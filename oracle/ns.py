@@ -1,4 +1,4 @@
-"""Oracle for the NS time-stepper operators of the reference (TEST / BASELINE ONLY).
+"""Oracle for the NS time-stepper operators of the reference (test and CPU-baseline infrastructure only).
 
 Restates ``Anisotropic Resistivity Tomography/scripts/naiver_stokes_3D.py`` (and the same
 functions of ``Urban Modelling/AI_HFM_v3.ipynb`` cell 19) in NumPy.  Arrays are (Z, Y, X);

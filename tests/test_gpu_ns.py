@@ -1,4 +1,4 @@
-"""NS time-stepper operators (rows B1-B7) on the GPU against the oracle, and a full
+"""NS time-stepper operators on the GPU against the oracle, and a full
 reference time step."""
 import numpy as np
 import pytest
