@@ -1,4 +1,4 @@
-// TMA-pipelined plane-marching stencil kernels for the large levels (X >= 64).
+// TMA-pipelined plane-marching stencil kernels for the large levels (X >= 48).
 //
 // A block owns a TY x TX tile of the (y, x) plane (8 x 64 for float32, 16 x 64 for 16-bit
 // storage) and marches through a chunk of z
@@ -567,7 +567,8 @@ int go(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
 }
 
 // Grid (plane tiles, z chunks, instances): z chunks sized for about 3 resident blocks per SM
-// and four waves, at least 2 planes each.
+// and four waves, at least 2 planes each.  (Eight waves, which shrink the partly filled last
+// wave, measured slower: every chunk re-reads its two halo planes and refills its pipeline.)
 template <class T>
 dim3 tma_grid(TmaArgs<T> &a, Grid3 g, int B) {
   constexpr int TY = Geo<T>::TY;
