@@ -47,6 +47,21 @@ int sm_count() {
   return cache[dev];
 }
 
+int set_max_dynamic_smem(const void *kernel, int bytes, const char *what) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, const void *>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e, what);
+  std::lock_guard<std::mutex> lk(mu);
+  for (const auto &d : done)
+    if (d.first == dev && d.second == kernel) return HFM_OK;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return cuda_status(e, what);
+  done.emplace_back(dev, kernel);
+  return HFM_OK;
+}
+
 DevOp make_devop(const hfm_operator &op, int64_t coef_stride) {
   DevOp d;
   memset(&d, 0, sizeof(d));

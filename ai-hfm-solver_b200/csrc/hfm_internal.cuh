@@ -36,6 +36,9 @@ void set_capturing(bool on);
   } while (0)
 
 int sm_count();  // SMs of the current device (cached per device)
+// Raise a kernel's dynamic shared-memory limit on the current device, once per device and
+// kernel (a process that drives several GPUs needs it on each).
+int set_max_dynamic_smem(const void *kernel, int bytes, const char *what);
 
 // ------------------------------------------------------------------ storage types
 template <class T> struct St;

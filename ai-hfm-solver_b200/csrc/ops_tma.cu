@@ -553,14 +553,10 @@ int make_map(CUtensorMap *m, const void *ptr, int X, int Y, int Z, int B, int64_
 template <int KIND, class T, int MODE, int CORR>
 int go(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
   using G = Geo<T, KIND == HFM_OP_SIGMA7, CORR != 0, MODE == M_PRE2>;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
   const int smem = G::NS * G::STAGE;
-  std::call_once(once, [&] {
-    attr_err = cudaFuncSetAttribute(k_tma<KIND, T, MODE, CORR>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  });
-  if (attr_err != cudaSuccess) return cuda_status(attr_err, "cudaFuncSetAttribute(k_tma)");
+  int st = set_max_dynamic_smem((const void *)k_tma<KIND, T, MODE, CORR>, smem,
+                                "cudaFuncSetAttribute(k_tma)");
+  if (st) return st;
   k_tma<KIND, T, MODE, CORR><<<grid, G::THREADS, smem, s>>>(a);
   HFM_CHECK_LAUNCH("k_tma");
   return HFM_OK;

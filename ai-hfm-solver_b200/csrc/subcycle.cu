@@ -188,9 +188,9 @@ int launch_subcycle(SubArgs<T> a, int B, cudaStream_t s) {
     soff += 3 * n[l];
   }
   const size_t smem = subcycle_smem_bytes(n, a.nlev, (int)sizeof(T));
-  static cudaError_t attr = cudaFuncSetAttribute(k_subcycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)kSubcycleMaxSmem);
-  if (attr != cudaSuccess) return cuda_status(attr, "cudaFuncSetAttribute(k_subcycle)");
+  int st = set_max_dynamic_smem((const void *)k_subcycle<T>, (int)kSubcycleMaxSmem,
+                                "cudaFuncSetAttribute(k_subcycle)");
+  if (st) return st;
   if (smem > kSubcycleMaxSmem) return fail(HFM_ERR_BAD_ARG, "subcycle: levels exceed shared memory");
   k_subcycle<T><<<B, kSubThreads, smem, s>>>(a);
   HFM_CHECK_LAUNCH("k_subcycle");
