@@ -15,11 +15,13 @@
 // coordinates.  Every TMA x coordinate is a multiple of 16 bytes (x0 - HX with x0 a multiple
 // of 64 and HX = 16 / sizeof(T)); no store uses TMA.
 //
-// All waits are bounded: an mbarrier wait that does not complete within kMaxSpin polls sets
-// the library's device timeout counter, drains the stages this block has in flight (again
-// bounded) and returns.
+// All waits are bounded: a plane wait that does not complete within the wait budget (2^20
+// polls unless hfm_set_wait_budget lowers it) sets the library's device timeout counter; the
+// block then drains the copies it has issued (waits of up to 2^20 polls each, so no copy lands
+// in shared memory after the block has exited) and returns.
 #include <cuda.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "hfm_internal.cuh"
@@ -27,6 +29,7 @@
 namespace hfm {
 
 static __device__ int g_tma_timeouts;
+static std::atomic<int> g_wait_budget{1 << 20};
 
 namespace {
 
@@ -83,6 +86,7 @@ template <class T> struct TmaArgs {
   float omega, corr_sign;
   int has_phi, has_f, has_sigma, zero_xend, zero_xend_out, top_copy, dot_phi, dot_rhs;
   unsigned stage_bytes;
+  int wait_budget;  // polls of a plane wait before the block gives up (hfm_set_wait_budget)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -98,8 +102,8 @@ __device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int i = 0; i < kMaxSpin; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int budget) {
+  for (int i = 0; i < budget; ++i) {
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n"
@@ -250,15 +254,15 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
     }
   }
   int p_waited = p_first - 1;  // last plane whose loads completed
-  auto wait_plane = [&](int p) -> bool {
+  auto wait_plane = [&](int p, int budget) -> bool {
     const int q = p - p_first;
-    const bool w = mbar_wait(smem_u32(&bars[q % NS]), (uint32_t)((q / NS) & 1));
+    const bool w = mbar_wait(smem_u32(&bars[q % NS]), (uint32_t)((q / NS) & 1), budget);
     if (w) p_waited = p;
     return w;
   };
   auto stage_of = [&](int p) -> char * { return smem + ((p - p_first) % NS) * G::STAGE; };
-  bool ok = wait_plane(z0 - 1);
-  ok = wait_plane(z0) && ok;
+  bool ok = wait_plane(z0 - 1, a.wait_budget);
+  ok = wait_plane(z0, a.wait_budget) && ok;
   // a timeout is acted on by the whole block at once, so no thread is left at a barrier
   if (__syncthreads_or(!ok)) ok = false;
 
@@ -344,7 +348,7 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
       issue_plane<T, CORR, SIG, PRE2>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
       ++p_next;
     }
-    mine = wait_plane(z + 1);
+    mine = wait_plane(z + 1, a.wait_budget);
     const char *sm_ = stage_of(z - 1);
     const char *sc = stage_of(z);
     const char *sp = stage_of(z + 1);
@@ -500,7 +504,7 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
     // drain: wait (bounded) for the planes whose loads are still in flight, so that no
     // copy lands in shared memory after this block has exited; thread 0 issued them all
     if (tid == 0)
-      for (int p = p_waited + 1; p < p_next; ++p) wait_plane(p);
+      for (int p = p_waited + 1; p < p_next; ++p) wait_plane(p, kMaxSpin);
     return;
   }
   if ((MODE != M_SMOOTH || a.dot_rhs) && a.partials) {
@@ -631,6 +635,7 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
   if (a.has_f) bytes += (unsigned)(G::FN * sizeof(T));
   if (corr) bytes += (unsigned)(G::CCN * sizeof(T));
   a.stage_bytes = bytes;
+  a.wait_budget = g_wait_budget.load();
   a.op = op;
   a.out = out;
   a.coarse = coarse;
@@ -688,6 +693,7 @@ int tma_launch_pre2(const DevOp &op, const T *f, const T *invd, T *out, int64_t 
   a.has_phi = 1;
   a.has_sigma = 1;
   a.stage_bytes = (unsigned)((2 * G::PHI + G::SXN + G::SYN + G::SZN) * sizeof(T));
+  a.wait_budget = g_wait_budget.load();
   a.op = op;
   a.out = out;
   a.active = active;
@@ -716,6 +722,12 @@ template int tma_launch_pre2<__half>(const DevOp &, const __half *, const __half
                                      int64_t, int, Grid3, float, const int *, cudaStream_t);
 
 }  // namespace hfm
+
+extern "C" int hfm_set_wait_budget(int polls) {
+  if (polls < 0 || polls > (1 << 20)) return hfm::fail(HFM_ERR_BAD_ARG, "hfm_set_wait_budget: 0 .. 2^20 polls");
+  hfm::g_wait_budget.store(polls);
+  return HFM_OK;
+}
 
 extern "C" int hfm_device_timeouts(int *count, int reset) {
   if (!count) return hfm::fail(HFM_ERR_BAD_ARG, "NULL");

@@ -88,6 +88,11 @@ int64_t hfm_kernel_launch_count(void);
 /* Bounded device-side waits that expired on the current device (TMA pipeline stages); a
  * non-zero count means results of the affected launches are invalid.  reset != 0 clears it. */
 int hfm_device_timeouts(int *count, int reset);
+/* Poll budget of those waits for launches made after the call (default and maximum 2^20).
+ * Budget 0 makes every such wait expire at once - the failure path, for tests: each block
+ * stops, lets the copies it issued land, counts the timeout and returns; results of those
+ * launches are invalid.  No counterpart in the reference. */
+int hfm_set_wait_budget(int polls);
 
 /* ------------------------------------------------ stateless operators (drop-in layers) */
 /* Conv3D(1, kernel_size=3, strides=1, padding='SAME') with frozen weights and zero bias:
