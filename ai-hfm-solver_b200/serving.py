@@ -19,6 +19,8 @@ hierarchies live in HBM, sized so the buckets fit an HBM budget (admission by fo
 
 A request that arrives while others are on the GPU therefore joins the next launch of its
 bucket: iteration-level continuous batching, not a queue that waits for a batch to drain.
+Requests whose inputs are in host memory start their host -> device copy on arrival (copy
+stream), so the copies of queued requests overlap the buckets' work.
 Each slot's arithmetic depends only on its own data (fixed-order per-slot reductions), so a
 result is the same alone and in the mix.
 
@@ -130,11 +132,18 @@ class _Bucket:
     def ready(self):
         return not self.inflight or self.event.query()
 
-    def admit(self, req, now):
+    def admit(self, req, now, staged=None):
+        """Load ``req`` into a free slot.  ``staged`` = (sigma, rhs, event): its inputs were
+        already copied to the device on the server's copy stream (end-to-end mode)."""
         slot = self.free.pop()
         with torch.cuda.stream(self.stream):
             sig, rhs = req.sigma, req.rhs
-            if not sig.is_cuda:  # end-to-end mode: host -> device copy is part of the request
+            if staged is not None:
+                sig, rhs, ev = staged
+                self.stream.wait_event(ev)
+                sig.record_stream(self.stream)
+                rhs.record_stream(self.stream)
+            elif not sig.is_cuda:  # host inputs not staged yet: copy them now
                 sig = sig.to("cuda", non_blocking=True)
                 rhs = rhs.to("cuda", non_blocking=True)
             self.mg.set_operator(Sigma7(sig[0], sig[1], sig[2]), slot=slot)
@@ -220,6 +229,7 @@ class SolveServer:
             want[big] = max(1, want[big] // 2)
         self.footprint = {n: per[n] * want[n] for n in edges}
         self.buckets = {n: _Bucket(n, self.cfg, want[n], keep_solutions) for n in edges}
+        self.copy_stream = torch.cuda.Stream()
 
     def close(self):
         for b in self.buckets.values():
@@ -231,6 +241,7 @@ class SolveServer:
         clock = time.perf_counter
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         queued = {n: collections.deque() for n in self.buckets}
+        staged = {}  # rid -> device copies of host inputs (end-to-end mode)
         results = []
         torch.cuda.synchronize()
         t0 = clock()
@@ -241,6 +252,15 @@ class SolveServer:
             while pending and (not realtime or pending[0].arrival <= now):
                 r = pending.popleft()
                 queued[r.n].append(r)
+                if not r.sigma.is_cuda:
+                    # host inputs start their copy to the device on arrival, on a stream of their
+                    # own, so admission into a slot later does not wait for it
+                    with torch.cuda.stream(self.copy_stream):
+                        sd = r.sigma.to("cuda", non_blocking=True)
+                        rd = r.rhs.to("cuda", non_blocking=True)
+                        ev = torch.cuda.Event()
+                        ev.record(self.copy_stream)
+                    staged[r.rid] = (sd, rd, ev)
             idle = True
             for b in buckets:
                 if b.copies:
@@ -252,7 +272,8 @@ class SolveServer:
                 results.extend(b.harvest(clock, t0, host_out))
                 q = queued[b.n]
                 while q and b.free:
-                    b.admit(q.popleft(), clock() - t0)
+                    r = q.popleft()
+                    b.admit(r, clock() - t0, staged.pop(r.rid, None))
                 b.launch(self.cycles_per_tick)
                 if b.inflight:
                     idle = False
