@@ -217,7 +217,7 @@ class SolveServer:
     def __init__(self, cfg=None, edges=EDGES, slots=64, budget_bytes=120e9,
                  cycles_per_tick=4, keep_solutions=False):
         self.cfg = cfg or SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6,
-                                       max_cycles=600)
+                                       max_cycles=600, inner_tol=1e-3)
         self.cycles_per_tick = cycles_per_tick
         per = {n: footprint_bytes(self.cfg, L.OP_SIGMA7, (n, n, n), 1) for n in edges}
         want = {n: (slots[n] if isinstance(slots, dict) else slots) for n in edges}
@@ -288,7 +288,8 @@ class SolveServer:
 def solve_one_at_a_time(requests, cfg=None, time_budget_s=None, keep_solutions=False):
     """The plain path: one request at a time through a single-slot float32 handle per edge.
     Returns (results, seconds)."""
-    cfg = cfg or SolverConfig(cycle="V", accel="ir", storage="f32", tol=1e-6, max_cycles=600)
+    cfg = cfg or SolverConfig(cycle="V", accel="ir", storage="f32", tol=1e-6, max_cycles=600,
+                              inner_tol=1e-3)
     handles = {}
     results = []
     torch.cuda.synchronize()

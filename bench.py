@@ -241,7 +241,11 @@ def run_serve(args, pkg, torch, rank, world, local):
     sv, M, L = pkg.serving, pkg.multigrid, pkg._lib
     dev = torch.device("cuda", local)
     reqs = sv.make_stream(count=args.requests, rate=args.rate, seed=stream_seed(rank), device=dev)
-    cfg = M.SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6, max_cycles=600)
+    # inner CG solves to 1e-3 of their starting residual: three refinement steps meet 1e-6
+    # with fewer iterations than one tight inner solve (measured over inner tolerances 1e-6 ..
+    # 1e-1 on this stream); the plain path uses the same setting
+    cfg = M.SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6, max_cycles=600,
+                         inner_tol=1e-3)
     server = sv.SolveServer(cfg=cfg, slots=64, budget_bytes=120e9, cycles_per_tick=4)
 
     def barrier():
@@ -298,7 +302,8 @@ def run_serve(args, pkg, torch, rank, world, local):
     server.close()
 
     # plain path: one request at a time, float32 storage, bounded sample of the same stream
-    pcfg = M.SolverConfig(cycle="V", accel="ir", storage="f32", tol=1e-6, max_cycles=600)
+    pcfg = M.SolverConfig(cycle="V", accel="ir", storage="f32", tol=1e-6, max_cycles=600,
+                          inner_tol=1e-3)
     sv.solve_one_at_a_time(reqs[:10], cfg=pcfg)  # warm-up (graph capture per edge)
     plain, pdt = sv.solve_one_at_a_time(reqs, cfg=pcfg, time_budget_s=8.0)
     plain_sps = len(plain) / pdt
@@ -314,7 +319,7 @@ def run_serve(args, pkg, torch, rank, world, local):
                                "Poisson %.0f req/s, HBM budget 120 GB" % (len(reqs), args.rate),
                    "solver": "float64 iterative refinement around PCG + V(2,2) Jacobi omega=2/3 "
                              "(avg restriction, nearest prolongation, coarsest 4^3 / 3^3), "
-                             "bf16 inner storage, float32 accumulation",
+                             "bf16 inner storage, float32 accumulation, inner solves to 1e-3",
                    "tol": 1e-6, "slots_per_edge": {str(n): b.slots for n, b in server.buckets.items()},
                    "l2": "inputs larger than L2 (stream inputs %.1f GB resident)" %
                          (sum(r.sigma.numel() * 4 + r.rhs.numel() * 4 for r in reqs) / 1e9),
