@@ -244,13 +244,14 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
                T *coarse, int64_t stride, int64_t coarse_stride, int B, Grid3 g, float omega,
                unsigned flags, const int *active, double *partials, int *nblk_out,
                cudaStream_t s);
-// The coarse end of a V-cycle in one kernel (subcycle.cu): levels l0 .. coarsest of a SIGMA7
-// hierarchy, one block per instance, all fields in shared memory.
+// The coarse end of a V-cycle in one kernel (subcycle.cu): levels l0 .. coarsest of a SIGMA7,
+// CONST7 or K27 hierarchy, one block per instance, all fields in shared memory.
 constexpr int kMaxSubLevels = 8;
 constexpr size_t kSubcycleMaxSmem = 200 * 1024;
 template <class T> struct SubLevel {
   int Z, Y, X, n;
-  float cz, cy, cx;          // face multipliers of this level (c_d times the level's scale)
+  float cz, cy, cx;          // SIGMA7: face multipliers of this level (c_d times its scale)
+  float k[27];               // CONST7 (k[0..2] = kz, ky, kx) / K27 weights of this level
   const T *sx, *sy, *sz;     // the level's conductivities, instance stride n
   int o_phi, o_tmp, o_rhs;   // float offsets of the level's fields in shared memory
   int o_sig;                 // element offset of its conductivities in the T region
@@ -265,8 +266,8 @@ template <class T> struct SubArgs {
   int nu_pre, nu_post, coarse_sweeps;
   int sig_byte_offset;
 };
-size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size);
-template <class T> int launch_subcycle(SubArgs<T> a, int B, cudaStream_t s);
+size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size, bool sigma);
+template <class T> int launch_subcycle(int kind, SubArgs<T> a, int B, cudaStream_t s);
 
 // The first two Jacobi sweeps from a zero iterate in one pass (SIGMA7, TMA-eligible grids):
 // out = J(phi1) with phi1 = omega f * invd, invd = 1 / diag of the level.

@@ -828,17 +828,25 @@ class Engine : public EngineBase {
   }
 
   // First level of the fused coarse V-cycle (subcycle.cu), or -1: the deepest levels of at
-  // most 4096 cells of a SIGMA7 hierarchy, at least two of them, below the fine level.
+  // most 4096 cells of a SIGMA7, CONST7 or K27 hierarchy, at least two of them, below the fine
+  // level.
   int fused_first_level() {
     const hfm_mg_config &c = m_->cfg;
-    if (kind() != HFM_OP_SIGMA7 || (c.options & HFM_OPT_NO_FUSED_COARSE)) return -1;
+    const int k = kind();
+    if ((k != HFM_OP_SIGMA7 && k != HFM_OP_CONST7 && k != HFM_OP_K27) ||
+        (c.options & HFM_OPT_NO_FUSED_COARSE))
+      return -1;
+    // one block per instance: with few instances the separate kernels, which spread a level
+    // over many SMs, are as fast (measured: a single 64 x 128 x 128 pressure solve)
+    if (m_->slots < 8) return -1;
     if (n(m_->L - 1) > coarse_smem_limit()) return -1;
     int l0 = m_->L - 1;
     while (l0 - 1 >= 1 && n(l0 - 1) <= 4096 && m_->L - (l0 - 1) <= kMaxSubLevels) --l0;
     if (l0 >= m_->L - 1) return -1;
     int ns[kMaxSubLevels];
     for (int l = l0; l < m_->L; ++l) ns[l - l0] = (int)n(l);
-    if (subcycle_smem_bytes(ns, m_->L - l0, (int)sizeof(T)) > kSubcycleMaxSmem) return -1;
+    if (subcycle_smem_bytes(ns, m_->L - l0, (int)sizeof(T), k == HFM_OP_SIGMA7) > kSubcycleMaxSmem)
+      return -1;
     return l0;
   }
 
@@ -860,6 +868,7 @@ class Engine : public EngineBase {
       q.sx = (const T *)op.coef[0];
       q.sy = (const T *)op.coef[1];
       q.sz = (const T *)op.coef[2];
+      for (int j = 0; j < 27; ++j) q.k[j] = op.k[j];  // CONST7 / K27 weights, scale applied
     }
     a.rhs = rhs(l0);
     a.out = buf(l0, 0);
@@ -870,7 +879,7 @@ class Engine : public EngineBase {
     a.nu_post = c.nu_post;
     a.coarse_sweeps = c.coarse_sweeps;
     cur_[l0] = 0;
-    return launch_subcycle<T>(a, m_->slots, s);
+    return launch_subcycle<T>(kind(), a, m_->slots, s);
   }
 
   int vcycle(int l, bool zero, bool fcycle, int check_level0, cudaStream_t s) {

@@ -9,8 +9,10 @@
 // 2x2x2 averaging restriction, recursion, coarsest level `coarse_sweeps` sweeps from zero with
 // coarse_omega, nearest prolongation + correction fused with the first post-sweep, the
 // remaining post-sweeps); iterates stay in float32 between sweeps (the multi-kernel path
-// rounds them to the storage type).  SIGMA7 operator: face coefficient c_d (s_i + s_j) / 2,
-// wall face c_d s_i, ghost phi = 0.
+// rounds them to the storage type).  Operators as the other kernels evaluate them, ghost
+// phi = 0: SIGMA7 face coefficients c_d (s_i + s_j) / 2 (wall face c_d s_i); CONST7 the
+// anisotropic 7-point stencil with diagonal 2 (kz + ky + kx); K27 any 3x3x3 kernel, diagonal
+// its centre weight.
 #include "hfm_internal.cuh"
 
 namespace hfm {
@@ -19,7 +21,7 @@ namespace {
 
 constexpr int kSubThreads = 512;
 
-template <class T>
+template <int KIND, class T>
 __device__ __forceinline__ float sub_apply(const SubLevel<T> &L, const float *ph, const float *cor,
                                            const SubLevel<T> *Lc, const T *S, int z, int y, int x,
                                            float *diag) {
@@ -30,6 +32,26 @@ __device__ __forceinline__ float sub_apply(const SubLevel<T> &L, const float *ph
     if (cor) v -= cor[((zz >> 1) * Lc->Y + (yy >> 1)) * Lc->X + (xx >> 1)];
     return v;
   };
+  if (KIND == HFM_OP_K27) {
+    float acc = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float wgt = L.k[9 * a + 3 * b + c];
+          if (wgt != 0.f) acc += wgt * P(z + a - 1, y + b - 1, x + c - 1);
+        }
+    *diag = L.k[13];
+    return acc;
+  }
+  if (KIND == HFM_OP_CONST7) {
+    const float kz = L.k[0], ky = L.k[1], kx = L.k[2], d = 2.f * (kz + ky + kx);
+    *diag = d;
+    return d * P(z, y, x) - kz * (P(z - 1, y, x) + P(z + 1, y, x)) -
+           ky * (P(z, y - 1, x) + P(z, y + 1, x)) - kx * (P(z, y, x - 1) + P(z, y, x + 1));
+  }
   const T *sx = S + L.o_sig, *sy = sx + L.n, *sz = sy + L.n;
   const int i = (z * Y + y) * X + x;
   const float vx = St<T>::to(sx[i]), vy = St<T>::to(sy[i]), vz = St<T>::to(sz[i]);
@@ -46,14 +68,14 @@ __device__ __forceinline__ float sub_apply(const SubLevel<T> &L, const float *ph
 }
 
 // out = phi' + om (f - A phi') / diag with phi' = in - P(cor) (in / cor may be null)
-template <class T>
+template <int KIND, class T>
 __device__ void sub_sweep(const SubLevel<T> &L, const float *in, const float *cor,
                           const SubLevel<T> *Lc, const float *f, float *out, float om,
                           const T *S) {
   for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
     const int x = i % L.X, t = i / L.X, y = t % L.Y, z = t / L.Y;
     float dg;
-    const float ax = sub_apply<T>(L, in, cor, Lc, S, z, y, x, &dg);
+    const float ax = sub_apply<KIND, T>(L, in, cor, Lc, S, z, y, x, &dg);
     float pc = in ? in[i] : 0.f;
     if (cor) pc -= cor[((z >> 1) * Lc->Y + (y >> 1)) * Lc->X + (x >> 1)];
     out[i] = pc + om * __fdividef(f[i] - ax, dg);
@@ -62,7 +84,7 @@ __device__ void sub_sweep(const SubLevel<T> &L, const float *in, const float *co
 }
 
 // fc = R(A phi - f): 0.125 times the sum over each coarse cell's eight fine residuals
-template <class T>
+template <int KIND, class T>
 __device__ void sub_resid_restrict(const SubLevel<T> &L, const float *ph, const float *f,
                                    const SubLevel<T> &Lc, float *fc, const T *S) {
   for (int j = threadIdx.x; j < Lc.n; j += blockDim.x) {
@@ -76,14 +98,14 @@ __device__ void sub_resid_restrict(const SubLevel<T> &L, const float *ph, const 
         for (int c = 0; c < 2; ++c) {
           const int z = 2 * zc + a, y = 2 * yc + b, x = 2 * xc + c;
           float dg;
-          sum += sub_apply<T>(L, ph, nullptr, nullptr, S, z, y, x, &dg) - f[(z * L.Y + y) * L.X + x];
+          sum += sub_apply<KIND, T>(L, ph, nullptr, nullptr, S, z, y, x, &dg) - f[(z * L.Y + y) * L.X + x];
         }
     fc[j] = 0.125f * sum;
   }
   __syncthreads();
 }
 
-template <class T>
+template <int KIND, class T>
 __global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant__ SubArgs<T> a) {
   const int64_t inst = blockIdx.x;
   if (a.active && !a.active[inst]) return;
@@ -91,7 +113,7 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant_
   float *F = reinterpret_cast<float *>(sub_smem);
   T *S = reinterpret_cast<T *>(sub_smem + a.sig_byte_offset);
   const int nl = a.nlev;
-  for (int l = 0; l < nl; ++l) {
+  for (int l = 0; l < nl && KIND == HFM_OP_SIGMA7; ++l) {
     const SubLevel<T> &L = a.lv[l];
     const int64_t g = inst * (int64_t)L.n;
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
@@ -113,12 +135,12 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant_
     const float *f = F + L.o_rhs;
     int c = 0;
     for (int k = 0; k < a.nu_pre; ++k) {
-      sub_sweep<T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, f, buf[c ^ 1], a.omega, S);
+      sub_sweep<KIND, T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, f, buf[c ^ 1], a.omega, S);
       c ^= 1;
     }
     cur[l] = c;
     zero[l] = a.nu_pre == 0;
-    sub_resid_restrict<T>(L, zero[l] ? nullptr : buf[c], f, a.lv[l + 1], F + a.lv[l + 1].o_rhs, S);
+    sub_resid_restrict<KIND, T>(L, zero[l] ? nullptr : buf[c], f, a.lv[l + 1], F + a.lv[l + 1].o_rhs, S);
   }
   // coarsest: coarse_sweeps sweeps from zero
   {
@@ -126,7 +148,7 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant_
     float *buf[2] = {F + L.o_phi, F + L.o_tmp};
     int c = 0;
     for (int k = 0; k < a.coarse_sweeps; ++k) {
-      sub_sweep<T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1],
+      sub_sweep<KIND, T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1],
                    a.coarse_omega, S);
       c ^= 1;
     }
@@ -146,8 +168,8 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant_
     int c = cur[l];
     for (int k = 0; k < post; ++k) {
       const float om = a.nu_post == 0 ? 0.f : a.omega;
-      if (k == 0) sub_sweep<T>(L, zero[l] ? nullptr : buf[c], coarse, &Lc, F + L.o_rhs, buf[c ^ 1], om, S);
-      else sub_sweep<T>(L, buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1], om, S);
+      if (k == 0) sub_sweep<KIND, T>(L, zero[l] ? nullptr : buf[c], coarse, &Lc, F + L.o_rhs, buf[c ^ 1], om, S);
+      else sub_sweep<KIND, T>(L, buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1], om, S);
       c ^= 1;
     }
     cur[l] = c;
@@ -159,21 +181,31 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant_
 
 }  // namespace
 
-size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size) {
+size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size, bool sigma) {
   size_t f = 0, sg = 0;
   for (int l = 0; l < nlev; ++l) {
     f += (size_t)3 * n[l];
-    sg += (size_t)3 * n[l];
+    if (sigma) sg += (size_t)3 * n[l];
   }
   const size_t fbytes = ((f * 4 + 15) / 16) * 16;
   return fbytes + sg * (size_t)elem_size;
 }
 
+template <int KIND, class T>
+int go_subcycle(const SubArgs<T> &a, int B, size_t smem, cudaStream_t s) {
+  int st = set_max_dynamic_smem((const void *)k_subcycle<KIND, T>, (int)kSubcycleMaxSmem,
+                                "cudaFuncSetAttribute(k_subcycle)");
+  if (st) return st;
+  k_subcycle<KIND, T><<<B, kSubThreads, smem, s>>>(a);
+  HFM_CHECK_LAUNCH("k_subcycle");
+  return HFM_OK;
+}
+
 template <class T>
-int launch_subcycle(SubArgs<T> a, int B, cudaStream_t s) {
+int launch_subcycle(int kind, SubArgs<T> a, int B, cudaStream_t s) {
   int n[kMaxSubLevels];
   for (int l = 0; l < a.nlev; ++l) n[l] = a.lv[l].n;
-  // shared-memory layout: float fields of every level, then the conductivities (type T)
+  // shared-memory layout: float fields of every level, then (SIGMA7) the conductivities
   int off = 0;
   for (int l = 0; l < a.nlev; ++l) {
     a.lv[l].o_phi = off;
@@ -187,18 +219,18 @@ int launch_subcycle(SubArgs<T> a, int B, cudaStream_t s) {
     a.lv[l].o_sig = soff;
     soff += 3 * n[l];
   }
-  const size_t smem = subcycle_smem_bytes(n, a.nlev, (int)sizeof(T));
-  int st = set_max_dynamic_smem((const void *)k_subcycle<T>, (int)kSubcycleMaxSmem,
-                                "cudaFuncSetAttribute(k_subcycle)");
-  if (st) return st;
+  const size_t smem = subcycle_smem_bytes(n, a.nlev, (int)sizeof(T), kind == HFM_OP_SIGMA7);
   if (smem > kSubcycleMaxSmem) return fail(HFM_ERR_BAD_ARG, "subcycle: levels exceed shared memory");
-  k_subcycle<T><<<B, kSubThreads, smem, s>>>(a);
-  HFM_CHECK_LAUNCH("k_subcycle");
-  return HFM_OK;
+  switch (kind) {
+    case HFM_OP_SIGMA7: return go_subcycle<HFM_OP_SIGMA7, T>(a, B, smem, s);
+    case HFM_OP_CONST7: return go_subcycle<HFM_OP_CONST7, T>(a, B, smem, s);
+    case HFM_OP_K27: return go_subcycle<HFM_OP_K27, T>(a, B, smem, s);
+    default: return fail(HFM_ERR_UNSUPPORTED, "subcycle: operator kind");
+  }
 }
 
-template int launch_subcycle<float>(SubArgs<float>, int, cudaStream_t);
-template int launch_subcycle<__nv_bfloat16>(SubArgs<__nv_bfloat16>, int, cudaStream_t);
-template int launch_subcycle<__half>(SubArgs<__half>, int, cudaStream_t);
+template int launch_subcycle<float>(int, SubArgs<float>, int, cudaStream_t);
+template int launch_subcycle<__nv_bfloat16>(int, SubArgs<__nv_bfloat16>, int, cudaStream_t);
+template int launch_subcycle<__half>(int, SubArgs<__half>, int, cudaStream_t);
 
 }  // namespace hfm

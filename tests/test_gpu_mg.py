@@ -338,14 +338,23 @@ def test_fused_coarse_cycle_matches_separate_kernels(hfm, T, cycle, storage):
     for fused in (True, False):
         cfg = M.SolverConfig(cycle=cycle, storage=storage, tol=1e-300, max_cycles=10,
                              cycles_per_launch=1, fused_coarse=fused)
-        with M.Multigrid((32, 32, 32), hfm._lib.OP_SIGMA7, cfg, slots=2) as h:
-            for s in range(2):
+        # 8 instances: the fused path runs from 8 instances per handle up
+        with M.Multigrid((32, 32, 32), hfm._lib.OP_SIGMA7, cfg, slots=8) as h:
+            for s in range(8):
                 h.set_operator(hfm.ops.Sigma7(*(dev(T, sig[k]) for k in range(3))), slot=s)
                 h.load(s, dev(T, f))
             h.run(3)
-            outs.append([h.fetch(s).cpu().numpy() for s in range(2)])
+            outs.append([h.fetch(s).cpu().numpy() for s in (0, 7)])
     close(outs[0][0], outs[1][0], rtol=1e-5 if storage == "f32" else 2e-2)
     np.testing.assert_array_equal(outs[0][0], outs[0][1])
+    if cycle == "V" and storage == "f32":
+        # and the fused path against the oracle's V-cycles directly
+        oop = mg.Sigma7(sig[0], sig[1], sig[2], dtype=np.float32)
+        ops_ = mg.hierarchy(oop, len(mg.level_shapes((32, 32, 32))), 0.5)
+        ref = np.zeros_like(f)
+        for _ in range(3):
+            ref = mg.vcycle(ops_, 0, ref, f, mg.CycleConfig(2, 2, 2.0 / 3.0, 32))
+        close(outs[0][0], ref)
 
 
 @pytest.mark.parametrize("storage", ["f32", "bf16", "f16"])
@@ -385,3 +394,28 @@ def test_sawtooth_aspect_ratio_coarsest(hfm, T):
                                 fine_smooth=False, zero_xend=True)
     assert levels[-1] == (1, 4, 4)
     close(outs[-1], ref)
+
+
+@pytest.mark.parametrize("form", ["k27", "const7"])
+def test_fused_coarse_cycle_other_operators(hfm, T, form):
+    """The fused coarse V-cycle with the 27-point pressure kernel and the constant 7-point
+    operator: F-cycles (whose V parts use it) agree with the separate-kernel path."""
+    n = 32
+    rng = np.random.default_rng(12)
+    f = rng.standard_normal((n, n, n)).astype(np.float32)
+    M, ops, L = hfm.multigrid, hfm.ops, hfm._lib
+    if form == "k27":
+        kind, op = L.OP_K27, ops.Stencil27(W.w5_pressure27())
+    else:
+        kind, op = L.OP_CONST7, ops.Const7(50.0, 100.0, 200.0)
+    outs = []
+    for fused in (True, False):
+        cfg = M.SolverConfig(cycle="F", tol=1e-300, max_cycles=10, cycles_per_launch=1,
+                             fused_coarse=fused)
+        with M.Multigrid((n, n, n), kind, cfg, slots=8) as h:  # >= 8: the fused path runs
+            h.set_operator(op)
+            for s in range(8):
+                h.load(s, dev(T, f))
+            h.run(3)
+            outs.append(h.fetch(5).cpu().numpy())
+    close(outs[0], outs[1], rtol=1e-5)
