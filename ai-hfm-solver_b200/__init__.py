@@ -15,7 +15,8 @@ __all__ = ["_lib", "weights", "problems", "ops", "multigrid"]
 
 def __getattr__(name):
     # ops / multigrid import torch; keep the package importable for the build step.
-    if name in ("ops", "multigrid", "serving", "precision", "tomography", "ns", "kolmogorov"):
+    if name in ("ops", "multigrid", "serving", "precision", "tomography", "ns", "kolmogorov",
+                "slab"):
         import importlib
         return importlib.import_module("." + name, __name__)
     raise AttributeError(name)

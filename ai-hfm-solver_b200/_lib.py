@@ -91,6 +91,9 @@ SIGNATURES = {
     "hfm_norm2_f64": (I, [P, I64, I, P, P, P]),
     "hfm_max_abs": (I, [P, I64, I, P, P, P]),
     "hfm_norm2_f64_noalloc": (I, [P, I64, I, P, P]),
+    "hfm_dot_f64": (I, [P, P, I64, I, I64, P, P, P]),
+    "hfm_cg_update_xr": (I, [P, P, P, P, P, P, I64, I, I64, P]),
+    "hfm_cg_update_p": (I, [P, P, P, P, I64, I, I64, P]),
     "hfm_ns_momentum": (I, [P, P, P, P, P, P, P, P, P, I, I, I, P, P, P, P, F, P]),
     "hfm_ns_pressure_gradient": (I, [P, P, P, P, I, I, I, P, P, P, P]),
     "hfm_ns_divergence": (I, [P, P, P, P, I, I, I, P, P, P, I, P]),

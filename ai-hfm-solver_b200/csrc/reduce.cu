@@ -47,6 +47,28 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// partials[inst][block] = sum of x*y over the block's cells of instance inst (float64).
+__global__ void __launch_bounds__(kThreads)
+    k_dot(const float *__restrict__ x, const float *__restrict__ y, int64_t n, int64_t stride,
+          double *__restrict__ partials) {
+  __shared__ double sh[kThreads / 32];
+  const int64_t inst = blockIdx.y;
+  const float *xi = x + inst * stride;
+  const float *yi = y + inst * stride;
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    acc += (double)__ldg(xi + i) * (double)__ldg(yi + i);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < kThreads / 32 ? sh[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) partials[inst * gridDim.x + blockIdx.x] = v;
+  }
+}
+
 // out[inst] = sum of partials[inst][0..nblk) in a fixed tree order.
 __global__ void k_finalize_sum(const double *__restrict__ partials, int nblk,
                                double *__restrict__ out) {
@@ -254,6 +276,17 @@ extern "C" int hfm_norm2_f64_noalloc(const float *x, int64_t n, int B, double *o
   k_sqrt_inplace<<<(B + 127) / 128, 128, 0, s>>>(out, B);
   HFM_CHECK_LAUNCH("k_sqrt_inplace");
   return HFM_OK;
+}
+
+extern "C" int hfm_dot_f64(const float *x, const float *y, int64_t n, int B, int64_t stride,
+                           double *out, void *scratch, hfm_stream_t stream) {
+  if (!x || !y || !out || !scratch || n <= 0 || B <= 0 || (B > 1 && stride < n))
+    return fail(HFM_ERR_BAD_ARG, "hfm_dot_f64: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nb = reduce_blocks_for(n);
+  k_dot<<<dim3(nb, B), kThreads, 0, s>>>(x, y, n, stride, (double *)scratch);
+  HFM_CHECK_LAUNCH("k_dot");
+  return launch_finalize_sum((double *)scratch, nb, B, out, s);
 }
 
 extern "C" int hfm_max_abs(const float *x, int64_t n, int B, float *out, void *scratch,

@@ -190,6 +190,11 @@ int hfm_norm2_f64(const float *x, int64_t n, int B, double *out, void *scratch,
                   hfm_stream_t stream); /* sqrt(sum x^2), accumulated in float64 */
 int hfm_max_abs(const float *x, int64_t n, int B, float *out, void *scratch,
                 hfm_stream_t stream);
+/* Per-instance sum of x * y in float64 (fixed order, scratch as above); instance i starts at
+ * x + i * stride (stride >= n when B > 1).  The dot products of the Z-slab conjugate-gradient
+ * solver, whose slabs are instances with the halo planes outside the n interior cells. */
+int hfm_dot_f64(const float *x, const float *y, int64_t n, int B, int64_t stride, double *out,
+                void *scratch, hfm_stream_t stream);
 
 /* hfm_norm2_f64 for callers that cannot allocate device memory: no counterpart in the
  * reference.  Some callers have no way to obtain scratch - a C or Fortran host code that
@@ -207,6 +212,21 @@ int hfm_max_abs(const float *x, int64_t n, int B, float *out, void *scratch,
  * bitwise equal to hfm_norm2_f64's. */
 #define HFM_NORM2_NOALLOC_SCRATCH_BYTES (512u * 1024u)
 int hfm_norm2_f64_noalloc(const float *x, int64_t n, int B, double *out, hfm_stream_t stream);
+
+/* ---------------------------------------------------------- Z-slab conjugate gradients */
+/* Vector updates of a conjugate-gradient solve whose grid is cut into B slabs along Z (one
+ * slab per instance, instance i at base + i * stride, n interior cells each).  They replace
+ * nothing in the reference, whose parallel solver (Anisotropic Resistivity Tomography/
+ * scripts/parallel_naiver_stokes_3D.py:745-823) runs stationary cycles with a host halo update
+ * (halo_exchange.py:635-719, structured_halo_update_3D) after every stencil call.  The
+ * coefficient is num[0] / den[0] read on the device (float64 sums already reduced over every
+ * slab of the solve), so no host round trip sits between the dot product and the update.
+ *   hfm_cg_update_xr:  a = num / den;  x += a p;  r -= a q
+ *   hfm_cg_update_p:   b = num / den (0 when den is NULL or 0);  p = z + b p */
+int hfm_cg_update_xr(float *x, float *r, const float *p, const float *q, const double *num,
+                     const double *den, int64_t n, int B, int64_t stride, hfm_stream_t stream);
+int hfm_cg_update_p(float *p, const float *z, const double *num, const double *den, int64_t n,
+                    int B, int64_t stride, hfm_stream_t stream);
 
 /* ---------------------------------------------------------------- NS time-stepper operators */
 /* Operators of scripts/naiver_stokes_3D.py (and Urban Modelling/AI_HFM_v3.ipynb cell 19) on
