@@ -40,7 +40,7 @@ import torch.distributed as dist
 
 from . import _lib as L
 from .multigrid import SolverConfig
-from .ops import Const7, Sigma7, Stencil27
+from .ops import Const7, Stencil27
 
 GHOST = 2
 
@@ -286,10 +286,11 @@ class SlabMultigrid:
     Cycle parameters come from ``SolverConfig`` (``nu_pre``, ``nu_post`` >= 1, ``omega``,
     ``coarse_sweeps``, ``coarse_omega``, ``coarse_scale``, ``n_levels``, ``min_coarse_edge``,
     ``tol``, ``max_cycles``).  Fields passed in and out are the interiors of the slabs held
-    here, (S, Zl, Y, X) with Zl = Z / world."""
+    here, (S, Zl, Y, X) with Zl = Z / world.  ``graphs`` (default: when every slab is in this
+    process on a GPU) replays the CG iteration as one CUDA graph; NCCL ranks run it eagerly."""
 
     def __init__(self, shape, op, cfg=None, group=None, device=None, agglomerate_cells=32 ** 3,
-                 kernels=None):
+                 kernels=None, graphs=None):
         self.cfg = cfg or SolverConfig()
         if self.cfg.cycle != "V" or self.cfg.accel not in ("none", "cg"):
             raise ValueError("the slab solver runs V-cycles, stationary or with cg")
@@ -349,7 +350,11 @@ class SlabMultigrid:
         self._r = torch.zeros(shp, device=self.device)
         self._p = torch.zeros(shp, device=self.device)
         self._q = torch.zeros(shp, device=self.device)
-        self._sums = torch.zeros((4, S), dtype=torch.float64, device=self.device)
+        self._sums = torch.zeros(S, dtype=torch.float64, device=self.device)
+        self._scal = torch.zeros(4, dtype=torch.float64, device=self.device)  # rz rz_old pq rr
+        self._graph = None
+        self.graphs = (isinstance(self.group, LocalSlabs) and self.device.type == "cuda"
+                       if graphs is None else bool(graphs))
         self._scratch = torch.zeros(max(8, self.k.scratch_bytes(shp)), dtype=torch.uint8,
                                     device=self.device)
 
@@ -446,22 +451,47 @@ class SlabMultigrid:
         out = self._vcycle(0, cur, self._r)
         return out[:, G:G + lv.Zl].clone()
 
-    def _global_dot(self, x, y, row):
-        out = self._sums[row]
-        self.k.dot(x, y, out, self._scratch)
-        tot = out.sum().reshape(1) if out.numel() > 1 else out.clone()
-        return self.group.allreduce(tot)
+    def _global_dot(self, x, y, dst):
+        """dst (one float64 on the device) = sum over every slab of every rank of x * y."""
+        self.k.dot(x, y, self._sums, self._scratch)
+        if self._sums.numel() > 1:
+            torch.sum(self._sums, dim=0, keepdim=True, out=dst)
+        else:
+            dst.copy_(self._sums)
+        return self.group.allreduce(dst)
+
+    def _cg_iteration(self, first):
+        """z = V(0, r); p = z + (rz / rz_old) p; q = A p; x += a p, r -= a q with
+        a = rz / (p . q); rr = r . r.  Every scalar stays in device memory."""
+        lv = self.levels[0]
+        x, r, p, q = self._x, self._r, self._p, self._q
+        rz, rz_old, pq, rr = (self._scal[i:i + 1] for i in range(4))
+        z = self._vcycle(0, None, r)
+        self._global_dot(r, z, rz)
+        if first:
+            self.k.update_p(p, z, None, None)
+        else:
+            self.k.update_p(p, z, rz, rz_old)
+        rz_old.copy_(rz)
+        lv.group.halo(p)
+        for s in range(lv.S):
+            self.k.apply(lv, s, p, q)
+        self._global_dot(p, q, pq)
+        self.k.update_xr(x, r, p, q, rz, pq)
+        self._global_dot(r, r, rr)
 
     def solve(self, b, phi0=None):
         """Solve A x = b to ``cfg.tol`` relative residual.  Returns (x slabs, stats) with
-        stats = {"iterations", "rel_resid", "converged", "history"}."""
+        stats = {"iterations", "rel_resid", "converged", "history"}.  With ``graphs`` the
+        conjugate-gradient iterations after the first replay one captured CUDA graph (same
+        kernels, same results); only the convergence check reads back to the host."""
         G = GHOST
         cfg = self.cfg
         lv = self.levels[0]
         b_pad = torch.zeros_like(self._r)
         self._load(b_pad, b)
-        nb2 = float(self._global_dot(b_pad, b_pad, 0).item())
-        nb = math.sqrt(nb2)
+        rr = self._scal[3:4]
+        nb = math.sqrt(float(self._global_dot(b_pad, b_pad, rr).item()))
         x = self._x
         x.zero_()
         if phi0 is not None:
@@ -474,7 +504,7 @@ class SlabMultigrid:
         for s in range(lv.S):
             self.k.residual(lv, s, x, b_pad, r)        # A x - b
         r.neg_()                                       # b - A x
-        hist = [math.sqrt(float(self._global_dot(r, r, 1).item())) / nb]
+        hist = [math.sqrt(float(self._global_dot(r, r, rr).item())) / nb]
         it = 0
         if cfg.accel == "none":
             cur = x
@@ -482,24 +512,22 @@ class SlabMultigrid:
                 cur = self._vcycle(0, cur, b_pad)
                 for s in range(lv.S):
                     self.k.residual(lv, s, cur, b_pad, r)
-                hist.append(math.sqrt(float(self._global_dot(r, r, 1).item())) / nb)
+                hist.append(math.sqrt(float(self._global_dot(r, r, rr).item())) / nb)
                 it += 1
             if cur is not x:
                 x.copy_(cur)
         else:
-            p, q = self._p, self._q
-            rz_old = None
             while hist[-1] >= cfg.tol and it < cfg.max_cycles:
-                z = self._vcycle(0, None, r)
-                rz = self._global_dot(r, z, 2)
-                self.k.update_p(p, z, rz, rz_old)
-                rz_old = rz
-                lv.group.halo(p)
-                for s in range(lv.S):
-                    self.k.apply(lv, s, p, q)
-                pq = self._global_dot(p, q, 3)
-                self.k.update_xr(x, r, p, q, rz, pq)
-                hist.append(math.sqrt(float(self._global_dot(r, r, 1).item())) / nb)
+                if it > 0 and self.graphs:
+                    if self._graph is None:
+                        g = torch.cuda.CUDAGraph()
+                        with torch.cuda.graph(g):
+                            self._cg_iteration(False)
+                        self._graph = g
+                    self._graph.replay()
+                else:
+                    self._cg_iteration(it == 0)
+                hist.append(math.sqrt(float(rr.item())) / nb)
                 it += 1
         return x[:, G:G + lv.Zl].clone(), {"iterations": it, "rel_resid": hist[-1],
                                            "converged": hist[-1] < cfg.tol, "history": hist}

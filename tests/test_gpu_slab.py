@@ -8,8 +8,8 @@ ranks.  Checked here:
 * one V-cycle gives the same bits over 1, 2 and 4 slabs, with agglomerated or distributed
   coarse levels, for the variable-coefficient, constant 7-point and 27-point operators, and
   agrees with the float32 oracle's one-domain V-cycle to 1e-5 of the field's largest value;
-* PCG over 4 slabs takes the iterations of the one-slab solve and reaches the tolerance on the
-  whole grid (residual recomputed with the float64 oracle operator); the one-GPU handle
+* PCG over 4 slabs takes the iterations of the one-slab solve, gives the same bits eagerly and
+  as a replayed CUDA graph, and reaches the tolerance on the whole grid (residual recomputed with the float64 oracle operator); the one-GPU handle
   (``hfm_mg_solve``, same cycle) lands within one iteration and 1e-3 of the same solution.
 """
 import ctypes as C
@@ -143,6 +143,16 @@ def test_pcg_over_slabs(hfm, T):
         res[world] = (x.reshape(shape).cpu().numpy(), st)
     assert res[1][1]["iterations"] == res[4][1]["iterations"]
     x4 = res[4][0]
+    # the captured CG iteration replays the eager kernels: same bits, also on a second solve
+    mg, grp = _make(hfm, T, "sigma7", shape, 4, 32 ** 3, cfg, sig)
+    mg.graphs = False
+    xe, ste = mg.solve(hfm.slab.split(T.from_numpy(f).cuda(), grp))
+    assert ste["history"] == res[4][1]["history"]
+    np.testing.assert_array_equal(xe.reshape(shape).cpu().numpy(), x4)
+    mg.graphs = True
+    for _ in range(2):
+        xg, stg = mg.solve(hfm.slab.split(T.from_numpy(f).cuda(), grp))
+        np.testing.assert_array_equal(xg.reshape(shape).cpu().numpy(), x4)
     np.testing.assert_allclose(x4, res[1][0], rtol=0, atol=1e-5 * np.abs(x4).max())
     oop = M.Sigma7(*sig, dtype=np.float64)
     assert M.rel_residual(oop, x4.astype(np.float64), f) < 1.5e-6
