@@ -13,6 +13,10 @@ ranks.  Checked here:
   (``hfm_mg_solve``, same cycle) lands within one iteration and 1e-3 of the same solution.
 """
 import ctypes as C
+import datetime
+import os
+import socket
+import sys
 
 import numpy as np
 import pytest
@@ -180,3 +184,50 @@ def test_stationary_cycles_over_slabs(hfm, T):
         out[world] = (x.reshape(shape).cpu().numpy(), st["iterations"])
     assert out[1][1] == out[2][1]
     np.testing.assert_array_equal(out[1][0], out[2][0])
+
+
+def _nccl_rank(port, q):
+    ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+    import __graft_entry__ as ge
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        hfm = ge.load_package()
+        S, P = hfm.slab, hfm.problems
+        shape = (64, 64, 64)
+        sig = [torch.from_numpy(a).cuda() for a in P.anisotropic_sigma(shape, 8, 1.0)]
+        f = torch.from_numpy(P.dipole(shape, 8)).cuda()
+        cfg = hfm.multigrid.SolverConfig(accel="cg", tol=1e-6)
+        out = []
+        for grp in (S.DistSlabs(), S.LocalSlabs(1)):
+            mg = S.SlabMultigrid(shape, S.SlabSigma7(*(S.split(a, grp) for a in sig)), cfg,
+                                 group=grp, agglomerate_cells=16 ** 3)
+            x, st = mg.solve(S.split(f, grp))
+            out.append((x.cpu().numpy(), st["history"], mg.graphs))
+        q.put(out)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_nccl_group_of_one_equals_local(hfm):
+    """``DistSlabs`` on an NCCL group of one rank (all-gather of the coarse levels and the dot
+    all-reduces through NCCL, eager) gives the bits of ``LocalSlabs(1)`` (graph replay).  A
+    single rank has no halo partner; the send / recv path runs in the CPU suite on gloo."""
+    import torch.multiprocessing as mp
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_rank, args=(port, q))
+    p.start()
+    (xd, hd, gd), (xl, hl, gl) = q.get(timeout=300)
+    p.join(timeout=60)
+    assert p.exitcode == 0
+    assert not gd and gl
+    assert hd == hl
+    np.testing.assert_array_equal(xd, xl)

@@ -9,8 +9,9 @@ conjugate gradients over slabs are checked without a GPU:
 * preconditioned CG and stationary cycles take the oracle's iteration count and agree with its
   solution to 1e-5 of the largest value (dot products are summed per slab, so the last bits
   differ);
-* two gloo ranks (``DistSlabs``, halo planes by send / recv, coarse levels by all-gather) give
-  the same bits as one process.
+* two and four gloo ranks (``DistSlabs``, halo planes by send / recv, coarse levels by
+  all-gather) give the same bits as one process; with four, the middle ranks exchange with
+  both neighbours.
 """
 import datetime
 import os
@@ -131,10 +132,9 @@ def test_pcg_and_stationary_match_oracle(kind, world, agg):
     assert err < 1e-5, err
 
 
-# ------------------------------------------------------------------------- two gloo ranks
+# ------------------------------------------------------------------------------ gloo ranks
 def _free_port():
-    import socket as so
-    with so.socket() as s:
+    with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         return s.getsockname()[1]
 
@@ -161,10 +161,10 @@ def _rank_main(rank, world, port, agg, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("agg", [0, 600])
-def test_two_gloo_ranks_equal_one_process(agg):
+@pytest.mark.parametrize("world,agg", [(2, 0), (2, 600), (4, 0), (4, 600)])
+def test_gloo_ranks_equal_one_process(world, agg):
     import torch.multiprocessing as mp
-    world, port = 2, _free_port()
+    port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_rank_main, args=(r, world, port, agg, q)) for r in range(world)]
@@ -177,12 +177,12 @@ def test_two_gloo_ranks_equal_one_process(agg):
     pkg = _pkg()
     cfg, ocfg = _cfgs(pkg, "cg")
     b, phi0, sig, op = _problem("sigma7", seed=7)
-    assert out[0][1] == out[1][1] == (4 if agg == 0 else 2)
+    assert {o[1] for o in out} == {4 if agg == 0 else 2}
     v = np.concatenate([o[2] for o in out]).reshape(SHAPE)
     np.testing.assert_array_equal(v, M.vcycle(_oracle_ops(op, pkg, cfg), 0, phi0, b, ocfg))
-    mg, grp = _solver(pkg, "sigma7", sig, 2, agg, cfg)
+    mg, grp = _solver(pkg, "sigma7", sig, world, agg, cfg)
     x1, st1 = mg.solve(pkg.slab.split(torch.from_numpy(b), grp))
     x = np.concatenate([o[3] for o in out])
-    assert out[0][4] == out[1][4] == st1["iterations"]
-    assert out[0][5] == out[1][5]                  # every rank saw the same residuals
+    assert {o[4] for o in out} == {st1["iterations"]}
+    assert all(o[5] == out[0][5] for o in out)     # every rank saw the same residuals
     np.testing.assert_allclose(x, x1.numpy(), rtol=0, atol=1e-6 * np.abs(x).max())
