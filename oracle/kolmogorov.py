@@ -55,12 +55,13 @@ def level_shapes(shape, min_edge=1):
     return shapes
 
 
-def sawtooth2d(w9, values, b, n_levels):
+def sawtooth2d(w9, values, b, n_levels, keep=None):
     """One cycle of ``Multigrid_2D.ipynb#c18`` (j_itr = 1): r = A v - b, restriction to the
     coarsest level, w = 0 there, one Jacobi per level on the way up against the restricted
     residual, one on the fine level against r, v -= w, then one Jacobi on v against b.  The
     same weights on every level, zero padding, omega = 1 (the reference's update
-    ``w - A(w)/d + r/d``)."""
+    ``w - A(w)/d + r/d``).  ``keep`` (a dict) receives the residuals and corrections per level
+    (level 0 finest)."""
     f32 = np.float32
     r = conv2d(values, w9) - np.asarray(b, f32)
     rs = [r]
@@ -68,8 +69,12 @@ def sawtooth2d(w9, values, b, n_levels):
         rs.append(restrict2d(rs[-1]))
     w = np.zeros_like(rs[-1])
     w = jacobi2d(w9, w, rs[-1])
+    ws = {n_levels - 1: w}
     for lvl in range(n_levels - 2, -1, -1):
         w = jacobi2d(w9, prolong2d(w), rs[lvl])
+        ws[lvl] = w
+    if keep is not None:
+        keep["r"], keep["w"] = rs, ws
     values = np.asarray(values, f32) - w
     return jacobi2d(w9, values, b)
 

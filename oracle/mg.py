@@ -196,14 +196,16 @@ def residual(op, phi, b):
 # Reference sawtooth cycle
 # --------------------------------------------------------------------------------------
 def sawtooth_cycle(ops, phi, b, fine_smooth=True, zero_xend=False, top_copy=False,
-                   coarse_zero_shape=None, keep=None):
+                   coarse_zero_shape=None, keep=None, coarse_sweeps=1):
     """One cycle of the reference multigrid (``Anisotropic_3d_Multigrid_7point.ipynb:
     406-449``; ``BGS_multigrid_v1.ipynb`` cell 42; pressure form ``naiver_stokes_3D.py:
     646-703``).
 
     1. ``r = A phi - b`` (NS form: ``r[..., X-1] = 0``);
     2. restrict ``r`` level by level down to ``ops[-1]``;
-    3. coarsest: ``w = 0`` then one Jacobi against its residual;
+    3. coarsest: ``w = 0`` then one Jacobi against its residual (``coarse_sweeps`` of them:
+       the serial run of ``parallel_multigrid_advection_diffusion_3D.ipynb`` cell 15 sweeps
+       its 2^3 level twice);
     4. every finer coarse level: ``w = P w`` then one Jacobi;
     5. fine: ``w = P w`` then (unless ``fine_smooth`` is False, the NS form) one Jacobi
        against ``r``;
@@ -223,7 +225,8 @@ def sawtooth_cycle(ops, phi, b, fine_smooth=True, zero_xend=False, top_copy=Fals
     for l in range(1, L):
         rs.append(tfops.restrict_avg(rs[-1], dt))
     w = np.zeros_like(rs[-1])
-    w = jacobi_ref(ops[-1], w, rs[-1])
+    for _ in range(coarse_sweeps):
+        w = jacobi_ref(ops[-1], w, rs[-1])
     ws = {L - 1: w}
     for l in range(L - 2, 0, -1):
         w = tfops.prolong_nearest(w, dt)

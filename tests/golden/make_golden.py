@@ -4,11 +4,17 @@ Run from the repository root: ``python tests/golden/make_golden.py``.
 
 Two kinds of fixture are written:
 
-* ``reference_pins.json`` - numbers the reference itself printed, typed in from its saved
-  notebook outputs (``Anisotropic Resistivity Tomography/notebooks/
-  Multigrid_3d_7point_source.ipynb`` cells 4, 5, 6 and 10: the 7-point kernel at
-  dt=0.1, Dx=200, Dy=100, Dz=50, dx=1; ``Anisotropic_3d_Multigrid_7point_BC_Rec.ipynb``
-  lines 196 and 279: parameter counts).  These pin the oracle's kernel layout.
+* ``reference_pins.json`` - numbers the reference itself printed in its saved notebook
+  outputs.  Typed in: ``Anisotropic Resistivity Tomography/notebooks/
+  Multigrid_3d_7point_source.ipynb`` cells 4, 5, 6 and 10 (the 7-point kernel at dt=0.1,
+  Dx=200, Dy=100, Dz=50, dx=1) and ``Anisotropic_3d_Multigrid_7point_BC_Rec.ipynb`` lines 196
+  and 279 (parameter counts): these pin the oracle's kernel layout.  Read from the notebook
+  files (the reference checkout must be present, ``HFM_REFERENCE_ROOT``): the corrections
+  ``w_2`` (2x2) and ``w_4`` (4x4) of one serial 2D sawtooth cycle
+  (``notebooks/Parallel_multigrid_2D.ipynb`` cell 20, printed by cells 50 and 52), and the
+  norm of the serial 3D solution after 100 sawtooth cycles
+  (``notebooks/parallel_multigrid_advection_diffusion_3D.ipynb`` cell 15, printed by cell
+  72).  These pin solution values.
 * ``oracle_small.npz`` - seeded small-grid inputs and the oracle's outputs for every
   operator and for a few reference cycles.  TensorFlow 2.0 (the reference's pinned
   dependency) is not installable here, so these are the oracle's values, cross-checked at
@@ -17,6 +23,7 @@ Two kinds of fixture are written:
 """
 import json
 import os
+import re
 import sys
 
 import numpy as np
@@ -35,6 +42,47 @@ def torch_conv_same(x, K):
     return torch.nn.functional.conv3d(t, k, padding=1)[0, 0].numpy()
 
 
+REFERENCE = os.environ.get("HFM_REFERENCE_ROOT", "/root/reference")
+NOTEBOOKS = os.path.join(REFERENCE, "Anisotropic Resistivity Tomography", "notebooks")
+
+
+def _cell_text(notebook, cell):
+    with open(os.path.join(NOTEBOOKS, notebook)) as f:
+        nb = json.load(f)
+    out = []
+    for o in nb["cells"][cell].get("outputs", []):
+        out.append("".join(o.get("text", [])) if "text" in o
+                   else "".join(o.get("data", {}).get("text/plain", [])))
+    return "".join(out)
+
+
+def _first_tensor(text):
+    """Numbers of the first printed ``tf.Tensor(...)`` in ``text``, with its shape."""
+    m = re.search(r"tf\.Tensor\((.*?), shape=\(([0-9, ]+)\)", text, re.S)
+    vals = [float(v) for v in re.findall(r"-?\d+\.\d*(?:e-?\d+)?", m.group(1))]
+    shape = tuple(int(v) for v in m.group(2).replace(" ", "").split(",") if v)
+    return np.array(vals).reshape(shape).tolist()
+
+
+def printed_solution_values():
+    w2 = _first_tensor(_cell_text("Parallel_multigrid_2D.ipynb", 50))
+    w4 = _first_tensor(_cell_text("Parallel_multigrid_2D.ipynb", 52))
+    lines = _cell_text("parallel_multigrid_advection_diffusion_3D.ipynb", 72).splitlines()
+    serial_norm = float(lines[1])     # print(serial_l1), after "ABE of subdomains"
+    return {
+        "mg2d_source": "notebooks/Parallel_multigrid_2D.ipynb cell 20 (128^2, dt=10, Dx=Dy=0.1, "
+                       "ub=1, 40x40 box at 43 as source and initial guess, levels 128..2, "
+                       "one cycle); values printed by cells 50 and 52",
+        "mg2d_w2": w2,
+        "mg2d_w4": w4,
+        "mg3d_source": "notebooks/parallel_multigrid_advection_diffusion_3D.ipynb cell 15 "
+                       "(128^3, 7-point Dx=Dy=Dz=100, 40^3 box at 43 as source and initial "
+                       "guess, levels 128..2 with two Jacobi sweeps at 2^3, 100 cycles); "
+                       "np.linalg.norm of the float32 result printed by cell 72",
+        "mg3d_norm_after_100": serial_norm,
+    }
+
+
 def main():
     pins = {
         "source": "notebooks/Multigrid_3d_7point_source.ipynb cells 4-6, 10 (dt=0.1, Dx=200, Dy=100, Dz=50, dx=1)",
@@ -49,6 +97,7 @@ def main():
         "params_conv3x3x3": 28,
         "params_restrict2x2x2": 9,
     }
+    pins.update(printed_solution_values())
     with open(os.path.join(HERE, "reference_pins.json"), "w") as f:
         json.dump(pins, f, indent=1)
 

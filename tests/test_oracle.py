@@ -30,6 +30,70 @@ def test_reference_printed_kernel(pins):
     np.testing.assert_allclose(K, np.array(pins["kernel_3x3x3"]), atol=1e-12)
 
 
+def test_oracle_reproduces_reference_2d_cycle_values(pins):
+    """The serial 2D run of ``notebooks/Parallel_multigrid_2D.ipynb`` (cell 20: 128^2,
+    advection-diffusion weights of cell 5, 40x40 box as source and initial guess, restriction
+    down to 2x2, one cycle) printed its 2x2 and 4x4 corrections (cells 50, 52).  The oracle's
+    cycle gives the same numbers to the 8 printed decimals."""
+    from oracle import kolmogorov as K2
+    T = np.zeros((128, 128), np.float32)
+    T[43:83, 43:83] = 1.0
+    keep = {}
+    K2.sawtooth2d(W.w2_2d_advection_diffusion(), T, T, 7, keep=keep)
+    w = keep["w"]
+    assert w[6].shape == (2, 2) and w[5].shape == (4, 4)
+    np.testing.assert_allclose(w[6], np.array(pins["mg2d_w2"]), rtol=0, atol=6e-9)
+    np.testing.assert_allclose(w[5], np.array(pins["mg2d_w4"]), rtol=0, atol=6e-9)
+
+
+def _float32_dot_32_lanes(x):
+    """sqrt(x . x) summed as a float32 BLAS dot with 4 x 8 fused multiply-add accumulators
+    (element i lands in lane i mod 32; lanes added register by register, then across the 8
+    lanes in order).  This is how the reference's ``np.linalg.norm`` of a float32 array is
+    evaluated on an AVX2 host; the result differs from the exact norm in the 5th digit."""
+    f = np.float32
+    x = np.asarray(x, np.float64).ravel()
+    acc = np.zeros(32, np.float32)
+    for blk in x.reshape(-1, 32):
+        acc = (acc.astype(np.float64) + blk * blk).astype(np.float32)
+    a = acc.reshape(4, 8)
+    v = (a[0] + a[1]) + (a[2] + a[3])
+    h = f(0)
+    for t in v:
+        h = f(h + t)
+    return f(np.sqrt(h))
+
+
+def test_oracle_reproduces_reference_3d_solution_norm(pins):
+    """The serial 3D run of ``notebooks/parallel_multigrid_advection_diffusion_3D.ipynb``
+    (cell 15: 128^3, 7-point operator with Dx = Dy = Dz = 100, 40^3 box as source and initial
+    guess, restriction down to 2^3 with two Jacobi sweeps there, 100 reference cycles)
+    printed the norm of its float32 solution (cell 72): 288.47165.  The oracle's solution
+    has that norm exactly when the norm is summed as the reference summed it, and within
+    1e-4 exactly (the printed number's own rounding); the same cycle with one coarsest sweep
+    misses by 3.6e-3, so the check separates the variants."""
+    K = W.w2_7point(Dx=100.0, Dy=100.0, Dz=100.0, dt=1.0)
+    assert K[1, 1, 1] == 600.0 and K[0, 1, 1] == -100.0
+    ops = mg.hierarchy(mg.Stencil27(K), 7, 1.0)
+    assert len(mg.level_shapes((128, 128, 128), min_edge=2)) == 7   # 128 ... 2
+    T = np.zeros((128, 128, 128), np.float32)
+    T[43:83, 43:83, 43:83] = 1.0
+    want = pins["mg3d_norm_after_100"]
+
+    def run(coarse_sweeps):
+        v = T.copy()
+        for _ in range(100):
+            v = mg.sawtooth_cycle(ops, v, T, coarse_sweeps=coarse_sweeps)
+        return v
+
+    v = run(2)
+    assert _float32_dot_32_lanes(v) == np.float32(want)
+    exact = float(np.linalg.norm(v.astype(np.float64)))
+    assert abs(exact - want) / want < 1e-4, exact
+    one = float(np.linalg.norm(run(1).astype(np.float64)))
+    assert abs(one - want) / want > 1e-3, one
+
+
 def test_product_weights_match_oracle(pkg):
     w = pkg.weights
     np.testing.assert_allclose(w.anisotropic7(), W.w2_7point(), rtol=1e-7)
