@@ -207,8 +207,9 @@ def run_reference(args):
     import __graft_entry__ as ge
     pkg = ge.load_package()
     dev = "cuda" if torch.cuda.is_available() else "cpu"
-    reqs = pkg.serving.make_stream(count=64, rate=args.rate, seed=1, device=dev) \
-        if dev == "cuda" else None
+    # the stream's generator runs on the GPU when there is one (the same draws as the GPU
+    # arm's generator); on a host without one it runs on the CPU
+    reqs = pkg.serving.make_stream(count=64, rate=args.rate, seed=1, device=dev)
     from oracle import cpu_port, mg as omg
     cores = cpu_port.threads()
     per_step = 4
