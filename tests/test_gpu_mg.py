@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from oracle import mg, tfops, weights as W
+from oracle import mg, weights as W
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")

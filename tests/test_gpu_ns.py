@@ -3,7 +3,7 @@ reference time step."""
 import numpy as np
 import pytest
 
-from oracle import ns as ons, weights as OW
+from oracle import ns as ons
 
 pytestmark = pytest.mark.gpu
 SHAPE = (10, 12, 14)
