@@ -11,7 +11,9 @@ conjugate gradients over slabs are checked without a GPU:
   differ);
 * two and four gloo ranks (``DistSlabs``, halo planes by send / recv, coarse levels by
   all-gather) give the same bits as one process; with four, the middle ranks exchange with
-  both neighbours.
+  both neighbours;
+* two subgroups of two ranks each solve their own problem side by side (halo peers are the
+  subgroup's global ranks).
 """
 import datetime
 import os
@@ -186,3 +188,52 @@ def test_gloo_ranks_equal_one_process(world, agg):
     assert {o[4] for o in out} == {st1["iterations"]}
     assert all(o[5] == out[0][5] for o in out)     # every rank saw the same residuals
     np.testing.assert_allclose(x, x1.numpy(), rtol=0, atol=1e-6 * np.abs(x).max())
+
+
+def _subgroup_main(rank, port, q):
+    """Four gloo ranks as two independent 2-slab solves on subgroups {0, 1} and {2, 3}: the
+    halo peers are global ranks of the subgroup, and each pair solves its own problem."""
+    sys.path[:0] = [ROOT, HERE]
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=4,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        from _slab_oracle import OracleSlabKernels
+        groups = [dist.new_group([0, 1]), dist.new_group([2, 3])]
+        pkg = _pkg()
+        S = pkg.slab
+        grp = S.DistSlabs(groups[rank // 2])
+        cfg, _ = _cfgs(pkg, "cg")
+        b, _, sig, _ = _problem("sigma7", seed=20 + rank // 2)
+        mg = S.SlabMultigrid(SHAPE, _slab_op(pkg, "sigma7", sig, grp), cfg, group=grp,
+                             device="cpu", agglomerate_cells=600, kernels=OracleSlabKernels())
+        x, st = mg.solve(S.split(torch.from_numpy(b), grp))
+        q.put((rank, grp.rank, grp.world, x.numpy(), st["iterations"]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_subgroups_solve_independently():
+    import torch.multiprocessing as mp
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_subgroup_main, args=(r, port, q)) for r in range(4)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=240) for _ in range(4)], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [(o[1], o[2]) for o in out] == [(0, 2), (1, 2), (0, 2), (1, 2)]
+    pkg = _pkg()
+    cfg, _ = _cfgs(pkg, "cg")
+    for pair in (0, 1):
+        b, _, sig, _ = _problem("sigma7", seed=20 + pair)
+        mg, grp = _solver(pkg, "sigma7", sig, 2, 600, cfg)
+        x1, st1 = mg.solve(pkg.slab.split(torch.from_numpy(b), grp))
+        mine = out[2 * pair:2 * pair + 2]
+        assert {o[4] for o in mine} == {st1["iterations"]}
+        x = np.concatenate([o[3] for o in mine])
+        np.testing.assert_allclose(x, x1.numpy(), rtol=0, atol=1e-6 * np.abs(x).max())
