@@ -1,0 +1,65 @@
+"""A reference run replayed through this package's layer API, against what the reference
+printed.
+
+``notebooks/parallel_multigrid_advection_diffusion_3D.ipynb`` cell 15 runs 100 serial
+sawtooth cycles on 128^3: the 7-point operator with Dx = Dy = Dz = 100 (centre 600), a 40^3
+box of ones at offset 43 as both source and initial guess, restriction down to 2^3 with two
+Jacobi sweeps there, one on each finer level, the fine correction and one Jacobi on the
+iterate.  Cell 72 printed the norm of the float32 solution: 288.47165.  The loop below is the
+notebook's, with its ``CNN3D_A_<n>`` / ``CNN3D_res_<n>`` / ``CNN3D_prol_<n>`` models replaced
+by ``ops.Conv3DSame`` / ``ops.Restriction`` / ``ops.Prolongation`` (one object serves every
+size) and its arithmetic written in the same order.  The printed norm carries the rounding of
+a float32 ``np.linalg.norm`` (5e-5 here), so the exact norm is checked to 1e-4; the solution
+is also checked against the pinned oracle's to 1e-5 of its largest value.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mg as M
+
+pytestmark = pytest.mark.gpu
+
+
+def test_advection_diffusion_3d_serial_run(hfm):
+    import torch
+    ops, W = hfm.ops, hfm.weights
+    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.json")) as fh:
+        printed = json.load(fh)["mg3d_norm_after_100"]
+    w2 = W.anisotropic7(Dx=100.0, Dy=100.0, Dz=100.0)
+    d = float(w2[1, 1, 1])
+    assert d == 600.0
+    A, res, prol = ops.Conv3DSame(w2), ops.Restriction(), ops.Prolongation()
+    n = 128
+    T = torch.zeros((1, n, n, n, 1), device="cuda")
+    T[0, 43:83, 43:83, 43:83, 0] = 1.0
+    values, b = T.clone(), T
+    for _ in range(100):
+        w = torch.zeros((1, 2, 2, 2, 1), device="cuda")
+        r = A(values) - b
+        rs = [r]
+        for _ in range(6):                       # r_64 ... r_2
+            rs.append(res(rs[-1]))
+        for _ in range(2):                       # two sweeps on 2^3
+            w = w - A(w) / d + rs[6] / d
+        for lvl in range(5, 0, -1):              # 4^3 ... 64^3
+            w = prol(w)
+            w = w - A(w) / d + rs[lvl] / d
+        w = prol(w)
+        w = w - A(w) / d + r / d
+        values = values - w
+        values = values - A(values) / d + b / d
+    got = values[0, :, :, :, 0].double()
+    norm = float(got.norm())
+    assert abs(norm - printed) / printed < 1e-4, norm
+
+    Tn = np.zeros((n, n, n), np.float32)
+    Tn[43:83, 43:83, 43:83] = 1.0
+    hier = M.hierarchy(M.Stencil27(w2), 7, 1.0)
+    v = Tn.copy()
+    for _ in range(100):
+        v = M.sawtooth_cycle(hier, v, Tn, coarse_sweeps=2)
+    err = np.abs(got.cpu().numpy() - v).max() / np.abs(v).max()
+    assert err < 1e-5, err
