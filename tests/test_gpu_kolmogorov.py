@@ -102,29 +102,6 @@ def test_reference_2d_cycle_matches_oracle(hfm, T):
     close(v[0].cpu().numpy(), ref, 1e-5)
 
 
-def test_reference_2d_cycle_printed_corrections(hfm, T):
-    """One serial cycle of ``notebooks/Parallel_multigrid_2D.ipynb`` (cell 20: 128^2, the
-    cell-5 weights, 40 x 40 box as source and initial guess, restriction down to 2 x 2): the
-    2 x 2 and 4 x 4 corrections the reference printed (cells 50 and 52), to their 8 decimals,
-    and the new values against the oracle."""
-    import json
-    import os
-    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.json")) as fh:
-        pins = json.load(fh)
-    KM = hfm.kolmogorov
-    mg = KM.Multigrid2D((128, 128), hfm.weights.advection_diffusion_2d(), storage="f32",
-                        periodic=False, coarse_scale=1.0, min_edge=2, omega=1.0)
-    assert mg.L == 7 and mg.shapes[-1] == (2, 2)
-    b = np.zeros((128, 128), np.float32)
-    b[43:83, 43:83] = 1.0
-    bd = T.from_numpy(b).cuda().view(1, 128, 128)
-    v = mg.sawtooth(bd.clone(), bd)
-    np.testing.assert_allclose(mg.w[6][0].cpu().numpy(), np.array(pins["mg2d_w2"]), rtol=0, atol=6e-9)
-    np.testing.assert_allclose(mg.w[5][0].cpu().numpy(), np.array(pins["mg2d_w4"]), rtol=0, atol=6e-9)
-    ref = K2.sawtooth2d(W.w2_2d_advection_diffusion(), b, b, 7)
-    close(v[0].cpu().numpy(), ref, 1e-5)
-
-
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
 def test_periodic_pressure_cycles(hfm, T, storage):
     """Outer iterations p -= V(A p - f) on the periodic 5-point Poisson problem agree with the

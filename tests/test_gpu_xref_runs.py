@@ -1,5 +1,9 @@
-"""A reference run replayed through this package's layer API, against what the reference
-printed.
+"""Reference runs replayed on the GPU, against what the reference printed.
+
+``notebooks/Parallel_multigrid_2D.ipynb`` cell 20 runs one serial 2D sawtooth cycle on 128^2
+(the cell-5 advection-diffusion weights, a 40 x 40 box of ones at offset 43 as both source
+and initial guess, restriction down to 2 x 2); cells 50 and 52 printed the 2 x 2 and 4 x 4
+corrections to 8 decimals.  ``kolmogorov.Multigrid2D.sawtooth`` runs that cycle.
 
 ``notebooks/parallel_multigrid_advection_diffusion_3D.ipynb`` cell 15 runs 100 serial
 sawtooth cycles on 128^3: the 7-point operator with Dx = Dy = Dz = 100 (centre 600), a 40^3
@@ -18,16 +22,40 @@ import os
 import numpy as np
 import pytest
 
-from oracle import mg as M
+from oracle import kolmogorov as K2, mg as M, weights as OW
 
 pytestmark = pytest.mark.gpu
+
+
+def _printed():
+    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.json")) as fh:
+        return json.load(fh)
+
+
+def test_2d_cycle_printed_corrections(hfm):
+    import torch
+    pins = _printed()
+    mg = hfm.kolmogorov.Multigrid2D((128, 128), hfm.weights.advection_diffusion_2d(),
+                                    storage="f32", periodic=False, coarse_scale=1.0, min_edge=2,
+                                    omega=1.0)
+    assert mg.L == 7 and mg.shapes[-1] == (2, 2)
+    b = np.zeros((128, 128), np.float32)
+    b[43:83, 43:83] = 1.0
+    bd = torch.from_numpy(b).cuda().view(1, 128, 128)
+    v = mg.sawtooth(bd.clone(), bd)
+    np.testing.assert_allclose(mg.w[6][0].cpu().numpy(), np.array(pins["mg2d_w2"]), rtol=0,
+                               atol=6e-9)
+    np.testing.assert_allclose(mg.w[5][0].cpu().numpy(), np.array(pins["mg2d_w4"]), rtol=0,
+                               atol=6e-9)
+    ref = K2.sawtooth2d(OW.w2_2d_advection_diffusion(), b, b, 7)
+    err = np.abs(v[0].cpu().numpy() - ref).max() / np.abs(ref).max()
+    assert err < 1e-5, err
 
 
 def test_advection_diffusion_3d_serial_run(hfm):
     import torch
     ops, W = hfm.ops, hfm.weights
-    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.json")) as fh:
-        printed = json.load(fh)["mg3d_norm_after_100"]
+    printed = _printed()["mg3d_norm_after_100"]
     w2 = W.anisotropic7(Dx=100.0, Dy=100.0, Dz=100.0)
     d = float(w2[1, 1, 1])
     assert d == 600.0
