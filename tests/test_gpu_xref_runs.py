@@ -3,7 +3,9 @@
 ``notebooks/Parallel_multigrid_2D.ipynb`` cell 20 runs one serial 2D sawtooth cycle on 128^2
 (the cell-5 advection-diffusion weights, a 40 x 40 box of ones at offset 43 as both source
 and initial guess, restriction down to 2 x 2); cells 50 and 52 printed the 2 x 2 and 4 x 4
-corrections to 8 decimals.  ``kolmogorov.Multigrid2D.sawtooth`` runs that cycle.
+corrections to 8 decimals.  ``kolmogorov.Multigrid2D.sawtooth`` runs that cycle; its
+corrections are checked to 1e-8 (the last printed digit; a few float32 ulps of values near
+0.02).
 
 ``notebooks/parallel_multigrid_advection_diffusion_3D.ipynb`` cell 15 runs 100 serial
 sawtooth cycles on 128^3: the 7-point operator with Dx = Dy = Dz = 100 (centre 600), a 40^3
@@ -44,9 +46,9 @@ def test_2d_cycle_printed_corrections(hfm):
     bd = torch.from_numpy(b).cuda().view(1, 128, 128)
     v = mg.sawtooth(bd.clone(), bd)
     np.testing.assert_allclose(mg.w[6][0].cpu().numpy(), np.array(pins["mg2d_w2"]), rtol=0,
-                               atol=6e-9)
+                               atol=1e-8)
     np.testing.assert_allclose(mg.w[5][0].cpu().numpy(), np.array(pins["mg2d_w4"]), rtol=0,
-                               atol=6e-9)
+                               atol=1e-8)
     ref = K2.sawtooth2d(OW.w2_2d_advection_diffusion(), b, b, 7)
     err = np.abs(v[0].cpu().numpy() - ref).max() / np.abs(ref).max()
     assert err < 1e-5, err
