@@ -968,9 +968,14 @@ class Engine : public EngineBase {
       if ((st = launch_restrict<T>(f, n(l - 1), rhs(l), n(l), m_->slots, g(l - 1), m_->active, s)))
         return st;
     }
-    // 3. coarsest: one Jacobi sweep from w = 0
-    if ((st = smooth(L - 1, src(nullptr, n(L - 1)), rhs(L - 1), buf(L - 1, 0), c.omega, 0u, s)))
-      return st;
+    // 3. coarsest: one Jacobi sweep from w = 0 (coarse_sweeps of them with
+    //    HFM_OPT_SAWTOOTH_COARSE_SWEEPS), the last one landing in buffer 0
+    const int ncs = (c.options & HFM_OPT_SAWTOOTH_COARSE_SWEEPS) ? c.coarse_sweeps : 1;
+    for (int k = 0; k < ncs; ++k) {
+      const int dst = (ncs - 1 - k) & 1;
+      PhiSrc<T> p = src(k == 0 ? nullptr : buf(L - 1, dst ^ 1), n(L - 1));
+      if ((st = smooth(L - 1, p, rhs(L - 1), buf(L - 1, dst), c.omega, 0u, s))) return st;
+    }
     // 4. coarse levels: w = P w; one Jacobi
     for (int l = L - 2; l >= 1; --l) {
       PhiSrc<T> p = with_coarse(src(nullptr, n(l)), l + 1, buf(l + 1, 0), 1.f);

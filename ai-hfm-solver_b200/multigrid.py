@@ -45,16 +45,21 @@ class SolverConfig:
     inner_max_cycles: int = 200
     fused_coarse: bool = True   # deep V-cycle levels (<= 4096 cells) in one fused kernel
     fused_pre: bool = True      # first two pre-sweeps from zero in one pass (SIGMA7, TMA levels)
+    sawtooth_coarse_sweeps: int = 1  # Jacobi sweeps on the sawtooth's coarsest level (1 =
+                                     # Anisotropic_3d_Multigrid_7point.ipynb; 2 = the serial
+                                     # run of parallel_multigrid_advection_diffusion_3D.ipynb)
 
     @staticmethod
-    def reference(n_levels, fine_smooth=True, top_copy=False, zero_xend=False, cycles=1000):
+    def reference(n_levels, fine_smooth=True, top_copy=False, zero_xend=False, cycles=1000,
+                  coarse_sweeps=1):
         """The reference sawtooth cycle: omega 1, one Jacobi per level, same operator on every
-        level (``Anisotropic_3d_Multigrid_7point.ipynb:402-449``)."""
+        level (``Anisotropic_3d_Multigrid_7point.ipynb:402-449``); ``coarse_sweeps`` Jacobi
+        sweeps on the coarsest level."""
         return SolverConfig(cycle="sawtooth", n_levels=n_levels, nu_pre=0, nu_post=1,
                             omega=1.0, coarse_omega=1.0, coarse_scale=1.0,
                             sawtooth_fine_smooth=fine_smooth, top_copy=top_copy,
                             zero_xend=zero_xend, tol=1e-300, max_cycles=cycles,
-                            cycles_per_launch=2)
+                            cycles_per_launch=2, sawtooth_coarse_sweeps=coarse_sweeps)
 
     def struct(self, op_kind):
         c = L.HfmMgConfig()
@@ -78,6 +83,9 @@ class SolverConfig:
         c.inner_max_cycles = self.inner_max_cycles
         c.options = (0 if self.fused_coarse else L.OPT_NO_FUSED_COARSE) | \
             (0 if self.fused_pre else L.OPT_NO_FUSED_PRE)
+        if self.cycle == "sawtooth" and self.sawtooth_coarse_sweeps != 1:
+            c.options |= L.OPT_SAWTOOTH_COARSE_SWEEPS
+            c.coarse_sweeps = self.sawtooth_coarse_sweeps
         return c
 
 

@@ -372,7 +372,8 @@ typedef struct {
   int n_levels;           /* 0 = automatic (halve while extents even and min > min_coarse_edge) */
   int min_coarse_edge;    /* default 4 */
   int nu_pre, nu_post;    /* V/F smoothing sweeps (default 2, 2) */
-  int coarse_sweeps;      /* Jacobi sweeps on the coarsest level (V/F; sawtooth uses 1) */
+  int coarse_sweeps;      /* Jacobi sweeps on the coarsest level (V/F; sawtooth uses 1
+                             unless HFM_OPT_SAWTOOTH_COARSE_SWEEPS) */
   float omega;            /* smoother weight (default 2/3; sawtooth reference 1) */
   float coarse_omega;
   float coarse_scale;     /* level l operator scaled by coarse_scale^l (1 = reference) */
@@ -394,6 +395,10 @@ typedef struct {
 /* options: run the first two pre-smoothing sweeps from zero as two passes instead of one
  * (by default the pointwise first sweep phi1 = omega f / diag is formed inside the second) */
 #define HFM_OPT_NO_FUSED_PRE 2
+/* options: the sawtooth cycle sweeps its coarsest level coarse_sweeps times from zero instead
+ * of once (the serial run of notebooks/parallel_multigrid_advection_diffusion_3D.ipynb cell 15
+ * sweeps its 2^3 level twice; Anisotropic_3d_Multigrid_7point.ipynb:424-432 once) */
+#define HFM_OPT_SAWTOOTH_COARSE_SWEEPS 4
 
 typedef struct {
   int active;       /* 1 while the slot is still iterating */

@@ -16,7 +16,8 @@ notebook's, with its ``CNN3D_A_<n>`` / ``CNN3D_res_<n>`` / ``CNN3D_prol_<n>`` mo
 by ``ops.Conv3DSame`` / ``ops.Restriction`` / ``ops.Prolongation`` (one object serves every
 size) and its arithmetic written in the same order.  The printed norm carries the rounding of
 a float32 ``np.linalg.norm`` (5e-5 here), so the exact norm is checked to 1e-4; the solution
-is also checked against the pinned oracle's to 1e-5 of its largest value.
+is also checked against the pinned oracle's to 1e-5 of its largest value.  The same run goes
+through the multigrid handle too (``SolverConfig.reference(coarse_sweeps=2)``).
 """
 import json
 import os
@@ -54,6 +55,23 @@ def test_2d_cycle_printed_corrections(hfm):
     assert err < 1e-5, err
 
 
+_ORACLE_3D = {}
+
+
+def _oracle_3d(w2):
+    """The pinned oracle's solution of the 3D serial run (computed once per session)."""
+    if "v" not in _ORACLE_3D:
+        n = 128
+        Tn = np.zeros((n, n, n), np.float32)
+        Tn[43:83, 43:83, 43:83] = 1.0
+        hier = M.hierarchy(M.Stencil27(w2), 7, 1.0)
+        v = Tn.copy()
+        for _ in range(100):
+            v = M.sawtooth_cycle(hier, v, Tn, coarse_sweeps=2)
+        _ORACLE_3D["v"] = v
+    return _ORACLE_3D["v"]
+
+
 def test_advection_diffusion_3d_serial_run(hfm):
     import torch
     ops, W = hfm.ops, hfm.weights
@@ -85,11 +103,31 @@ def test_advection_diffusion_3d_serial_run(hfm):
     norm = float(got.norm())
     assert abs(norm - printed) / printed < 1e-4, norm
 
-    Tn = np.zeros((n, n, n), np.float32)
-    Tn[43:83, 43:83, 43:83] = 1.0
-    hier = M.hierarchy(M.Stencil27(w2), 7, 1.0)
-    v = Tn.copy()
-    for _ in range(100):
-        v = M.sawtooth_cycle(hier, v, Tn, coarse_sweeps=2)
+    v = _oracle_3d(w2)
+    err = np.abs(got.cpu().numpy() - v).max() / np.abs(v).max()
+    assert err < 1e-5, err
+
+
+def test_advection_diffusion_3d_serial_run_on_the_handle(hfm):
+    """The same run through the multigrid handle (``hfm_mg_*``: the sawtooth cycle with two
+    coarsest sweeps, 100 cycles captured in CUDA graphs)."""
+    import torch
+    Mg, W = hfm.multigrid, hfm.weights
+    printed = _printed()["mg3d_norm_after_100"]
+    w2 = W.anisotropic7(Dx=100.0, Dy=100.0, Dz=100.0)
+    n = 128
+    T = torch.zeros((1, n, n, n), device="cuda")
+    T[0, 43:83, 43:83, 43:83] = 1.0
+    # max_cycles above the 100 run, so that the slot stays active through the last one
+    cfg = Mg.SolverConfig.reference(n_levels=7, cycles=102, coarse_sweeps=2)
+    with Mg.Multigrid((n, n, n), hfm._lib.OP_K27, cfg, slots=1) as h:
+        assert h.levels[-1] == (2, 2, 2)
+        h.set_operator(hfm.ops.Stencil27(w2))
+        h.load(0, T, T)
+        h.run(100)
+        got = h.fetch(0).double()
+    norm = float(got.norm())
+    assert abs(norm - printed) / printed < 1e-4, norm
+    v = _oracle_3d(w2)
     err = np.abs(got.cpu().numpy() - v).max() / np.abs(v).max()
     assert err < 1e-5, err
