@@ -73,3 +73,33 @@ def test_bad_arguments_fail_without_gpu(lib, pkg):
     cfg.cycle = L.CYCLE_F
     assert lib.hfm_mg_create(C.byref(cfg), 8, 8, 8, 1, C.byref(h)) == L.ERR_BAD_ARG
     assert b"F-cycle" in lib.hfm_last_error()
+
+
+def test_slab_entry_points_validate_without_gpu(lib, pkg):
+    """The Z-slab CG helpers reject bad pointers and strides on the host."""
+    L = pkg._lib
+    f = lib.hfm_dot_f64
+    assert f(None, None, 16, 1, 16, None, None, None) == L.ERR_BAD_ARG
+    buf = (C.c_float * 64)()
+    out = (C.c_double * 2)()
+    scratch = (C.c_char * 64)()
+    # two instances whose stride is shorter than an instance overlap
+    assert f(buf, buf, 32, 2, 16, out, scratch, None) == L.ERR_BAD_ARG
+    assert b"hfm_dot_f64" in lib.hfm_last_error()
+    d = (C.c_double * 1)()
+    assert lib.hfm_cg_update_xr(buf, buf, buf, buf, None, d, 16, 1, 16, None) == L.ERR_BAD_ARG
+    assert lib.hfm_cg_update_p(buf, buf, None, d, 16, 1, 16, None) == L.ERR_BAD_ARG
+    assert lib.hfm_cg_update_p(buf, buf, d, d, 0, 1, 16, None) == L.ERR_BAD_ARG
+    assert b"hfm_cg_update_p" in lib.hfm_last_error()
+
+
+def test_sawtooth_coarse_sweeps_option(pkg):
+    """SolverConfig.reference(coarse_sweeps=k) sets the option bit only when k != 1, so the
+    reference cycle's single coarsest sweep stays the default."""
+    M, L = pkg.multigrid, pkg._lib
+    one = M.SolverConfig.reference(n_levels=5).struct(L.OP_K27)
+    assert not one.options & L.OPT_SAWTOOTH_COARSE_SWEEPS
+    two = M.SolverConfig.reference(n_levels=5, coarse_sweeps=2).struct(L.OP_K27)
+    assert two.options & L.OPT_SAWTOOTH_COARSE_SWEEPS and two.coarse_sweeps == 2
+    v = M.SolverConfig(cycle="V", sawtooth_coarse_sweeps=3).struct(L.OP_SIGMA7)
+    assert not v.options & L.OPT_SAWTOOTH_COARSE_SWEEPS and v.coarse_sweeps == 32
