@@ -192,7 +192,10 @@ int hfm_max_abs(const float *x, int64_t n, int B, float *out, void *scratch,
                 hfm_stream_t stream);
 /* Per-instance sum of x * y in float64 (fixed order, scratch as above); instance i starts at
  * x + i * stride (stride >= n when B > 1).  The dot products of the Z-slab conjugate-gradient
- * solver, whose slabs are instances with the halo planes outside the n interior cells. */
+ * solver, whose slabs are instances with the halo planes outside the n interior cells.  No
+ * counterpart in the reference: its cycles run a fixed count (multi_itr,
+ * Anisotropic_3d_Multigrid_7point.ipynb:402-405) and its parallel runs compare norms only
+ * afterwards on the host (parallel_multigrid_advection_diffusion_3D.ipynb cell 72). */
 int hfm_dot_f64(const float *x, const float *y, int64_t n, int B, int64_t stride, double *out,
                 void *scratch, hfm_stream_t stream);
 
