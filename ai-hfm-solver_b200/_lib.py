@@ -69,6 +69,7 @@ SIGNATURES = {
     "hfm_kernel_launch_count": (I64, []),
     "hfm_set_wait_budget": (I, [I]),
     "hfm_device_timeouts": (I, [C.POINTER(I), I]),
+    "hfm_device_drain_timeouts": (I, [C.POINTER(I), I]),
     "hfm_conv3d_k3": (I, [P, P, I, I, I, I, P, P]),
     "hfm_restrict_avg": (I, [P, P, I, I, I, I, P]),
     "hfm_prolong_nearest": (I, [P, P, I, I, I, I, P]),

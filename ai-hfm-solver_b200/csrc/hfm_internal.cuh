@@ -36,6 +36,10 @@ void set_capturing(bool on);
   } while (0)
 
 int sm_count();  // SMs of the current device (cached per device)
+// Device address (current device) of the two TMA wait-failure counters: [0] plane waits that
+// expired, [1] drain waits that expired.  Kernels that must not report success after a
+// failed wait read them.
+int wait_fail_counters(const int **out);
 // Raise a kernel's dynamic shared-memory limit on the current device, once per device and
 // kernel (a process that drives several GPUs needs it on each).
 int set_max_dynamic_smem(const void *kernel, int bytes, const char *what);

@@ -75,8 +75,15 @@ __global__ void k_init_state(SlotState *st, int *active, int slot, const double 
 }
 
 // Sum the residual partials of each slot, update its state, switch it off when done.
+// A TMA plane or drain wait expired somewhere on this device since the counters were last
+// cleared (wf = the two wait-failure counters): the slot's data may come from an incomplete
+// stage, so it ends with HFM_ERR_TIMEOUT instead of a status computed from that data.
+__device__ __forceinline__ bool waits_failed(const int *wf) {
+  return wf && (*(volatile const int *)&wf[0] | *(volatile const int *)&wf[1]);
+}
+
 __global__ void k_check(const double *__restrict__ partials, int nblk, SlotState *st,
-                        int *active, double tol, int max_cycles, int which_buf) {
+                        int *active, double tol, int max_cycles, int which_buf, const int *wf) {
   const int inst = blockIdx.x;
   if (!active[inst]) return;
   __shared__ double sh[32];
@@ -92,7 +99,11 @@ __global__ void k_check(const double *__restrict__ partials, int nblk, SlotState
     double rel = sqrt(tot) / s.norm_b;
     s.rel = rel;
     s.rr = tot;
-    if (!(rel == rel) || isinf(rel)) {
+    if (waits_failed(wf)) {
+      s.status = HFM_ERR_TIMEOUT;
+      s.sol_buf = which_buf;
+      active[inst] = 0;
+    } else if (!(rel == rel) || isinf(rel)) {
       s.status = HFM_ERR_NAN;
       s.sol_buf = which_buf;
       active[inst] = 0;
@@ -117,7 +128,7 @@ __global__ void k_check(const double *__restrict__ partials, int nblk, SlotState
 // the slot to the outer (float64) step.
 __global__ void k_check_inner(const double *__restrict__ partials, int nblk, SlotState *st,
                               int *active, int *outer_mask, double tol, double inner_tol,
-                              int inner_max) {
+                              int inner_max, const int *wf) {
   const int inst = blockIdx.x;
   if (!active[inst]) return;
   __shared__ double sh[32];
@@ -135,7 +146,10 @@ __global__ void k_check_inner(const double *__restrict__ partials, int nblk, Slo
     s.inner_cycles += 1;
     const double r = sqrt(tot);
     const double target = fmax(inner_tol * s.inner_norm, 0.3 * tol * s.norm_b);
-    if (!(r == r) || isinf(r)) {
+    if (waits_failed(wf)) {
+      s.status = HFM_ERR_TIMEOUT;
+      active[inst] = 0;
+    } else if (!(r == r) || isinf(r)) {
       s.status = HFM_ERR_NAN;
       active[inst] = 0;
     } else if (r < target || s.inner_cycles >= inner_max) {
@@ -149,7 +163,8 @@ __global__ void k_check_inner(const double *__restrict__ partials, int nblk, Slo
 // Outer step bookkeeping: relative residual of the float64 solution; finish, or start the
 // next inner solve from its residual.
 __global__ void k_check_outer(const double *__restrict__ partials, int nblk, SlotState *st,
-                              int *active, int *outer_mask, double tol, int max_cycles) {
+                              int *active, int *outer_mask, double tol, int max_cycles,
+                              const int *wf) {
   const int inst = blockIdx.x;
   if (!outer_mask[inst]) return;
   __shared__ double sh[32];
@@ -168,7 +183,9 @@ __global__ void k_check_outer(const double *__restrict__ partials, int nblk, Slo
     s.outer += 1;
     s.first = 0;
     outer_mask[inst] = 0;
-    if (!(rel == rel) || isinf(rel)) {
+    if (waits_failed(wf)) {
+      s.status = HFM_ERR_TIMEOUT;
+    } else if (!(rel == rel) || isinf(rel)) {
       s.status = HFM_ERR_NAN;
     } else if (rel < tol) {
       s.status = HFM_OK;
@@ -732,6 +749,7 @@ struct hfm_mg {
   int64_t partials_per_slot = 0;
   double *scal = nullptr;  // per-slot scratch scalars (rz_new), and ||b||^2 at load
   double *gscale = nullptr;  // fp16 storage: geometric mean of each slot's conductivities
+  const int *wait_fail = nullptr;  // the device's TMA wait-failure counters (read by checks)
   hfm_operator fine_desc;
   cudaStream_t cap = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
@@ -792,7 +810,7 @@ class Engine : public EngineBase {
 
   int check(int nblk, int which, cudaStream_t s) {
     k_check<<<m_->slots, 256, 0, s>>>(m_->partials, nblk, m_->state, m_->active, m_->cfg.tol,
-                                      m_->cfg.max_cycles, which);
+                                      m_->cfg.max_cycles, which, m_->wait_fail);
     HFM_CHECK_LAUNCH("k_check");
     return HFM_OK;
   }
@@ -1028,7 +1046,7 @@ class Engine : public EngineBase {
     }
     HFM_CHECK_LAUNCH("k_residual64");
     k_check_outer<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
-                                    m_->cfg.tol, m_->cfg.max_cycles);
+                                    m_->cfg.tol, m_->cfg.max_cycles, m_->wait_fail);
     HFM_CHECK_LAUNCH("k_check_outer");
     k_ir_start_inner<<<ib, 256, 0, s>>>(m_->cg[0], it, m_->state, m_->active);
     HFM_CHECK_LAUNCH("k_ir_start_inner");
@@ -1086,7 +1104,8 @@ class Engine : public EngineBase {
     HFM_CHECK_LAUNCH("k_cg_xr");
     if (!ir) return check(vb, 0, s);
     k_check_inner<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
-                                    m_->cfg.tol, m_->cfg.inner_tol, m_->cfg.inner_max_cycles);
+                                    m_->cfg.tol, m_->cfg.inner_tol, m_->cfg.inner_max_cycles,
+                                    m_->wait_fail);
     HFM_CHECK_LAUNCH("k_check_inner");
     return HFM_OK;
   }
@@ -1558,6 +1577,7 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
         cudaMemset(m->state, 0, (size_t)slots * sizeof(SlotState)) != cudaSuccess)
       st = fail(HFM_ERR_CUDA, "cudaMemset failed");
   }
+  if (!st) st = wait_fail_counters(&m->wait_fail);
   if (!st && cudaStreamCreateWithFlags(&m->cap, cudaStreamNonBlocking) != cudaSuccess)
     st = fail(HFM_ERR_CUDA, "cudaStreamCreate failed");
   if (!st) {

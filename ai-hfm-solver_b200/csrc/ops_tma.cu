@@ -16,19 +16,25 @@
 // of 64 and HX = 16 / sizeof(T)); no store uses TMA.
 //
 // All waits are bounded: a plane wait that does not complete within the wait budget (2^20
-// polls unless hfm_set_wait_budget lowers it) sets the library's device timeout counter; the
-// block then drains the copies it has issued (waits of up to 2^20 polls each, so no copy lands
-// in shared memory after the block has exited) and returns.
+// polls unless hfm_set_wait_budget lowers it) counts one timeout in the library's device
+// counters; the block then drains the copies it has issued (waits of up to 2^20 polls each)
+// and returns.  When every drain wait completes, no copy lands in shared memory after the
+// block has exited; a drain wait that itself expires is counted separately (the block exits
+// with copies possibly still in flight, and the context is suspect).  The multigrid handle's
+// check kernels read both counters and mark their slots HFM_ERR_TIMEOUT while either is
+// non-zero.
 #include <cuda.h>
 
 #include <atomic>
 #include <mutex>
+#include <vector>
 
 #include "hfm_internal.cuh"
 
 namespace hfm {
 
-static __device__ int g_tma_timeouts;
+// [0]: plane waits that expired, [1]: drain waits that expired (see the file comment)
+static __device__ int g_tma_wait_fail[2];
 static std::atomic<int> g_wait_budget{1 << 20};
 
 namespace {
@@ -500,11 +506,14 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
   }
   if (ok && __syncthreads_or(!mine)) ok = false;  // the last plane's wait
   if (!ok) {
-    if (tid == 0) atomicAdd(&g_tma_timeouts, 1);
+    if (tid == 0) atomicAdd(&g_tma_wait_fail[0], 1);
     // drain: wait (bounded) for the planes whose loads are still in flight, so that no
     // copy lands in shared memory after this block has exited; thread 0 issued them all
-    if (tid == 0)
-      for (int p = p_waited + 1; p < p_next; ++p) wait_plane(p, kMaxSpin);
+    if (tid == 0) {
+      bool drained = true;
+      for (int p = p_waited + 1; p < p_next; ++p) drained = wait_plane(p, kMaxSpin) && drained;
+      if (!drained) atomicAdd(&g_tma_wait_fail[1], 1);
+    }
     return;
   }
   if ((MODE != M_SMOOTH || a.dot_rhs) && a.partials) {
@@ -729,12 +738,43 @@ extern "C" int hfm_set_wait_budget(int polls) {
   return HFM_OK;
 }
 
-extern "C" int hfm_device_timeouts(int *count, int reset) {
-  if (!count) return hfm::fail(HFM_ERR_BAD_ARG, "NULL");
-  HFM_CUDA(cudaMemcpyFromSymbol(count, hfm::g_tma_timeouts, sizeof(int)));
+namespace hfm {
+
+// Device address of g_tma_wait_fail on the current device (looked up once per device with
+// that device current: in host code the array's name only stands for the symbol).
+int wait_fail_counters(const int **out) {
+  static std::mutex mu;
+  static std::vector<const int *> ptrs;
+  int dev = 0;
+  HFM_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)ptrs.size() <= dev) ptrs.resize(dev + 1, nullptr);
+  if (!ptrs[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_tma_wait_fail);
+    if (e != cudaSuccess || !p) return cuda_status(e, "cudaGetSymbolAddress(wait counters)");
+    ptrs[dev] = (const int *)p;
+  }
+  *out = ptrs[dev];
+  return HFM_OK;
+}
+
+static int read_wait_counter(int which, int *count, int reset) {
+  if (!count) return fail(HFM_ERR_BAD_ARG, "NULL");
+  HFM_CUDA(cudaMemcpyFromSymbol(count, g_tma_wait_fail, sizeof(int), which * sizeof(int)));
   if (reset) {
     int zero = 0;
-    HFM_CUDA(cudaMemcpyToSymbol(hfm::g_tma_timeouts, &zero, sizeof(int)));
+    HFM_CUDA(cudaMemcpyToSymbol(g_tma_wait_fail, &zero, sizeof(int), which * sizeof(int)));
   }
   return HFM_OK;
+}
+
+}  // namespace hfm
+
+extern "C" int hfm_device_timeouts(int *count, int reset) {
+  return hfm::read_wait_counter(0, count, reset);
+}
+
+extern "C" int hfm_device_drain_timeouts(int *count, int reset) {
+  return hfm::read_wait_counter(1, count, reset);
 }

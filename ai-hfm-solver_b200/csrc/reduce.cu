@@ -210,14 +210,19 @@ HFM_RED_INST(__half)
 // ------------------------------------------------------------------------- C ABI
 using namespace hfm;
 
+// The per-instance reductions launch one grid row per instance (gridDim.y = B), so B is
+// limited to the grid's y extent.
+constexpr int kMaxInstances = 65535;
+
 extern "C" size_t hfm_reduce_scratch_bytes(int64_t n, int B) {
-  if (n <= 0 || B <= 0) return 0;
+  if (n <= 0 || B <= 0 || B > kMaxInstances) return 0;
   return (size_t)reduce_blocks_for(n) * (size_t)B * sizeof(double);
 }
 
 extern "C" int hfm_norm2_f64(const float *x, int64_t n, int B, double *out, void *scratch,
                              hfm_stream_t stream) {
   if (!x || !out || !scratch || n <= 0 || B <= 0) return fail(HFM_ERR_BAD_ARG, "hfm_norm2_f64: bad argument");
+  if (B > kMaxInstances) return fail(HFM_ERR_BAD_ARG, "hfm_norm2_f64: at most 65535 instances");
   cudaStream_t s = (cudaStream_t)stream;
   int nb = 0;
   int st = launch_sumsq_partials<float>(x, n, n, B, (double *)scratch, &nb, nullptr, s);
@@ -257,6 +262,7 @@ int noalloc_scratch(double **out) {
 extern "C" int hfm_norm2_f64_noalloc(const float *x, int64_t n, int B, double *out,
                                      hfm_stream_t stream) {
   if (!x || !out || n <= 0 || B <= 0) return fail(HFM_ERR_BAD_ARG, "hfm_norm2_f64_noalloc: bad argument");
+  if (B > kMaxInstances) return fail(HFM_ERR_BAD_ARG, "hfm_norm2_f64_noalloc: at most 65535 instances");
   const size_t need = hfm_reduce_scratch_bytes(n, B);
   if (need > HFM_NORM2_NOALLOC_SCRATCH_BYTES)
     return fail(HFM_ERR_BAD_ARG,
@@ -282,6 +288,7 @@ extern "C" int hfm_dot_f64(const float *x, const float *y, int64_t n, int B, int
                            double *out, void *scratch, hfm_stream_t stream) {
   if (!x || !y || !out || !scratch || n <= 0 || B <= 0 || (B > 1 && stride < n))
     return fail(HFM_ERR_BAD_ARG, "hfm_dot_f64: bad argument");
+  if (B > kMaxInstances) return fail(HFM_ERR_BAD_ARG, "hfm_dot_f64: at most 65535 instances");
   cudaStream_t s = (cudaStream_t)stream;
   const int nb = reduce_blocks_for(n);
   k_dot<<<dim3(nb, B), kThreads, 0, s>>>(x, y, n, stride, (double *)scratch);
@@ -292,6 +299,7 @@ extern "C" int hfm_dot_f64(const float *x, const float *y, int64_t n, int B, int
 extern "C" int hfm_max_abs(const float *x, int64_t n, int B, float *out, void *scratch,
                            hfm_stream_t stream) {
   if (!x || !out || !scratch || n <= 0 || B <= 0) return fail(HFM_ERR_BAD_ARG, "hfm_max_abs: bad argument");
+  if (B > kMaxInstances) return fail(HFM_ERR_BAD_ARG, "hfm_max_abs: at most 65535 instances");
   cudaStream_t s = (cudaStream_t)stream;
   int nb = reduce_blocks_for(n);
   k_maxabs<<<dim3(nb, B), kThreads, 0, s>>>(x, n, (float *)scratch);

@@ -204,12 +204,13 @@ class Multigrid:
 
     def solve(self, rhs):
         """Solve every slot for ``rhs`` of shape ``(slots, Z, Y, X)``; returns (phi, stats).
-        A slot that does not reach tolerance keeps its status in stats (no exception)."""
+        A slot that does not reach tolerance, meets NaN or sees an expired device wait keeps
+        its status in stats (no exception)."""
         _check_field(rhs, "rhs")
         phi = torch.empty_like(rhs)
         st = L.lib().hfm_mg_solve(self._h, C.c_void_p(rhs.data_ptr()), C.c_void_p(phi.data_ptr()),
                                   self._stats, _stream())
-        if st not in (L.OK, L.ERR_NOT_CONVERGED, L.ERR_NAN):
+        if st not in (L.OK, L.ERR_NOT_CONVERGED, L.ERR_NAN, L.ERR_TIMEOUT):
             L.check(st, "hfm_mg_solve")
         stats = [dict(active=s.active, status=s.status, cycles=s.cycles, outer=s.outer,
                       norm_b=s.norm_b, rel_resid=s.rel_resid) for s in self._stats]

@@ -220,6 +220,13 @@ class NSStepper:
         self.mg.set_operator(Stencil27(self.Kp))
         self.itime = 0
         self.p_cycles = []
+        self.p_status = []  # per step: the pressure solve's status (0 = reached p_tol)
+        self.p_rel = []     # and its relative residual
+        # the reference's clock (naiver_stokes_3D.py:519-523, 549, 572): ctime_old is
+        # nrestart * dt after a restart, and each step adds dt + ctime_old to ctime
+        self.nrestart = 0
+        self.ctime_old = 0.0
+        self.ctime = 0.0
 
     def close(self):
         self.mg.close()
@@ -231,6 +238,8 @@ class NSStepper:
             self.mg.run(c.multi_itr)
             self.mg.fetch(0, self.p)
             self.p_cycles.append(c.multi_itr)
+            self.p_status.append(L.OK)  # a fixed cycle count, no tolerance (as the reference)
+            self.p_rel.append(float("nan"))
         else:
             self.mg.load(0, self.rhs, self.p)
             while True:
@@ -240,6 +249,8 @@ class NSStepper:
                     break
             self.mg.fetch(0, self.p)
             self.p_cycles.append(st["cycles"])
+            self.p_status.append(st["status"])
+            self.p_rel.append(st["rel_resid"])
 
     def step(self):
         """One time step in the reference's order (naiver_stokes_3D.py:571-727)."""
@@ -272,22 +283,38 @@ class NSStepper:
         pressure_gradient(p, u, v, w, self.Kx, self.Ky, self.Kz)
         boundary_condition_velocity(u, v, w, c.ub)
         bluff_body(u, v, w, self.sigma, c.dt)
+        self.ctime = self.ctime + c.dt + self.ctime_old
         self.itime += 1
 
-    # reference checkpoint layout: u, v, w, p saved as (Z, Y, X) float32 .npy per output step
-    # (save_data, naiver_stokes_3D.py:488-497; restart :531-549)
-    def save(self, directory, itime=None):
+    # reference checkpoint layout: u, v, w, p saved as (Z, Y, X) float32 .npy files named
+    # <field><step> (save_data, naiver_stokes_3D.py:488-497; restart :531-549)
+    def save(self, directory, itime=None, n_out=None):
+        """Write u, v, w, p as ``u<itime>.npy`` ... in ``directory``.  ``itime`` defaults to
+        the steps taken so far; with ``n_out`` the files are written only when ``itime`` is a
+        multiple of it, as ``save_data`` does.  Returns True when files were written."""
         it = self.itime if itime is None else itime
+        if n_out is not None and it % n_out != 0:
+            return False
         os.makedirs(directory, exist_ok=True)
         for name in ("u", "v", "w", "p"):
             np.save(os.path.join(directory, "%s%d.npy" % (name, it)),
                     getattr(self, name).cpu().numpy())
+        return True
 
     def restart(self, directory, itime):
+        """Read ``u<itime>.npy`` ... (cast to float32) into the fields and continue from step
+        ``itime``: nrestart = itime, ctime_old = nrestart * dt (naiver_stokes_3D.py:531-549)."""
+        arrays = {}
         for name in ("u", "v", "w", "p"):
             a = np.load(os.path.join(directory, "%s%d.npy" % (name, itime))).astype(np.float32)
+            if a.shape != self.shape:
+                raise ValueError("%s%d.npy has shape %s, the stepper %s" % (name, itime, a.shape, self.shape))
+            arrays[name] = a
+        for name, a in arrays.items():
             getattr(self, name).copy_(torch.from_numpy(a))
         self.itime = itime
+        self.nrestart = itime
+        self.ctime_old = itime * self.cfg.dt
 
     def max_divergence(self):
         b = torch.empty_like(self.u)

@@ -86,8 +86,17 @@ int hfm_device_sm_count(int *sm_count); /* current device's SM count */
 /* Kernels this library has enqueued since load (a CUDA-graph launch counts its kernel nodes). */
 int64_t hfm_kernel_launch_count(void);
 /* Bounded device-side waits that expired on the current device (TMA pipeline stages); a
- * non-zero count means results of the affected launches are invalid.  reset != 0 clears it. */
+ * non-zero count means results of the affected launches are invalid.  reset != 0 clears it.
+ * While this count or the drain count below is non-zero, every multigrid handle's
+ * convergence check on this device marks its active slots HFM_ERR_TIMEOUT and switches
+ * them off (no slot reports success after a failed wait); clear both to resume. */
 int hfm_device_timeouts(int *count, int reset);
+/* Drain waits that expired: after a plane wait expires, the block waits (bounded) for the
+ * copies it already issued; if that wait expires as well, the block exits with copies
+ * possibly still in flight and this count is raised.  A non-zero value means the context is
+ * suspect: stop issuing work on the device and report it.  reset != 0 clears it.  No
+ * counterpart in the reference. */
+int hfm_device_drain_timeouts(int *count, int reset);
 /* Poll budget of those waits for launches made after the call (default and maximum 2^20).
  * Budget 0 makes every such wait expire at once - the failure path, for tests: each block
  * stops, lets the copies it issued land, counts the timeout and returns; results of those
@@ -184,7 +193,9 @@ int hfm_stencil27_jacobi(const float *phi, const float *rhs, float *out, float *
 /* Per-instance reductions over n elements of each of B instances (HFM3 diagnostics
  * np.max(w), np.max(r): Urban Modelling/AI_HFM_v3.ipynb:2622-2627).  Results land in device
  * memory (B values).  `scratch` is caller device memory of hfm_reduce_scratch_bytes(n, B)
- * bytes; the summation order is fixed, so results do not depend on other work in flight. */
+ * bytes; the summation order is fixed, so results do not depend on other work in flight.
+ * B is at most 65535 (one grid row per instance); larger B returns HFM_ERR_BAD_ARG and
+ * hfm_reduce_scratch_bytes returns 0 for it. */
 size_t hfm_reduce_scratch_bytes(int64_t n, int B);
 int hfm_norm2_f64(const float *x, int64_t n, int B, double *out, void *scratch,
                   hfm_stream_t stream); /* sqrt(sum x^2), accumulated in float64 */

@@ -94,9 +94,11 @@ def divergence_rhs(u, v, w, Su, Sv, Sw):
     return bc_source(b)
 
 
-def step(u, v, w, p, sigma, dt, ub, Kdif, Kx, Ky, Kz, Su, Sv, Sw, Kp, n_levels, multi_itr):
+def step(u, v, w, p, sigma, dt, ub, Kdif, Kx, Ky, Kz, Su, Sv, Sw, Kp, n_levels, multi_itr,
+         pressure=None):
     """One reference time step (naiver_stokes_3D.py:571-727) with the reference's pressure
-    multigrid (sawtooth NS form)."""
+    multigrid (sawtooth NS form, ``multi_itr`` cycles), or with ``pressure(p, b) -> p``
+    solving the pressure equation instead when it is given."""
     from . import mg
     u, v, w = bc_velocity(u, v, w, ub)
     p = bc_pressure(p)
@@ -105,9 +107,12 @@ def step(u, v, w, p, sigma, dt, ub, Kdif, Kx, Ky, Kz, Su, Sv, Sw, Kp, n_levels, 
     u, v, w = pressure_gradient(p, u, v, w, Kx, Ky, Kz)
     u, v, w = bc_velocity(u, v, w, ub)
     b = divergence_rhs(u, v, w, Su, Sv, Sw)
-    ops = mg.hierarchy(mg.Stencil27(Kp), n_levels)
-    for _ in range(multi_itr):
-        p = mg.sawtooth_cycle(ops, p, b, fine_smooth=False, zero_xend=True)
+    if pressure is not None:
+        p = pressure(p, b)
+    else:
+        ops = mg.hierarchy(mg.Stencil27(Kp), n_levels)
+        for _ in range(multi_itr):
+            p = mg.sawtooth_cycle(ops, p, b, fine_smooth=False, zero_xend=True)
     p = bc_pressure(p)
     u, v, w = pressure_gradient(p, u, v, w, Kx, Ky, Kz)
     u, v, w = bc_velocity(u, v, w, ub)

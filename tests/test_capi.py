@@ -93,6 +93,23 @@ def test_slab_entry_points_validate_without_gpu(lib, pkg):
     assert b"hfm_cg_update_p" in lib.hfm_last_error()
 
 
+def test_reductions_reject_more_instances_than_grid_rows(lib, pkg):
+    """One grid row per instance: B = 65536 is refused on the host with HFM_ERR_BAD_ARG, not
+    left to fail as a launch error."""
+    L = pkg._lib
+    buf = (C.c_float * 64)()
+    out = (C.c_double * 2)()
+    scratch = (C.c_char * 64)()
+    B = 65536
+    assert lib.hfm_reduce_scratch_bytes(8, B) == 0
+    assert lib.hfm_reduce_scratch_bytes(8, B - 1) > 0
+    assert lib.hfm_norm2_f64(buf, 8, B, out, scratch, None) == L.ERR_BAD_ARG
+    assert b"65535" in lib.hfm_last_error()
+    assert lib.hfm_norm2_f64_noalloc(buf, 8, B, out, None) == L.ERR_BAD_ARG
+    assert lib.hfm_dot_f64(buf, buf, 8, B, 8, out, scratch, None) == L.ERR_BAD_ARG
+    assert lib.hfm_max_abs(buf, 8, B, buf, scratch, None) == L.ERR_BAD_ARG
+
+
 def test_sawtooth_coarse_sweeps_option(pkg):
     """SolverConfig.reference(coarse_sweeps=k) sets the option bit only when k != 1, so the
     reference cycle's single coarsest sweep stays the default."""

@@ -42,3 +42,43 @@ def test_expired_waits_are_counted_and_the_context_survives(hfm):
         oop = mg.Sigma7(sig[0, i], sig[1, i], sig[2, i], dtype=np.float64)
         ref = mg.jacobi(oop, x[i].astype(np.float64), b[i].astype(np.float64), 0.8)
         assert np.abs(y[i] - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("accel,storage", [("cg", "f32"), ("ir", "bf16")])
+def test_handle_reports_timeout_after_expired_waits(hfm, accel, storage):
+    """A solve whose TMA waits expire ends every slot with HFM_ERR_TIMEOUT (never with a status
+    computed from an incomplete stage); after the counters are cleared a new handle solves."""
+    import torch
+    L, M, ops = hfm._lib, hfm.multigrid, hfm.ops
+    n, B = 64, 2  # TMA-eligible fine level
+    sig = np.stack([hfm.problems.anisotropic_sigma((n, n, n), seed=5 + i, log_std=1.0)
+                    for i in range(B)], axis=1)
+    f = np.stack([hfm.problems.dipole((n, n, n), seed=5 + i) for i in range(B)])
+    sd = torch.from_numpy(sig).cuda()
+    fd = torch.from_numpy(f).cuda()
+    op = ops.Sigma7(sd[0], sd[1], sd[2])
+    cfg = M.SolverConfig(cycle="V", accel=accel, storage=storage, tol=1e-6, max_cycles=60)
+    cnt, drain = C.c_int(0), C.c_int(0)
+    L.call("hfm_device_timeouts", C.byref(cnt), 1)
+    L.call("hfm_device_drain_timeouts", C.byref(drain), 1)
+    L.call("hfm_set_wait_budget", 0)  # graphs captured from here on carry budget 0
+    try:
+        with M.Multigrid((n, n, n), L.OP_SIGMA7, cfg, slots=B) as h:
+            h.set_operator(op)
+            _, stats = h.solve(fd)
+    finally:
+        L.call("hfm_set_wait_budget", 1 << 20)
+    L.call("hfm_device_timeouts", C.byref(cnt), 1)
+    L.call("hfm_device_drain_timeouts", C.byref(drain), 1)
+    assert cnt.value > 0 and drain.value == 0
+    assert [s["status"] for s in stats] == [L.ERR_TIMEOUT] * B, stats
+    assert not any(s["active"] for s in stats)
+    with M.Multigrid((n, n, n), L.OP_SIGMA7, cfg, slots=B) as h:
+        h.set_operator(op)
+        phi, stats = h.solve(fd)
+    assert [s["status"] for s in stats] == [L.OK] * B, stats
+    L.call("hfm_device_timeouts", C.byref(cnt), 0)
+    assert cnt.value == 0
+    for i in range(B):
+        oop = mg.Sigma7(sig[0, i], sig[1, i], sig[2, i], dtype=np.float64)
+        assert mg.rel_residual(oop, phi[i].double().cpu().numpy(), f[i]) < 2e-6

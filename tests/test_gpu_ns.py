@@ -1,5 +1,7 @@
 """NS time-stepper operators on the GPU against the oracle, and a full
 reference time step."""
+import os
+
 import numpy as np
 import pytest
 
@@ -138,3 +140,53 @@ def test_petrov_galerkin_dissipation_and_momentum(env):
         s2.step()
     assert all(bool(torch.isfinite(t).all()) for t in (s2.u, s2.v, s2.w, s2.p))
     s2.close()
+
+
+def test_checkpoint_restart_continues_bitwise(env, tmp_path):
+    """N steps, save in the reference's .npy layout, a fresh stepper restarts from the files
+    and takes N more: the fields equal those of 2N uninterrupted steps bit for bit, and the
+    restart clock follows naiver_stokes_3D.py:531-549, 572 (ctime_old = nrestart dt, each step
+    adds dt + ctime_old)."""
+    hfm, torch, _ = env
+    ns = hfm.ns
+    shape, N = (16, 32, 32), 3
+    cfg = ns.NSConfig(dt=0.5, dx=1.0, Re=0.05, ub=1.0, diffusion="7", pressure="fcycle", p_tol=1e-5)
+    sig = ns.obstacle_mask(shape, n_boxes=4, footprint=(3, 6), height=(4, 10), sigma=1e5, seed=2)
+    ref = ns.NSStepper(shape, cfg, sigma=sig)
+    try:
+        for _ in range(2 * N):
+            ref.step()
+        want = {k: getattr(ref, k).cpu().numpy() for k in ("u", "v", "w", "p")}
+    finally:
+        ref.close()
+    a = ns.NSStepper(shape, cfg, sigma=sig)
+    try:
+        for _ in range(N):
+            a.step()
+        assert not a.save(str(tmp_path), n_out=2)  # step 3 is not a multiple of n_out = 2
+        assert a.save(str(tmp_path), n_out=N)
+        assert sorted(os.listdir(tmp_path)) == ["p3.npy", "u3.npy", "v3.npy", "w3.npy"]
+        assert np.load(tmp_path / "u3.npy").shape == shape
+    finally:
+        a.close()
+    b = ns.NSStepper(shape, cfg, sigma=sig)
+    try:
+        b.restart(str(tmp_path), N)
+        assert b.itime == N and b.nrestart == N and b.ctime_old == N * cfg.dt
+        for _ in range(N):
+            b.step()
+        assert b.itime == 2 * N
+        # the reference's accumulation: ctime = ctime + dt + ctime_old at every step
+        clock = 0.0
+        for _ in range(N):
+            clock = clock + cfg.dt + N * cfg.dt
+        assert b.ctime == clock
+        for k, v in want.items():
+            np.testing.assert_array_equal(getattr(b, k).cpu().numpy(), v, err_msg=k)
+        with pytest.raises(ValueError):
+            np.save(tmp_path / "u9.npy", np.zeros((4, 4, 4), np.float32))
+            for k in ("v", "w", "p"):
+                np.save(tmp_path / ("%s9.npy" % k), np.zeros(shape, np.float32))
+            b.restart(str(tmp_path), 9)
+    finally:
+        b.close()

@@ -315,3 +315,25 @@ def test_mesh_mask_follows_reference_loop(pkg):
                     ref[0][k][j][i][0] = 100000
     got = ns.mask_from_mesh(mesh, (nz, ny, nx), device="cpu").numpy()
     np.testing.assert_array_equal(got, ref[0, ..., 0])
+
+
+def test_load_mesh_mask_reads_reference_mesh_file(pkg, tmp_path):
+    """ns.load_mesh_mask on a mesh_<n>_sk.npy-style file written here: the file's array goes
+    through the reference's loop (naiver_stokes_3D.py:527, 560-564) unchanged."""
+    pytest.importorskip("torch")
+    ns = pkg.ns
+    nx, ny, nz = 10, 9, 6
+    rng = np.random.default_rng(11)
+    mesh = (rng.random((1, nx + 32, ny + 32, nz + 3, 1)) > 0.4).astype(np.float32)
+    path = tmp_path / "mesh_10_sk.npy"
+    np.save(path, mesh)
+    ref = np.zeros((nz, ny, nx))
+    for i in range(1, nx - 1):
+        for j in range(1, ny - 1):
+            for k in range(1, nz - 1):
+                if mesh[0][i + 16][j + 16][k][0] == 0:
+                    ref[k][j][i] = 100000
+    got = ns.load_mesh_mask(str(path), (nz, ny, nx), device="cpu").numpy()
+    assert got.dtype == np.float32
+    np.testing.assert_array_equal(got, ref)
+    assert (got > 0).sum() > 0

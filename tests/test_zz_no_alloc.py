@@ -38,7 +38,8 @@ def test_noalloc_norm_matches_scratch_version_twice(hfm):
     for B, n in ((7, 300001), (3, 4096)):
         x = torch.randn(B * n, device="cuda", dtype=torch.float32)
         got, ref = _norm_both(hfm, x, B)
-        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=0)
+        # same kernels, same summation order: the same bits
+        np.testing.assert_array_equal(got, ref)
         np.testing.assert_allclose(got, np.linalg.norm(x.view(B, n).double().cpu().numpy(), axis=1),
                                    rtol=1e-12)
 
@@ -55,3 +56,11 @@ def test_noalloc_norm_rejects_oversize(hfm):
                                    C.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert st == L.ERR_BAD_ARG
     assert b"static" in lib.hfm_last_error()
+    # one grid row per instance: 65536 instances are rejected before any launch, even when
+    # their partial sums would fit the array
+    n, B = 8, 65536
+    st = lib.hfm_norm2_f64_noalloc(C.c_void_p(x.data_ptr()), n, B, C.c_void_p(out.data_ptr()),
+                                   C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == L.ERR_BAD_ARG
+    assert b"65535" in lib.hfm_last_error()
+    assert lib.hfm_reduce_scratch_bytes(n, B) == 0
