@@ -14,13 +14,13 @@ OK, ERR_BAD_ARG, ERR_OOM, ERR_NOT_CONVERGED, ERR_NAN, ERR_TIMEOUT, ERR_CUDA, ERR
 # hfm_dtype
 F32, BF16, F16, F64 = range(4)
 # hfm_op_kind
-OP_CONST7, OP_SIGMA7, OP_DIR7, OP_K27 = range(4)
+OP_CONST7, OP_SIGMA7, OP_DIR7, OP_K27, OP_FACE7 = range(5)
 # flags
 FLAG_ZERO_XEND, FLAG_TOP_COPY, FLAG_ZERO_GUESS, FLAG_PERIODIC, FLAG_SAME_LEVEL_CORR = 1, 2, 4, 8, 16
 # hfm_cycle / hfm_accel
 CYCLE_SAWTOOTH, CYCLE_V, CYCLE_F = range(3)
 ACCEL_NONE, ACCEL_CG, ACCEL_IR = range(3)
-OPT_NO_FUSED_COARSE, OPT_NO_FUSED_PRE, OPT_SAWTOOTH_COARSE_SWEEPS = 1, 2, 4
+OPT_NO_FUSED_COARSE, OPT_NO_FUSED_PRE, OPT_SAWTOOTH_COARSE_SWEEPS, OPT_NO_FACES = 1, 2, 4, 8
 
 
 class HfmOperator(C.Structure):
@@ -77,6 +77,11 @@ SIGNATURES = {
     "hfm_op_residual": (I, [P, P, P, P, I, I, I, I, U, P]),
     "hfm_op_jacobi": (I, [P, P, P, P, P, I, I, I, I, F, I, U, P]),
     "hfm_op_jacobi_typed": (I, [P, I, P, P, P, I, I, I, I, F, U, P]),
+    "hfm_op_residual_typed": (I, [P, I, P, P, P, I, I, I, I, U, P]),
+    "hfm_residual_restrict_typed": (I, [P, I, P, P, P, P, I, I, I, I, U, P]),
+    "hfm_prolong_correct_smooth_typed": (I, [P, I, P, P, P, P, I, I, I, I, F, U, P]),
+    "hfm_sigma7_faces": (I, [I, P, P, P, F, F, F, P, P, P, I, I, I, I, P]),
+    "hfm_face7_elems": (I, [I, I, I, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
     "hfm_residual_restrict": (I, [P, P, P, P, P, I, I, I, I, U, P]),
     "hfm_prolong_correct_smooth": (I, [P, P, P, P, P, I, I, I, I, F, U, P]),
     "hfm_stencil7_const_apply": (I, [P, P, I, I, I, I, F, F, F, P]),

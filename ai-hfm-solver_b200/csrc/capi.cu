@@ -108,10 +108,49 @@ int check_op(const hfm_operator *op) {
       for (int i = 0; i < 7; ++i)
         if (!op->coef[i]) return fail(HFM_ERR_BAD_ARG, "DIR7 needs seven coefficient arrays");
       return HFM_OK;
+    case HFM_OP_FACE7:
+      for (int i = 0; i < 3; ++i)
+        if (!op->coef[i]) return fail(HFM_ERR_BAD_ARG, "FACE7 needs Fx, Fy, Fz");
+      return HFM_OK;
     default:
       return fail(HFM_ERR_BAD_ARG, "unknown operator kind");
   }
 }
+
+// Operator of a typed (storage-dtype) call: the coefficient arrays are stored as dtype.
+int check_op_typed(const hfm_operator *op, int dtype, const char *who) {
+  if (!op) return fail(HFM_ERR_BAD_ARG, std::string(who) + ": operator is NULL");
+  if (dtype != HFM_F32 && dtype != HFM_BF16 && dtype != HFM_F16)
+    return fail(HFM_ERR_BAD_ARG, std::string(who) + ": dtype must be F32, BF16 or F16");
+  int na = 0;
+  switch (op->kind) {
+    case HFM_OP_SIGMA7: case HFM_OP_FACE7: na = 3; break;
+    case HFM_OP_DIR7: na = 7; break;
+    case HFM_OP_CONST7: case HFM_OP_K27: na = 0; break;
+    default: return fail(HFM_ERR_BAD_ARG, "unknown operator kind");
+  }
+  if (na && op->coef_dtype != dtype)
+    return fail(HFM_ERR_BAD_ARG, std::string(who) + ": coef_dtype must equal dtype");
+  for (int i = 0; i < na; ++i)
+    if (!op->coef[i]) return fail(HFM_ERR_BAD_ARG, std::string(who) + ": missing coefficient array");
+  return HFM_OK;
+}
+
+template <class T> PhiSrc<T> typed_src(const void *phi, int64_t n, unsigned flags) {
+  PhiSrc<T> p;
+  memset(&p, 0, sizeof(p));
+  p.base = (flags & HFM_FLAG_ZERO_GUESS) ? nullptr : (const T *)phi;
+  p.base_stride = n;
+  p.zero_xend = (flags & HFM_FLAG_ZERO_XEND) ? 1 : 0;
+  return p;
+}
+
+#define HFM_BY_DTYPE(dtype, BODY)                                  \
+  switch (dtype) {                                                 \
+    case HFM_F32: { using T = float; BODY; }                       \
+    case HFM_BF16: { using T = __nv_bfloat16; BODY; }              \
+    default: { using T = __half; BODY; }                           \
+  }
 
 PhiSrc<float> plain_src(const float *phi, int64_t stride, unsigned flags) {
   PhiSrc<float> p;
@@ -244,33 +283,67 @@ int hfm_op_jacobi_typed(const hfm_operator *op, int dtype, const void *phi, cons
   if ((st = check_grid(B, Z, Y, X))) return st;
   if (!op || !rhs || !out || (!phi && !(flags & HFM_FLAG_ZERO_GUESS)))
     return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: NULL argument");
-  if (dtype != HFM_F32 && dtype != HFM_BF16 && dtype != HFM_F16)
-    return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: dtype must be F32, BF16 or F16");
-  if (op->kind == HFM_OP_SIGMA7 || op->kind == HFM_OP_DIR7) {
-    if (op->coef_dtype != dtype) return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: coef_dtype must equal dtype");
-    for (int i = 0; i < (op->kind == HFM_OP_SIGMA7 ? 3 : 7); ++i)
-      if (!op->coef[i]) return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: missing coefficient array");
-  } else if (op->kind != HFM_OP_CONST7 && op->kind != HFM_OP_K27) {
-    return fail(HFM_ERR_BAD_ARG, "unknown operator kind");
-  }
+  if ((st = check_op_typed(op, dtype, "hfm_op_jacobi_typed"))) return st;
   if (phi == out) return fail(HFM_ERR_BAD_ARG, "hfm_op_jacobi_typed: phi aliases out");
   const int64_t n = (int64_t)Z * Y * X;
   DevOp d = make_devop(*op, n);
-  const void *base = (flags & HFM_FLAG_ZERO_GUESS) ? nullptr : phi;
-#define HFM_TYPED(T)                                                                         \
-  {                                                                                          \
-    PhiSrc<T> p;                                                                             \
-    memset(&p, 0, sizeof(p));                                                                \
-    p.base = (const T *)base;                                                                \
-    p.base_stride = n;                                                                       \
-    p.zero_xend = (flags & HFM_FLAG_ZERO_XEND) ? 1 : 0;                                      \
-    return launch_smooth<T>(op->kind, d, p, (const T *)rhs, n, (T *)out, n, B, Grid3{Z, Y, X}, \
-                            omega, flags, nullptr, (cudaStream_t)stream);                    \
-  }
-  if (dtype == HFM_F32) HFM_TYPED(float)
-  if (dtype == HFM_BF16) HFM_TYPED(__nv_bfloat16)
-  HFM_TYPED(__half)
-#undef HFM_TYPED
+  HFM_BY_DTYPE(dtype, return launch_smooth<T>(op->kind, d, typed_src<T>(phi, n, flags),
+                                              (const T *)rhs, n, (T *)out, n, B, Grid3{Z, Y, X},
+                                              omega, flags, nullptr, (cudaStream_t)stream))
+}
+
+int hfm_op_residual_typed(const hfm_operator *op, int dtype, const void *phi, const void *b,
+                          void *r, int B, int Z, int Y, int X, unsigned flags,
+                          hfm_stream_t stream) {
+  int st;
+  if ((st = check_grid(B, Z, Y, X))) return st;
+  if (!phi || !b || !r) return fail(HFM_ERR_BAD_ARG, "hfm_op_residual_typed: NULL field");
+  if ((st = check_op_typed(op, dtype, "hfm_op_residual_typed"))) return st;
+  const int64_t n = (int64_t)Z * Y * X;
+  DevOp d = make_devop(*op, n);
+  HFM_BY_DTYPE(dtype, return launch_residual<T>(op->kind, d, typed_src<T>(phi, n, flags), (const T *)b,
+                                                n, (T *)r, n, B, Grid3{Z, Y, X}, flags, nullptr,
+                                                nullptr, nullptr, (cudaStream_t)stream))
+}
+
+int hfm_residual_restrict_typed(const hfm_operator *op, int dtype, const void *phi,
+                                const void *b, void *r_fine, void *r_coarse, int B, int Z,
+                                int Y, int X, unsigned flags, hfm_stream_t stream) {
+  int st;
+  if ((st = check_grid(B, Z, Y, X))) return st;
+  if (!phi || !b || !r_coarse) return fail(HFM_ERR_BAD_ARG, "hfm_residual_restrict_typed: NULL field");
+  if ((st = check_op_typed(op, dtype, "hfm_residual_restrict_typed"))) return st;
+  const int64_t n = (int64_t)Z * Y * X;
+  DevOp d = make_devop(*op, n);
+  HFM_BY_DTYPE(dtype, return launch_residual_restrict<T>(
+                          op->kind, d, typed_src<T>(phi, n, flags & HFM_FLAG_ZERO_GUESS),
+                          (const T *)b, n, (T *)r_fine, n, (T *)r_coarse, n / 8, B,
+                          Grid3{Z, Y, X}, flags, nullptr, nullptr, nullptr, (cudaStream_t)stream))
+}
+
+int hfm_prolong_correct_smooth_typed(const hfm_operator *op, int dtype, const void *phi,
+                                     const void *w_coarse, const void *rhs, void *out, int B,
+                                     int Z, int Y, int X, float omega, unsigned flags,
+                                     hfm_stream_t stream) {
+  int st;
+  if ((st = check_grid(B, Z, Y, X))) return st;
+  if (!w_coarse || !rhs || !out) return fail(HFM_ERR_BAD_ARG, "hfm_prolong_correct_smooth_typed: NULL field");
+  if ((Z | Y | X) & 1) return fail(HFM_ERR_BAD_ARG, "hfm_prolong_correct_smooth_typed: fine extents must be even");
+  if (phi == out) return fail(HFM_ERR_BAD_ARG, "hfm_prolong_correct_smooth_typed: phi aliases out");
+  if ((st = check_op_typed(op, dtype, "hfm_prolong_correct_smooth_typed"))) return st;
+  const int64_t n = (int64_t)Z * Y * X;
+  DevOp d = make_devop(*op, n);
+  HFM_BY_DTYPE(dtype, {
+    PhiSrc<T> p = typed_src<T>(phi, n, flags);
+    p.corr = (const T *)w_coarse;
+    p.corr_stride = n / 8;
+    p.corr_coarse = 1;
+    p.corr_sign = phi ? -1.f : 1.f;
+    p.Yc = Y / 2;
+    p.Xc = X / 2;
+    return launch_smooth<T>(op->kind, d, p, (const T *)rhs, n, (T *)out, n, B, Grid3{Z, Y, X},
+                            omega, flags, nullptr, (cudaStream_t)stream);
+  })
 }
 
 int hfm_residual_restrict(const hfm_operator *op, const float *phi, const float *b,

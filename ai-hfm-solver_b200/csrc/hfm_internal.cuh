@@ -111,6 +111,11 @@ template <class T> struct PhiSrc {
   }
 };
 
+// FACE7 arrays: elements per instance of Fx [Z][Y][X + 8], Fy [Z][Y + 1][X], Fz [Z + 1][Y][X].
+__host__ __device__ __forceinline__ int64_t face7_nx(int Z, int Y, int X) { return (int64_t)Z * Y * (X + 8); }
+__host__ __device__ __forceinline__ int64_t face7_ny(int Z, int Y, int X) { return (int64_t)Z * (Y + 1) * X; }
+__host__ __device__ __forceinline__ int64_t face7_nz(int Z, int Y, int X) { return (int64_t)(Z + 1) * Y * X; }
+
 // Evaluate (A phi')(z,y,x) and the Jacobi diagonal for operator KIND.
 template <int KIND, class T, class F>
 __device__ __forceinline__ float op_apply_at(const DevOp &op, const F &phi, int64_t inst,
@@ -157,6 +162,19 @@ __device__ __forceinline__ float op_apply_at(const DevOp &op, const F &phi, int6
     float azm = cz * (z > 0 ? 0.5f * (vz + St<T>::ld(sz + i - P2)) : vz);
     float azp = cz * (z < Z - 1 ? 0.5f * (vz + St<T>::ld(sz + i + P2)) : vz);
     *diag = axm + axp + aym + ayp + azm + azp;
+    return axm * (pc - P(z, y, x - 1)) + axp * (pc - P(z, y, x + 1)) +
+           aym * (pc - P(z, y - 1, x)) + ayp * (pc - P(z, y + 1, x)) +
+           azm * (pc - P(z - 1, y, x)) + azp * (pc - P(z + 1, y, x));
+  } else if (KIND == HFM_OP_FACE7) {
+    const T *fx = (const T *)op.coef[0] + inst * face7_nx(Z, Y, X) + ((int64_t)z * Y + y) * (X + 8) + x;
+    const T *fy = (const T *)op.coef[1] + inst * face7_ny(Z, Y, X) + ((int64_t)z * (Y + 1) + y) * X + x;
+    const T *fz = (const T *)op.coef[2] + inst * face7_nz(Z, Y, X) + ((int64_t)z * Y + y) * X + x;
+    const float s = op.scale;
+    const float axm = s * St<T>::ld(fx), axp = s * St<T>::ld(fx + 1);
+    const float aym = s * St<T>::ld(fy), ayp = s * St<T>::ld(fy + X);
+    const float azm = s * St<T>::ld(fz), azp = s * St<T>::ld(fz + (int64_t)Y * X);
+    float pc = P(z, y, x);
+    *diag = ((axm + axp) + (aym + ayp)) + (azm + azp);
     return axm * (pc - P(z, y, x - 1)) + axp * (pc - P(z, y, x + 1)) +
            aym * (pc - P(z, y - 1, x)) + ayp * (pc - P(z, y + 1, x)) +
            azm * (pc - P(z - 1, y, x)) + azp * (pc - P(z + 1, y, x));
@@ -241,6 +259,10 @@ bool vec_aligned(int kind, const DevOp &op, const PhiSrc<T> &phi, const void *rh
       if (!al(op.coef[k])) return false;
     if ((op.coef_stride * es) % bytes) return false;
   }
+  if (kind == HFM_OP_FACE7) {  // instance strides follow from the extents (rows of X + 8 / X)
+    for (int k = 0; k < 3; ++k)
+      if (!al(op.coef[k])) return false;
+  }
   return true;
 }
 template <class T>
@@ -276,8 +298,23 @@ template <class T> int launch_subcycle(int kind, SubArgs<T> a, int B, cudaStream
 // The first two Jacobi sweeps from a zero iterate in one pass (SIGMA7, TMA-eligible grids):
 // out = J(phi1) with phi1 = omega f * invd, invd = 1 / diag of the level.
 template <class T>
-int tma_launch_pre2(const DevOp &op, const T *f, const T *invd, T *out, int64_t stride, int B,
-                    Grid3 g, float omega, const int *active, cudaStream_t s);
+int tma_launch_pre2(int kind, const DevOp &op, const T *f, const T *invd, T *out, int64_t stride,
+                    int B, Grid3 g, float omega, const int *active, cudaStream_t s);
+// The FACE7 plane-marching kernel takes neither the x-end rule, the top copy nor the p . A p
+// sums; launches that need them run the generic kernels.
+template <class T>
+bool face_tma_ok(int kind, const PhiSrc<T> &phi, unsigned flags) {
+  return kind != HFM_OP_FACE7 ||
+         (!phi.zero_xend && !(flags & (HFM_FLAG_ZERO_XEND | HFM_FLAG_TOP_COPY | HFM_INT_DOT_PHI)));
+}
+
+// FACE7 arrays of the SIGMA7 operator (faces.cu) from conductivities of type TS (instance
+// stride s_stride), stored as T; `div` (per-slot divisors, may be null) divides the
+// conductivities of instance slot0 + b first.
+template <class TS, class T>
+int launch_sigma_faces(const TS *sx, const TS *sy, const TS *sz, int64_t s_stride, float cz,
+                       float cy, float cx, const double *div, int slot0, T *fx, T *fy, T *fz,
+                       int B, Grid3 g, cudaStream_t s);
 
 // Upper bound of blocks per instance of any residual launch on grid g (partials sizing).
 int64_t max_partial_blocks(Grid3 g, int B);

@@ -713,7 +713,18 @@ struct Level {
   void *coef[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   void *invd = nullptr;  // SIGMA7: 1 / diagonal of the level's operator (two-sweep pass)
   DevOp op;
+  // 16-bit SIGMA7 levels the plane-marching kernels take: the FACE7 arrays of the level's
+  // operator (scale folded in) and that operator, used by every sweep and residual there
+  void *face[3] = {nullptr, nullptr, nullptr};
+  DevOp fop;
 };
+
+// A level of a handle holds FACE7 arrays: 16-bit SIGMA7 storage, the option not set, and a
+// grid the face plane-marching kernel takes.
+static bool face_level(const hfm_mg_config &c, Grid3 g) {
+  return c.op_kind == HFM_OP_SIGMA7 && (c.storage == HFM_BF16 || c.storage == HFM_F16) &&
+         !(c.options & HFM_OPT_NO_FACES) && tma_eligible(HFM_OP_FACE7, g, FAST_SMOOTH, nullptr, 0, 2);
+}
 
 class EngineBase {
  public:
@@ -779,6 +790,9 @@ class Engine : public EngineBase {
   Grid3 g(int l) { return Grid3{m_->lv[l].Z, m_->lv[l].Y, m_->lv[l].X}; }
   int64_t n(int l) { return m_->lv[l].n; }
   int kind() { return m_->cfg.op_kind; }
+  // the operator level l runs: FACE7 where the level holds face arrays
+  int lk(int l) { return m_->lv[l].face[0] ? HFM_OP_FACE7 : kind(); }
+  const DevOp &lo(int l) { return m_->lv[l].face[0] ? m_->lv[l].fop : m_->lv[l].op; }
   // bf16 refinement: the storage-type copy of the CG residual is written by the kernels that
   // produce r (outer residual, k_cg_xr) instead of a separate conversion pass
   bool fused_rhs() const {
@@ -804,7 +818,7 @@ class Engine : public EngineBase {
 
   int smooth(int l, const PhiSrc<T> &p, const T *f, T *out, float omega, unsigned flags,
              cudaStream_t s, double *partials = nullptr, int *nblk = nullptr) {
-    return launch_smooth<T>(kind(), m_->lv[l].op, p, f, n(l), out, n(l), m_->slots, g(l),
+    return launch_smooth<T>(lk(l), lo(l), p, f, n(l), out, n(l), m_->slots, g(l),
                             omega, flags, m_->active, s, partials, nblk);
   }
 
@@ -837,12 +851,10 @@ class Engine : public EngineBase {
   bool pre2_ok(int l) {
     if (kind() != HFM_OP_SIGMA7 || !m_->lv[l].invd || (m_->cfg.options & HFM_OPT_NO_FUSED_PRE))
       return false;
-    if (!tma_eligible(HFM_OP_SIGMA7, g(l), FAST_SMOOTH, nullptr, 0, (int)sizeof(T))) return false;
+    if (!tma_eligible(lk(l), g(l), FAST_SMOOTH, nullptr, 0, (int)sizeof(T))) return false;
     PhiSrc<T> p = src(rhs(l), n(l));
-    return vec_aligned<T>(HFM_OP_SIGMA7, m_->lv[l].op, p, m_->lv[l].invd, buf(l, 0), nullptr,
-                          n(l), 16) &&
-           vec_aligned<T>(HFM_OP_SIGMA7, m_->lv[l].op, p, m_->lv[l].invd, buf(l, 1), nullptr,
-                          n(l), 16);
+    return vec_aligned<T>(lk(l), lo(l), p, m_->lv[l].invd, buf(l, 0), nullptr, n(l), 16) &&
+           vec_aligned<T>(lk(l), lo(l), p, m_->lv[l].invd, buf(l, 1), nullptr, n(l), 16);
   }
 
   // First level of the fused coarse V-cycle (subcycle.cu), or -1: the deepest levels of at
@@ -912,7 +924,7 @@ class Engine : public EngineBase {
     int k0 = 0;
     if (zero && c.nu_pre >= 2 && !xend && pre2_ok(l)) {
       // the first two sweeps from zero in one pass (phi1 = omega f / diag is pointwise)
-      if ((st = tma_launch_pre2<T>(m_->lv[l].op, rhs(l), (const T *)m_->lv[l].invd,
+      if ((st = tma_launch_pre2<T>(lk(l), lo(l), rhs(l), (const T *)m_->lv[l].invd,
                                    buf(l, cur_[l] ^ 1), n(l), m_->slots, g(l), c.omega,
                                    m_->active, s)))
         return st;
@@ -933,13 +945,13 @@ class Engine : public EngineBase {
       // residual of the iterate with its x = X-1 plane read as zero, zero there, restricted
       T *rf = (T *)m_->saw[0];
       p.zero_xend = 1;
-      if ((st = launch_residual<T>(kind(), m_->lv[l].op, p, rhs(l), n(l), rf, n(l), m_->slots,
+      if ((st = launch_residual<T>(lk(l), lo(l), p, rhs(l), n(l), rf, n(l), m_->slots,
                                    g(l), HFM_FLAG_ZERO_XEND, m_->active,
                                    chk ? m_->partials : nullptr, &nblk, s)))
         return st;
       if ((st = launch_restrict<T>(rf, n(l), rhs(l + 1), n(l + 1), m_->slots, g(l), m_->active, s)))
         return st;
-    } else if ((st = launch_residual_restrict<T>(kind(), m_->lv[l].op, p, rhs(l), n(l), nullptr, 0,
+    } else if ((st = launch_residual_restrict<T>(lk(l), lo(l), p, rhs(l), n(l), nullptr, 0,
                                                  rhs(l + 1), n(l + 1), m_->slots, g(l), 0u,
                                                  m_->active, chk ? m_->partials : nullptr, &nblk, s)))
       return st;
@@ -975,7 +987,7 @@ class Engine : public EngineBase {
     int st, nblk = 0;
     const unsigned xend = c.flags & HFM_FLAG_ZERO_XEND;
     // 1. r = A phi - b (NS: r[..., X-1] = 0), residual norm for the stopping test
-    if ((st = launch_residual<T>(kind(), m_->lv[0].op, src(buf(0, cur_[0]), n(0)), rhs(0), n(0),
+    if ((st = launch_residual<T>(lk(0), lo(0), src(buf(0, cur_[0]), n(0)), rhs(0), n(0),
                                  r0, n(0), m_->slots, g(0), xend, m_->active, m_->partials,
                                  &nblk, s)))
       return st;
@@ -1157,6 +1169,7 @@ class Engine : public EngineBase {
       return fail(HFM_ERR_BAD_ARG, "coefficients must be float32 or float64");
     // slot < 0: every slot at once (the arrays hold all slots), one launch per level
     const int lo = slot < 0 ? 0 : slot, cnt = slot < 0 ? m_->slots : 1;
+    const hfm_operator fine_src = op;  // the caller's conductivities (fine-level faces)
     // fp16 cycles used as a preconditioner store sigma / g (their output is rescaled by 1/g);
     // stationary fp16 cycles keep sigma itself, their iterate is the solution
     const bool normalize = std::is_same<T, __half>::value && m_->cfg.accel != HFM_ACCEL_NONE;
@@ -1207,6 +1220,41 @@ class Engine : public EngineBase {
           (const T *)op.coef[2] + lo * nl, op.c[0] * op.scale, op.c[1] * op.scale,
           op.c[2] * op.scale, g(l).Z, g(l).Y, g(l).X, nl * cnt, (T *)m_->lv[l].invd + lo * nl);
       HFM_CHECK_LAUNCH("k_invdiag");
+    }
+    // FACE7 arrays of the levels that hold them: the fine level's faces from the caller's
+    // float32 / float64 conductivities (divided by the slot's geometric mean for normalised
+    // fp16 cycles), coarse levels' from their restricted conductivities; the level's scale
+    // is folded into the faces
+    for (int l = 0; l < m_->L; ++l) {
+      Level &L_ = m_->lv[l];
+      if (!L_.face[0]) continue;
+      const DevOp &op = L_.op;
+      const float s_ = op.scale;
+      const float cz = op.c[0] * s_, cy = op.c[1] * s_, cx = op.c[2] * s_;
+      const int64_t nx = face7_nx(g(l).Z, g(l).Y, g(l).X), ny = face7_ny(g(l).Z, g(l).Y, g(l).X),
+                    nz = face7_nz(g(l).Z, g(l).Y, g(l).X);
+      T *fx = (T *)L_.face[0] + lo * nx, *fy = (T *)L_.face[1] + lo * ny, *fz = (T *)L_.face[2] + lo * nz;
+      const double *div = normalize ? m_->gscale : nullptr;
+      int st;
+      if (l == 0 && fine_src.coef_dtype == HFM_F64)
+        st = launch_sigma_faces<double, T>((const double *)fine_src.coef[0], (const double *)fine_src.coef[1],
+                                           (const double *)fine_src.coef[2], n(0), cz, cy, cx, div, lo,
+                                           fx, fy, fz, cnt, g(0), s);
+      else if (l == 0)
+        st = launch_sigma_faces<float, T>((const float *)fine_src.coef[0], (const float *)fine_src.coef[1],
+                                          (const float *)fine_src.coef[2], n(0), cz, cy, cx, div, lo,
+                                          fx, fy, fz, cnt, g(0), s);
+      else
+        st = launch_sigma_faces<T, T>((const T *)op.coef[0] + lo * n(l), (const T *)op.coef[1] + lo * n(l),
+                                      (const T *)op.coef[2] + lo * n(l), n(l), cz, cy, cx, nullptr, 0,
+                                      fx, fy, fz, cnt, g(l), s);
+      if (st) return st;
+      hfm_operator fo;
+      memset(&fo, 0, sizeof(fo));
+      fo.kind = HFM_OP_FACE7;
+      fo.scale = 1.f;
+      for (int a = 0; a < 3; ++a) fo.coef[a] = L_.face[a];
+      L_.fop = make_devop(fo, 0);
     }
     return HFM_OK;
   }
@@ -1495,6 +1543,9 @@ size_t hfm_mg_footprint_bytes(const hfm_mg_config *c, int Z, int Y, int X, int s
     size_t nl = (size_t)lv[l].n();
     size_t fields = 3 + (c->op_kind == HFM_OP_SIGMA7 ? 4 : 0) + (c->op_kind == HFM_OP_DIR7 ? 7 : 0);
     tot += nl * fields * es;
+    if (face_level(*c, lv[l]))
+      tot += (size_t)(face7_nx(lv[l].Z, lv[l].Y, lv[l].X) + face7_ny(lv[l].Z, lv[l].Y, lv[l].X) +
+                      face7_nz(lv[l].Z, lv[l].Y, lv[l].X)) * es;
   }
   const size_t nf = (size_t)Z * Y * X;
   if (c->accel != HFM_ACCEL_NONE) {
@@ -1545,6 +1596,11 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
     if (cfg->op_kind == HFM_OP_SIGMA7) {
       for (int a = 0; a < 3; ++a) L.coef[a] = dalloc(m.get(), b, &st);
       L.invd = dalloc(m.get(), b, &st);
+    }
+    if (face_level(*cfg, lv[l])) {
+      L.face[0] = dalloc(m.get(), (size_t)face7_nx(L.Z, L.Y, L.X) * slots * es, &st);
+      L.face[1] = dalloc(m.get(), (size_t)face7_ny(L.Z, L.Y, L.X) * slots * es, &st);
+      L.face[2] = dalloc(m.get(), (size_t)face7_nz(L.Z, L.Y, L.X) * slots * es, &st);
     }
     if (cfg->op_kind == HFM_OP_DIR7)
       for (int a = 0; a < 7; ++a) L.coef[a] = dalloc(m.get(), b, &st);

@@ -184,6 +184,108 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// The same transfers with 16-byte accesses for rows of a multiple of VEC = 16 / sizeof(T)
+// fine values (16-byte aligned fine pointer and stride, 8-byte aligned coarse ones): a thread
+// owns HC = VEC / 2 consecutive coarse cells of one coarse row.  Restriction loads VEC fine
+// values from each of its four fine rows (two y, two z) and sums in the order of k_restrict
+// (z, then y, then x), so both give the same bits; prolongation loads HC coarse values and
+// stores VEC fine values into each of the four rows.
+template <class T> struct Vec16 {
+  static constexpr int VEC = 16 / (int)sizeof(T), HC = VEC / 2;
+  static __device__ __forceinline__ void ld(const T *p, float (&v)[VEC]) {
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    if constexpr (sizeof(T) == 4) {
+      v[0] = __uint_as_float(u.x); v[1] = __uint_as_float(u.y);
+      v[2] = __uint_as_float(u.z); v[3] = __uint_as_float(u.w);
+    } else {
+      const T *h = reinterpret_cast<const T *>(&u);
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) v[k] = St<T>::to(h[k]);
+    }
+  }
+};
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_restrict_v(const T *__restrict__ f, int64_t fs, T *__restrict__ c, int64_t cs, int Z, int Y,
+                 int X, const int *__restrict__ active) {
+  constexpr int VEC = Vec16<T>::VEC, HC = Vec16<T>::HC;
+  const int64_t inst = blockIdx.y;
+  if (active && !active[inst]) return;
+  const int Zc = Z >> 1, Yc = Y >> 1, Xc = X >> 1, Xv = Xc / HC;
+  const int64_t nv = (int64_t)Zc * Yc * Xv;
+  const T *fi = f + inst * fs;
+  T *ci = c + inst * cs;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nv;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const int xv = (int)(j % Xv);
+    const int64_t t = j / Xv;
+    const int yc = (int)(t % Yc), zc = (int)(t / Yc);
+    float sum[HC];
+#pragma unroll
+    for (int k = 0; k < HC; ++k) sum[k] = 0.f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb) {
+        float v[VEC];
+        Vec16<T>::ld(fi + ((int64_t)(2 * zc + a) * Y + 2 * yc + bb) * X + (int64_t)VEC * xv, v);
+#pragma unroll
+        for (int k = 0; k < HC; ++k) {
+          sum[k] += 0.125f * v[2 * k];
+          sum[k] += 0.125f * v[2 * k + 1];
+        }
+      }
+    alignas(8) T out[HC];
+#pragma unroll
+    for (int k = 0; k < HC; ++k) out[k] = St<T>::from(sum[k]);
+    *reinterpret_cast<uint2 *>(ci + ((int64_t)zc * Yc + yc) * Xc + (int64_t)HC * xv) =
+        *reinterpret_cast<const uint2 *>(out);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_prolong_v(const T *__restrict__ c, int64_t cs, T *__restrict__ f, int64_t fs, int Zc,
+                int Yc, int Xc, const int *__restrict__ active) {
+  constexpr int VEC = Vec16<T>::VEC, HC = Vec16<T>::HC;
+  const int64_t inst = blockIdx.y;
+  if (active && !active[inst]) return;
+  const int Y = 2 * Yc, X = 2 * Xc, Xv = Xc / HC;
+  const int64_t nv = (int64_t)Zc * Yc * Xv;
+  const T *ci = c + inst * cs;
+  T *fi = f + inst * fs;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nv;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const int xv = (int)(j % Xv);
+    const int64_t t = j / Xv;
+    const int yc = (int)(t % Yc), zc = (int)(t / Yc);
+    const uint2 u = *reinterpret_cast<const uint2 *>(ci + ((int64_t)zc * Yc + yc) * Xc + (int64_t)HC * xv);
+    const T *h = reinterpret_cast<const T *>(&u);
+    alignas(16) T w[VEC];
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) w[k] = h[k >> 1];
+    const uint4 o = *reinterpret_cast<const uint4 *>(w);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+        *reinterpret_cast<uint4 *>(fi + ((int64_t)(2 * zc + a) * Y + 2 * yc + bb) * X + (int64_t)VEC * xv) = o;
+  }
+}
+
+// The vector transfers apply: X (fine) a multiple of VEC, fine pointer and instance stride
+// 16-byte aligned, coarse ones 8-byte aligned.
+template <class T>
+bool transfer_vec_ok(const T *fine, int64_t f_stride, const T *coarse, int64_t c_stride, int X, int B) {
+  constexpr int VEC = Vec16<T>::VEC;
+  const int64_t es = (int64_t)sizeof(T);
+  if (X % VEC) return false;
+  if ((uintptr_t)fine % 16 || (uintptr_t)coarse % 8) return false;
+  if (B > 1 && ((f_stride * es) % 16 || (c_stride * es) % 8)) return false;
+  return true;
+}
+
 // Small-grid Jacobi: the level lives in shared memory, one block per instance.
 template <int KIND, class T>
 __global__ void k_coarse_jacobi(DevOp op, const T *__restrict__ rhs, int64_t rhs_stride,
@@ -242,6 +344,7 @@ int64_t max_partial_blocks(Grid3 g, int B) {
     case HFM_OP_SIGMA7: { constexpr int K_ = HFM_OP_SIGMA7; __VA_ARGS__; break; } \
     case HFM_OP_DIR7: { constexpr int K_ = HFM_OP_DIR7; __VA_ARGS__; break; }     \
     case HFM_OP_K27: { constexpr int K_ = HFM_OP_K27; __VA_ARGS__; break; }       \
+    case HFM_OP_FACE7: { constexpr int K_ = HFM_OP_FACE7; __VA_ARGS__; break; }   \
     default: return fail(HFM_ERR_BAD_ARG, "unknown operator kind");          \
   }
 
@@ -254,6 +357,7 @@ int launch_smooth(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
   if ((!phi.base || phi.base_stride == out_stride) && (phi.base || phi.corr || rhs) &&
       (!rhs || rhs_stride == out_stride) &&
       tma_eligible(kind, g, FAST_SMOOTH, phi.corr, phi.corr_coarse, (int)sizeof(T)) &&
+      face_tma_ok<T>(kind, phi, flags) &&
       vec_aligned<T>(kind, op, phi, rhs, out, nullptr, out_stride, 16))
     return tma_launch<T>(kind, FAST_SMOOTH, op, phi, rhs, out, nullptr, out_stride, 0, B, g,
                          omega, flags, active, partials, nblk_out, s);
@@ -278,6 +382,7 @@ int launch_residual(int kind, const DevOp &op, const PhiSrc<T> &phi, const T *b,
                     const int *active, double *partials, int *nblk_out, cudaStream_t s) {
   if (phi.base && !phi.corr && !phi.zero_xend && r && phi.base_stride == r_stride &&
       (!b || b_stride == r_stride) && tma_eligible(kind, g, FAST_RESID, nullptr, 0, (int)sizeof(T)) &&
+      face_tma_ok<T>(kind, phi, flags) &&
       vec_aligned<T>(kind, op, phi, b, r, nullptr, r_stride, 16))
     return tma_launch<T>(kind, FAST_RESID, op, phi, b, r, nullptr, r_stride, 0, B, g, 0.f,
                          flags, active, partials, nblk_out, s);
@@ -313,6 +418,7 @@ int launch_residual_restrict(int kind, const DevOp &op, const PhiSrc<T> &phi, co
   if (phi.base && !phi.corr && !phi.zero_xend && b && phi.base_stride == b_stride &&
       (!r_fine || rf_stride == b_stride) && rc_stride == b_stride / 8 &&
       tma_eligible(kind, g, FAST_RESTRICT, nullptr, 0, (int)sizeof(T)) &&
+      face_tma_ok<T>(kind, phi, flags) &&
       vec_aligned<T>(kind, op, phi, b, r_fine, nullptr, b_stride, 16))
     return tma_launch<T>(kind, FAST_RESTRICT, op, phi, b, r_fine, r_coarse, b_stride, rc_stride,
                          B, g, 0.f, flags, active, partials, nblk_out, s);
@@ -338,6 +444,13 @@ int launch_restrict(const T *fine, int64_t f_stride, T *coarse, int64_t c_stride
                     Grid3 g, const int *active, cudaStream_t s) {
   int64_t nc = (int64_t)(g.Z / 2) * (g.Y / 2) * (g.X / 2);
   if (nc == 0) return HFM_OK;
+  if (transfer_vec_ok<T>(fine, f_stride, coarse, c_stride, g.X, B)) {
+    dim3 grid(blocks_for(nc / Vec16<T>::HC, B), B);
+    k_restrict_v<T><<<grid, kThreads, 0, s>>>(fine, f_stride, coarse, c_stride, g.Z, g.Y, g.X,
+                                              active);
+    HFM_CHECK_LAUNCH("k_restrict_v");
+    return HFM_OK;
+  }
   dim3 grid(blocks_for(nc, B), B);
   k_restrict<T><<<grid, kThreads, 0, s>>>(fine, f_stride, coarse, c_stride, g.Z, g.Y, g.X,
                                           active);
@@ -348,6 +461,13 @@ int launch_restrict(const T *fine, int64_t f_stride, T *coarse, int64_t c_stride
 template <class T>
 int launch_prolong(const T *coarse, int64_t c_stride, T *fine, int64_t f_stride, int B,
                    Grid3 gc, const int *active, cudaStream_t s) {
+  if (transfer_vec_ok<T>(fine, f_stride, coarse, c_stride, 2 * gc.X, B)) {
+    dim3 grid(blocks_for(gc.n() / Vec16<T>::HC, B), B);
+    k_prolong_v<T><<<grid, kThreads, 0, s>>>(coarse, c_stride, fine, f_stride, gc.Z, gc.Y,
+                                             gc.X, active);
+    HFM_CHECK_LAUNCH("k_prolong_v");
+    return HFM_OK;
+  }
   dim3 grid(blocks_for(gc.n() * 8, B), B);
   k_prolong<T><<<grid, kThreads, 0, s>>>(coarse, c_stride, fine, f_stride, gc.Z, gc.Y, gc.X,
                                          active);

@@ -522,6 +522,8 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
   }
 }
 
+#include "tma_face.cuh"
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -575,6 +577,18 @@ int go(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
   return HFM_OK;
 }
 
+template <class T, int MODE, int CORR>
+int go_face(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
+  using G = GeoF<CORR != 0, MODE == M_PRE2>;
+  const int smem = G::NS * G::STAGE;
+  int st = set_max_dynamic_smem((const void *)k_tma_face<T, MODE, CORR>, smem,
+                                "cudaFuncSetAttribute(k_tma_face)");
+  if (st) return st;
+  k_tma_face<T, MODE, CORR><<<grid, G::THREADS, smem, s>>>(a);
+  HFM_CHECK_LAUNCH("k_tma_face");
+  return HFM_OK;
+}
+
 // Grid (plane tiles, z chunks, instances): z chunks sized for about 3 resident blocks per SM
 // and four waves, at least 2 planes each.  (Eight waves, which shrink the partly filled last
 // wave, measured slower: every chunk re-reads its two halo planes and refills its pipeline.)
@@ -596,7 +610,10 @@ dim3 tma_grid(TmaArgs<T> &a, Grid3 g, int B) {
 }  // namespace
 
 bool tma_eligible(int kind, Grid3 g, int mode, const void *corr, int corr_coarse, int es) {
-  if (kind != HFM_OP_CONST7 && kind != HFM_OP_SIGMA7 && kind != HFM_OP_K27) return false;
+  if (kind != HFM_OP_CONST7 && kind != HFM_OP_SIGMA7 && kind != HFM_OP_K27 &&
+      kind != HFM_OP_FACE7)
+    return false;
+  if (kind == HFM_OP_FACE7 && es != 2) return false;  // the face kernel is 16-bit only
   // grids narrower than a tile (48 <= X < 64) use the same boxes: the columns past X are
   // zero-filled, not read.  Below X = 48 the register-queue kernels are as fast or faster
   // (measured: 32^3 and 24^3 levels of 64 instances).
@@ -610,11 +627,81 @@ bool tma_eligible(int kind, Grid3 g, int mode, const void *corr, int corr_coarse
   return true;
 }
 
+// The FACE7 kernel (16-bit storage): tensor maps of phi (or f for the fused first two
+// sweeps, with invd), the face arrays Fx [Z][Y][X + 8], Fy [Z][Y + 1][X], Fz [Z + 1][Y][X],
+// the right-hand side and the coarse correction.  Callers exclude the x-end rule, the top
+// copy and the p . A p sums (face_tma_ok).
+template <class T>
+int tma_launch_face(int mode, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
+                    const T *invd, T *out, T *coarse, int64_t stride, int64_t coarse_stride,
+                    int B, Grid3 g, float omega, unsigned flags, const int *active,
+                    double *partials, int *nblk_out, cudaStream_t s) {
+  using G = GeoF<false, false>;
+  constexpr int TY = G::TY;
+  TmaArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  int st;
+  const bool pre2 = mode == M_PRE2;
+  const T *base = pre2 ? rhs : phi.base;
+  a.has_phi = base != nullptr;
+  if (a.has_phi && (st = make_map<T>(&a.m_phi, base, g.X, g.Y, g.Z, B, pre2 ? stride : phi.base_stride,
+                                     G::PW, TY + 2)))
+    return st;
+  if ((st = make_map<T>(&a.m_sx, op.coef[0], g.X + 8, g.Y, g.Z, B, face7_nx(g.Z, g.Y, g.X), G::FXW, TY)))
+    return st;
+  if ((st = make_map<T>(&a.m_sy, op.coef[1], g.X, g.Y + 1, g.Z, B, face7_ny(g.Z, g.Y, g.X), TX, TY + 1)))
+    return st;
+  if ((st = make_map<T>(&a.m_sz, op.coef[2], g.X, g.Y, g.Z + 1, B, face7_nz(g.Z, g.Y, g.X), TX, TY)))
+    return st;
+  a.has_f = !pre2 && rhs != nullptr;
+  if (a.has_f && (st = make_map<T>(&a.m_f, rhs, g.X, g.Y, g.Z, B, stride, TX, TY))) return st;
+  const int corr = (!pre2 && phi.corr) ? 1 : 0;
+  if (corr && (st = make_map<T>(&a.m_cc, phi.corr, g.X / 2, g.Y / 2, g.Z / 2, B, phi.corr_stride,
+                                G::CW, TY / 2 + 2)))
+    return st;
+  if (pre2 && (st = make_map<T>(&a.m_ds, invd, g.X, g.Y, g.Z, B, stride, G::PW, TY + 2))) return st;
+  unsigned bytes = (unsigned)((G::FXN + G::FYN + G::FZN) * sizeof(T));
+  if (a.has_phi) bytes += (unsigned)(G::PHI * sizeof(T));
+  if (a.has_f) bytes += (unsigned)(G::FN * sizeof(T));
+  if (corr) bytes += (unsigned)(G::CCN * sizeof(T));
+  if (pre2) bytes += (unsigned)(G::PHI * sizeof(T));
+  a.stage_bytes = bytes;
+  a.wait_budget = g_wait_budget.load();
+  a.op = op;
+  a.out = out;
+  a.coarse = coarse;
+  a.partials = partials;
+  a.active = active;
+  a.stride = stride;
+  a.coarse_stride = coarse_stride;
+  a.Z = g.Z;
+  a.Y = g.Y;
+  a.X = g.X;
+  a.omega = omega;
+  a.corr_sign = phi.corr_sign;
+  a.dot_rhs = ((mode == M_SMOOTH || pre2) && (flags & HFM_INT_DOT_RHS) && partials) ? 1 : 0;
+  dim3 grid = tma_grid(a, g, B);
+  if (nblk_out) *nblk_out = grid.x * grid.y;
+  if (pre2) return go_face<T, M_PRE2, 0>(a, grid, s);
+  if (mode == M_SMOOTH) {
+    if (corr) return go_face<T, M_SMOOTH, 1>(a, grid, s);
+    return go_face<T, M_SMOOTH, 0>(a, grid, s);
+  }
+  if (mode == M_RESID) return go_face<T, M_RESID, 0>(a, grid, s);
+  return go_face<T, M_RESTRICT, 0>(a, grid, s);
+}
+
 template <class T>
 int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const T *rhs, T *out,
                T *coarse, int64_t stride, int64_t coarse_stride, int B, Grid3 g, float omega,
                unsigned flags, const int *active, double *partials, int *nblk_out,
                cudaStream_t s) {
+  if (kind == HFM_OP_FACE7) {
+    if constexpr (sizeof(T) == 2)
+      return tma_launch_face<T>(mode, op, phi, rhs, nullptr, out, coarse, stride, coarse_stride,
+                                B, g, omega, flags, active, partials, nblk_out, s);
+    return fail(HFM_ERR_UNSUPPORTED, "tma path: FACE7 needs 16-bit storage");
+  }
   using G = Geo<T>;  // tile extents (identical for every stage layout)
   constexpr int TY = G::TY;
   TmaArgs<T> a;
@@ -687,8 +774,17 @@ int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const 
 }
 
 template <class T>
-int tma_launch_pre2(const DevOp &op, const T *f, const T *invd, T *out, int64_t stride, int B,
-                    Grid3 g, float omega, const int *active, cudaStream_t s) {
+int tma_launch_pre2(int kind, const DevOp &op, const T *f, const T *invd, T *out, int64_t stride,
+                    int B, Grid3 g, float omega, const int *active, cudaStream_t s) {
+  if (kind == HFM_OP_FACE7) {
+    if constexpr (sizeof(T) == 2) {
+      PhiSrc<T> none;
+      memset(&none, 0, sizeof(none));
+      return tma_launch_face<T>(M_PRE2, op, none, f, invd, out, nullptr, stride, 0, B, g, omega,
+                                0u, active, nullptr, nullptr, s);
+    }
+    return fail(HFM_ERR_UNSUPPORTED, "tma path: FACE7 needs 16-bit storage");
+  }
   using G = Geo<T, true, false, true>;
   constexpr int TY = G::TY;
   TmaArgs<T> a;
@@ -722,12 +818,12 @@ int tma_launch_pre2(const DevOp &op, const T *f, const T *invd, T *out, int64_t 
 HFM_TMA_INST(float)
 HFM_TMA_INST(__nv_bfloat16)
 HFM_TMA_INST(__half)
-template int tma_launch_pre2<float>(const DevOp &, const float *, const float *, float *, int64_t,
-                                    int, Grid3, float, const int *, cudaStream_t);
-template int tma_launch_pre2<__nv_bfloat16>(const DevOp &, const __nv_bfloat16 *,
+template int tma_launch_pre2<float>(int, const DevOp &, const float *, const float *, float *,
+                                    int64_t, int, Grid3, float, const int *, cudaStream_t);
+template int tma_launch_pre2<__nv_bfloat16>(int, const DevOp &, const __nv_bfloat16 *,
                                             const __nv_bfloat16 *, __nv_bfloat16 *, int64_t, int,
                                             Grid3, float, const int *, cudaStream_t);
-template int tma_launch_pre2<__half>(const DevOp &, const __half *, const __half *, __half *,
+template int tma_launch_pre2<__half>(int, const DevOp &, const __half *, const __half *, __half *,
                                      int64_t, int, Grid3, float, const int *, cudaStream_t);
 
 }  // namespace hfm

@@ -1,11 +1,16 @@
 """Time one libhfm kernel on a synthetic batch with CUDA events (and serve as the ncu target).
 
     python ai-hfm-solver_b200/kernel_bench.py --kernel smooth --form sigma7 --n 64 --batch 64
+    python ai-hfm-solver_b200/kernel_bench.py --kernel smooth --form face7 --dtype bf16 --n 128
 
-Kernels: ``smooth`` (one weighted-Jacobi sweep), ``resid`` (A phi - b), ``restrict``
-(fused residual + restriction), ``correct`` (fused prolongation + correction + sweep),
-``apply27`` (27-point conv).  Prints one JSON line with the time per launch, the algorithmic
-bytes per launch and the achieved GB/s.  Inputs are larger than L2 for the default sizes.
+Kernels: ``smooth`` (one weighted-Jacobi sweep), ``resid`` (A phi - b), ``restrict`` (fused
+residual + restriction), ``correct`` (fused prolongation + correction + sweep), ``apply27``
+(27-point conv), ``transfer-r`` / ``transfer-p`` (standalone restriction / prolongation).
+Forms: ``sigma7`` (per-cell conductivities), ``face7`` (stored faces; 16-bit storage),
+``const7``, ``k27``.  ``--dtype`` selects the storage of fields and coefficients (the typed
+entry points for bf16 / f16).  Prints one JSON line with the time per launch, the
+algorithmic bytes per launch (every array read once and every output written once, at its
+actual size) and the achieved GB/s.  Inputs are larger than L2 for the default sizes.
 """
 import argparse
 import ctypes as C
@@ -16,80 +21,109 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 
-# algorithmic bytes per fine cell, float32
-BYTES = {("smooth", "sigma7"): 24, ("smooth", "const7"): 12, ("smooth", "k27"): 12,
-         ("resid", "sigma7"): 24, ("resid", "const7"): 12, ("resid", "k27"): 12,
-         ("restrict", "sigma7"): 20.5, ("restrict", "const7"): 8.5,
-         ("correct", "sigma7"): 24.5, ("correct", "const7"): 12.5, ("correct", "k27"): 12.5,
-         ("apply27", "k27"): 8}
-
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel", default="smooth")
-    ap.add_argument("--form", default="sigma7")
+    ap.add_argument("--form", default="sigma7", choices=["sigma7", "face7", "const7", "k27"])
     ap.add_argument("--n", type=int, default=64)
     ap.add_argument("--shape", default=None, help="Z,Y,X (overrides --n)")
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--dtype", default="f32", choices=["f32", "bf16", "f16"],
-                    help="storage of fields and conductivities (smooth only)")
+                    help="storage of fields and coefficients")
     a = ap.parse_args()
     import torch
     import __graft_entry__ as ge
     hfm = ge.load_package()
-    ops, W = hfm.ops, hfm.weights
+    ops, W, L = hfm.ops, hfm.weights, hfm._lib
     Z, Y, X = (tuple(int(v) for v in a.shape.split(",")) if a.shape else (a.n, a.n, a.n))
     B = a.batch
+    n = Z * Y * X
     dev = torch.device("cuda")
     g = torch.Generator(device=dev).manual_seed(0)
-    x = torch.randn((B, Z, Y, X), device=dev, generator=g)
-    b = torch.randn((B, Z, Y, X), device=dev, generator=g)
-    if a.form == "sigma7":
-        s = torch.exp(torch.randn((3, B, Z, Y, X), device=dev, generator=g))
-        op = ops.Sigma7(s[0], s[1], s[2])
-    elif a.form == "const7":
-        op = ops.Const7(50.0, 100.0, 200.0)
-    else:
-        op = ops.Stencil27(W.pressure27())
-    out = torch.empty_like(x)
-    wc = torch.randn((B, Z // 2, Y // 2, X // 2), device=dev, generator=g)
-    st = op.struct()
-    stream = ops._stream()
-    L = hfm._lib
-    P = lambda t: C.c_void_p(t.data_ptr() if t is not None else 0)
-
     tdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[a.dtype]
-    if a.kernel == "smooth" and a.dtype != "f32":
-        xt, bt, ot = x.to(tdt), b.to(tdt), out.to(tdt)
-        keep = []
+    code = {"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[a.dtype]
+    E = torch.tensor([], dtype=tdt).element_size()
+    x = torch.randn((B, Z, Y, X), device=dev, generator=g).to(tdt)
+    b = torch.randn((B, Z, Y, X), device=dev, generator=g).to(tdt)
+    out = torch.empty_like(x)
+    wc = torch.randn((B, Z // 2, Y // 2, X // 2), device=dev, generator=g).to(tdt)
+    P = lambda t: C.c_void_p(t.data_ptr() if t is not None else 0)
+    stream = ops._stream()
+    st = L.HfmOperator()
+    st.scale = 1.0
+    st.coef_dtype = code
+    coef_bytes = 0  # coefficient bytes per launch
+    keep = []
+    if a.form in ("sigma7", "face7"):
+        s = torch.exp(torch.randn((3, B, Z, Y, X), device=dev, generator=g))
         if a.form == "sigma7":
             keep = [s[k].to(tdt).contiguous() for k in range(3)]
-            for k in range(3):
-                st.coef[k] = keep[k].data_ptr()
-        st.coef_dtype = {"bf16": L.BF16, "f16": L.F16}[a.dtype]
-        dcode = st.coef_dtype
-        fn = lambda: L.call("hfm_op_jacobi_typed", C.byref(st), dcode, P(xt), P(bt), P(ot), B, Z, Y,
-                            X, 2.0 / 3.0, 0, stream)
-        BYTES[("smooth", a.form)] = BYTES[("smooth", a.form)] * (2 / 4)
-    elif a.kernel == "smooth":
-        fn = lambda: L.call("hfm_op_jacobi", C.byref(st), P(x), P(b), P(out), P(None), B, Z, Y, X,
-                            2.0 / 3.0, 1, 0, stream)
+            st.kind = L.OP_SIGMA7
+            coef_bytes = 3 * B * n * E
+        else:
+            if a.dtype == "f32":
+                raise SystemExit("face7 kernels are 16-bit")
+            keep = [torch.empty((B, Z, Y, X + 8), dtype=tdt, device=dev),
+                    torch.empty((B, Z, Y + 1, X), dtype=tdt, device=dev),
+                    torch.empty((B, Z + 1, Y, X), dtype=tdt, device=dev)]
+            L.call("hfm_sigma7_faces", code, P(s[0]), P(s[1]), P(s[2]), 1.0, 1.0, 1.0,
+                   *(P(t) for t in keep), B, Z, Y, X, stream)
+            st.kind = L.OP_FACE7
+            coef_bytes = sum(t.numel() for t in keep) * E
+        for k in range(3):
+            st.c[k] = 1.0
+            st.coef[k] = keep[k].data_ptr()
+        del s
+    elif a.form == "const7":
+        st.kind = L.OP_CONST7
+        st.k[0], st.k[1], st.k[2] = 50.0, 100.0, 200.0
+    else:
+        st.kind = L.OP_K27
+        for i, v in enumerate(W.pressure27().reshape(27)):
+            st.k[i] = float(v)
+    field = B * n * E
+    typed = a.dtype != "f32"
+    if a.kernel == "smooth":
+        fn = (lambda: L.call("hfm_op_jacobi_typed", C.byref(st), code, P(x), P(b), P(out), B, Z, Y, X,
+                             2.0 / 3.0, 0, stream)) if typed else \
+             (lambda: L.call("hfm_op_jacobi", C.byref(st), P(x), P(b), P(out), P(None), B, Z, Y, X,
+                             2.0 / 3.0, 1, 0, stream))
+        nbytes = 3 * field + coef_bytes
     elif a.kernel == "resid":
-        fn = lambda: L.call("hfm_op_residual", C.byref(st), P(x), P(b), P(out), B, Z, Y, X, 0, stream)
+        fn = (lambda: L.call("hfm_op_residual_typed", C.byref(st), code, P(x), P(b), P(out), B, Z, Y,
+                             X, 0, stream)) if typed else \
+             (lambda: L.call("hfm_op_residual", C.byref(st), P(x), P(b), P(out), B, Z, Y, X, 0, stream))
+        nbytes = 3 * field + coef_bytes
     elif a.kernel == "restrict":
-        fn = lambda: L.call("hfm_residual_restrict", C.byref(st), P(x), P(b), P(None), P(wc),
-                            B, Z, Y, X, 0, stream)
+        fn = (lambda: L.call("hfm_residual_restrict_typed", C.byref(st), code, P(x), P(b), P(None),
+                             P(wc), B, Z, Y, X, 0, stream)) if typed else \
+             (lambda: L.call("hfm_residual_restrict", C.byref(st), P(x), P(b), P(None), P(wc),
+                             B, Z, Y, X, 0, stream))
+        nbytes = 2 * field + field / 8 + coef_bytes
     elif a.kernel == "correct":
-        fn = lambda: L.call("hfm_prolong_correct_smooth", C.byref(st), P(x), P(wc), P(b), P(out),
-                            B, Z, Y, X, 2.0 / 3.0, 0, stream)
+        fn = (lambda: L.call("hfm_prolong_correct_smooth_typed", C.byref(st), code, P(x), P(wc), P(b),
+                             P(out), B, Z, Y, X, 2.0 / 3.0, 0, stream)) if typed else \
+             (lambda: L.call("hfm_prolong_correct_smooth", C.byref(st), P(x), P(wc), P(b), P(out),
+                             B, Z, Y, X, 2.0 / 3.0, 0, stream))
+        nbytes = 3 * field + field / 8 + coef_bytes
     elif a.kernel == "apply27":
-        keep = W.pressure27().reshape(27).copy()
+        w27 = W.pressure27().reshape(27).copy()
         fn = lambda: L.call("hfm_conv3d_k3", P(x), P(out), B, Z, Y, X,
-                            keep.ctypes.data_as(C.c_void_p), stream)
+                            w27.ctypes.data_as(C.c_void_p), stream)
+        nbytes = 2 * field
+    elif a.kernel == "transfer-r":
+        fn = lambda: L.call("hfm_restrict_avg", P(x), P(wc), B, Z, Y, X, stream)
+        nbytes = field + field / 8
+    elif a.kernel == "transfer-p":
+        fn = lambda: L.call("hfm_prolong_nearest", P(wc), P(out), B, Z // 2, Y // 2, X // 2, stream)
+        nbytes = field + field / 8
     else:
         raise SystemExit("unknown kernel " + a.kernel)
+    if a.kernel in ("apply27", "transfer-r", "transfer-p") and typed:
+        raise SystemExit("%s runs in float32 only" % a.kernel)
     for _ in range(a.warmup):
         fn()
     torch.cuda.synchronize()
@@ -100,10 +134,9 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.reps
-    cells = B * Z * Y * X
-    nbytes = BYTES.get((a.kernel, a.form), 0) * cells
-    print(json.dumps({"kernel": a.kernel, "form": a.form, "shape": [B, Z, Y, X],
+    print(json.dumps({"kernel": a.kernel, "form": a.form, "dtype": a.dtype, "shape": [B, Z, Y, X],
                       "ms_per_launch": ms, "bytes_per_launch": nbytes,
+                      "bytes_per_cell": nbytes / (B * n),
                       "gbs": nbytes / (ms / 1e3) / 1e9 if ms > 0 else None}))
 
 

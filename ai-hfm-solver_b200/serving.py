@@ -91,9 +91,12 @@ def dipole_field(n, rng, device, margin=4):
 
 
 def make_stream(count=1024, rate=2000.0, edges=EDGES, log_std=(0.5, 2.0), seed=0,
-                device="cuda"):
+                device="cuda", only=None):
     """The serving workload: ``count`` requests, edge uniform over ``edges``, log-std uniform
-    in ``log_std``, own sigma and dipole each, Poisson arrivals at ``rate`` per second."""
+    in ``log_std``, own sigma and dipole each, Poisson arrivals at ``rate`` per second.
+    With ``only`` (a set of request ids) the fields are built for those requests alone; the
+    others keep their edge, arrival and log-std with ``sigma = rhs = None`` (the draws, and
+    so every request, are the same either way)."""
     rng = np.random.default_rng(seed)
     gen = torch.Generator(device=device)
     t = 0.0
@@ -102,10 +105,35 @@ def make_stream(count=1024, rate=2000.0, edges=EDGES, log_std=(0.5, 2.0), seed=0
         t += rng.exponential(1.0 / rate)
         n = int(rng.choice(edges))
         ls = float(rng.uniform(*log_std))
+        if only is not None and i not in only:
+            _dipole_draws(n, rng)
+            reqs.append(SolveRequest(i, n, t, None, None, ls))
+            continue
         gen.manual_seed(seed * 1000003 + i)
         reqs.append(SolveRequest(i, n, t, sigma_field(n, gen, ls, device),
                                  dipole_field(n, rng, device), ls))
     return reqs
+
+
+def _dipole_draws(n, rng, margin=4):
+    """The random draws of ``dipole_field`` without building the field."""
+    lo, hi = margin, n - margin
+    p = tuple(int(v) for v in rng.integers(lo, hi, 3))
+    q = p
+    while q == p:
+        q = tuple(int(v) for v in rng.integers(lo, hi, 3))
+
+
+def with_rate(requests, rate, seed=0):
+    """The same requests with Poisson arrivals re-drawn at ``rate`` per second (order kept):
+    the stream at a lower offered load."""
+    rng = np.random.default_rng(seed + 7)
+    t = 0.0
+    out = []
+    for r in requests:
+        t += rng.exponential(1.0 / rate)
+        out.append(SolveRequest(r.rid, r.n, t, r.sigma, r.rhs, r.log_std))
+    return out
 
 
 class _Bucket:

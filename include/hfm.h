@@ -48,7 +48,8 @@ typedef enum {
   HFM_OP_CONST7 = 0, /* anisotropic 7-point, constant coefficients kz, ky, kx (7point.ipynb w2) */
   HFM_OP_SIGMA7 = 1, /* 7-point from per-cell conductivities sx, sy, sz (face means) */
   HFM_OP_DIR7 = 2,   /* six per-cell directional coefficient arrays + diagonal (BGS form) */
-  HFM_OP_K27 = 3     /* arbitrary frozen 3x3x3 kernel (27-point pressure / diffusion) */
+  HFM_OP_K27 = 3,    /* arbitrary frozen 3x3x3 kernel (27-point pressure / diffusion) */
+  HFM_OP_FACE7 = 4   /* 7-point from stored face coefficients, walls included (below) */
 } hfm_op_kind;
 
 /* Flags for residual / smoothing calls. */
@@ -66,6 +67,17 @@ typedef enum {
  *   DIR7:   coef[0..6] = A_xm, A_xp, A_ym, A_yp, A_zm, A_zp, A_tot (BGS_multigrid_v1 cell 38),
  *           (A phi)_c = sum_d A_d (phi_c - phi_nb(d)), diagonal A_tot.
  *   K27:    k[0..26] = w27; Jacobi diagonal = k[13].
+ *   FACE7:  coef[0..2] = Fx, Fy, Fz, the coefficients of every cell face, walls included:
+ *           Fx per instance [Z][Y][X + 8]: element i = 0 .. X of a row is the face between
+ *             cells i-1 and i (i = 0 and i = X are the walls; elements past X are unused);
+ *           Fy per instance [Z][Y + 1][X]: row j = 0 .. Y is the face between rows j-1, j;
+ *           Fz per instance [Z + 1][Y][X]: plane k = 0 .. Z likewise.
+ *           (A phi)_c = sum over the six faces F of c of F (phi_c - phi_nb), phi_nb = 0
+ *           outside the grid; the Jacobi diagonal is the sum of the six faces.  The
+ *           SIGMA7 operator in this form is hfm_sigma7_faces' output; in 16-bit storage it
+ *           rounds each face once (SIGMA7 in 16-bit storage rounds the conductivities).
+ *           Instance strides follow from the extents.  No counterpart in the reference,
+ *           whose per-direction arrays (BGS_multigrid_v1.ipynb cell 38) are per cell.
  *   scale multiplies the operator (1 = reference; coarse levels of a handle use
  *   coarse_scale^level).  coef_dtype is the storage type of coef arrays (HFM_F32 for the
  *   stateless calls). */
@@ -145,6 +157,32 @@ int hfm_op_jacobi(const hfm_operator *op, const float *phi, const float *rhs, fl
 int hfm_op_jacobi_typed(const hfm_operator *op, int dtype, const void *phi, const void *rhs,
                         void *out, int B, int Z, int Y, int X, float omega, unsigned flags,
                         hfm_stream_t stream);
+
+/* The residual and the two fused transfer operators with fields and coefficients stored as
+ * `dtype` (as hfm_op_jacobi_typed): r = A phi - b; r_coarse = R (A phi - b) (r_fine may be
+ * NULL); out = J(phi - P w_coarse).  The other kernels of the reduced-precision inner cycles,
+ * exposed for direct use, testing and measurement.  op->coef_dtype must equal dtype. */
+int hfm_op_residual_typed(const hfm_operator *op, int dtype, const void *phi, const void *b,
+                          void *r, int B, int Z, int Y, int X, unsigned flags,
+                          hfm_stream_t stream);
+int hfm_residual_restrict_typed(const hfm_operator *op, int dtype, const void *phi,
+                                const void *b, void *r_fine, void *r_coarse, int B, int Z,
+                                int Y, int X, unsigned flags, hfm_stream_t stream);
+int hfm_prolong_correct_smooth_typed(const hfm_operator *op, int dtype, const void *phi,
+                                     const void *w_coarse, const void *rhs, void *out, int B,
+                                     int Z, int Y, int X, float omega, unsigned flags,
+                                     hfm_stream_t stream);
+
+/* Face coefficients of the SIGMA7 operator (face means c_d (s_i + s_j) / 2, wall faces
+ * c_d s_i; Anisotropic Resistivity Tomography/README:14-26) in the FACE7 layout, stored in
+ * `dtype` (F32, BF16 or F16; each face computed in float32 from the float32 sx, sy, sz and
+ * rounded once).  fx, fy, fz hold B instances of hfm_face7_elems' sizes; elements of Fx
+ * past X are written as zero. */
+int hfm_sigma7_faces(int dtype, const float *sx, const float *sy, const float *sz, float cz,
+                     float cy, float cx, void *fx, void *fy, void *fz, int B, int Z, int Y,
+                     int X, hfm_stream_t stream);
+/* Elements per instance of the FACE7 arrays Fx, Fy, Fz for extents (Z, Y, X). */
+int hfm_face7_elems(int Z, int Y, int X, int64_t *nfx, int64_t *nfy, int64_t *nfz);
 
 /* Fused residual + restriction: r_coarse = R (A phi - b) on the even grid (Z, Y, X), and
  * r_fine = A phi - b when r_fine is not NULL (7point.ipynb:409-419). */
@@ -413,6 +451,12 @@ typedef struct {
  * of once (the serial run of notebooks/parallel_multigrid_advection_diffusion_3D.ipynb cell 15
  * sweeps its 2^3 level twice; Anisotropic_3d_Multigrid_7point.ipynb:424-432 once) */
 #define HFM_OPT_SAWTOOTH_COARSE_SWEEPS 4
+/* options: 16-bit SIGMA7 handles keep the per-cell conductivities on every level (by default
+ * the levels the plane-marching kernels take - X >= 48, Y >= 16 - also hold the FACE7 face
+ * arrays of their operator, formed from float32 conductivities on the fine level, and run
+ * the face kernels there: each face rounded once to the storage type instead of forming
+ * faces from rounded conductivities) */
+#define HFM_OPT_NO_FACES 8
 
 typedef struct {
   int active;       /* 1 while the slot is still iterating */

@@ -109,6 +109,74 @@ class Sigma7:
         return Sigma7(*s, c=self.c, scale=self.scale * coarse_scale, dtype=self.dtype)
 
 
+def round_bf16(a):
+    """float32 values rounded to the nearest bfloat16 (ties to even), as float32."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def round_storage(a, storage):
+    """float32 values rounded to the storage type ("f32", "bf16" or "f16"), as float32."""
+    a = np.asarray(a, np.float32)
+    if storage == "bf16":
+        return round_bf16(a)
+    if storage == "f16":
+        return a.astype(np.float16).astype(np.float32)
+    return a
+
+
+def sigma7_faces(sx, sy, sz, c=(1.0, 1.0, 1.0), storage="f32"):
+    """The face arrays of the SIGMA7 operator in the library's FACE7 layout: Fx
+    (..., Z, Y, X + 8) with element i = 0 .. X the face between cells i-1 and i (walls at 0
+    and X, zero past X), Fy (..., Z, Y + 1, X), Fz (..., Z + 1, Y, X).  Each face is formed in
+    float32 as the kernels form it, c_d (0.5 (s_i + s_j)), a wall face c_d s_i (README face
+    formula, ``Anisotropic Resistivity Tomography/README:14-26``), then rounded once to
+    ``storage``.  Returns float32 arrays holding the rounded values."""
+    f32 = np.float32
+    cz, cy, cx = (f32(v) for v in c)
+    half = f32(0.5)
+
+    def axis_faces(a, ax, cc):
+        a = np.asarray(a, f32)
+        n = a.shape[ax]
+        shp = list(a.shape)
+        shp[ax] = n + 1
+        out = np.empty(shp, f32)
+        sl = lambda i, j: tuple([slice(None)] * (a.ndim + ax) + [slice(i, j)] +
+                                [slice(None)] * (-ax - 1))
+        out[sl(0, 1)] = cc * a[sl(0, 1)]
+        out[sl(n, n + 1)] = cc * a[sl(n - 1, n)]
+        if n > 1:
+            out[sl(1, n)] = cc * (half * (a[sl(0, n - 1)] + a[sl(1, n)]))
+        return round_storage(out, storage)
+
+    fx = axis_faces(sx, -1, cx)
+    fx = np.concatenate([fx, np.zeros(fx.shape[:-1] + (7,), f32)], axis=-1)
+    return fx, axis_faces(sy, -2, cy), axis_faces(sz, -3, cz)
+
+
+class Face7:
+    """The 7-point operator from stored face coefficients (the library's FACE7 form):
+    ``(A phi)_c = sum over the six faces F of c of F (phi_c - phi_nb)``, ghost phi = 0, the
+    diagonal the sum of the six faces.  With ``sigma7_faces`` arrays it is the SIGMA7
+    operator with every face rounded to the storage type."""
+
+    def __init__(self, fx, fy, fz, scale=1.0, dtype=np.float64):
+        self.dtype = dtype
+        fx, fy, fz = (np.asarray(a, dtype) * dtype(scale) for a in (fx, fy, fz))
+        X = fx.shape[-1] - 8
+        self.faces = [(fx[..., :X], fx[..., 1:X + 1]), (fy[..., :-1, :], fy[..., 1:, :]),
+                      (fz[..., :-1, :, :], fz[..., 1:, :, :])]
+        d = np.zeros_like(self.faces[0][0])
+        for lo, hi in self.faces:
+            d = d + lo + hi
+        self.diag = d
+
+    def apply(self, x):
+        return Sigma7.apply(self, x)
+
+
 class Dir7:
     """The reference's variable-coefficient form verbatim: six per-cell coefficient arrays
     ``A_MAT_{xm1,xp1,ym1,yp1,zm1,zp1}`` and their sum ``A_MAT_TOT``

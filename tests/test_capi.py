@@ -120,3 +120,34 @@ def test_sawtooth_coarse_sweeps_option(pkg):
     assert two.options & L.OPT_SAWTOOTH_COARSE_SWEEPS and two.coarse_sweeps == 2
     v = M.SolverConfig(cycle="V", sawtooth_coarse_sweeps=3).struct(L.OP_SIGMA7)
     assert not v.options & L.OPT_SAWTOOTH_COARSE_SWEEPS and v.coarse_sweeps == 32
+
+
+def test_face7_host_calls(lib, pkg):
+    """FACE7 array sizes, argument checks of the face builder, and the handle footprint that
+    counts the face arrays of 16-bit SIGMA7 levels (none with HFM_OPT_NO_FACES or float32)."""
+    L = pkg._lib
+    a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+    assert lib.hfm_face7_elems(4, 5, 6, C.byref(a), C.byref(b), C.byref(c)) == L.OK
+    assert (a.value, b.value, c.value) == (4 * 5 * 14, 4 * 6 * 6, 5 * 5 * 6)
+    assert lib.hfm_face7_elems(0, 5, 6, C.byref(a), C.byref(b), C.byref(c)) == L.ERR_BAD_ARG
+    buf = (C.c_float * 64)()
+    assert lib.hfm_sigma7_faces(L.BF16, None, buf, buf, 1.0, 1.0, 1.0, buf, buf, buf, 1, 2, 2, 2,
+                                None) == L.ERR_BAD_ARG
+    assert lib.hfm_sigma7_faces(L.F64, buf, buf, buf, 1.0, 1.0, 1.0, buf, buf, buf, 1, 2, 2, 2,
+                                None) == L.ERR_BAD_ARG
+    assert b"dtype" in lib.hfm_last_error()
+    cfg = L.HfmMgConfig()
+    lib.hfm_mg_config_default(C.byref(cfg))
+    cfg.storage = L.BF16
+    with_faces = lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1)
+    cfg.options = L.OPT_NO_FACES
+    without = lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1)
+    # faces on the 128^3 and 64^3 levels (X >= 48): 3 arrays of about n cells, 2 bytes each
+    extra = 2 * (128 * 128 * 136 + 128 * 129 * 128 + 129 * 128 * 128 +
+                 64 * 64 * 72 + 64 * 65 * 64 + 65 * 64 * 64)
+    assert with_faces - without == extra
+    cfg.options = 0
+    cfg.storage = L.F32
+    f32 = lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1)
+    cfg.options = L.OPT_NO_FACES
+    assert lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1) == f32

@@ -203,3 +203,18 @@ def test_reduced_precision_storage_smoother(hfm, T, storage):
 
 def ops_sigma(hfm, T, sig):
     return hfm.ops.Sigma7(*(dev(T, sig[k]) for k in range(3)))
+
+
+@pytest.mark.parametrize("shape", [(3, 17, 24, 64), (2, 16, 9, 40), (1, 6, 6, 14)])
+def test_transfers_vector_and_scalar_paths(hfm, T, shape):
+    """Restriction and prolongation on batched grids whose rows take the 16-byte vector
+    kernels (X a multiple of 4) and one that does not (X = 14), odd Z / Y floored: against
+    the oracle's VALID average (same summation order: the bits of the float32 oracle) and
+    UpSampling3D (exact)."""
+    ops = hfm.ops
+    rng = np.random.default_rng(23)
+    x = rng.standard_normal(shape).astype(np.float32)
+    got = ops.restrict_avg(dev(T, x)).cpu().numpy()
+    np.testing.assert_array_equal(got, tfops.restrict_avg(x, np.float32))
+    up = ops.prolong_nearest(dev(T, x)).cpu().numpy()
+    np.testing.assert_array_equal(up, tfops.prolong_nearest(x))
