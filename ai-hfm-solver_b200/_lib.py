@@ -10,7 +10,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libhfm.so")
 
 # hfm_status
-OK, ERR_BAD_ARG, ERR_OOM, ERR_NOT_CONVERGED, ERR_NAN, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED = range(8)
+(OK, ERR_BAD_ARG, ERR_OOM, ERR_NOT_CONVERGED, ERR_NAN, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED,
+ ERR_CANCELLED) = range(9)
 # hfm_dtype
 F32, BF16, F16, F64 = range(4)
 # hfm_op_kind
@@ -20,7 +21,8 @@ FLAG_ZERO_XEND, FLAG_TOP_COPY, FLAG_ZERO_GUESS, FLAG_PERIODIC, FLAG_SAME_LEVEL_C
 # hfm_cycle / hfm_accel
 CYCLE_SAWTOOTH, CYCLE_V, CYCLE_F = range(3)
 ACCEL_NONE, ACCEL_CG, ACCEL_IR = range(3)
-OPT_NO_FUSED_COARSE, OPT_NO_FUSED_PRE, OPT_SAWTOOTH_COARSE_SWEEPS, OPT_NO_FACES = 1, 2, 4, 8
+(OPT_NO_FUSED_COARSE, OPT_NO_FUSED_PRE, OPT_SAWTOOTH_COARSE_SWEEPS, OPT_NO_FACES,
+ OPT_NO_PERSISTENT) = 1, 2, 4, 8, 16
 
 
 class HfmOperator(C.Structure):
@@ -43,6 +45,20 @@ class HfmSlotStats(C.Structure):
                 ("outer", C.c_int), ("norm_b", C.c_double), ("rel_resid", C.c_double)]
 
 
+SERVE_MAX_EDGES = 16
+
+
+class HfmServeConfig(C.Structure):
+    _fields_ = [("n_edges", C.c_int), ("edges", C.c_int * SERVE_MAX_EDGES), ("slots", C.c_int),
+                ("budget_bytes", C.c_double), ("cycles_per_tick", C.c_int),
+                ("solver", HfmMgConfig)]
+
+
+class HfmServeResult(C.Structure):
+    _fields_ = [("ticket", C.c_int64), ("status", C.c_int), ("cycles", C.c_int),
+                ("outer", C.c_int), ("rel_resid", C.c_double)]
+
+
 class HfmError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), msg))
@@ -52,7 +68,7 @@ class HfmError(RuntimeError):
 STATUS_NAMES = {OK: "HFM_OK", ERR_BAD_ARG: "HFM_ERR_BAD_ARG", ERR_OOM: "HFM_ERR_OOM",
                 ERR_NOT_CONVERGED: "HFM_ERR_NOT_CONVERGED", ERR_NAN: "HFM_ERR_NAN",
                 ERR_TIMEOUT: "HFM_ERR_TIMEOUT", ERR_CUDA: "HFM_ERR_CUDA",
-                ERR_UNSUPPORTED: "HFM_ERR_UNSUPPORTED"}
+                ERR_UNSUPPORTED: "HFM_ERR_UNSUPPORTED", ERR_CANCELLED: "HFM_ERR_CANCELLED"}
 
 P = C.c_void_p
 I = C.c_int
@@ -83,6 +99,14 @@ SIGNATURES = {
     "hfm_sigma7_faces": (I, [I, P, P, P, F, F, F, P, P, P, I, I, I, I, P]),
     "hfm_face7_elems": (I, [I, I, I, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
     "hfm_residual_restrict": (I, [P, P, P, P, P, I, I, I, I, U, P]),
+    "hfm_serve_config_default": (None, [P]),
+    "hfm_serve_create": (I, [P, P]),
+    "hfm_serve_bucket_slots": (I, [P, I, C.POINTER(I)]),
+    "hfm_serve_submit": (I, [P, I, P, P, P, P, P, C.POINTER(I64)]),
+    "hfm_serve_poll": (I, [P, P, I, C.POINTER(I)]),
+    "hfm_serve_cancel": (I, [P, I64]),
+    "hfm_serve_pending": (I, [P, C.POINTER(I), C.POINTER(I)]),
+    "hfm_serve_destroy": (I, [P]),
     "hfm_prolong_correct_smooth": (I, [P, P, P, P, P, I, I, I, I, F, U, P]),
     "hfm_stencil7_const_apply": (I, [P, P, I, I, I, I, F, F, F, P]),
     "hfm_stencil7_const_residual": (I, [P, P, P, I, I, I, I, F, F, F, U, P]),

@@ -215,6 +215,7 @@ const char *hfm_status_string(int status) {
     case HFM_ERR_TIMEOUT: return "HFM_ERR_TIMEOUT";
     case HFM_ERR_CUDA: return "HFM_ERR_CUDA";
     case HFM_ERR_UNSUPPORTED: return "HFM_ERR_UNSUPPORTED";
+    case HFM_ERR_CANCELLED: return "HFM_ERR_CANCELLED";
     default: return "HFM_ERR_UNKNOWN";
   }
 }

@@ -40,6 +40,7 @@ int sm_count();  // SMs of the current device (cached per device)
 // expired, [1] drain waits that expired.  Kernels that must not report success after a
 // failed wait read them.
 int wait_fail_counters(const int **out);
+int current_wait_budget();  // polls of a bounded device wait (hfm_set_wait_budget)
 // Raise a kernel's dynamic shared-memory limit on the current device, once per device and
 // kernel (a process that drives several GPUs needs it on each).
 int set_max_dynamic_smem(const void *kernel, int bytes, const char *what);
@@ -294,6 +295,40 @@ template <class T> struct SubArgs {
 };
 size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size, bool sigma);
 template <class T> int launch_subcycle(int kind, SubArgs<T> a, int B, cudaStream_t s);
+
+// The small end of a V-cycle as one persistent kernel (subcycle.cu): a level l1 that the
+// plane-marching TMA kernels do not take, with the fused coarse cycle directly below it.
+// Work items (step, instance, z tile) in step order; an item starts once every item of its
+// instance's earlier steps is done (per-instance counters, bounded waits).
+constexpr int kSmallMaxSteps = 16;
+enum { SK_PRE2 = 0, SK_SMOOTH = 1, SK_RESTRICT = 2, SK_SUB = 3 };
+template <class T> struct SmallArgs {
+  SubArgs<T> sub;            // levels below l1: rhs = the restricted residual, out = the correction
+  DevOp op;                  // level l1's operator (coefficients of type T, instance stride n)
+  int Z, Y, X;               // level l1
+  int64_t n;
+  const T *f;                // right-hand side of level l1
+  const T *invd;             // level l1's 1 / diagonal (SK_PRE2)
+  T *buf[2];                 // level l1's iterate buffers
+  int nsteps;
+  int kind[kSmallMaxSteps];  // SK_*
+  int src[kSmallMaxSteps];   // iterate read (-1: zero)
+  int dst[kSmallMaxSteps];   // iterate written
+  int corr[kSmallMaxSteps];  // SK_SMOOTH: subtract the prolonged coarse correction
+  int dot[kSmallMaxSteps];   // SK_SMOOTH: partial sums of out * f into `partials`
+  float om[kSmallMaxSteps];
+  int base[kSmallMaxSteps + 1];  // first item of each step
+  int need[kSmallMaxSteps];      // items of an instance done before the step may start
+  int tiles, zc;             // z tiles of level l1 (zc planes each, even)
+  const int *active;
+  double *partials;          // [instance][tile]
+  int *ticket;               // next work item (zeroed before the launch)
+  int *done;                 // items done per instance (zeroed before the launch)
+  int wait_budget;
+  int *wait_fail;            // the device's wait-failure counters
+};
+// Blocks the persistent kernel is launched with, for SUB shared memory `smem`.
+template <class T> int launch_small(int kind, SmallArgs<T> a, int B, cudaStream_t s);
 
 // The first two Jacobi sweeps from a zero iterate in one pass (SIGMA7, TMA-eligible grids):
 // out = J(phi1) with phi1 = omega f * invd, invd = 1 / diag of the level.

@@ -83,7 +83,8 @@ __device__ __forceinline__ bool waits_failed(const int *wf) {
 }
 
 __global__ void k_check(const double *__restrict__ partials, int nblk, SlotState *st,
-                        int *active, double tol, int max_cycles, int which_buf, const int *wf) {
+                        int *active, double tol, int max_cycles, int which_buf, const int *wf,
+                        const double *rz_new = nullptr) {
   const int inst = blockIdx.x;
   if (!active[inst]) return;
   __shared__ double sh[32];
@@ -99,6 +100,7 @@ __global__ void k_check(const double *__restrict__ partials, int nblk, SlotState
     double rel = sqrt(tot) / s.norm_b;
     s.rel = rel;
     s.rr = tot;
+    if (rz_new) s.rz = rz_new[inst];  // CG: this iteration's r . z becomes the current one
     if (waits_failed(wf)) {
       s.status = HFM_ERR_TIMEOUT;
       s.sol_buf = which_buf;
@@ -128,7 +130,7 @@ __global__ void k_check(const double *__restrict__ partials, int nblk, SlotState
 // the slot to the outer (float64) step.
 __global__ void k_check_inner(const double *__restrict__ partials, int nblk, SlotState *st,
                               int *active, int *outer_mask, double tol, double inner_tol,
-                              int inner_max, const int *wf) {
+                              int inner_max, const int *wf, const double *rz_new) {
   const int inst = blockIdx.x;
   if (!active[inst]) return;
   __shared__ double sh[32];
@@ -142,6 +144,7 @@ __global__ void k_check_inner(const double *__restrict__ partials, int nblk, Slo
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sh[w];
     SlotState s = st[inst];
     s.rr = tot;
+    s.rz = rz_new[inst];  // this iteration's r . z becomes the current one
     s.cycles += 1;
     s.inner_cycles += 1;
     const double r = sqrt(tot);
@@ -569,38 +572,40 @@ __global__ void k_dot_partials(const float *__restrict__ a, const TZ *__restrict
   HFM_END_ITEMS
 }
 
-// which: 0 -> rz (new), 1 -> pq
-__global__ void k_scalar_sum(const double *__restrict__ partials, int nblk, SlotState *st,
-                             const int *active, int which, double *rz_new) {
-  const int inst = blockIdx.x;
-  if (!active[inst]) return;
+// Sum of one slot's nblk partial sums in a fixed order (256 threads: a thread-strided sum, a
+// warp tree, then the warps in order), so every block that computes it gets the same value.
+__device__ double slot_sum(const double *__restrict__ p, int nblk) {
   __shared__ double sh[32];
+  __shared__ double res;
+  __syncthreads();  // sh / res are reused across items
   double acc = 0.0;
-  for (int i = threadIdx.x; i < nblk; i += blockDim.x) acc += partials[(int64_t)inst * nblk + i];
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) acc += p[i];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
-    if (which == 0) {
-      rz_new[inst] = t;
-    } else {  // p.q of this iteration; rz_new becomes the current r.z (beta used the old one)
-      st[inst].pq = t;
-      st[inst].rz = rz_new[inst];
-    }
+    res = t;
   }
+  __syncthreads();
+  return res;
 }
 
-// p = z + beta p (beta = rz_new / rz; first iteration p = z); rz <- rz_new.
+// p = z + beta p (beta = rz_new / rz; first iteration p = z).  rz_new = r . z is summed here
+// from the slot's nblk_rz partials (every item of the slot sums them in the same order) and
+// stored in rz_new[slot] by the slot's first chunk; the check at the end of the iteration
+// makes it the current rz.
 template <class TZ>
 __global__ void k_cg_p(const TZ *__restrict__ z, float *__restrict__ p, Items it, SlotState *st,
-                       const double *rz_new, const int *active, int scaled,
-                       const double *gscale) {
+                       const double *__restrict__ rz_part, int nblk_rz, double *rz_new,
+                       const int *active, int scaled, const double *gscale) {
   HFM_FOR_ITEMS(it, active[slot])
+  const double rzn = slot_sum(rz_part + (int64_t)slot * nblk_rz, nblk_rz);
+  if (ch == 0 && threadIdx.x == 0) rz_new[slot] = rzn;
   const SlotState s = st[slot];
   const bool first = s.inner_cycles == 0 || s.rz == 0.0;
-  const float beta = first ? 0.f : (float)(rz_new[slot] / s.rz);
+  const float beta = first ? 0.f : (float)(rzn / s.rz);
   const float zs = pc_out(s, it.n, scaled, gscale, slot);
   if (v4) {
     for (int64_t i = lo + 4 * threadIdx.x; i < hi; i += 4 * blockDim.x) {
@@ -626,13 +631,16 @@ __global__ void k_cg_p(const TZ *__restrict__ z, float *__restrict__ p, Items it
 
 // x += alpha p, r -= alpha q, partial sums of r^2; with `rstore` also the storage-type copy of
 // the new r that the next iteration's cycle reads (bf16 refinement: no separate conversion).
+// alpha = rz_new / p.q, with p.q summed here from the slot's nblk_pq partials of the operator
+// pass (a buffer of its own: this kernel writes its r^2 partials into `partials`).
 template <class T>
 __global__ void k_cg_xr(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
                         const float *__restrict__ q, T *__restrict__ rstore, Items it,
-                        const SlotState *st, double *partials, const int *active) {
+                        const double *__restrict__ pq_part, int nblk_pq,
+                        const double *__restrict__ rz_new, double *partials, const int *active) {
   HFM_FOR_ITEMS(it, active[slot])
-  const SlotState s = st[slot];
-  const float alpha = (s.pq != 0.0) ? (float)(s.rz / s.pq) : 0.f;
+  const double pq = slot_sum(pq_part + (int64_t)slot * nblk_pq, nblk_pq);
+  const float alpha = (pq != 0.0) ? (float)(rz_new[slot] / pq) : 0.f;
   double acc = 0.0;
   if (v4) {
     for (int64_t i = lo + 4 * threadIdx.x; i < hi; i += 4 * blockDim.x) {
@@ -757,6 +765,8 @@ struct hfm_mg {
   hfm::SlotState *state = nullptr;
   hfm_slot_stats *stats_dev = nullptr;  // packed per-slot statistics for asynchronous queries
   double *partials = nullptr;
+  double *partials2 = nullptr;  // CG: the p . q partials (read while `partials` is rewritten)
+  int *small_ctr = nullptr;     // persistent small-end kernel: work ticket, per-slot counts
   int64_t partials_per_slot = 0;
   double *scal = nullptr;  // per-slot scratch scalars (rz_new), and ||b||^2 at load
   double *gscale = nullptr;  // fp16 storage: geometric mean of each slot's conductivities
@@ -822,9 +832,9 @@ class Engine : public EngineBase {
                             omega, flags, m_->active, s, partials, nblk);
   }
 
-  int check(int nblk, int which, cudaStream_t s) {
+  int check(int nblk, int which, cudaStream_t s, const double *rz_new = nullptr) {
     k_check<<<m_->slots, 256, 0, s>>>(m_->partials, nblk, m_->state, m_->active, m_->cfg.tol,
-                                      m_->cfg.max_cycles, which, m_->wait_fail);
+                                      m_->cfg.max_cycles, which, m_->wait_fail, rz_new);
     HFM_CHECK_LAUNCH("k_check");
     return HFM_OK;
   }
@@ -881,6 +891,14 @@ class Engine : public EngineBase {
   }
 
   int fused_vcycle(int l0, cudaStream_t s) {
+    SubArgs<T> a = make_sub(l0);
+    cur_[l0] = 0;
+    return launch_subcycle<T>(kind(), a, m_->slots, s);
+  }
+
+  // Arguments of the fused coarse cycle from level l0 down (right-hand side rhs(l0), result
+  // in buf(l0, 0)).
+  SubArgs<T> make_sub(int l0) {
     const hfm_mg_config &c = m_->cfg;
     SubArgs<T> a;
     memset(&a, 0, sizeof(a));
@@ -908,14 +926,108 @@ class Engine : public EngineBase {
     a.nu_pre = c.nu_pre;
     a.nu_post = c.nu_post;
     a.coarse_sweeps = c.coarse_sweeps;
-    cur_[l0] = 0;
-    return launch_subcycle<T>(kind(), a, m_->slots, s);
+    return a;
+  }
+
+  // The small end as one persistent kernel: level l (which the TMA kernels do not take) and
+  // the fused coarse cycle directly below it.
+  bool small_ok(int l) {
+    const hfm_mg_config &c = m_->cfg;
+    if ((c.options & HFM_OPT_NO_PERSISTENT) || fused_l0_ < 0 || l + 1 != fused_l0_) return false;
+    if (lk(l) == HFM_OP_FACE7) return false;
+    if (tma_eligible(lk(l), g(l), FAST_SMOOTH, nullptr, 0, (int)sizeof(T))) return false;
+    if ((g(l).Z | g(l).Y | g(l).X) & 1) return false;
+    if (l == 0 && (c.flags & HFM_FLAG_ZERO_XEND)) return false;
+    if (c.nu_pre + std::max(c.nu_post, 1) + 2 > kSmallMaxSteps) return false;
+    return true;
+  }
+
+  int small_vcycle(int l, cudaStream_t s) {
+    const hfm_mg_config &c = m_->cfg;
+    const int B = m_->slots;
+    SmallArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    a.sub = make_sub(l + 1);
+    a.op = lo(l);
+    a.Z = g(l).Z;
+    a.Y = g(l).Y;
+    a.X = g(l).X;
+    a.n = n(l);
+    a.f = rhs(l);
+    a.invd = (const T *)m_->lv[l].invd;
+    a.buf[0] = buf(l, 0);
+    a.buf[1] = buf(l, 1);
+    a.active = m_->active;
+    // z tiles: about two items per SM and step over the instances, an even number of planes
+    const int want = std::max(1, (2 * sm_count() + B - 1) / B);
+    int zc = (a.Z + want - 1) / want;
+    zc += zc & 1;
+    zc = std::max(2, std::min(zc, a.Z));
+    a.zc = zc;
+    a.tiles = (a.Z + zc - 1) / zc;
+    const bool dot = want_rz_ && l == 0;
+    int ns = 0, cur = 0;
+    bool zero = true;
+    auto add = [&](int kind, int corr, int dotk, float om) {
+      a.kind[ns] = kind;
+      a.src[ns] = zero ? -1 : cur;
+      a.dst[ns] = cur ^ 1;
+      a.corr[ns] = corr;
+      a.dot[ns] = dotk;
+      a.om[ns] = om;
+      ++ns;
+    };
+    int k0 = 0;
+    if (c.nu_pre >= 2 && kind() == HFM_OP_SIGMA7 && a.invd && !(c.options & HFM_OPT_NO_FUSED_PRE)) {
+      add(SK_PRE2, 0, 0, c.omega);  // phi1 = omega f / diag formed inside the second sweep
+      cur ^= 1;
+      zero = false;
+      k0 = 2;
+    }
+    for (int k = k0; k < c.nu_pre; ++k) {
+      add(SK_SMOOTH, 0, 0, c.omega);
+      cur ^= 1;
+      zero = false;
+    }
+    a.kind[ns] = SK_RESTRICT;
+    a.src[ns] = zero ? -1 : cur;
+    ++ns;
+    a.kind[ns] = SK_SUB;
+    ++ns;
+    const int post = std::max(c.nu_post, 1);
+    for (int k = 0; k < post; ++k) {
+      add(SK_SMOOTH, k == 0, dot && k == post - 1, c.nu_post == 0 ? 0.f : c.omega);
+      cur ^= 1;
+      zero = false;
+    }
+    a.nsteps = ns;
+    int per_inst = 0;
+    for (int i = 0; i < ns; ++i) {
+      const int cnt = a.kind[i] == SK_SUB ? 1 : a.tiles;
+      a.base[i] = B * per_inst;
+      a.need[i] = per_inst;
+      per_inst += cnt;
+    }
+    a.base[ns] = B * per_inst;
+    a.partials = dot ? m_->partials : nullptr;
+    a.ticket = m_->small_ctr;
+    a.done = m_->small_ctr + 1;
+    a.wait_budget = current_wait_budget();
+    a.wait_fail = const_cast<int *>(m_->wait_fail);
+    HFM_CUDA(cudaMemsetAsync(m_->small_ctr, 0, (size_t)(B + 1) * sizeof(int), s));
+    int st = launch_small<T>(kind(), a, B, s);
+    if (st) return st;
+    if (dot) nblk_rz_ = a.tiles;
+    cur_[l] = cur;
+    cur_[l + 1] = 0;
+    return HFM_OK;
   }
 
   int vcycle(int l, bool zero, bool fcycle, int check_level0, cudaStream_t s) {
     const hfm_mg_config &c = m_->cfg;
     int st;
     if (l == m_->L - 1) return coarse_solve(l, s);
+    if (zero && !fcycle && !(l == 0 && check_level0) && small_ok(l)) return small_vcycle(l, s);
     if (zero && !fcycle && l > 0 && l == fused_l0_) return fused_vcycle(l, s);
     if (zero) cur_[l] = 0;
     // NS outflow rule on the fine level (as the reference cycle applies it): the iterate is
@@ -1087,37 +1199,37 @@ class Engine : public EngineBase {
     want_rz_ = false;
     if (st) return st;
     const T *z = buf(0, cur_[0]);
-    // rz_new = r . z ; p = z + beta p
-    if (nblk_rz_ > 0) {
-      k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, nblk_rz_, m_->state, m_->active, 0, m_->scal);
-    } else {
+    // rz_new = r . z (summed inside k_cg_p from the last sweep's partials, or from a separate
+    // dot pass); p = z + beta p
+    const double *rz_part = m_->partials;
+    int nblk_rz = nblk_rz_;
+    if (nblk_rz_ <= 0) {
       k_dot_partials<T><<<ib, 256, 0, s>>>(r, z, it, m_->partials, m_->active, m_->state, scaled,
                                            m_->gscale);
       HFM_CHECK_LAUNCH("k_dot_partials");
-      k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, 0, m_->scal);
+      nblk_rz = vb;
     }
-    k_cg_p<T><<<ib, 256, 0, s>>>(z, p, it, m_->state, m_->scal, m_->active, scaled, m_->gscale);
+    k_cg_p<T><<<ib, 256, 0, s>>>(z, p, it, m_->state, rz_part, nblk_rz, m_->scal, m_->active,
+                                 scaled, m_->gscale);
     HFM_CHECK_LAUNCH("k_cg_p");
     // q = A p with the partial sums of p . q in the same pass (float32 operator on the fine
-    // level); the p.q reduction also makes rz_new the current r.z
+    // level), into a partials buffer of their own
     PhiSrc<float> pp;
     memset(&pp, 0, sizeof(pp));
     pp.base = p;
     pp.base_stride = nf;
     int nblk_pq = 0;
     if ((st = launch_residual<float>(kind(), fine32_, pp, nullptr, 0, q, nf, B, g(0), HFM_INT_DOT_PHI,
-                                     m_->active, m_->partials, &nblk_pq, s)))
+                                     m_->active, m_->partials2, &nblk_pq, s)))
       return st;
-    k_scalar_sum<<<B, 256, 0, s>>>(m_->partials, nblk_pq, m_->state, m_->active, 1, m_->scal);
-    HFM_CHECK_LAUNCH("k_scalar_sum");
-    // x += alpha p ; r -= alpha q ; ||r||
-    k_cg_xr<T><<<ib, 256, 0, s>>>(x, r, p, q, fused_rhs() ? rhs(0) : nullptr, it, m_->state,
-                                  m_->partials, m_->active);
+    // x += alpha p ; r -= alpha q ; ||r||  (alpha from rz_new and the p . q partials)
+    k_cg_xr<T><<<ib, 256, 0, s>>>(x, r, p, q, fused_rhs() ? rhs(0) : nullptr, it, m_->partials2,
+                                  nblk_pq, m_->scal, m_->partials, m_->active);
     HFM_CHECK_LAUNCH("k_cg_xr");
-    if (!ir) return check(vb, 0, s);
+    if (!ir) return check(vb, 0, s, m_->scal);
     k_check_inner<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
                                     m_->cfg.tol, m_->cfg.inner_tol, m_->cfg.inner_max_cycles,
-                                    m_->wait_fail);
+                                    m_->wait_fail, m_->scal);
     HFM_CHECK_LAUNCH("k_check_inner");
     return HFM_OK;
   }
@@ -1556,7 +1668,8 @@ size_t hfm_mg_footprint_bytes(const hfm_mg_config *c, int Z, int Y, int X, int s
     tot += nf * 2 * es;
   }
   tot *= (size_t)slots;
-  tot += (size_t)slots * (sizeof(SlotState) + 64) + (size_t)slots * 4096 * 8;
+  tot += (size_t)slots * (sizeof(SlotState) + 64) +
+         (size_t)slots * 4096 * 8 * (c->accel != HFM_ACCEL_NONE ? 2 : 1);
   return tot;
 }
 
@@ -1622,7 +1735,10 @@ int hfm_mg_create(const hfm_mg_config *cfg, int Z, int Y, int X, int slots, hfm_
   m->partials_per_slot = std::max<int64_t>(std::max<int64_t>(4096, max_partial_blocks(lv[0], slots)),
                                           item_chunks(lv[0].n()));
   m->partials = (double *)dalloc(m.get(), (size_t)slots * m->partials_per_slot * 8, &st);
+  if (cfg->accel != HFM_ACCEL_NONE)
+    m->partials2 = (double *)dalloc(m.get(), (size_t)slots * m->partials_per_slot * 8, &st);
   m->active = (int *)dalloc(m.get(), (size_t)slots * 4, &st);
+  m->small_ctr = (int *)dalloc(m.get(), (size_t)(slots + 1) * 4, &st);
   m->state = (SlotState *)dalloc(m.get(), (size_t)slots * sizeof(SlotState), &st);
   m->stats_dev = (hfm_slot_stats *)dalloc(m.get(), (size_t)slots * sizeof(hfm_slot_stats), &st);
   m->scal = (double *)dalloc(m.get(), (size_t)(slots + 1) * 8, &st);

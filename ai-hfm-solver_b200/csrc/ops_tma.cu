@@ -836,6 +836,8 @@ extern "C" int hfm_set_wait_budget(int polls) {
 
 namespace hfm {
 
+int current_wait_budget() { return g_wait_budget.load(); }
+
 // Device address of g_tma_wait_fail on the current device (looked up once per device with
 // that device current: in host code the array's name only stands for the symbol).
 int wait_fail_counters(const int **out) {

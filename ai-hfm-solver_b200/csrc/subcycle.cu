@@ -13,6 +13,8 @@
 // phi = 0: SIGMA7 face coefficients c_d (s_i + s_j) / 2 (wall face c_d s_i); CONST7 the
 // anisotropic 7-point stencil with diagonal 2 (kz + ky + kx); K27 any 3x3x3 kernel, diagonal
 // its centre weight.
+#include <algorithm>
+
 #include "hfm_internal.cuh"
 
 namespace hfm {
@@ -105,11 +107,21 @@ __device__ void sub_resid_restrict(const SubLevel<T> &L, const float *ph, const 
   __syncthreads();
 }
 
-template <int KIND, class T>
-__global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant__ SubArgs<T> a) {
-  const int64_t inst = blockIdx.x;
-  if (a.active && !a.active[inst]) return;
-  extern __shared__ __align__(16) unsigned char sub_smem[];
+// A 16-bit or float32 value read through L2 (ld.global.cg): data another block of the same
+// launch may have written (the persistent kernel's restricted residual).
+template <class T> __device__ __forceinline__ T ld_l2(const T *p);
+template <> __device__ __forceinline__ float ld_l2<float>(const float *p) { return __ldcg(p); }
+template <> __device__ __forceinline__ __nv_bfloat16 ld_l2<__nv_bfloat16>(const __nv_bfloat16 *p) {
+  return __ushort_as_bfloat16(__ldcg(reinterpret_cast<const unsigned short *>(p)));
+}
+template <> __device__ __forceinline__ __half ld_l2<__half>(const __half *p) {
+  return __ushort_as_half(__ldcg(reinterpret_cast<const unsigned short *>(p)));
+}
+
+// The coarse-end V-cycle of one instance with the block's shared memory `sub_smem`.  COH:
+// the right-hand side was written by other blocks of the same launch (read through L2).
+template <int KIND, class T, bool COH>
+__device__ void subcycle_body(const SubArgs<T> &a, int64_t inst, unsigned char *sub_smem) {
   float *F = reinterpret_cast<float *>(sub_smem);
   T *S = reinterpret_cast<T *>(sub_smem + a.sig_byte_offset);
   const int nl = a.nlev;
@@ -122,8 +134,10 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant_
       S[L.o_sig + 2 * L.n + i] = L.sz[g + i];
     }
   }
-  for (int i = threadIdx.x; i < a.lv[0].n; i += blockDim.x)
-    F[a.lv[0].o_rhs + i] = St<T>::to(a.rhs[inst * (int64_t)a.lv[0].n + i]);
+  for (int i = threadIdx.x; i < a.lv[0].n; i += blockDim.x) {
+    const T *src = a.rhs + inst * (int64_t)a.lv[0].n + i;
+    F[a.lv[0].o_rhs + i] = St<T>::to(COH ? ld_l2<T>(src) : *src);
+  }
   __syncthreads();
 
   int cur[kMaxSubLevels];    // 0: iterate in phi, 1: in tmp
@@ -179,6 +193,14 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant_
     a.out[inst * (int64_t)a.lv[0].n + i] = St<T>::from(res[i]);
 }
 
+template <int KIND, class T>
+__global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant__ SubArgs<T> a) {
+  const int64_t inst = blockIdx.x;
+  if (a.active && !a.active[inst]) return;
+  extern __shared__ __align__(16) unsigned char sub_smem[];
+  subcycle_body<KIND, T, false>(a, inst, sub_smem);
+}
+
 }  // namespace
 
 size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size, bool sigma) {
@@ -200,6 +222,221 @@ int go_subcycle(const SubArgs<T> &a, int B, size_t smem, cudaStream_t s) {
   HFM_CHECK_LAUNCH("k_subcycle");
   return HFM_OK;
 }
+
+// Shared-memory layout of the coarse-end cycle: float fields of every level, then (SIGMA7)
+// the conductivities.  Returns the bytes, 0 if they exceed the limit.
+template <class T> size_t layout_sub(int kind, SubArgs<T> &a) {
+  int n[kMaxSubLevels];
+  for (int l = 0; l < a.nlev; ++l) n[l] = a.lv[l].n;
+  int off = 0;
+  for (int l = 0; l < a.nlev; ++l) {
+    a.lv[l].o_phi = off;
+    a.lv[l].o_tmp = off + n[l];
+    a.lv[l].o_rhs = off + 2 * n[l];
+    off += 3 * n[l];
+  }
+  a.sig_byte_offset = ((off * 4 + 15) / 16) * 16;
+  int soff = 0;
+  for (int l = 0; l < a.nlev; ++l) {
+    a.lv[l].o_sig = soff;
+    soff += 3 * n[l];
+  }
+  const size_t smem = subcycle_smem_bytes(n, a.nlev, (int)sizeof(T), kind == HFM_OP_SIGMA7);
+  return smem > kSubcycleMaxSmem ? 0 : smem;
+}
+
+// ------------------------------------------------------------------ persistent small end
+// Level l1 of a V-cycle and the coarse end below it in one launch.  A block takes work items
+// in order from a global ticket: (step, instance, z tile) for the sweeps and the residual +
+// restriction of level l1, (SUB, instance) for the coarse end, which runs in the block's
+// shared memory exactly as k_subcycle does.  Items are numbered step by step, so an item
+// only waits for items with smaller numbers - items other running blocks have already taken
+// - and the waits always end; each is still bounded (the wait budget), and one that runs out
+// is counted in the device's wait-failure counters (the handle then ends its slots with
+// HFM_ERR_TIMEOUT) and the item is skipped.  Iterates, the restricted residual and the
+// correction written in this launch are read through L2; conductivities, 1 / diag and f are
+// read-only here.
+
+// Iterate source of a sweep of the persistent kernel: phi' = (src or 0) - P(wc), or the
+// fused first sweep's phi1 = omega f / diag.
+template <class T> struct SmallPhi {
+  const T *base, *corr, *f, *invd;
+  int64_t stride, cstride;
+  int Yc, Xc;
+  float omega;
+  int pre2;
+  __device__ __forceinline__ float operator()(int64_t inst, int z, int y, int x, int Y, int X) const {
+    const int64_t i = inst * stride + ((int64_t)z * Y + y) * X + x;
+    if (pre2) return omega * St<T>::ld(f + i) * St<T>::ld(invd + i);
+    float v = base ? St<T>::to(ld_l2<T>(base + i)) : 0.f;
+    if (corr) v -= St<T>::to(ld_l2<T>(corr + inst * cstride + ((int64_t)(z >> 1) * Yc + (y >> 1)) * Xc + (x >> 1)));
+    return v;
+  }
+};
+
+template <int KIND, class T>
+__device__ void small_sweep(const SmallArgs<T> &a, int sidx, int64_t inst, int tile) {
+  const int X = a.X, Y = a.Y, Z = a.Z;
+  const int z0 = tile * a.zc, z1 = min(Z, z0 + a.zc);
+  SmallPhi<T> ph;
+  ph.base = a.src[sidx] >= 0 ? a.buf[a.src[sidx]] : nullptr;
+  ph.corr = a.corr[sidx] ? a.sub.out : nullptr;
+  ph.f = a.f;
+  ph.invd = a.invd;
+  ph.stride = a.n;
+  ph.cstride = a.sub.lv[0].n;
+  ph.Yc = a.sub.lv[0].Y;
+  ph.Xc = a.sub.lv[0].X;
+  ph.omega = a.om[sidx];
+  ph.pre2 = a.kind[sidx] == SK_PRE2;
+  T *out = a.buf[a.dst[sidx]] + inst * a.n;
+  const float om = a.om[sidx];
+  double acc = 0.0;
+  const int64_t cells = (int64_t)(z1 - z0) * Y * X;
+  for (int64_t k = threadIdx.x; k < cells; k += blockDim.x) {
+    const int x = (int)(k % X);
+    const int64_t t = k / X;
+    const int y = (int)(t % Y), z = z0 + (int)(t / Y);
+    float dg;
+    const float ax = op_apply_at<KIND, T>(a.op, ph, inst, z, y, x, Z, Y, X, &dg);
+    const int64_t i = ((int64_t)z * Y + y) * X + x;
+    const float fv = St<T>::ld(a.f + inst * a.n + i);
+    const float pc = ph(inst, z, y, x, Y, X);
+    const float v = pc + om * __fdividef(fv - ax, dg);
+    out[i] = St<T>::from(v);
+    if (a.dot[sidx]) acc += (double)v * fv;
+  }
+  if (a.dot[sidx] && a.partials) {
+    __shared__ double sh[32];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tot = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sh[w];
+      a.partials[inst * a.tiles + tile] = tot;
+    }
+  }
+}
+
+// r_c = R(A phi - f) for the coarse planes of z tile `tile` (zc even).
+template <int KIND, class T>
+__device__ void small_restrict(const SmallArgs<T> &a, int sidx, int64_t inst, int tile) {
+  const int X = a.X, Y = a.Y, Z = a.Z;
+  const SubLevel<T> &C = a.sub.lv[0];
+  SmallPhi<T> ph;
+  ph.base = a.src[sidx] >= 0 ? a.buf[a.src[sidx]] : nullptr;
+  ph.corr = nullptr;
+  ph.f = a.f;
+  ph.invd = a.invd;
+  ph.stride = a.n;
+  ph.pre2 = 0;
+  T *fc = const_cast<T *>(a.sub.rhs) + inst * (int64_t)C.n;
+  const int c0 = tile * a.zc / 2, c1 = min(C.Z, (tile * a.zc + a.zc) / 2);
+  const int64_t cells = (int64_t)(c1 - c0) * C.Y * C.X;
+  for (int64_t k = threadIdx.x; k < cells; k += blockDim.x) {
+    const int xc = (int)(k % C.X);
+    const int64_t t = k / C.X;
+    const int yc = (int)(t % C.Y), zcc = c0 + (int)(t / C.Y);
+    float sum = 0.f;
+#pragma unroll
+    for (int aa = 0; aa < 2; ++aa)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int z = 2 * zcc + aa, y = 2 * yc + bb, x = 2 * xc + cc;
+          float dg;
+          const float ax = op_apply_at<KIND, T>(a.op, ph, inst, z, y, x, Z, Y, X, &dg);
+          sum += 0.125f * (ax - St<T>::ld(a.f + inst * a.n + ((int64_t)z * Y + y) * X + x));
+        }
+    fc[((int64_t)zcc * C.Y + yc) * C.X + xc] = St<T>::from(sum);
+  }
+}
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <int KIND, class T>
+__global__ void __launch_bounds__(kSubThreads) k_small(const __grid_constant__ SmallArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char sub_smem[];
+  __shared__ int item_sh, ok_sh;
+  const int total = a.base[a.nsteps];
+  for (;;) {
+    if (threadIdx.x == 0) item_sh = atomicAdd(a.ticket, 1);
+    __syncthreads();
+    const int item = item_sh;
+    if (item >= total) break;
+    int s = 0;
+    while (item >= a.base[s + 1]) ++s;
+    const int cnt = a.kind[s] == SK_SUB ? 1 : a.tiles;
+    const int local = item - a.base[s];
+    const int64_t inst = local / cnt;
+    const int tile = local % cnt;
+    if (a.active && !a.active[inst]) {
+      __syncthreads();  // item_sh is rewritten by the next take
+      continue;
+    }
+    if (threadIdx.x == 0) {
+      int ok = 1;
+      if (a.need[s] > 0) {
+        ok = 0;
+        for (int i = 0; i < a.wait_budget; ++i)
+          if (ld_acquire(a.done + inst) >= a.need[s]) {
+            ok = 1;
+            break;
+          }
+        if (!ok) atomicAdd(a.wait_fail, 1);
+      }
+      ok_sh = ok;
+    }
+    __syncthreads();
+    if (ok_sh) {
+      if (a.kind[s] == SK_SUB) subcycle_body<KIND, T, true>(a.sub, inst, sub_smem);
+      else if (a.kind[s] == SK_RESTRICT) small_restrict<KIND, T>(a, s, inst, tile);
+      else small_sweep<KIND, T>(a, s, inst, tile);
+    }
+    // publish: every thread's writes, then the instance's count
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(a.done + inst, 1);
+  }
+}
+
+template <int KIND, class T>
+int go_small(const SmallArgs<T> &a, size_t smem, cudaStream_t s) {
+  const void *fn = (const void *)k_small<KIND, T>;
+  int st = set_max_dynamic_smem(fn, (int)kSubcycleMaxSmem, "cudaFuncSetAttribute(k_small)");
+  if (st) return st;
+  int per_sm = 0;
+  HFM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSubThreads, smem));
+  if (per_sm < 1) per_sm = 1;
+  const int total = a.base[a.nsteps];
+  const int blocks = std::min(total, per_sm * sm_count());
+  k_small<KIND, T><<<blocks, kSubThreads, smem, s>>>(a);
+  HFM_CHECK_LAUNCH("k_small");
+  return HFM_OK;
+}
+
+template <class T>
+int launch_small(int kind, SmallArgs<T> a, int B, cudaStream_t s) {
+  const size_t smem = layout_sub<T>(kind, a.sub);
+  if (!smem) return fail(HFM_ERR_BAD_ARG, "small-level kernel: coarse levels exceed shared memory");
+  (void)B;
+  switch (kind) {
+    case HFM_OP_SIGMA7: return go_small<HFM_OP_SIGMA7, T>(a, smem, s);
+    case HFM_OP_CONST7: return go_small<HFM_OP_CONST7, T>(a, smem, s);
+    case HFM_OP_K27: return go_small<HFM_OP_K27, T>(a, smem, s);
+    default: return fail(HFM_ERR_UNSUPPORTED, "small-level kernel: operator kind");
+  }
+}
+
+template int launch_small<float>(int, SmallArgs<float>, int, cudaStream_t);
+template int launch_small<__nv_bfloat16>(int, SmallArgs<__nv_bfloat16>, int, cudaStream_t);
+template int launch_small<__half>(int, SmallArgs<__half>, int, cudaStream_t);
 
 template <class T>
 int launch_subcycle(int kind, SubArgs<T> a, int B, cudaStream_t s) {

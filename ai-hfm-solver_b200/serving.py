@@ -313,6 +313,91 @@ class SolveServer:
         return results
 
 
+class NativeServer:
+    """The library's own serving loop (``hfm_serve_*``, the C ABI a non-Python host calls):
+    the same buckets, admission by footprint and per-bucket graph launches as
+    ``SolveServer``, driven by ``hfm_serve_poll``."""
+
+    def __init__(self, cfg=None, edges=EDGES, slots=64, budget_bytes=120e9, cycles_per_tick=4):
+        c = L.HfmServeConfig()
+        L.lib().hfm_serve_config_default(C.byref(c))
+        c.n_edges = len(edges)
+        for i, e in enumerate(edges):
+            c.edges[i] = int(e)
+        c.slots = int(slots)
+        c.budget_bytes = float(budget_bytes)
+        c.cycles_per_tick = int(cycles_per_tick)
+        if cfg is not None:
+            c.solver = cfg.struct(L.OP_SIGMA7)
+        h = C.c_void_p()
+        L.call("hfm_serve_create", C.byref(c), C.byref(h))
+        self._h = h
+        self._keep = {}  # ticket -> (inputs, output): valid until the request is reported
+
+    def bucket_slots(self, edge):
+        v = C.c_int()
+        L.call("hfm_serve_bucket_slots", self._h, int(edge), C.byref(v))
+        return v.value
+
+    def submit(self, req):
+        """Queue ``req`` (device tensors); returns its ticket."""
+        sig = req.sigma.contiguous()
+        rhs = req.rhs.contiguous()
+        x = torch.empty((req.n,) * 3, dtype=torch.float64, device=sig.device)
+        torch.cuda.current_stream().synchronize()  # the buckets read the inputs on their streams
+        t = C.c_int64()
+        P = lambda a: C.c_void_p(a.data_ptr())
+        L.call("hfm_serve_submit", self._h, int(req.n), P(sig[0]), P(sig[1]), P(sig[2]), P(rhs),
+               P(x), C.byref(t))
+        self._keep[t.value] = (sig, rhs, x)
+        return t.value
+
+    def poll(self, cap=256):
+        """Finished requests: a list of dicts (ticket, status, cycles, outer, rel_resid, x)."""
+        buf = (L.HfmServeResult * cap)()
+        n = C.c_int()
+        L.call("hfm_serve_poll", self._h, buf, cap, C.byref(n))
+        out = []
+        for r in buf[:n.value]:
+            _, _, x = self._keep.pop(r.ticket)
+            out.append(dict(ticket=r.ticket, status=r.status, cycles=r.cycles, outer=r.outer,
+                            rel_resid=r.rel_resid, x=x))
+        return out
+
+    def cancel(self, ticket):
+        L.call("hfm_serve_cancel", self._h, int(ticket))
+
+    def pending(self):
+        q, r = C.c_int(), C.c_int()
+        L.call("hfm_serve_pending", self._h, C.byref(q), C.byref(r))
+        return q.value, r.value
+
+    def serve(self, requests, timeout_s=600.0):
+        """Submit every request, poll until all are reported; {ticket: result}, and the
+        tickets in request order."""
+        tickets = [self.submit(r) for r in requests]
+        done = {}
+        t0 = time.perf_counter()
+        while len(done) < len(tickets):
+            for r in self.poll():
+                done[r["ticket"]] = r
+            if time.perf_counter() - t0 > timeout_s:
+                raise TimeoutError("hfm_serve_poll: requests still pending after %.0f s" % timeout_s)
+        return done, tickets
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            L.lib().hfm_serve_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def solve_one_at_a_time(requests, cfg=None, time_budget_s=None, keep_solutions=False):
     """The plain path: one request at a time through a single-slot float32 handle per edge.
     Returns (results, seconds)."""

@@ -37,7 +37,8 @@ typedef enum {
   HFM_ERR_NAN = 4,           /* NaN/Inf found in a residual norm */
   HFM_ERR_TIMEOUT = 5,       /* a bounded device-side wait expired */
   HFM_ERR_CUDA = 6,          /* CUDA runtime error (message in hfm_last_error) */
-  HFM_ERR_UNSUPPORTED = 7
+  HFM_ERR_UNSUPPORTED = 7,
+  HFM_ERR_CANCELLED = 8      /* a served request cancelled before it finished */
 } hfm_status;
 
 typedef enum { HFM_F32 = 0, HFM_BF16 = 1, HFM_F16 = 2, HFM_F64 = 3 } hfm_dtype;
@@ -457,6 +458,13 @@ typedef struct {
  * the face kernels there: each face rounded once to the storage type instead of forming
  * faces from rounded conductivities) */
 #define HFM_OPT_NO_FACES 8
+/* options: run the small end of a V-cycle - the level above the fused coarse cycle when the
+ * plane-marching TMA kernels do not take it (X < 48), and the fused coarse cycle - as
+ * separate launches (by default one persistent kernel walks an (instance, step, tile) work
+ * list of that level's sweeps, its residual + restriction, the coarse cycle of every
+ * instance and the correction, with per-instance dependency counters; handles of at least
+ * 8 slots, zero-guess V-cycles such as a CG preconditioner's) */
+#define HFM_OPT_NO_PERSISTENT 16
 
 typedef struct {
   int active;       /* 1 while the slot is still iterating */
@@ -507,6 +515,66 @@ int hfm_mg_fetch_f64(hfm_mg *mg, int slot, double *phi_out, hfm_stream_t stream)
 /* Read an internal level buffer of a slot (0 = phi / w, 1 = rhs / r) for per-level checks. */
 int hfm_mg_read_level(hfm_mg *mg, int slot, int level, int which, float *out,
                       hfm_stream_t stream);
+
+/* ------------------------------------------------------------------ serving */
+/* Continuous batching of anisotropic forward solves -div(sigma grad phi) = f (SIGMA7, cubic
+ * grids of several edges) for hosts that are not Python: one resident multigrid handle
+ * ("bucket") per edge with a number of slots, sized so the buckets fit an HBM budget
+ * (admission by footprint: the largest buckets halve their slots until the sum fits).
+ * hfm_serve_poll never blocks: it retires the finished slots of every bucket whose last
+ * launch has completed (copying each solution to the request's output), admits queued
+ * requests into free slots and relaunches the bucket (cycles_per_tick iterations as one
+ * CUDA graph, each bucket on a stream of its own), so a request that arrives while others
+ * run joins its bucket's next launch.  Each slot's arithmetic depends only on its own data,
+ * so a result is the same alone and in the mix.  No counterpart in the reference (which
+ * solves one problem per script run); the Python server (serving.py) runs the same loop.
+ * A server is not thread-safe; use it from one host thread. */
+typedef struct hfm_server hfm_server;
+#define HFM_SERVE_MAX_EDGES 16
+typedef struct {
+  int n_edges;               /* cubic edges served, one bucket each */
+  int edges[HFM_SERVE_MAX_EDGES];
+  int slots;                 /* slots per bucket before admission by footprint (default 64) */
+  double budget_bytes;       /* HBM budget of all buckets (default 120e9) */
+  int cycles_per_tick;       /* iterations per bucket launch (default 4) */
+  hfm_mg_config solver;      /* bucket solver; op_kind must be SIGMA7 and accel IR (default:
+                                V(2,2) PCG in float64 refinement, bf16 storage, tol 1e-6,
+                                inner_tol 1e-3, max_cycles 600) */
+} hfm_serve_config;
+
+typedef struct {
+  int64_t ticket;            /* from hfm_serve_submit */
+  int status;                /* HFM_OK, HFM_ERR_NOT_CONVERGED, HFM_ERR_NAN, HFM_ERR_TIMEOUT,
+                                HFM_ERR_CANCELLED */
+  int cycles;                /* CG iterations done */
+  int outer;                 /* float64 refinement steps done */
+  double rel_resid;          /* float64 relative residual ||b - A x|| / ||b|| */
+} hfm_serve_result;
+
+void hfm_serve_config_default(hfm_serve_config *cfg);
+/* Create the buckets on the current device (edges 32, 48, 64, 96, 128 by default). */
+int hfm_serve_create(const hfm_serve_config *cfg, hfm_server **out);
+/* Slots the bucket of `edge` holds after admission by footprint. */
+int hfm_serve_bucket_slots(const hfm_server *srv, int edge, int *slots);
+/* Queue a request of edge n: conductivities sx, sy, sz and right-hand side f (device
+ * float32, n^3 each, [z][y][x]) and the output x (device float64, n^3).  The caller owns
+ * all five arrays: its writes to the inputs must be complete before the call (the buckets
+ * read them on their own streams), and it keeps them valid and unchanged until the request
+ * is reported by hfm_serve_poll; x is complete when reported.  Returns a ticket (increasing
+ * from 0). */
+int hfm_serve_submit(hfm_server *srv, int n, const float *sx, const float *sy, const float *sz,
+                     const float *f, double *x, int64_t *ticket);
+/* Advance every bucket without blocking; report up to `cap` finished requests in done[]
+ * (their x is complete in device memory) and their number in *n_done. */
+int hfm_serve_poll(hfm_server *srv, hfm_serve_result *done, int cap, int *n_done);
+/* Cancel a queued or running request: it is reported by a later poll with
+ * HFM_ERR_CANCELLED (x not written).  HFM_ERR_BAD_ARG for an unknown or finished ticket. */
+int hfm_serve_cancel(hfm_server *srv, int64_t ticket);
+/* Requests queued (waiting for a slot) and running (in a slot or copying out). */
+int hfm_serve_pending(const hfm_server *srv, int *queued, int *running);
+/* Wait for the device work of every bucket, then free the buckets (pending requests are
+ * dropped unreported). */
+int hfm_serve_destroy(hfm_server *srv);
 
 #ifdef __cplusplus
 }

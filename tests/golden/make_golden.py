@@ -1,6 +1,7 @@
 """Generate the golden fixtures in this directory.
 
-Run from the repository root: ``python tests/golden/make_golden.py``.
+Run from the repository root with the reference checkout named by ``HFM_REFERENCE_ROOT``:
+``HFM_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py``.
 
 Two kinds of fixture are written:
 
@@ -42,12 +43,16 @@ def torch_conv_same(x, K):
     return torch.nn.functional.conv3d(t, k, padding=1)[0, 0].numpy()
 
 
-REFERENCE = os.environ.get("HFM_REFERENCE_ROOT", "/root/reference")
-NOTEBOOKS = os.path.join(REFERENCE, "Anisotropic Resistivity Tomography", "notebooks")
+def _notebooks():
+    """The reference checkout's notebook folder: HFM_REFERENCE_ROOT must name the checkout."""
+    root = os.environ.get("HFM_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("set HFM_REFERENCE_ROOT to the bc1chen/AI-HFM-Solver checkout")
+    return os.path.join(root, "Anisotropic Resistivity Tomography", "notebooks")
 
 
 def _cell_text(notebook, cell):
-    with open(os.path.join(NOTEBOOKS, notebook)) as f:
+    with open(os.path.join(_notebooks(), notebook)) as f:
         nb = json.load(f)
     out = []
     for o in nb["cells"][cell].get("outputs", []):

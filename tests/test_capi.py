@@ -151,3 +151,33 @@ def test_face7_host_calls(lib, pkg):
     f32 = lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1)
     cfg.options = L.OPT_NO_FACES
     assert lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1) == f32
+
+
+def test_serve_config_and_validation_without_gpu(lib, pkg):
+    """hfm_serve_*: the default configuration and the host-side checks that run before any
+    device allocation."""
+    L = pkg._lib
+    c = L.HfmServeConfig()
+    lib.hfm_serve_config_default(C.byref(c))
+    assert list(c.edges[:c.n_edges]) == [32, 48, 64, 96, 128]
+    assert c.slots == 64 and c.budget_bytes == 120e9 and c.cycles_per_tick == 4
+    assert c.solver.accel == L.ACCEL_IR and c.solver.storage == L.BF16
+    assert c.solver.tol == 1e-6 and c.solver.inner_tol == 1e-3 and c.solver.max_cycles == 600
+    h = C.c_void_p()
+    bad = L.HfmServeConfig.from_buffer_copy(c)
+    bad.n_edges = 0
+    assert lib.hfm_serve_create(C.byref(bad), C.byref(h)) == L.ERR_BAD_ARG
+    bad = L.HfmServeConfig.from_buffer_copy(c)
+    bad.edges[1] = 32
+    assert lib.hfm_serve_create(C.byref(bad), C.byref(h)) == L.ERR_BAD_ARG
+    assert b"repeated" in lib.hfm_last_error()
+    bad = L.HfmServeConfig.from_buffer_copy(c)
+    bad.solver.accel = L.ACCEL_CG
+    assert lib.hfm_serve_create(C.byref(bad), C.byref(h)) == L.ERR_UNSUPPORTED
+    bad = L.HfmServeConfig.from_buffer_copy(c)
+    bad.budget_bytes = 1e6  # less than one 128^3 slot
+    assert lib.hfm_serve_create(C.byref(bad), C.byref(h)) == L.ERR_OOM
+    n = C.c_int()
+    assert lib.hfm_serve_poll(None, None, 0, C.byref(n)) == L.ERR_BAD_ARG
+    assert lib.hfm_serve_cancel(None, 0) == L.ERR_BAD_ARG
+    assert lib.hfm_status_string(L.ERR_CANCELLED) == b"HFM_ERR_CANCELLED"

@@ -61,3 +61,52 @@ def test_budget_limits_slots_and_queues(hfm, S):
     assert all(r.status == 0 for r in res)
     # with two slots, later requests waited: admission time after arrival
     assert max(r.admitted - reqs[r.rid].arrival for r in res) > 0
+
+
+def test_native_server_same_bits_as_python_server(hfm, S):
+    """The C-ABI serving loop (hfm_serve_*) over the same buckets gives every request the
+    Python server's float64 solution bit for bit, and reaches the tolerance."""
+    sv, torch = S
+    edges = (16, 32)
+    reqs = sv.make_stream(count=10, rate=1e6, edges=edges, log_std=(0.5, 2.0), seed=21)
+    py = sv.SolveServer(edges=edges, slots=4, keep_solutions=True, cycles_per_tick=4)
+    try:
+        ref = {r.rid: r for r in py.serve(reqs, realtime=False)}
+    finally:
+        py.close()
+    nat = sv.NativeServer(cfg=py.cfg, edges=edges, slots=4, cycles_per_tick=4)
+    try:
+        assert nat.bucket_slots(16) == 4 and nat.bucket_slots(32) == 4
+        done, tickets = nat.serve(reqs)
+        assert nat.pending() == (0, 0)
+    finally:
+        nat.close()
+    for req, t in zip(reqs, tickets):
+        d = done[t]
+        assert d["status"] == 0, d
+        assert (d["cycles"], d["outer"]) == (ref[req.rid].cycles, ref[req.rid].outer)
+        np.testing.assert_array_equal(d["x"].cpu().numpy(), ref[req.rid].phi.cpu().numpy())
+        assert _check_true_residual(req, d["x"], 1e-6) < 1e-6
+
+
+def test_native_server_cancel(hfm, S):
+    """A queued and a running request cancelled through hfm_serve_cancel are reported as
+    HFM_ERR_CANCELLED; the others finish; a finished ticket cannot be cancelled."""
+    sv, torch = S
+    L = hfm._lib
+    reqs = sv.make_stream(count=4, rate=1e6, edges=(32,), log_std=(1.0, 1.0), seed=23)
+    nat = sv.NativeServer(edges=(32,), slots=2, cycles_per_tick=2)
+    try:
+        t = [nat.submit(r) for r in reqs]
+        done = {d["ticket"]: d for d in nat.poll()}   # admits two, launches
+        nat.cancel(t[3])                              # still queued
+        nat.cancel(t[0])                              # running
+        while len(done) < 4:
+            for d in nat.poll():
+                done[d["ticket"]] = d
+        with pytest.raises(L.HfmError):
+            nat.cancel(t[1])
+    finally:
+        nat.close()
+    assert done[t[0]]["status"] == L.ERR_CANCELLED and done[t[3]]["status"] == L.ERR_CANCELLED
+    assert done[t[1]]["status"] == 0 and done[t[2]]["status"] == 0
