@@ -357,6 +357,80 @@ __global__ void k_residual64(DevOp op, const double *__restrict__ x, const doubl
   HFM_END_ITEMS
 }
 
+// The same float64 outer residual for SIGMA7 with X % 4 == 0: a thread takes four
+// consecutive cells of a row (one index computation, 32-byte loads of x64 / b64 and 16-byte
+// loads of the conductivities), rows of a slot indexed in 32 bits (n < 2^31).
+template <class T>
+__global__ void k_residual64_sigma4(DevOp op, const double *__restrict__ x,
+                                    const double *__restrict__ b, float *__restrict__ rout,
+                                    T *__restrict__ rstore, int Z, int Y, int X, Items it,
+                                    const int *__restrict__ mask, double *__restrict__ partials) {
+  HFM_FOR_ITEMS(it, mask[slot])
+  const double *xi = x + base;
+  const float *sx = (const float *)op.coef[0] + (int64_t)slot * op.coef_stride;
+  const float *sy = (const float *)op.coef[1] + (int64_t)slot * op.coef_stride;
+  const float *sz = (const float *)op.coef[2] + (int64_t)slot * op.coef_stride;
+  const double sc = op.scale;
+  const double cz = op.c[0] * sc, cy = op.c[1] * sc, cx = op.c[2] * sc;
+  const int PL = X * Y;
+  double acc = 0.0;
+  for (int64_t i64 = lo + 4 * threadIdx.x; i64 < hi; i64 += 4 * blockDim.x) {
+    const int i = (int)i64;
+    const int row = i / X, xx = i - row * X;
+    const int yy = row % Y, zz = row / Y;
+    auto ld4d = [](const double *p, double (&v)[4]) {
+      const double2 a = *reinterpret_cast<const double2 *>(p), c = *reinterpret_cast<const double2 *>(p + 2);
+      v[0] = a.x; v[1] = a.y; v[2] = c.x; v[3] = c.y;
+    };
+    auto ld4f = [](const float *p, double (&v)[4]) {
+      const float4 a = *reinterpret_cast<const float4 *>(p);
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    };
+    double pc[4], pym[4] = {0, 0, 0, 0}, pyp[4] = {0, 0, 0, 0}, pzm[4] = {0, 0, 0, 0}, pzp[4] = {0, 0, 0, 0};
+    double vx[4], vy[4], vz[4], sym[4], syp[4], szm[4], szp[4];
+    ld4d(xi + i, pc);
+    ld4f(sx + i, vx);
+    ld4f(sy + i, vy);
+    ld4f(sz + i, vz);
+    const bool ylo = yy > 0, yhi = yy < Y - 1, zlo = zz > 0, zhi = zz < Z - 1;
+    if (ylo) ld4d(xi + i - X, pym);
+    if (yhi) ld4d(xi + i + X, pyp);
+    if (zlo) ld4d(xi + i - PL, pzm);
+    if (zhi) ld4d(xi + i + PL, pzp);
+    ld4f(ylo ? sy + i - X : sy + i, sym);
+    ld4f(yhi ? sy + i + X : sy + i, syp);
+    ld4f(zlo ? sz + i - PL : sz + i, szm);
+    ld4f(zhi ? sz + i + PL : sz + i, szp);
+    const double pl = xx > 0 ? xi[i - 1] : 0.0, pr = xx + 4 < X ? xi[i + 4] : 0.0;
+    const double sl = xx > 0 ? (double)sx[i - 1] : 0.0, sr = xx + 4 < X ? (double)sx[i + 4] : 0.0;
+    double bb[4];
+    ld4d(b + base + i, bb);
+    float rr[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int xe = xx + e;
+      const double vxl = e == 0 ? sl : vx[e - 1], vxr = e == 3 ? sr : vx[e + 1];
+      const double axm = cx * (xe > 0 ? 0.5 * (vx[e] + vxl) : vx[e]);
+      const double axp = cx * (xe < X - 1 ? 0.5 * (vx[e] + vxr) : vx[e]);
+      const double aym = cy * (ylo ? 0.5 * (vy[e] + sym[e]) : vy[e]);
+      const double ayp = cy * (yhi ? 0.5 * (vy[e] + syp[e]) : vy[e]);
+      const double azm = cz * (zlo ? 0.5 * (vz[e] + szm[e]) : vz[e]);
+      const double azp = cz * (zhi ? 0.5 * (vz[e] + szp[e]) : vz[e]);
+      const double xl = e == 0 ? pl : pc[e - 1], xr = e == 3 ? pr : pc[e + 1];
+      const double ax = axm * (pc[e] - xl) + axp * (pc[e] - xr) + aym * (pc[e] - pym[e]) +
+                        ayp * (pc[e] - pyp[e]) + azm * (pc[e] - pzm[e]) + azp * (pc[e] - pzp[e]);
+      const double r = bb[e] - ax;
+      rr[e] = (float)r;
+      acc += r * r;
+    }
+    *reinterpret_cast<float4 *>(rout + base + i) = make_float4(rr[0], rr[1], rr[2], rr[3]);
+    if (rstore) st4v<T>(rstore + base + i, make_float4(rr[0], rr[1], rr[2], rr[3]));
+  }
+  const double t = block_reduce_sum(acc);
+  if (threadIdx.x == 0) partials[(int64_t)slot * it.CH + ch] = t;
+  HFM_END_ITEMS
+}
+
 template <class T>
 __global__ void k_fetch(const T *__restrict__ b0, const T *__restrict__ b1,
                         const float *__restrict__ bx, int64_t n, const SlotState *st,
@@ -1155,8 +1229,14 @@ class Engine : public EngineBase {
     HFM_CHECK_LAUNCH("k_ir_update");
     DevOp d = fine32_;
     T *rs = fused_rhs() ? rhs(0) : nullptr;
+    const bool vec4 = (g(0).X % 4) == 0 && nf < ((int64_t)1 << 31);
     switch (kind()) {
       case HFM_OP_SIGMA7:
+        if (vec4) {
+          k_residual64_sigma4<T><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], rs, g(0).Z,
+                                                    g(0).Y, g(0).X, it, m_->outer, m_->partials);
+          break;
+        }
         k_residual64<HFM_OP_SIGMA7, T><<<ib, 256, 0, s>>>(d, m_->x64, m_->b64, m_->cg[1], rs, g(0).Z,
                                                            g(0).Y, g(0).X, it, m_->outer, m_->partials);
         break;

@@ -5,7 +5,10 @@
 
 Kernels: ``smooth`` (one weighted-Jacobi sweep), ``resid`` (A phi - b), ``restrict`` (fused
 residual + restriction), ``correct`` (fused prolongation + correction + sweep), ``apply27``
-(27-point conv), ``transfer-r`` / ``transfer-p`` (standalone restriction / prolongation).
+(27-point conv), ``transfer-r`` / ``transfer-p`` (standalone restriction / prolongation),
+``ns-step`` (time steps of the obstacle flow at --shape, default 64,128,128: 24 boxes, 7-point
+diffusion, F-cycle pressure solve to 1e-5; --reps steps in one timed region, the target of a
+launch list).
 Forms: ``sigma7`` (per-cell conductivities), ``face7`` (stored faces; 16-bit storage),
 ``const7``, ``k27``.  ``--dtype`` selects the storage of fields and coefficients (the typed
 entry points for bf16 / f16).  Prints one JSON line with the time per launch, the
@@ -38,6 +41,8 @@ def main():
     import __graft_entry__ as ge
     hfm = ge.load_package()
     ops, W, L = hfm.ops, hfm.weights, hfm._lib
+    if a.kernel == "ns-step":
+        return ns_step(hfm, torch, a)
     Z, Y, X = (tuple(int(v) for v in a.shape.split(",")) if a.shape else (a.n, a.n, a.n))
     B = a.batch
     n = Z * Y * X
@@ -138,6 +143,30 @@ def main():
                       "ms_per_launch": ms, "bytes_per_launch": nbytes,
                       "bytes_per_cell": nbytes / (B * n),
                       "gbs": nbytes / (ms / 1e3) / 1e9 if ms > 0 else None}))
+
+
+def ns_step(hfm, torch, a):
+    """Time steps of the obstacle flow (the obstacle-flow configuration's settings)."""
+    ns = hfm.ns
+    shape = tuple(int(v) for v in a.shape.split(",")) if a.shape else (64, 128, 128)
+    cfg = ns.NSConfig(dt=0.5, dx=1.0, Re=0.05, ub=1.0, diffusion="7", pressure="fcycle", p_tol=1e-5)
+    sig = ns.obstacle_mask(shape, n_boxes=24, footprint=(4, 16), height=(8, 40), sigma=1e5, seed=0)
+    st = ns.NSStepper(shape, cfg, sigma=sig)
+    try:
+        for _ in range(a.warmup):
+            st.step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.reps):
+            st.step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.reps
+        print(json.dumps({"kernel": "ns-step", "shape": list(shape), "ms_per_step": ms,
+                          "pressure_cycles": st.p_cycles[-a.reps:]}))
+    finally:
+        st.close()
 
 
 if __name__ == "__main__":
