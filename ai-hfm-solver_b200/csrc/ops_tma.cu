@@ -27,6 +27,7 @@
 
 #include <atomic>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "hfm_internal.cuh"

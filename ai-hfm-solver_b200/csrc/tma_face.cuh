@@ -176,6 +176,46 @@ __device__ __forceinline__ float face_cell_coarse(const uint32_t (&cv)[2], uint3
   return s;
 }
 
+// S and D of the thread's 8 cells with float32 neighbour values (the faces converted): the
+// fused first two sweeps in fp16 storage, where omega f / diag can exceed the fp16 range (a
+// residual spike, normalised to O(sqrt(n)), over a small diagonal) and is kept in float32 as
+// the conductivity-form kernel keeps it.
+template <class T>
+__device__ __forceinline__ void face_cells_f32(const float (&c)[8], float xl, float xr,
+                                               const float (&ym)[8], const float (&yp)[8],
+                                               const float (&zm)[8], const float (&zp)[8],
+                                               const uint32_t (&fx)[4], uint32_t fx8,
+                                               const uint32_t (&fyl)[4], const uint32_t (&fyh)[4],
+                                               const uint32_t (&fzl)[4], const uint32_t (&fzh)[4],
+                                               float (&S)[8], float (&D)[8]) {
+  float Fx[9], Fyl[8], Fyh[8], Fzl[8], Fzh[8];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float2 v = cvt2<T>(fx[k]);
+    Fx[2 * k] = v.x; Fx[2 * k + 1] = v.y;
+    v = cvt2<T>(fyl[k]);
+    Fyl[2 * k] = v.x; Fyl[2 * k + 1] = v.y;
+    v = cvt2<T>(fyh[k]);
+    Fyh[2 * k] = v.x; Fyh[2 * k + 1] = v.y;
+    v = cvt2<T>(fzl[k]);
+    Fzl[2 * k] = v.x; Fzl[2 * k + 1] = v.y;
+    v = cvt2<T>(fzh[k]);
+    Fzh[2 * k] = v.x; Fzh[2 * k + 1] = v.y;
+  }
+  Fx[8] = cvt2<T>(fx8).x;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    float s = Fx[e] * (e == 0 ? xl : c[e - 1]);
+    s = fmaf(Fx[e + 1], e == 7 ? xr : c[e + 1], s);
+    s = fmaf(Fyl[e], ym[e], s);
+    s = fmaf(Fyh[e], yp[e], s);
+    s = fmaf(Fzl[e], zm[e], s);
+    s = fmaf(Fzh[e], zp[e], s);
+    S[e] = s;
+    D[e] = ((((Fx[e] + Fx[e + 1]) + Fyl[e]) + Fyh[e]) + Fzl[e]) + Fzh[e];
+  }
+}
+
 template <class T, int MODE, int CORR>
 __global__ void __launch_bounds__(GeoF<false, false>::THREADS, GeoF<false, false>::MINB)
     k_tma_face(const __grid_constant__ TmaArgs<T> a) {
@@ -231,9 +271,10 @@ __global__ void __launch_bounds__(GeoF<false, false>::THREADS, GeoF<false, false
   auto phi_row = [&](const char *st, int ry, uint32_t (&w)[4]) {
     ld8w(st + G::O_PHI + (ry * G::PW + G::HX + V * c) * 2, w);
   };
-  // PRE2: g = f * (1 / diag) of a tile row, rounded to the storage type (the first sweep's
-  // phi1 = omega g, stored as the separate two-sweep form would store it); lo / hi: the
-  // single neighbours left and right of the row's 8 values
+  // PRE2: g = f * (1 / diag) of a tile row; bf16 rounds it to the storage type (the first
+  // sweep's phi1 = omega g, stored as the separate two-sweep form would store it), fp16 keeps
+  // it in float32 (pre_rowf: omega f / diag can exceed the fp16 range); pre_one / pre_onef:
+  // the single neighbours left and right of the row's 8 values
   auto pre_row = [&](const char *st, int ry, uint32_t (&w)[4]) {
     uint32_t f[4], d[4];
     ld8w(st + G::O_PHI + (ry * G::PW + G::HX + V * c) * 2, f);
@@ -241,6 +282,21 @@ __global__ void __launch_bounds__(GeoF<false, false>::THREADS, GeoF<false, false
 #pragma unroll
     for (int k = 0; k < 4; ++k)
       w[k] = pack2<T>(M::template fma<0, 0>(f[k], d[k], 0.f), M::template fma<1, 1>(f[k], d[k], 0.f));
+  };
+  auto pre_rowf = [&](const char *st, int ry, float (&g)[8]) {
+    uint32_t f[4], d[4];
+    ld8w(st + G::O_PHI + (ry * G::PW + G::HX + V * c) * 2, f);
+    ld8w(st + G::O_DS + (ry * G::PW + G::HX + V * c) * 2, d);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 fv = cvt2<T>(f[k]), dv = cvt2<T>(d[k]);
+      g[2 * k] = fv.x * dv.x;
+      g[2 * k + 1] = fv.y * dv.y;
+    }
+  };
+  auto pre_onef = [&](const char *st, int ry, int col) -> float {
+    return cvt2<T>(ld1w(st + G::O_PHI + (ry * G::PW + col) * 2)).x *
+           cvt2<T>(ld1w(st + G::O_DS + (ry * G::PW + col) * 2)).x;
   };
   auto pre_one = [&](const char *st, int ry, int col) -> uint32_t {
     const uint32_t f = ld1w(st + G::O_PHI + (ry * G::PW + col) * 2);
@@ -274,8 +330,21 @@ __global__ void __launch_bounds__(GeoF<false, false>::THREADS, GeoF<false, false
     const char *sp = stage_of(z + 1);
 
     // neighbours (phi, or g for PRE2), faces, right-hand side
+    constexpr bool PRE2F = PRE2 && std::is_same<T, __half>::value;  // fp16: g in float32
     uint32_t pc[4], pym[4], pyp[4], pzm[4], pzp[4], pl, pr;
-    if (PRE2) {
+    float gc[8], gym[8], gyp[8], gzm[8], gzp[8], gl = 0.f, gr = 0.f;
+    if (PRE2F) {
+      pre_rowf(sc, r + 1, gc);
+      pre_rowf(sc, r, gym);
+      pre_rowf(sc, r + 2, gyp);
+      pre_rowf(sm_, r + 1, gzm);
+      pre_rowf(sp, r + 1, gzp);
+      gl = pre_onef(sc, r + 1, G::HX + V * c - 1);
+      gr = pre_onef(sc, r + 1, G::HX + V * c + V);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) pc[k] = pym[k] = pyp[k] = pzm[k] = pzp[k] = 0u;
+      pl = pr = 0u;
+    } else if (PRE2) {
       pre_row(sc, r + 1, pc);
       pre_row(sc, r, pym);
       pre_row(sc, r + 2, pyp);
@@ -310,20 +379,26 @@ __global__ void __launch_bounds__(GeoF<false, false>::THREADS, GeoF<false, false
       fr[0] = fr[1] = fr[2] = fr[3] = 0u;
 
     float S[8], D[8];
-    face_cell<T, 0>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
-    face_cell<T, 1>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
-    face_cell<T, 2>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
-    face_cell<T, 3>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
-    face_cell<T, 4>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
-    face_cell<T, 5>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
-    face_cell<T, 6>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
-    face_cell<T, 7>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
     float pcf[8];  // the centre values in float32
+    if (PRE2F) {
+      face_cells_f32<T>(gc, gl, gr, gym, gyp, gzm, gzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const float2 v = cvt2<T>(pc[k]);
-      pcf[2 * k] = v.x;
-      pcf[2 * k + 1] = v.y;
+      for (int e = 0; e < 8; ++e) pcf[e] = gc[e];
+    } else {
+      face_cell<T, 0>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
+      face_cell<T, 1>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
+      face_cell<T, 2>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
+      face_cell<T, 3>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
+      face_cell<T, 4>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
+      face_cell<T, 5>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
+      face_cell<T, 6>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
+      face_cell<T, 7>(pc, pl, pr, pym, pyp, pzm, pzp, fx, fx8, fyl, fyh, fzl, fzh, S, D);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float2 v = cvt2<T>(pc[k]);
+        pcf[2 * k] = v.x;
+        pcf[2 * k + 1] = v.y;
+      }
     }
     if (PRE2) {  // phi1 = omega g: the products above are omega-free
 #pragma unroll

@@ -61,7 +61,10 @@ def test_vcycles_match_separate_launches_and_oracle(hfm, T, n):
 def test_solves_match_separate_launches(hfm, T, storage, n):
     """PCG (float32) or float64 refinement (16-bit) with the persistent small end on 8 slots -
     at 32^3 the whole preconditioner V-cycle is one persistent launch, its last sweep summing
-    r . z - reaches 1e-6 in the separate launches' iteration counts (within 2)."""
+    r . z - reaches 1e-6 in the separate launches' iteration counts: within 2 in float32;
+    with 16-bit inner cycles within 20 %, since the persistent kernel keeps the first
+    sweep's iterate in float32 where the separate launches store it in the storage type,
+    and the inner CG's counts move with such roundings."""
     M, L = hfm.multigrid, hfm._lib
     B = 8
     sig, f = _problems(hfm, n, B, 50, log_std=1.5)
@@ -86,7 +89,9 @@ def test_solves_match_separate_launches(hfm, T, storage, n):
         assert st["status"] == 0, (s, st)
         op64 = mg.Sigma7(sig[0, s], sig[1, s], sig[2, s], dtype=np.float64)
         assert mg.rel_residual(op64, x, f[s]) < 1.5e-6
-        assert abs(st["cycles"] - res[False][1][s]["cycles"]) <= 2, (st, res[False][1][s])
+        c1, c0 = st["cycles"], res[False][1][s]["cycles"]
+        band = 2 if storage == "f32" else max(2, 0.2 * c0)
+        assert abs(c1 - c0) <= band, (s, st, res[False][1][s])
 
 
 def test_expired_dependency_waits_end_slots_with_timeout(hfm, T):
