@@ -60,6 +60,12 @@ def parse():
     p.add_argument("--rate", type=float, default=2000.0)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--nu", type=int, default=2,
+                   help="smoothing sweeps before and after the coarse correction, V(nu, nu)")
+    p.add_argument("--no-faces", action="store_true",
+                   help="16-bit cycles keep the conductivity form on the plane-marching levels")
+    p.add_argument("--no-persistent", action="store_true",
+                   help="the small end of the V-cycle as separate launches")
     p.add_argument("--quick", action="store_true",
                    help="served leg only (no plain / e2e / roofline / CPU legs), for profiling")
     return p.parse_args()
@@ -423,7 +429,8 @@ def run_serve(args, pkg, torch, rank, world, local):
     # with fewer iterations than one tight inner solve (measured over inner tolerances 1e-6 ..
     # 1e-1 on this stream); the plain path uses the same setting
     cfg = M.SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6, max_cycles=600,
-                         inner_tol=1e-3)
+                         inner_tol=1e-3, nu_pre=args.nu, nu_post=args.nu,
+                         faces=not args.no_faces, persistent=not args.no_persistent)
     server = sv.SolveServer(cfg=cfg, slots=64, budget_bytes=120e9, cycles_per_tick=4)
 
     def barrier():
@@ -460,7 +467,9 @@ def run_serve(args, pkg, torch, rank, world, local):
         return {"metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
                 "p50_ms": round(lat["p50_ms"], 3), "p99_ms": round(lat["p99_ms"], 3),
-                "failed": len(bad), "gpu_launches": int(launches), "quick": True}
+                "failed": len(bad), "gpu_launches": int(launches), "quick": True,
+                "nu": args.nu, "faces": cfg.faces, "persistent": cfg.persistent,
+                "iterations_mean": round(float(np.mean([r.cycles for r in all_res])), 2)}
     # service latency at an offered load below the throughput (the same requests, Poisson
     # arrivals at 500 req/s): queueing no longer dominates p50 / p99
     low = server.serve(sv.with_rate(reqs, 500.0, seed=rank), realtime=True)
@@ -486,7 +495,7 @@ def run_serve(args, pkg, torch, rank, world, local):
 
     # plain path: one request at a time, float32 storage, bounded sample of the same stream
     pcfg = M.SolverConfig(cycle="V", accel="ir", storage="f32", tol=1e-6, max_cycles=600,
-                          inner_tol=1e-3)
+                          inner_tol=1e-3, nu_pre=args.nu, nu_post=args.nu)
     sv.solve_one_at_a_time(reqs[:10], cfg=pcfg)  # warm-up (graph capture per edge)
     plain, pdt = sv.solve_one_at_a_time(reqs, cfg=pcfg, time_budget_s=8.0)
     plain_sps = len(plain) / pdt
