@@ -225,6 +225,11 @@ int launch_restrict(const T *fine, int64_t f_stride, T *coarse, int64_t c_stride
 template <class T>
 int launch_prolong(const T *coarse, int64_t c_stride, T *fine, int64_t f_stride, int B,
                    Grid3 gc, const int *active, cudaStream_t s);
+// Three same-shape arrays (the conductivities) restricted by one launch where the vector
+// kernel applies.
+template <class T>
+int launch_restrict3(const T *const fine[3], int64_t f_stride, T *const coarse[3], int64_t c_stride,
+                     int B, Grid3 g, cudaStream_t s);
 // Jacobi sweeps on a small grid held in shared memory, one block per instance.
 template <class T>
 int launch_coarse_jacobi(int kind, const DevOp &op, const T *rhs, int64_t rhs_stride,

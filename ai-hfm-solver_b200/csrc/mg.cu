@@ -514,15 +514,61 @@ __global__ void k_log_mean(const void *sx, const void *sy, const void *sz, int d
   }
 }
 
+// Admission of a slot's conductivities in one launch: blockIdx.y picks sx / sy / sz; each
+// cell is stored in the storage type (divided by the slot's geometric mean when gscale is
+// given) and, where the handle keeps one, as a float32 copy for the float32 operator.
+template <class T> struct Admit3 {
+  const void *src[3];
+  T *dst[3];
+  float *dst32[3];
+};
 template <class T>
-__global__ void k_convert_scaled(const void *__restrict__ src, int dt, T *__restrict__ dst,
-                                 int64_t n, int count, int slot0, const double *gscale) {
+__global__ void k_admit_convert(Admit3<T> a, int dt, int64_t n, int count, int slot0,
+                                const double *gscale) {
+  const void *src = a.src[blockIdx.y];
+  T *dst = a.dst[blockIdx.y];
+  float *d32 = a.dst32[blockIdx.y];
   const int64_t tot = n * count;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < tot;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const double g = gscale[slot0 + i / n];
     const double v = dt == HFM_F64 ? ((const double *)src)[i] : (double)((const float *)src)[i];
-    dst[i] = St<T>::from((float)(v / g));
+    dst[i] = St<T>::from(gscale ? (float)(v / gscale[slot0 + i / n]) : (float)v);
+    if (d32) d32[i] = (float)v;
+  }
+}
+
+// 1 / diagonal of every SIGMA7 level of the slots [slot0, slot0 + gridDim.y) in one launch:
+// the blocks of blockIdx.x are split over the levels by the prefix sums in first[]; indices
+// inside one instance are 32-bit (an instance has fewer than 2^31 cells).
+struct InvdLevels {
+  const void *sx[kMaxLevels], *sy[kMaxLevels], *sz[kMaxLevels];
+  void *out[kMaxLevels];
+  float cz[kMaxLevels], cy[kMaxLevels], cx[kMaxLevels];
+  int Z[kMaxLevels], Y[kMaxLevels], X[kMaxLevels];
+  int first[kMaxLevels + 1];
+  int L;
+};
+template <class T>
+__global__ void __launch_bounds__(256) k_invdiag_levels(const InvdLevels d, int slot0) {
+  int l = 0;
+  while (l + 1 < d.L && (int)blockIdx.x >= d.first[l + 1]) ++l;
+  const int Z = d.Z[l], Y = d.Y[l], X = d.X[l], P = X * Y, n = P * Z;
+  const int64_t o = (int64_t)(slot0 + blockIdx.y) * n;
+  const T *sx = (const T *)d.sx[l] + o, *sy = (const T *)d.sy[l] + o, *sz = (const T *)d.sz[l] + o;
+  T *out = (T *)d.out[l] + o;
+  const float cz = d.cz[l], cy = d.cy[l], cx = d.cx[l];
+  const float hz = 0.5f * cz, hy = 0.5f * cy, hx = 0.5f * cx;
+  const int nb = d.first[l + 1] - d.first[l];
+  for (int i = ((int)blockIdx.x - d.first[l]) * 256 + (int)threadIdx.x; i < n; i += nb * 256) {
+    const int x = i % X, t = i / X, y = t % Y, z = t / Y;
+    const float vx = St<T>::to(sx[i]), vy = St<T>::to(sy[i]), vz = St<T>::to(sz[i]);
+    const float axm = x > 0 ? hx * (vx + St<T>::to(sx[i - 1])) : cx * vx;
+    const float axp = x < X - 1 ? hx * (vx + St<T>::to(sx[i + 1])) : cx * vx;
+    const float aym = y > 0 ? hy * (vy + St<T>::to(sy[i - X])) : cy * vy;
+    const float ayp = y < Y - 1 ? hy * (vy + St<T>::to(sy[i + X])) : cy * vy;
+    const float azm = z > 0 ? hz * (vz + St<T>::to(sz[i - P])) : cz * vz;
+    const float azp = z < Z - 1 ? hz * (vz + St<T>::to(sz[i + P])) : cz * vz;
+    out[i] = St<T>::from(1.f / (((axm + axp) + (aym + ayp)) + (azm + azp)));
   }
 }
 
@@ -581,32 +627,6 @@ __global__ void k_fetch_all(const T *__restrict__ b0, const T *__restrict__ b1,
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     out[o + i] = bx ? bx[o + i] : St<T>::to(which ? b1[o + i] : b0[o + i]);
-}
-
-// 1 / diagonal of a SIGMA7 level (faces c_d (s_i + s_j) / 2, wall faces c_d s_i), for cells
-// [0, total) of consecutive instances of n = Z Y X cells each.
-template <class T>
-__global__ void k_invdiag(const T *__restrict__ sx, const T *__restrict__ sy,
-                          const T *__restrict__ sz, float cz, float cy, float cx, int Z, int Y,
-                          int X, int64_t total, T *__restrict__ out) {
-  const int64_t n = (int64_t)Z * Y * X;
-  const float hz = 0.5f * cz, hy = 0.5f * cy, hx = 0.5f * cx;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = k % n;
-    const int x = (int)(i % X);
-    const int64_t t = i / X;
-    const int y = (int)(t % Y), z = (int)(t / Y);
-    const float vx = St<T>::to(sx[k]), vy = St<T>::to(sy[k]), vz = St<T>::to(sz[k]);
-    const float axm = x > 0 ? hx * (vx + St<T>::to(sx[k - 1])) : cx * vx;
-    const float axp = x < X - 1 ? hx * (vx + St<T>::to(sx[k + 1])) : cx * vx;
-    const float aym = y > 0 ? hy * (vy + St<T>::to(sy[k - X])) : cy * vy;
-    const float ayp = y < Y - 1 ? hy * (vy + St<T>::to(sy[k + X])) : cy * vy;
-    const int64_t P = (int64_t)X * Y;
-    const float azm = z > 0 ? hz * (vz + St<T>::to(sz[k - P])) : cz * vz;
-    const float azp = z < Z - 1 ? hz * (vz + St<T>::to(sz[k + P])) : cz * vz;
-    out[k] = St<T>::from(1.f / (((axm + axp) + (aym + ayp)) + (azm + azp)));
-  }
 }
 
 // ----------------------------------------------------------------- CG vector kernels
@@ -1007,7 +1027,7 @@ class Engine : public EngineBase {
   // the fused coarse cycle directly below it.
   bool small_ok(int l) {
     const hfm_mg_config &c = m_->cfg;
-    if ((c.options & HFM_OPT_NO_PERSISTENT) || fused_l0_ < 0 || l + 1 != fused_l0_) return false;
+    if (!(c.options & HFM_OPT_PERSISTENT) || fused_l0_ < 0 || l + 1 != fused_l0_) return false;
     if (lk(l) == HFM_OP_FACE7) return false;
     if (tma_eligible(lk(l), g(l), FAST_SMOOTH, nullptr, 0, (int)sizeof(T))) return false;
     if ((g(l).Z | g(l).Y | g(l).X) & 1) return false;
@@ -1372,25 +1392,25 @@ class Engine : public EngineBase {
                                      m_->gscale);
       HFM_CHECK_LAUNCH("k_log_mean");
     }
-    for (int a = 0; a < 3; ++a) {
-      int st = HFM_OK;
-      if (normalize) {
-        k_convert_scaled<T><<<vec_blocks(n(0) * cnt, 1), 256, 0, s>>>(
-            op.coef[a], op.coef_dtype, (T *)m_->lv[0].coef[a] + lo * n(0), n(0), cnt, lo, m_->gscale);
-        HFM_CHECK_LAUNCH("k_convert_scaled");
-      } else {
-        st = launch_convert<T>(op.coef[a], op.coef_dtype, (T *)m_->lv[0].coef[a] + lo * n(0),
-                               n(0) * cnt, s);
+    {
+      Admit3<T> ad;
+      for (int a = 0; a < 3; ++a) {
+        ad.src[a] = op.coef[a];
+        ad.dst[a] = (T *)m_->lv[0].coef[a] + lo * n(0);
+        ad.dst32[a] = fine32_coef_[a] ? fine32_coef_[a] + lo * n(0) : nullptr;
       }
-      if (st) return st;
-      if (fine32_coef_[a] && (st = launch_convert<float>(op.coef[a], op.coef_dtype,
-                                                         fine32_coef_[a] + lo * n(0), n(0) * cnt, s)))
-        return st;
-      for (int l = 1; l < m_->L; ++l) {
-        st = launch_restrict<T>((T *)m_->lv[l - 1].coef[a] + lo * n(l - 1), n(l - 1),
-                                (T *)m_->lv[l].coef[a] + lo * n(l), n(l), cnt, g(l - 1), nullptr, s);
-        if (st) return st;
+      k_admit_convert<T><<<dim3(vec_blocks(n(0) * cnt, 3), 3), 256, 0, s>>>(
+          ad, op.coef_dtype, n(0), cnt, lo, normalize ? m_->gscale : nullptr);
+      HFM_CHECK_LAUNCH("k_admit_convert");
+    }
+    for (int l = 1; l < m_->L; ++l) {
+      const T *f3[3];
+      T *c3[3];
+      for (int a = 0; a < 3; ++a) {
+        f3[a] = (const T *)m_->lv[l - 1].coef[a] + lo * n(l - 1);
+        c3[a] = (T *)m_->lv[l].coef[a] + lo * n(l);
       }
+      if (int st = launch_restrict3<T>(f3, n(l - 1), c3, n(l), cnt, g(l - 1), s)) return st;
     }
     float sc = 1.f;
     for (int l = 0; l < m_->L; ++l) {
@@ -1403,15 +1423,27 @@ class Engine : public EngineBase {
     fine32_ = m_->lv[0].op;
     if (fine32_coef_[0])
       for (int a = 0; a < 3; ++a) fine32_.coef[a] = fine32_coef_[a];
-    // 1 / diagonal per level, for the fused first two sweeps of a cycle
-    for (int l = 0; l < m_->L; ++l) {
-      const DevOp &op = m_->lv[l].op;
-      const int64_t nl = n(l);
-      k_invdiag<T><<<vec_blocks(nl * cnt, 1), 256, 0, s>>>(
-          (const T *)op.coef[0] + lo * nl, (const T *)op.coef[1] + lo * nl,
-          (const T *)op.coef[2] + lo * nl, op.c[0] * op.scale, op.c[1] * op.scale,
-          op.c[2] * op.scale, g(l).Z, g(l).Y, g(l).X, nl * cnt, (T *)m_->lv[l].invd + lo * nl);
-      HFM_CHECK_LAUNCH("k_invdiag");
+    // 1 / diagonal of every level, for the fused first two sweeps of a cycle
+    {
+      InvdLevels d;
+      d.L = m_->L;
+      d.first[0] = 0;
+      for (int l = 0; l < m_->L; ++l) {
+        const DevOp &o = m_->lv[l].op;
+        d.sx[l] = o.coef[0];
+        d.sy[l] = o.coef[1];
+        d.sz[l] = o.coef[2];
+        d.out[l] = m_->lv[l].invd;
+        d.cz[l] = o.c[0] * o.scale;
+        d.cy[l] = o.c[1] * o.scale;
+        d.cx[l] = o.c[2] * o.scale;
+        d.Z[l] = g(l).Z;
+        d.Y[l] = g(l).Y;
+        d.X[l] = g(l).X;
+        d.first[l + 1] = d.first[l] + (int)std::min<int64_t>((n(l) + 1023) / 1024, 1024);
+      }
+      k_invdiag_levels<T><<<dim3(d.first[m_->L], cnt), 256, 0, s>>>(d, lo);
+      HFM_CHECK_LAUNCH("k_invdiag_levels");
     }
     // FACE7 arrays of the levels that hold them: the fine level's faces from the caller's
     // float32 / float64 conductivities (divided by the slot's geometric mean for normalised
@@ -1675,6 +1707,8 @@ std::vector<Grid3> plan_levels(const hfm_mg_config &c, int Z, int Y, int X) {
 int validate_cfg(const hfm_mg_config &c, int Z, int Y, int X, int slots) {
   if (Z <= 0 || Y <= 0 || X <= 0 || slots <= 0 || slots > 65535)
     return fail(HFM_ERR_BAD_ARG, "hfm_mg_create: bad extents or slot count");
+  if ((int64_t)Z * Y * X >= ((int64_t)1 << 31))
+    return fail(HFM_ERR_UNSUPPORTED, "hfm_mg_create: an instance holds at most 2^31 - 1 cells");
   if (c.op_kind != HFM_OP_CONST7 && c.op_kind != HFM_OP_SIGMA7 && c.op_kind != HFM_OP_K27 &&
       c.op_kind != HFM_OP_DIR7)
     return fail(HFM_ERR_UNSUPPORTED, "hfm_mg_create: unknown operator kind");

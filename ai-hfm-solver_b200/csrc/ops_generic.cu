@@ -205,17 +205,13 @@ template <class T> struct Vec16 {
   }
 };
 
+// One instance's vector restriction, the block's share of the grid-stride loop.
 template <class T>
-__global__ void __launch_bounds__(kThreads)
-    k_restrict_v(const T *__restrict__ f, int64_t fs, T *__restrict__ c, int64_t cs, int Z, int Y,
-                 int X, const int *__restrict__ active) {
+__device__ __forceinline__ void restrict_v_instance(const T *__restrict__ fi, T *__restrict__ ci,
+                                                    int Z, int Y, int X) {
   constexpr int VEC = Vec16<T>::VEC, HC = Vec16<T>::HC;
-  const int64_t inst = blockIdx.y;
-  if (active && !active[inst]) return;
   const int Zc = Z >> 1, Yc = Y >> 1, Xc = X >> 1, Xv = Xc / HC;
   const int64_t nv = (int64_t)Zc * Yc * Xv;
-  const T *fi = f + inst * fs;
-  T *ci = c + inst * cs;
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nv;
        j += (int64_t)gridDim.x * blockDim.x) {
     const int xv = (int)(j % Xv);
@@ -242,6 +238,28 @@ __global__ void __launch_bounds__(kThreads)
     *reinterpret_cast<uint2 *>(ci + ((int64_t)zc * Yc + yc) * Xc + (int64_t)HC * xv) =
         *reinterpret_cast<const uint2 *>(out);
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_restrict_v(const T *__restrict__ f, int64_t fs, T *__restrict__ c, int64_t cs, int Z, int Y,
+                 int X, const int *__restrict__ active) {
+  const int64_t inst = blockIdx.y;
+  if (active && !active[inst]) return;
+  restrict_v_instance<T>(f + inst * fs, c + inst * cs, Z, Y, X);
+}
+
+// Three arrays of the same shape restricted in one launch (blockIdx.z picks the array): the
+// conductivity hierarchy of a slot.
+template <class T> struct Arr3 {
+  const T *f[3];
+  T *c[3];
+};
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_restrict3_v(Arr3<T> a, int64_t fs, int64_t cs, int Z, int Y, int X) {
+  const int64_t inst = blockIdx.y;
+  restrict_v_instance<T>(a.f[blockIdx.z] + inst * fs, a.c[blockIdx.z] + inst * cs, Z, Y, X);
 }
 
 template <class T>
@@ -459,6 +477,31 @@ int launch_restrict(const T *fine, int64_t f_stride, T *coarse, int64_t c_stride
 }
 
 template <class T>
+int launch_restrict3(const T *const fine[3], int64_t f_stride, T *const coarse[3], int64_t c_stride,
+                     int B, Grid3 g, cudaStream_t s) {
+  const int64_t nc = (int64_t)(g.Z / 2) * (g.Y / 2) * (g.X / 2);
+  if (nc == 0) return HFM_OK;
+  bool vec = true;
+  for (int a = 0; a < 3; ++a) vec = vec && transfer_vec_ok<T>(fine[a], f_stride, coarse[a], c_stride, g.X, B);
+  if (!vec) {
+    for (int a = 0; a < 3; ++a) {
+      int st = launch_restrict<T>(fine[a], f_stride, coarse[a], c_stride, B, g, nullptr, s);
+      if (st) return st;
+    }
+    return HFM_OK;
+  }
+  Arr3<T> arr;
+  for (int a = 0; a < 3; ++a) {
+    arr.f[a] = fine[a];
+    arr.c[a] = coarse[a];
+  }
+  dim3 grid(blocks_for(nc / Vec16<T>::HC, B * 3), B, 3);
+  k_restrict3_v<T><<<grid, kThreads, 0, s>>>(arr, f_stride, c_stride, g.Z, g.Y, g.X);
+  HFM_CHECK_LAUNCH("k_restrict3_v");
+  return HFM_OK;
+}
+
+template <class T>
 int launch_prolong(const T *coarse, int64_t c_stride, T *fine, int64_t f_stride, int B,
                    Grid3 gc, const int *active, cudaStream_t s) {
   if (transfer_vec_ok<T>(fine, f_stride, coarse, c_stride, 2 * gc.X, B)) {
@@ -503,6 +546,8 @@ int launch_coarse_jacobi(int kind, const DevOp &op, const T *rhs, int64_t rhs_st
                                            int64_t, T *, int64_t, T *, int64_t, int, Grid3,  \
                                            unsigned, const int *, double *, int *,           \
                                            cudaStream_t);                                    \
+  template int launch_restrict3<T>(const T *const[3], int64_t, T *const[3], int64_t, int, Grid3,   \
+                                   cudaStream_t);                                           \
   template int launch_restrict<T>(const T *, int64_t, T *, int64_t, int, Grid3, const int *, \
                                   cudaStream_t);                                             \
   template int launch_prolong<T>(const T *, int64_t, T *, int64_t, int, Grid3, const int *,  \

@@ -64,8 +64,8 @@ def parse():
                    help="smoothing sweeps before and after the coarse correction, V(nu, nu)")
     p.add_argument("--no-faces", action="store_true",
                    help="16-bit cycles keep the conductivity form on the plane-marching levels")
-    p.add_argument("--no-persistent", action="store_true",
-                   help="the small end of the V-cycle as separate launches")
+    p.add_argument("--persistent", action="store_true",
+                   help="the small end of the V-cycle as one persistent kernel")
     p.add_argument("--quick", action="store_true",
                    help="served leg only (no plain / e2e / roofline / CPU legs), for profiling")
     return p.parse_args()
@@ -430,7 +430,7 @@ def run_serve(args, pkg, torch, rank, world, local):
     # 1e-1 on this stream); the plain path uses the same setting
     cfg = M.SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6, max_cycles=600,
                          inner_tol=1e-3, nu_pre=args.nu, nu_post=args.nu,
-                         faces=not args.no_faces, persistent=not args.no_persistent)
+                         faces=not args.no_faces, persistent=args.persistent)
     server = sv.SolveServer(cfg=cfg, slots=64, budget_bytes=120e9, cycles_per_tick=4)
 
     def barrier():

@@ -459,12 +459,14 @@ typedef struct {
  * faces from rounded conductivities) */
 #define HFM_OPT_NO_FACES 8
 /* options: run the small end of a V-cycle - the level above the fused coarse cycle when the
- * plane-marching TMA kernels do not take it (X < 48), and the fused coarse cycle - as
- * separate launches (by default one persistent kernel walks an (instance, step, tile) work
- * list of that level's sweeps, its residual + restriction, the coarse cycle of every
- * instance and the correction, with per-instance dependency counters; handles of at least
- * 8 slots, zero-guess V-cycles such as a CG preconditioner's) */
-#define HFM_OPT_NO_PERSISTENT 16
+ * plane-marching TMA kernels do not take it (X < 48), and the fused coarse cycle - as one
+ * persistent kernel that walks an (instance, step, tile) work list of that level's sweeps,
+ * its residual + restriction, the coarse cycle of every instance and the correction, with
+ * per-instance dependency counters (handles of at least 8 slots, zero-guess V-cycles such
+ * as a CG preconditioner's).  Off by default: the kernel holds every SM for a small amount
+ * of work, and handles that share the GPU (the buckets of a server) lose more than the
+ * launches it saves; by default the small end runs as separate launches. */
+#define HFM_OPT_PERSISTENT 16
 
 typedef struct {
   int active;       /* 1 while the slot is still iterating */

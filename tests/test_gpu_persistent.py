@@ -2,7 +2,7 @@
 plane-marching TMA kernels do not take it) and the coarse cycle itself, for every slot of a
 handle, in one launch that walks an (instance, step, tile) work list.
 
-Checked against the separate launches (HFM_OPT_NO_PERSISTENT) and the oracle: stationary
+Checked against the separate launches (without HFM_OPT_PERSISTENT) and the oracle: stationary
 V-cycles to the float32 evaluation error, solves to tolerance with the same iteration
 counts, and the bounded dependency waits: with a wait budget of zero every wait expires, the
 slots end with HFM_ERR_TIMEOUT, and the next handle solves normally.
@@ -103,7 +103,7 @@ def test_expired_dependency_waits_end_slots_with_timeout(hfm, T):
     sig, f = _problems(hfm, n, B, 60)
     op = hfm.ops.Sigma7(*(T.from_numpy(np.ascontiguousarray(sig[k])).cuda() for k in range(3)))
     fd = T.from_numpy(f).cuda()
-    cfg = M.SolverConfig(cycle="V", accel="cg", tol=1e-6, max_cycles=40)
+    cfg = M.SolverConfig(cycle="V", accel="cg", tol=1e-6, max_cycles=40, persistent=True)
     cnt, drain = C.c_int(0), C.c_int(0)
     L.call("hfm_device_timeouts", C.byref(cnt), 1)
     L.call("hfm_device_drain_timeouts", C.byref(drain), 1)
