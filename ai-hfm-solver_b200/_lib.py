@@ -22,7 +22,7 @@ FLAG_ZERO_XEND, FLAG_TOP_COPY, FLAG_ZERO_GUESS, FLAG_PERIODIC, FLAG_SAME_LEVEL_C
 CYCLE_SAWTOOTH, CYCLE_V, CYCLE_F = range(3)
 ACCEL_NONE, ACCEL_CG, ACCEL_IR = range(3)
 (OPT_NO_FUSED_COARSE, OPT_NO_FUSED_PRE, OPT_SAWTOOTH_COARSE_SWEEPS, OPT_NO_FACES,
- OPT_PERSISTENT) = 1, 2, 4, 8, 16
+ OPT_PERSISTENT, OPT_NO_TEMPORAL) = 1, 2, 4, 8, 16, 32
 
 
 class HfmOperator(C.Structure):
@@ -96,6 +96,7 @@ SIGNATURES = {
     "hfm_op_residual_typed": (I, [P, I, P, P, P, I, I, I, I, U, P]),
     "hfm_residual_restrict_typed": (I, [P, I, P, P, P, P, I, I, I, I, U, P]),
     "hfm_prolong_correct_smooth_typed": (I, [P, I, P, P, P, P, I, I, I, I, F, U, P]),
+    "hfm_face7_smooth2_typed": (I, [P, I, P, P, P, P, I, I, I, I, F, P]),
     "hfm_sigma7_faces": (I, [I, P, P, P, F, F, F, P, P, P, I, I, I, I, P]),
     "hfm_face7_elems": (I, [I, I, I, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
     "hfm_residual_restrict": (I, [P, P, P, P, P, I, I, I, I, U, P]),

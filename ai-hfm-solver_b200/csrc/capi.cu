@@ -347,6 +347,42 @@ int hfm_prolong_correct_smooth_typed(const hfm_operator *op, int dtype, const vo
   })
 }
 
+int hfm_face7_smooth2_typed(const hfm_operator *op, int dtype, const void *phi,
+                            const void *w_coarse, const void *rhs, void *out, int B, int Z,
+                            int Y, int X, float omega, hfm_stream_t stream) {
+  int st;
+  if ((st = check_grid(B, Z, Y, X))) return st;
+  if (!phi || !rhs || !out) return fail(HFM_ERR_BAD_ARG, "hfm_face7_smooth2_typed: NULL field");
+  if (phi == out) return fail(HFM_ERR_BAD_ARG, "hfm_face7_smooth2_typed: phi aliases out");
+  if ((st = check_op_typed(op, dtype, "hfm_face7_smooth2_typed"))) return st;
+  if (op->kind != HFM_OP_FACE7 || dtype == HFM_F32)
+    return fail(HFM_ERR_UNSUPPORTED, "hfm_face7_smooth2_typed: FACE7 in 16-bit storage only");
+  if (!face2_eligible(PAIR_SS, w_coarse != nullptr, Grid3{Z, Y, X}))
+    return fail(HFM_ERR_UNSUPPORTED, "hfm_face7_smooth2_typed: X >= 48 and a multiple of 8 "
+                                     "(16 with w_coarse), Y >= 16, Z >= 2, even with w_coarse");
+  for (const void *q : {phi, w_coarse, rhs, (const void *)out, op->coef[0], op->coef[1], op->coef[2]})
+    if ((uintptr_t)q & 15) return fail(HFM_ERR_BAD_ARG, "hfm_face7_smooth2_typed: fields must be 16-byte aligned");
+  const int64_t n = (int64_t)Z * Y * X;
+  DevOp d = make_devop(*op, n);
+  HFM_BY_DTYPE(dtype, {
+    PhiSrc<T> p;
+    memset(&p, 0, sizeof(p));
+    p.base = (const T *)phi;
+    p.base_stride = n;
+    if (w_coarse) {
+      p.corr = (const T *)w_coarse;
+      p.corr_stride = n / 8;
+      p.corr_coarse = 1;
+      p.corr_sign = -1.f;
+      p.Yc = Y / 2;
+      p.Xc = X / 2;
+    }
+    return tma_launch_face2<T>(PAIR_SS, d, p, (const T *)rhs, nullptr, (T *)out, nullptr, n, 0, B,
+                               Grid3{Z, Y, X}, omega, 0u, nullptr, nullptr, nullptr,
+                               (cudaStream_t)stream);
+  })
+}
+
 int hfm_residual_restrict(const hfm_operator *op, const float *phi, const float *b,
                           float *r_fine, float *r_coarse, int B, int Z, int Y, int X,
                           unsigned flags, hfm_stream_t stream) {

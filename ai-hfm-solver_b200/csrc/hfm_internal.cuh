@@ -337,6 +337,14 @@ template <class T> int launch_small(int kind, SmallArgs<T> a, int B, cudaStream_
 
 // The first two Jacobi sweeps from a zero iterate in one pass (SIGMA7, TMA-eligible grids):
 // out = J(phi1) with phi1 = omega f * invd, invd = 1 / diag of the level.
+// Two Jacobi sweeps of a FACE7 level in one pass (16-bit storage; tma_face2.cuh).
+enum { PAIR_SS = 0, PAIR_PR = 1 };
+bool face2_eligible(int pair, bool corr, Grid3 g);
+template <class T>
+int tma_launch_face2(int pair, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
+                     const T *invd, T *out, T *coarse, int64_t stride, int64_t coarse_stride,
+                     int B, Grid3 g, float omega, unsigned flags, const int *active,
+                     double *partials, int *nblk_out, cudaStream_t s);
 template <class T>
 int tma_launch_pre2(int kind, const DevOp &op, const T *f, const T *invd, T *out, int64_t stride,
                     int B, Grid3 g, float omega, const int *active, cudaStream_t s);

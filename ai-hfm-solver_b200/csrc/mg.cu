@@ -952,6 +952,16 @@ class Engine : public EngineBase {
 
   // Approximately solve A_l phi = rhs(l); `zero` says the current iterate is zero.
   // The fused first two sweeps run on the TMA path: SIGMA7 levels the TMA kernels take.
+  // Two sweeps per pass (tma_face2.cuh) on FACE7 levels, 16-bit storage.
+  bool face2_ok(int l, int pair, bool corr) {
+    if (sizeof(T) != 2 || lk(l) != HFM_OP_FACE7 || (m_->cfg.options & HFM_OPT_NO_TEMPORAL))
+      return false;
+    if (m_->cfg.flags & (HFM_FLAG_ZERO_XEND | HFM_FLAG_TOP_COPY)) return false;
+    if (!face2_eligible(pair, corr, g(l))) return false;
+    auto a16 = [](const void *q) { return ((uintptr_t)q & 15) == 0; };
+    return a16(buf(l, 0)) && a16(buf(l, 1)) && a16(rhs(l)) && (n(l) % 8) == 0;
+  }
+
   bool pre2_ok(int l) {
     if (kind() != HFM_OP_SIGMA7 || !m_->lv[l].invd || (m_->cfg.options & HFM_OPT_NO_FUSED_PRE))
       return false;
@@ -1128,12 +1138,25 @@ class Engine : public EngineBase {
     // read as zero on x = X-1 and the residual is zero there
     const int xend = (l == 0 && (c.flags & HFM_FLAG_ZERO_XEND)) ? 1 : 0;
     int k0 = 0;
+    const bool chk = (l == 0 && check_level0);
+    int nblk = 0;
+    bool restricted = false;
     if (zero && c.nu_pre >= 2 && !xend && pre2_ok(l)) {
-      // the first two sweeps from zero in one pass (phi1 = omega f / diag is pointwise)
-      if ((st = tma_launch_pre2<T>(lk(l), lo(l), rhs(l), (const T *)m_->lv[l].invd,
-                                   buf(l, cur_[l] ^ 1), n(l), m_->slots, g(l), c.omega,
-                                   m_->active, s)))
+      // the first two sweeps from zero in one pass (phi1 = omega f / diag is pointwise); with
+      // nu_pre = 2 on a FACE7 level also the residual and its restriction
+      if (c.nu_pre == 2 && face2_ok(l, PAIR_PR, false)) {
+        PhiSrc<T> none = src(nullptr, n(l));
+        if ((st = tma_launch_face2<T>(PAIR_PR, lo(l), none, rhs(l), (const T *)m_->lv[l].invd,
+                                      buf(l, cur_[l] ^ 1), rhs(l + 1), n(l), n(l + 1), m_->slots,
+                                      g(l), c.omega, 0u, m_->active,
+                                      chk ? m_->partials : nullptr, &nblk, s)))
+          return st;
+        restricted = true;
+      } else if ((st = tma_launch_pre2<T>(lk(l), lo(l), rhs(l), (const T *)m_->lv[l].invd,
+                                          buf(l, cur_[l] ^ 1), n(l), m_->slots, g(l), c.omega,
+                                          m_->active, s))) {
         return st;
+      }
       cur_[l] ^= 1;
       k0 = 2;
     }
@@ -1144,10 +1167,10 @@ class Engine : public EngineBase {
       cur_[l] ^= 1;
     }
     const bool still_zero = zero && c.nu_pre == 0;
-    int nblk = 0;
-    const bool chk = (l == 0 && check_level0);
     PhiSrc<T> p = src(still_zero ? nullptr : buf(l, cur_[l]), n(l));
-    if (xend) {
+    if (restricted) {
+      // done by the two-sweep pass
+    } else if (xend) {
       // residual of the iterate with its x = X-1 plane read as zero, zero there, restricted
       T *rf = (T *)m_->saw[0];
       p.zero_xend = 1;
@@ -1168,7 +1191,19 @@ class Engine : public EngineBase {
     } else {
       if ((st = vcycle(l + 1, true, false, 0, s))) return st;
     }
-    // correction fused with the first post-smoothing sweep (omega = 0 when nu_post == 0)
+    // correction fused with the first post-smoothing sweep (omega = 0 when nu_post == 0);
+    // with nu_post = 2 on a FACE7 level both post-sweeps in one pass
+    if (c.nu_post == 2 && !still_zero && !xend && face2_ok(l, PAIR_SS, true)) {
+      PhiSrc<T> q = with_coarse(src(buf(l, cur_[l]), n(l)), l + 1, buf(l + 1, cur_[l + 1]), -1.f);
+      const bool dot = want_rz_ && l == 0;
+      if ((st = tma_launch_face2<T>(PAIR_SS, lo(l), q, rhs(l), nullptr, buf(l, cur_[l] ^ 1),
+                                    nullptr, n(l), 0, m_->slots, g(l), c.omega,
+                                    dot ? HFM_INT_DOT_RHS : 0u, m_->active,
+                                    dot ? m_->partials : nullptr, dot ? &nblk_rz_ : nullptr, s)))
+        return st;
+      cur_[l] ^= 1;
+      return HFM_OK;
+    }
     const int post = std::max(c.nu_post, 1);
     for (int k = 0; k < post; ++k) {
       PhiSrc<T> q = src(still_zero && k == 0 ? nullptr : buf(l, cur_[l]), n(l));

@@ -524,6 +524,7 @@ __global__ void __launch_bounds__(Geo<T>::THREADS, Geo<T>::MINB) k_tma(const __g
 }
 
 #include "tma_face.cuh"
+#include "tma_face2.cuh"
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
@@ -692,6 +693,114 @@ int tma_launch_face(int mode, const DevOp &op, const PhiSrc<T> &phi, const T *rh
   return go_face<T, M_RESTRICT, 0>(a, grid, s);
 }
 
+template <class T, int PAIR, int CORR>
+int go_face2(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
+  using G = GeoF2<CORR != 0, PAIR == PAIR_PR>;
+  int st = set_max_dynamic_smem((const void *)k_tma_face2<T, PAIR, CORR>, G::SMEM,
+                                "cudaFuncSetAttribute(k_tma_face2)");
+  if (st) return st;
+  k_tma_face2<T, PAIR, CORR><<<grid, G::THREADS, G::SMEM, s>>>(a);
+  HFM_CHECK_LAUNCH("k_tma_face2");
+  return HFM_OK;
+}
+
+// Grid of the two-sweep kernel: every z chunk recomputes the first sweep on its two
+// neighbouring planes, so chunks are fewer and longer than tma_grid's - about two waves of
+// three resident blocks per SM, at least 4 planes each.
+static dim3 face2_grid(int &tiles_x, int &zc, Grid3 g, int B) {
+  constexpr int TY = GeoF2<false, false>::TY;
+  tiles_x = (g.X + TX - 1) / TX;
+  const int tiles = tiles_x * ((g.Y + TY - 1) / TY);
+  const int64_t slots = (int64_t)sm_count() * 3 * 2;
+  const int64_t chunks = (slots + (int64_t)tiles * B - 1) / ((int64_t)tiles * B);
+  zc = (int)((g.Z + chunks - 1) / chunks);
+  if (zc < 4) zc = 4;
+  if (zc & 1) ++zc;
+  if (zc > g.Z) zc = g.Z;
+  return dim3(tiles, (g.Z + zc - 1) / zc, B);
+}
+
+bool face2_eligible(int pair, bool corr, Grid3 g) {
+  if (g.X < 48 || g.Y < 16 || g.Z < 2 || (g.X % 8)) return false;
+  if (pair == PAIR_PR) return !((g.Y | g.Z) & 1);
+  if (corr) return (g.X % 16) == 0 && !((g.Y | g.Z) & 1);
+  return true;
+}
+
+// Two sweeps in one pass (tma_face2.cuh).  PAIR_SS: phi (with the coarse correction when
+// phi.corr is set) -> sweep -> sweep into out (z . r partials with HFM_INT_DOT_RHS); PAIR_PR:
+// the fused first two sweeps from zero of f = rhs (1/diag = invd) into out, and the
+// restricted residual of that iterate into coarse (|r|^2 partials when partials is given).
+template <class T>
+int tma_launch_face2(int pair, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
+                     const T *invd, T *out, T *coarse, int64_t stride, int64_t coarse_stride,
+                     int B, Grid3 g, float omega, unsigned flags, const int *active,
+                     double *partials, int *nblk_out, cudaStream_t s) {
+  if constexpr (sizeof(T) != 2) {
+    return fail(HFM_ERR_UNSUPPORTED, "two-sweep kernel: 16-bit storage only");
+  } else {
+    if (!op.coef[0] || !op.coef[1] || !op.coef[2])
+      return fail(HFM_ERR_BAD_ARG, "two-sweep kernel: FACE7 face arrays missing");
+    const bool pr = pair == PAIR_PR;
+    const int corr = (!pr && phi.corr) ? 1 : 0;
+    if (!face2_eligible(pair, corr != 0, g))
+      return fail(HFM_ERR_UNSUPPORTED, "two-sweep kernel: grid not eligible");
+    if (pr ? (!rhs || !invd || !coarse) : (!phi.base || !rhs))
+      return fail(HFM_ERR_BAD_ARG, "two-sweep kernel: missing operand");
+    if (corr && !phi.corr_coarse) return fail(HFM_ERR_UNSUPPORTED, "two-sweep kernel: coarse correction only");
+    using G = GeoF2<false, false>;
+    constexpr int TY = G::TY, PW = G::PW;
+    TmaArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    int st;
+    if ((st = make_map<T>(&a.m_phi, pr ? rhs : phi.base, g.X, g.Y, g.Z, B, pr ? stride : phi.base_stride,
+                          PW, TY + 4)))
+      return st;
+    if ((st = make_map<T>(&a.m_sx, op.coef[0], g.X + 8, g.Y, g.Z, B, face7_nx(g.Z, g.Y, g.X), PW, TY + 2)))
+      return st;
+    if ((st = make_map<T>(&a.m_sy, op.coef[1], g.X, g.Y + 1, g.Z, B, face7_ny(g.Z, g.Y, g.X), PW, TY + 3)))
+      return st;
+    if ((st = make_map<T>(&a.m_sz, op.coef[2], g.X, g.Y, g.Z + 1, B, face7_nz(g.Z, g.Y, g.X), PW, TY + 2)))
+      return st;
+    unsigned bytes = (unsigned)((G::PHI + G::FXN + G::FYN + G::FZN) * sizeof(T));
+    if (!pr) {
+      if ((st = make_map<T>(&a.m_f, rhs, g.X, g.Y, g.Z, B, stride, PW, TY + 2))) return st;
+      bytes += (unsigned)(G::FN * sizeof(T));
+    }
+    if (corr) {
+      if ((st = make_map<T>(&a.m_cc, phi.corr, g.X / 2, g.Y / 2, g.Z / 2, B, phi.corr_stride,
+                            G::CW, TY / 2 + 2)))
+        return st;
+      bytes += (unsigned)(G::CCN * sizeof(T));
+    }
+    if (pr) {
+      if ((st = make_map<T>(&a.m_ds, invd, g.X, g.Y, g.Z, B, stride, PW, TY + 4))) return st;
+      bytes += (unsigned)(G::PHI * sizeof(T));
+    }
+    a.stage_bytes = bytes;
+    a.wait_budget = g_wait_budget.load();
+    a.op = op;
+    a.out = out;
+    a.coarse = coarse;
+    a.partials = partials;
+    a.active = active;
+    a.stride = stride;
+    a.coarse_stride = coarse_stride;
+    a.Z = g.Z;
+    a.Y = g.Y;
+    a.X = g.X;
+    a.omega = omega;
+    a.corr_sign = phi.corr_sign;
+    a.dot_rhs = (!pr && (flags & HFM_INT_DOT_RHS) && partials) ? 1 : 0;
+    if (pr) a.partials = partials;
+    dim3 grid = face2_grid(a.tiles_x, a.zc, g, B);
+    if (nblk_out) *nblk_out = grid.x * grid.y;
+    if (pr) return go_face2<T, PAIR_PR, 0>(a, grid, s);
+    if (corr) return go_face2<T, PAIR_SS, 1>(a, grid, s);
+    return go_face2<T, PAIR_SS, 0>(a, grid, s);
+  }
+}
+
 template <class T>
 int tma_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const T *rhs, T *out,
                T *coarse, int64_t stride, int64_t coarse_stride, int B, Grid3 g, float omega,
@@ -819,6 +928,12 @@ int tma_launch_pre2(int kind, const DevOp &op, const T *f, const T *invd, T *out
 HFM_TMA_INST(float)
 HFM_TMA_INST(__nv_bfloat16)
 HFM_TMA_INST(__half)
+#define HFM_FACE2_INST(T)                                                                     \
+  template int tma_launch_face2<T>(int, const DevOp &, const PhiSrc<T> &, const T *, const T *, \
+                                   T *, T *, int64_t, int64_t, int, Grid3, float, unsigned,     \
+                                   const int *, double *, int *, cudaStream_t);
+HFM_FACE2_INST(__nv_bfloat16)
+HFM_FACE2_INST(__half)
 template int tma_launch_pre2<float>(int, const DevOp &, const float *, const float *, float *,
                                     int64_t, int, Grid3, float, const int *, cudaStream_t);
 template int tma_launch_pre2<__nv_bfloat16>(int, const DevOp &, const __nv_bfloat16 *,

@@ -66,6 +66,8 @@ def parse():
                    help="16-bit cycles keep the conductivity form on the plane-marching levels")
     p.add_argument("--persistent", action="store_true",
                    help="the small end of the V-cycle as one persistent kernel")
+    p.add_argument("--no-temporal", action="store_true",
+                   help="one Jacobi sweep per pass on the face-form levels")
     p.add_argument("--quick", action="store_true",
                    help="served leg only (no plain / e2e / roofline / CPU legs), for profiling")
     return p.parse_args()
@@ -149,11 +151,12 @@ def peak_hbm():
 
 
 def smoother_roofline(pkg, torch, dtype, slots, n, reps=20, form="sigma7"):
-    """CUDA-event time of one fine-level smoother sweep on a (slots, n^3) batch: the sigma
-    form (per-cell conductivities) or the face form the served 16-bit cycles run on their
-    plane-marching levels.  Algorithmic bytes: phi, f and phi' once each plus the
-    coefficient arrays at their actual size (3 n^3 conductivities, or the face arrays
-    n^2 (n + 8) + 2 n^2 (n + 1))."""
+    """CUDA-event time of one fine-level smoother launch on a (slots, n^3) batch: one sweep
+    of the sigma form (per-cell conductivities) or of the face form, or ("face7x2") the
+    served 16-bit cycles' post-smoothing pass - coarse correction and two sweeps of the face
+    form in one pass.  Algorithmic bytes: phi, f and the output once each, the coefficient
+    arrays at their actual size (3 n^3 conductivities, or the face arrays n^2 (n + 8) +
+    2 n^2 (n + 1)) and, for face7x2, the coarse correction (n^3 / 8)."""
     L, ops = pkg._lib, pkg.ops
     g = torch.Generator(device="cuda").manual_seed(1)
     tdt = {"f32": torch.float32, "bf16": torch.bfloat16}[dtype]
@@ -167,7 +170,7 @@ def smoother_roofline(pkg, torch, dtype, slots, n, reps=20, form="sigma7"):
     st.coef_dtype, st.scale = code, 1.0
     stream = ops._stream()
     P = lambda t: C.c_void_p(t.data_ptr())
-    if form == "face7":
+    if form in ("face7", "face7x2"):
         coef = [torch.empty((slots, n, n, n + 8), dtype=tdt, device="cuda"),
                 torch.empty((slots, n, n + 1, n), dtype=tdt, device="cuda"),
                 torch.empty((slots, n + 1, n, n), dtype=tdt, device="cuda")]
@@ -175,6 +178,9 @@ def smoother_roofline(pkg, torch, dtype, slots, n, reps=20, form="sigma7"):
                *(P(t) for t in coef), slots, n, n, n, stream)
         st.kind = L.OP_FACE7
         kname = "k_tma_face<%s,SMOOTH> fine-level weighted Jacobi, face form" % dtype
+        if form == "face7x2":
+            kname = ("k_tma_face2<%s,PAIR_SS,CORR> coarse correction + two weighted-Jacobi sweeps "
+                     "in one pass, face form" % dtype)
     else:
         coef = [t.to(tdt) for t in s]
         st.kind = L.OP_SIGMA7
@@ -183,20 +189,29 @@ def smoother_roofline(pkg, torch, dtype, slots, n, reps=20, form="sigma7"):
     for i in range(3):
         st.c[i] = 1.0
         st.coef[i] = coef[i].data_ptr()
-    fn = lambda: L.call("hfm_op_jacobi_typed", C.byref(st), code, P(x), P(b), P(y), slots, n, n, n,
-                        2.0 / 3.0, 0, stream)
+    w = None
+    if form == "face7x2":
+        w = torch.randn((slots, n // 2, n // 2, n // 2), device="cuda", generator=g).to(tdt)
+        fn = lambda: L.call("hfm_face7_smooth2_typed", C.byref(st), code, P(x), P(w), P(b), P(y),
+                            slots, n, n, n, 2.0 / 3.0, stream)
+    else:
+        fn = lambda: L.call("hfm_op_jacobi_typed", C.byref(st), code, P(x), P(b), P(y), slots, n,
+                            n, n, 2.0 / 3.0, 0, stream)
     ms = event_ms(torch, fn, reps=reps)
     bytes_alg = 3 * es * slots * n ** 3 + sum(t.numel() for t in coef) * es
+    if w is not None:
+        bytes_alg += w.numel() * es
     peak, src = peak_hbm()
     achieved = bytes_alg / (ms / 1e3) / 1e9
-    del x, b, y, coef
+    del x, b, y, coef, w
     key = "smooth_%s_%s_%dx%d^3" % (form, dtype, slots, n)
     traffic, tsrc = recorded_traffic(key)
     return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic,
             "traffic_note": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
             "traffic_source": tsrc, "kernel": "%s (%d x %d^3)" % (kname, slots, n),
-            "bytes_per_launch": bytes_alg, "ms_per_launch": round(ms, 4), "peak_source": src}
+            "bytes_per_launch": bytes_alg, "ms_per_launch": round(ms, 4), "peak_source": src,
+            "sweeps_per_launch": 2 if form == "face7x2" else 1}
 
 
 def recorded_traffic(key):
@@ -430,7 +445,8 @@ def run_serve(args, pkg, torch, rank, world, local):
     # 1e-1 on this stream); the plain path uses the same setting
     cfg = M.SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6, max_cycles=600,
                          inner_tol=1e-3, nu_pre=args.nu, nu_post=args.nu,
-                         faces=not args.no_faces, persistent=args.persistent)
+                         faces=not args.no_faces, persistent=args.persistent,
+                         temporal=not args.no_temporal)
     server = sv.SolveServer(cfg=cfg, slots=64, budget_bytes=120e9, cycles_per_tick=4)
 
     def barrier():
@@ -469,6 +485,7 @@ def run_serve(args, pkg, torch, rank, world, local):
                 "p50_ms": round(lat["p50_ms"], 3), "p99_ms": round(lat["p99_ms"], 3),
                 "failed": len(bad), "gpu_launches": int(launches), "quick": True,
                 "nu": args.nu, "faces": cfg.faces, "persistent": cfg.persistent,
+                "temporal": cfg.temporal,
                 "iterations_mean": round(float(np.mean([r.cycles for r in all_res])), 2)}
     # service latency at an offered load below the throughput (the same requests, Poisson
     # arrivals at 500 req/s): queueing no longer dominates p50 / p99
@@ -501,7 +518,11 @@ def run_serve(args, pkg, torch, rank, world, local):
     plain_sps = len(plain) / pdt
     # the served cycles' dominant kernel: the bf16 fine-level smoother of the 128^3 bucket,
     # in the face form those cycles run (and the conductivity form beside it)
-    roof = smoother_roofline(pkg, torch, "bf16", 64, 128, form="face7" if cfg.faces else "sigma7")
+    if cfg.faces and cfg.temporal and args.nu == 2:
+        roof = smoother_roofline(pkg, torch, "bf16", 64, 128, form="face7x2")
+    else:
+        roof = smoother_roofline(pkg, torch, "bf16", 64, 128, form="face7" if cfg.faces else "sigma7")
+    roof_face = smoother_roofline(pkg, torch, "bf16", 64, 128, form="face7")
     roof_sigma = smoother_roofline(pkg, torch, "bf16", 64, 128, form="sigma7")
     # the plain path's float32 smoother and grid transfers on one 512^3 grid (the >= 70 % of
     # HBM target)
@@ -533,7 +554,8 @@ def run_serve(args, pkg, torch, rank, world, local):
         "plain_p50_ms": round(sv.latency_stats(plain)["p50_ms"], 3),
         "plain_p99_ms": round(sv.latency_stats(plain)["p99_ms"], 3),
         "served_over_plain": round(value / world / plain_sps, 3),
-        "e2e": e2e, "roofline": roof, "roofline_sigma_bf16": roof_sigma,
+        "e2e": e2e, "roofline": roof, "roofline_face7_one_sweep_bf16": roof_face,
+        "roofline_sigma_bf16": roof_sigma,
         "roofline_plain_f32": roof_plain,
         "roofline_transfers_f32": roof_transfer,
         "gpu_launches": int(launches), "clocks": clk,

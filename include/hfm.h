@@ -174,6 +174,18 @@ int hfm_prolong_correct_smooth_typed(const hfm_operator *op, int dtype, const vo
                                      int Z, int Y, int X, float omega, unsigned flags,
                                      hfm_stream_t stream);
 
+/* Two weighted-Jacobi sweeps of a FACE7 operator in one pass over the grid (temporal
+ * blocking; the two iterations of the reference's sweep loop,
+ * Anisotropic_3d_Multigrid_7point.ipynb:424-444): out = J(J(phi - P w_coarse)), or
+ * out = J(J(phi)) when w_coarse is NULL.  16-bit storage (dtype BF16 / F16 = coef_dtype),
+ * bitwise equal to two hfm_op_jacobi_typed calls (the first with the correction, as
+ * hfm_prolong_correct_smooth_typed).  Grids: X >= 48 and a multiple of 8, Y >= 16, Z >= 2;
+ * with w_coarse also X a multiple of 16 and Y, Z even; others return HFM_ERR_UNSUPPORTED.
+ * Fields 16-byte aligned; phi must not alias out. */
+int hfm_face7_smooth2_typed(const hfm_operator *op, int dtype, const void *phi,
+                            const void *w_coarse, const void *rhs, void *out, int B, int Z,
+                            int Y, int X, float omega, hfm_stream_t stream);
+
 /* Face coefficients of the SIGMA7 operator (face means c_d (s_i + s_j) / 2, wall faces
  * c_d s_i; Anisotropic Resistivity Tomography/README:14-26) in the FACE7 layout, stored in
  * `dtype` (F32, BF16 or F16; each face computed in float32 from the float32 sx, sy, sz and
@@ -467,6 +479,12 @@ typedef struct {
  * of work, and handles that share the GPU (the buckets of a server) lose more than the
  * launches it saves; by default the small end runs as separate launches. */
 #define HFM_OPT_PERSISTENT 16
+/* options: run every Jacobi sweep of the FACE7 levels as its own pass (by default two sweeps
+ * share one pass over the level - temporal blocking: the correction and first post-sweep
+ * with the last post-sweep when nu_post = 2, and the fused first two pre-sweeps from zero
+ * with the residual and its restriction when nu_pre = 2; the first sweep is recomputed on
+ * a one-cell ring around each tile and kept in shared memory.  Results are identical.) */
+#define HFM_OPT_NO_TEMPORAL 32
 
 typedef struct {
   int active;       /* 1 while the slot is still iterating */

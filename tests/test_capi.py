@@ -153,6 +153,34 @@ def test_face7_host_calls(lib, pkg):
     assert lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1) == f32
 
 
+def test_face7_smooth2_validates_without_gpu(lib, pkg):
+    """The two-sweep entry point rejects null fields, aliasing, float32, other operator kinds
+    and grids the kernel does not take before it touches the device."""
+    L = pkg._lib
+    buf = (C.c_float * 64)()
+    addr = C.addressof(buf)
+    al = C.c_void_p((addr + 15) & ~15)
+    op = L.HfmOperator()
+    op.kind, op.coef_dtype, op.scale = L.OP_FACE7, L.BF16, 1.0
+    for i in range(3):
+        op.coef[i] = al.value
+    f = lambda *a: lib.hfm_face7_smooth2_typed(C.byref(op), *a)
+    assert f(L.BF16, None, None, al, al, 1, 4, 16, 64, 0.6, None) == L.ERR_BAD_ARG
+    assert f(L.BF16, al, None, al, al, 1, 4, 16, 64, 0.6, None) == L.ERR_BAD_ARG  # phi == out
+    other = C.c_void_p(al.value + 16)
+    assert f(L.BF16, al, None, al, other, 1, 4, 16, 40, 0.6, None) == L.ERR_UNSUPPORTED  # X < 48
+    assert f(L.BF16, al, None, al, other, 1, 4, 8, 64, 0.6, None) == L.ERR_UNSUPPORTED   # Y < 16
+    assert f(L.BF16, al, al, al, other, 1, 4, 16, 72, 0.6, None) == L.ERR_UNSUPPORTED    # X % 16
+    op.coef_dtype = L.F32
+    assert f(L.F32, al, None, al, other, 1, 4, 16, 64, 0.6, None) == L.ERR_UNSUPPORTED
+    op.coef_dtype, op.kind = L.BF16, L.OP_SIGMA7
+    assert f(L.BF16, al, None, al, other, 1, 4, 16, 64, 0.6, None) == L.ERR_UNSUPPORTED
+    op.kind = L.OP_FACE7
+    odd = C.c_void_p(al.value + 2)
+    assert f(L.BF16, odd, None, al, other, 1, 4, 16, 64, 0.6, None) == L.ERR_BAD_ARG
+    assert b"aligned" in lib.hfm_last_error()
+
+
 def test_serve_config_and_validation_without_gpu(lib, pkg):
     """hfm_serve_*: the default configuration and the host-side checks that run before any
     device allocation."""
