@@ -22,7 +22,7 @@ FLAG_ZERO_XEND, FLAG_TOP_COPY, FLAG_ZERO_GUESS, FLAG_PERIODIC, FLAG_SAME_LEVEL_C
 CYCLE_SAWTOOTH, CYCLE_V, CYCLE_F = range(3)
 ACCEL_NONE, ACCEL_CG, ACCEL_IR = range(3)
 (OPT_NO_FUSED_COARSE, OPT_NO_FUSED_PRE, OPT_SAWTOOTH_COARSE_SWEEPS, OPT_NO_FACES,
- OPT_PERSISTENT, OPT_NO_TEMPORAL) = 1, 2, 4, 8, 16, 32
+ OPT_PERSISTENT, OPT_TEMPORAL) = 1, 2, 4, 8, 16, 32
 
 
 class HfmOperator(C.Structure):

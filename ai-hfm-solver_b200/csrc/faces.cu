@@ -64,7 +64,53 @@ __global__ void k_sigma_faces(const TS *__restrict__ sx, const TS *__restrict__ 
   }
 }
 
+// 1 / diagonal of a FACE7 level: the cell's six faces summed in the order the face kernels
+// sum them (x left, x right, y below, y above, z below, z above, from zero), times the
+// operator's scale when it is not 1, so the fused first two sweeps divide by exactly the
+// diagonal the other sweeps use.
+template <class T>
+__global__ void k_invdiag_faces(const T *__restrict__ fx, const T *__restrict__ fy,
+                                const T *__restrict__ fz, float scale, int Z, int Y, int X,
+                                T *__restrict__ out, int64_t out_stride) {
+  const int64_t b = blockIdx.y;
+  const int n = Z * Y * X, P = Y * X;
+  fx += b * face7_nx(Z, Y, X);
+  fy += b * face7_ny(Z, Y, X);
+  fz += b * face7_nz(Z, Y, X);
+  out += b * out_stride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int x = i % X, t = i / X, y = t % Y, z = t / Y;
+    const int64_t ix = ((int64_t)z * Y + y) * (X + 8) + x, iy = ((int64_t)z * (Y + 1) + y) * X + x;
+    float d = __fadd_rn(St<T>::to(fx[ix]), 0.f);
+    d = __fadd_rn(St<T>::to(fx[ix + 1]), d);
+    d = __fadd_rn(St<T>::to(fy[iy]), d);
+    d = __fadd_rn(St<T>::to(fy[iy + X]), d);
+    d = __fadd_rn(St<T>::to(fz[i]), d);
+    d = __fadd_rn(St<T>::to(fz[(int64_t)i + P]), d);
+    if (scale != 1.f) d = __fmul_rn(d, scale);
+    out[i] = St<T>::from(1.f / d);
+  }
+}
+
 }  // namespace
+
+template <class T>
+int launch_invdiag_faces(const T *fx, const T *fy, const T *fz, float scale, T *out,
+                         int64_t out_stride, int B, Grid3 g, cudaStream_t s) {
+  int64_t nb = (g.n() + 255) / 256;
+  const int64_t cap = (int64_t)sm_count() * 8;
+  if (nb > cap) nb = cap;
+  if (nb < 1) nb = 1;
+  k_invdiag_faces<T><<<dim3((unsigned)nb, B), 256, 0, s>>>(fx, fy, fz, scale, g.Z, g.Y, g.X, out,
+                                                          out_stride);
+  HFM_CHECK_LAUNCH("k_invdiag_faces");
+  return HFM_OK;
+}
+template int launch_invdiag_faces<__nv_bfloat16>(const __nv_bfloat16 *, const __nv_bfloat16 *,
+                                                 const __nv_bfloat16 *, float, __nv_bfloat16 *,
+                                                 int64_t, int, Grid3, cudaStream_t);
+template int launch_invdiag_faces<__half>(const __half *, const __half *, const __half *, float,
+                                          __half *, int64_t, int, Grid3, cudaStream_t);
 
 template <class TS, class T>
 int launch_sigma_faces(const TS *sx, const TS *sy, const TS *sz, int64_t s_stride, float cz,

@@ -356,6 +356,10 @@ bool face_tma_ok(int kind, const PhiSrc<T> &phi, unsigned flags) {
          (!phi.zero_xend && !(flags & (HFM_FLAG_ZERO_XEND | HFM_FLAG_TOP_COPY | HFM_INT_DOT_PHI)));
 }
 
+// 1 / diagonal of a FACE7 level from its faces (faces.cu), the diagonal the face kernels use.
+template <class T>
+int launch_invdiag_faces(const T *fx, const T *fy, const T *fz, float scale, T *out,
+                         int64_t out_stride, int B, Grid3 g, cudaStream_t s);
 // FACE7 arrays of the SIGMA7 operator (faces.cu) from conductivities of type TS (instance
 // stride s_stride), stored as T; `div` (per-slot divisors, may be null) divides the
 // conductivities of instance slot0 + b first.

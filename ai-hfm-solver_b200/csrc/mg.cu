@@ -12,6 +12,7 @@
 // below tol (or that fails, or reaches max_cycles) is switched off by the check kernel and
 // every later kernel skips it, so the host only polls between graph launches.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -954,7 +955,7 @@ class Engine : public EngineBase {
   // The fused first two sweeps run on the TMA path: SIGMA7 levels the TMA kernels take.
   // Two sweeps per pass (tma_face2.cuh) on FACE7 levels, 16-bit storage.
   bool face2_ok(int l, int pair, bool corr) {
-    if (sizeof(T) != 2 || lk(l) != HFM_OP_FACE7 || (m_->cfg.options & HFM_OPT_NO_TEMPORAL))
+    if (sizeof(T) != 2 || lk(l) != HFM_OP_FACE7 || !(m_->cfg.options & HFM_OPT_TEMPORAL))
       return false;
     if (m_->cfg.flags & (HFM_FLAG_ZERO_XEND | HFM_FLAG_TOP_COPY)) return false;
     if (!face2_eligible(pair, corr, g(l))) return false;
@@ -1482,13 +1483,21 @@ class Engine : public EngineBase {
     }
     // FACE7 arrays of the levels that hold them: the fine level's faces from the caller's
     // float32 / float64 conductivities (divided by the slot's geometric mean for normalised
-    // fp16 cycles), coarse levels' from their restricted conductivities; the level's scale
-    // is folded into the faces
+    // fp16 cycles), coarse levels' from their restricted conductivities.  bf16 (float32's
+    // exponent range) folds the level's scale and c into the faces; fp16 divides them by
+    // kappa = scale * max(c) and keeps kappa as the operator's scale, so the stored faces stay
+    // in the range of the conductivities (c = 1/h^2 folded in would overflow fp16, and a
+    // coarse scale of 2^-l pushed small faces into its subnormals)
     for (int l = 0; l < m_->L; ++l) {
       Level &L_ = m_->lv[l];
       if (!L_.face[0]) continue;
       const DevOp &op = L_.op;
-      const float s_ = op.scale;
+      float s_ = op.scale, kappa = 1.f;
+      if (std::is_same<T, __half>::value) {
+        kappa = op.scale * std::max(std::fabs(op.c[0]), std::max(std::fabs(op.c[1]), std::fabs(op.c[2])));
+        if (!(kappa > 0.f) || !std::isfinite(kappa)) kappa = 1.f;
+        s_ = op.scale / kappa;
+      }
       const float cz = op.c[0] * s_, cy = op.c[1] * s_, cx = op.c[2] * s_;
       const int64_t nx = face7_nx(g(l).Z, g(l).Y, g(l).X), ny = face7_ny(g(l).Z, g(l).Y, g(l).X),
                     nz = face7_nz(g(l).Z, g(l).Y, g(l).X);
@@ -1511,9 +1520,15 @@ class Engine : public EngineBase {
       hfm_operator fo;
       memset(&fo, 0, sizeof(fo));
       fo.kind = HFM_OP_FACE7;
-      fo.scale = 1.f;
+      fo.scale = kappa;
       for (int a = 0; a < 3; ++a) fo.coef[a] = L_.face[a];
       L_.fop = make_devop(fo, 0);
+      // the fused first two sweeps divide by the diagonal of the stored faces
+      if constexpr (sizeof(T) == 2) {
+        if (L_.invd && (st = launch_invdiag_faces<T>(fx, fy, fz, kappa, (T *)L_.invd + lo * n(l), n(l),
+                                                     cnt, g(l), s)))
+          return st;
+      }
     }
     return HFM_OK;
   }

@@ -47,7 +47,7 @@ class SolverConfig:
     fused_pre: bool = True      # first two pre-sweeps from zero in one pass (SIGMA7, TMA levels)
     faces: bool = True          # 16-bit SIGMA7: face-coefficient kernels on the TMA levels
     persistent: bool = False    # small end of the V-cycle as one persistent kernel (>= 8 slots)
-    temporal: bool = True       # two Jacobi sweeps per pass on FACE7 levels (16-bit storage)
+    temporal: bool = False      # two Jacobi sweeps per pass on FACE7 levels (16-bit storage)
     sawtooth_coarse_sweeps: int = 1  # Jacobi sweeps on the sawtooth's coarsest level (1 =
                                      # Anisotropic_3d_Multigrid_7point.ipynb; 2 = the serial
                                      # run of parallel_multigrid_advection_diffusion_3D.ipynb)
@@ -88,7 +88,7 @@ class SolverConfig:
             (0 if self.fused_pre else L.OPT_NO_FUSED_PRE) | \
             (0 if self.faces else L.OPT_NO_FACES) | \
             (L.OPT_PERSISTENT if self.persistent else 0) | \
-            (0 if self.temporal else L.OPT_NO_TEMPORAL)
+            (L.OPT_TEMPORAL if self.temporal else 0)
         if self.cycle == "sawtooth" and self.sawtooth_coarse_sweeps != 1:
             c.options |= L.OPT_SAWTOOTH_COARSE_SWEEPS
             c.coarse_sweeps = self.sawtooth_coarse_sweeps

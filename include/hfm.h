@@ -479,12 +479,14 @@ typedef struct {
  * of work, and handles that share the GPU (the buckets of a server) lose more than the
  * launches it saves; by default the small end runs as separate launches. */
 #define HFM_OPT_PERSISTENT 16
-/* options: run every Jacobi sweep of the FACE7 levels as its own pass (by default two sweeps
- * share one pass over the level - temporal blocking: the correction and first post-sweep
- * with the last post-sweep when nu_post = 2, and the fused first two pre-sweeps from zero
- * with the residual and its restriction when nu_pre = 2; the first sweep is recomputed on
- * a one-cell ring around each tile and kept in shared memory.  Results are identical.) */
-#define HFM_OPT_NO_TEMPORAL 32
+/* options: two Jacobi sweeps per pass over the FACE7 levels (temporal blocking): the
+ * correction and first post-sweep with the last post-sweep when nu_post = 2, and the fused
+ * first two pre-sweeps from zero with the residual and its restriction when nu_pre = 2; the
+ * first sweep is recomputed on a one-cell ring around each tile and kept in shared memory.
+ * Results are identical to one sweep per pass.  Off by default: the pass halves the bytes
+ * but executes more instructions than two one-sweep passes, and the one-sweep face kernel
+ * is already close to the copy bandwidth, so it measured slower. */
+#define HFM_OPT_TEMPORAL 32
 
 typedef struct {
   int active;       /* 1 while the slot is still iterating */

@@ -6,7 +6,7 @@ with and without the coarse correction, on grids with partial tiles and several 
 The two-sweep kernel recomputes the first sweep on a one-cell ring around its tile, in the
 operation order of the tiles that own those cells, and stores it rounded to the storage type
 as the one-sweep launches do.  Stationary V-cycles of a 16-bit handle therefore give the same
-bits with and without HFM_OPT_NO_TEMPORAL: the post-sweep pair (coarse correction, sweep,
+bits with and without HFM_OPT_TEMPORAL: the post-sweep pair (coarse correction, sweep,
 sweep) on every FACE7 level and the pre-sweep pair (the fused first two sweeps from zero,
 residual, restriction) on the zero-guess coarse FACE7 levels.  Grids cover partial tiles in
 x (X = 48, X = 112) and y (Y = 24), several z chunks and several slots.
