@@ -693,13 +693,13 @@ int tma_launch_face(int mode, const DevOp &op, const PhiSrc<T> &phi, const T *rh
   return go_face<T, M_RESTRICT, 0>(a, grid, s);
 }
 
-template <class T, int PAIR, int CORR>
+template <class T, int PAIR, int CORR, int W>
 int go_face2(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
-  using G = GeoF2<CORR != 0, PAIR == PAIR_PR>;
-  int st = set_max_dynamic_smem((const void *)k_tma_face2<T, PAIR, CORR>, G::SMEM,
+  using G = GeoF2<CORR != 0, PAIR == PAIR_PR, W>;
+  int st = set_max_dynamic_smem((const void *)k_tma_face2<T, PAIR, CORR, W>, G::SMEM,
                                 "cudaFuncSetAttribute(k_tma_face2)");
   if (st) return st;
-  k_tma_face2<T, PAIR, CORR><<<grid, G::THREADS, G::SMEM, s>>>(a);
+  k_tma_face2<T, PAIR, CORR, W><<<grid, G::THREADS, G::SMEM, s>>>(a);
   HFM_CHECK_LAUNCH("k_tma_face2");
   return HFM_OK;
 }
@@ -707,9 +707,9 @@ int go_face2(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
 // Grid of the two-sweep kernel: every z chunk recomputes the first sweep on its two
 // neighbouring planes, so chunks are fewer and longer than tma_grid's - about two waves of
 // three resident blocks per SM, at least 4 planes each.
-static dim3 face2_grid(int &tiles_x, int &zc, Grid3 g, int B) {
-  constexpr int TY = GeoF2<false, false>::TY;
-  tiles_x = (g.X + TX - 1) / TX;
+static dim3 face2_grid(int &tiles_x, int &zc, Grid3 g, int B, int W) {
+  const int TY = 1024 / W;
+  tiles_x = (g.X + W - 1) / W;
   const int tiles = tiles_x * ((g.Y + TY - 1) / TY);
   const int64_t slots = (int64_t)sm_count() * 3 * 2;
   const int64_t chunks = (slots + (int64_t)tiles * B - 1) / ((int64_t)tiles * B);
@@ -727,10 +727,69 @@ bool face2_eligible(int pair, bool corr, Grid3 g) {
   return true;
 }
 
+template <class T, int W>
+int launch_face2_w(int pair, const DevOp &op, const PhiSrc<T> &phi, const T *rhs, const T *invd,
+                   T *out, T *coarse, int64_t stride, int64_t coarse_stride, int B, Grid3 g,
+                   float omega, unsigned flags, const int *active, double *partials,
+                   int *nblk_out, cudaStream_t s) {
+  const bool pr = pair == PAIR_PR;
+  const int corr = (!pr && phi.corr) ? 1 : 0;
+  using G = GeoF2<false, false, W>;
+  constexpr int TY = G::TY, PW = G::PW;
+  TmaArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  int st;
+  if ((st = make_map<T>(&a.m_phi, pr ? rhs : phi.base, g.X, g.Y, g.Z, B, pr ? stride : phi.base_stride,
+                        PW, TY + 4)))
+    return st;
+  if ((st = make_map<T>(&a.m_sx, op.coef[0], g.X + 8, g.Y, g.Z, B, face7_nx(g.Z, g.Y, g.X), PW, TY + 2)))
+    return st;
+  if ((st = make_map<T>(&a.m_sy, op.coef[1], g.X, g.Y + 1, g.Z, B, face7_ny(g.Z, g.Y, g.X), PW, TY + 3)))
+    return st;
+  if ((st = make_map<T>(&a.m_sz, op.coef[2], g.X, g.Y, g.Z + 1, B, face7_nz(g.Z, g.Y, g.X), PW, TY + 2)))
+    return st;
+  unsigned bytes = (unsigned)((G::PHI + G::FXN + G::FYN + G::FZN) * sizeof(T));
+  if (!pr) {
+    if ((st = make_map<T>(&a.m_f, rhs, g.X, g.Y, g.Z, B, stride, PW, TY + 2))) return st;
+    bytes += (unsigned)(G::FN * sizeof(T));
+  }
+  if (corr) {
+    if ((st = make_map<T>(&a.m_cc, phi.corr, g.X / 2, g.Y / 2, g.Z / 2, B, phi.corr_stride,
+                          G::CW, TY / 2 + 2)))
+      return st;
+    bytes += (unsigned)(G::CCN * sizeof(T));
+  }
+  if (pr) {
+    if ((st = make_map<T>(&a.m_ds, invd, g.X, g.Y, g.Z, B, stride, PW, TY + 4))) return st;
+    bytes += (unsigned)(G::PHI * sizeof(T));
+  }
+  a.stage_bytes = bytes;
+  a.wait_budget = g_wait_budget.load();
+  a.op = op;
+  a.out = out;
+  a.coarse = coarse;
+  a.partials = partials;
+  a.active = active;
+  a.stride = stride;
+  a.coarse_stride = coarse_stride;
+  a.Z = g.Z;
+  a.Y = g.Y;
+  a.X = g.X;
+  a.omega = omega;
+  a.corr_sign = phi.corr_sign;
+  a.dot_rhs = (!pr && (flags & HFM_INT_DOT_RHS) && partials) ? 1 : 0;
+  dim3 grid = face2_grid(a.tiles_x, a.zc, g, B, W);
+  if (nblk_out) *nblk_out = grid.x * grid.y;
+  if (pr) return go_face2<T, PAIR_PR, 0, W>(a, grid, s);
+  if (corr) return go_face2<T, PAIR_SS, 1, W>(a, grid, s);
+  return go_face2<T, PAIR_SS, 0, W>(a, grid, s);
+}
+
 // Two sweeps in one pass (tma_face2.cuh).  PAIR_SS: phi (with the coarse correction when
 // phi.corr is set) -> sweep -> sweep into out (z . r partials with HFM_INT_DOT_RHS); PAIR_PR:
 // the fused first two sweeps from zero of f = rhs (1/diag = invd) into out, and the
 // restricted residual of that iterate into coarse (|r|^2 partials when partials is given).
+// Tiles are 128 wide for 64 < X <= 128 (one tile per row), 64 wide otherwise.
 template <class T>
 int tma_launch_face2(int pair, const DevOp &op, const PhiSrc<T> &phi, const T *rhs,
                      const T *invd, T *out, T *coarse, int64_t stride, int64_t coarse_stride,
@@ -748,56 +807,11 @@ int tma_launch_face2(int pair, const DevOp &op, const PhiSrc<T> &phi, const T *r
     if (pr ? (!rhs || !invd || !coarse) : (!phi.base || !rhs))
       return fail(HFM_ERR_BAD_ARG, "two-sweep kernel: missing operand");
     if (corr && !phi.corr_coarse) return fail(HFM_ERR_UNSUPPORTED, "two-sweep kernel: coarse correction only");
-    using G = GeoF2<false, false>;
-    constexpr int TY = G::TY, PW = G::PW;
-    TmaArgs<T> a;
-    memset(&a, 0, sizeof(a));
-    int st;
-    if ((st = make_map<T>(&a.m_phi, pr ? rhs : phi.base, g.X, g.Y, g.Z, B, pr ? stride : phi.base_stride,
-                          PW, TY + 4)))
-      return st;
-    if ((st = make_map<T>(&a.m_sx, op.coef[0], g.X + 8, g.Y, g.Z, B, face7_nx(g.Z, g.Y, g.X), PW, TY + 2)))
-      return st;
-    if ((st = make_map<T>(&a.m_sy, op.coef[1], g.X, g.Y + 1, g.Z, B, face7_ny(g.Z, g.Y, g.X), PW, TY + 3)))
-      return st;
-    if ((st = make_map<T>(&a.m_sz, op.coef[2], g.X, g.Y, g.Z + 1, B, face7_nz(g.Z, g.Y, g.X), PW, TY + 2)))
-      return st;
-    unsigned bytes = (unsigned)((G::PHI + G::FXN + G::FYN + G::FZN) * sizeof(T));
-    if (!pr) {
-      if ((st = make_map<T>(&a.m_f, rhs, g.X, g.Y, g.Z, B, stride, PW, TY + 2))) return st;
-      bytes += (unsigned)(G::FN * sizeof(T));
-    }
-    if (corr) {
-      if ((st = make_map<T>(&a.m_cc, phi.corr, g.X / 2, g.Y / 2, g.Z / 2, B, phi.corr_stride,
-                            G::CW, TY / 2 + 2)))
-        return st;
-      bytes += (unsigned)(G::CCN * sizeof(T));
-    }
-    if (pr) {
-      if ((st = make_map<T>(&a.m_ds, invd, g.X, g.Y, g.Z, B, stride, PW, TY + 4))) return st;
-      bytes += (unsigned)(G::PHI * sizeof(T));
-    }
-    a.stage_bytes = bytes;
-    a.wait_budget = g_wait_budget.load();
-    a.op = op;
-    a.out = out;
-    a.coarse = coarse;
-    a.partials = partials;
-    a.active = active;
-    a.stride = stride;
-    a.coarse_stride = coarse_stride;
-    a.Z = g.Z;
-    a.Y = g.Y;
-    a.X = g.X;
-    a.omega = omega;
-    a.corr_sign = phi.corr_sign;
-    a.dot_rhs = (!pr && (flags & HFM_INT_DOT_RHS) && partials) ? 1 : 0;
-    if (pr) a.partials = partials;
-    dim3 grid = face2_grid(a.tiles_x, a.zc, g, B);
-    if (nblk_out) *nblk_out = grid.x * grid.y;
-    if (pr) return go_face2<T, PAIR_PR, 0>(a, grid, s);
-    if (corr) return go_face2<T, PAIR_SS, 1>(a, grid, s);
-    return go_face2<T, PAIR_SS, 0>(a, grid, s);
+    if (g.X > 64 && g.X <= 128)
+      return launch_face2_w<T, 128>(pair, op, phi, rhs, invd, out, coarse, stride, coarse_stride, B,
+                                    g, omega, flags, active, partials, nblk_out, s);
+    return launch_face2_w<T, 64>(pair, op, phi, rhs, invd, out, coarse, stride, coarse_stride, B, g,
+                                 omega, flags, active, partials, nblk_out, s);
   }
 }
 

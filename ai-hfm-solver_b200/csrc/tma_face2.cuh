@@ -24,15 +24,20 @@
 // first and last group of a row also its column -1 / 64 cell), the first 128 compute B.
 // Loads, waits and the timeout path are those of k_tma_face.
 
-template <bool CC, bool DS> struct GeoF2 {
+// W: tile width, 64 (16 rows) or 128 (8 rows); either way 128 threads own the tile's 1024
+// cells in the second sweep and 144 or 160 threads the first sweep's rows.  A tile as wide
+// as the grid has no ring columns inside the grid (they are zero), so grids with
+// 64 < X <= 128 take W = 128 and never run the single-cell path.
+template <bool CC, bool DS, int W = 64> struct GeoF2 {
   static constexpr int ES = 2;
-  static constexpr int TY = 16, VEC = 8, TPR = TX / VEC;
+  static constexpr int TW = W;
+  static constexpr int TY = 1024 / W, VEC = 8, TPR = W / VEC;
   static constexpr int BT = TPR * TY;               // threads of the second sweep
   static constexpr int AT = TPR * (TY + 2);         // threads of the first sweep
   static constexpr int THREADS = 160;               // AT rounded up to whole warps
   static constexpr int NS = 4, MINB = 3;
-  static constexpr int HX = 8, PW = TX + 2 * HX;
-  static constexpr int CW = TX / 2 + 2 * HX;
+  static constexpr int HX = 8, PW = W + 2 * HX;
+  static constexpr int CW = W / 2 + 2 * HX;
   static constexpr int PHI = (TY + 4) * PW;
   static constexpr int FXN = (TY + 2) * PW;
   static constexpr int FYN = (TY + 3) * PW;
@@ -53,10 +58,10 @@ template <bool CC, bool DS> struct GeoF2 {
   static constexpr int SMEM = NS * STAGE + 3 * AB;
 };
 
-template <class T, int PAIR, int CORR>
+template <class T, int PAIR, int CORR, int W>
 __device__ __forceinline__ void issue_plane_face2(const TmaArgs<T> &a, char *stage, uint32_t bar,
                                                   int p, int x0, int y0, int b) {
-  using G = GeoF2<CORR != 0, PAIR == PAIR_PR>;
+  using G = GeoF2<CORR != 0, PAIR == PAIR_PR, W>;
   mbar_expect(bar, a.stage_bytes);
   tma_load(smem_u32(stage + G::O_PHI), &a.m_phi, x0 - G::HX, y0 - 2, p, b, bar);
   tma_load(smem_u32(stage + G::O_FX), &a.m_sx, x0 - G::HX, y0 - 1, p, b, bar);
@@ -81,13 +86,13 @@ __device__ __forceinline__ float jacobi1(float S, float D, float pc, float fr, f
   return __fmaf_rn(om, __fmul_rn(u, rd), pc);
 }
 
-template <class T, int PAIR, int CORR>
+template <class T, int PAIR, int CORR, int W>
 __global__ void __launch_bounds__(GeoF2<false, false>::THREADS, GeoF2<false, false>::MINB)
     k_tma_face2(const __grid_constant__ TmaArgs<T> a) {
   constexpr bool PR = PAIR == PAIR_PR;
   constexpr bool PRE2F = PR && std::is_same<T, __half>::value;  // fp16: g in float32
-  using G = GeoF2<CORR != 0, PR>;
-  constexpr int TY = G::TY, V = G::VEC, NS = G::NS, PW = G::PW, HX = G::HX;
+  using G = GeoF2<CORR != 0, PR, W>;
+  constexpr int TY = G::TY, V = G::VEC, NS = G::NS, PW = G::PW, HX = G::HX, TX = G::TW;
   extern __shared__ __align__(128) char smem[];
   __shared__ __align__(8) uint64_t bars[NS];
   const int64_t inst = blockIdx.z;
@@ -116,7 +121,7 @@ __global__ void __launch_bounds__(GeoF2<false, false>::THREADS, GeoF2<false, fal
   if (tid == 0) {
     for (; p_next <= p_last && p_next < p_first + NS; ++p_next) {
       const int q = p_next - p_first;
-      issue_plane_face2<T, PAIR, CORR>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
+      issue_plane_face2<T, PAIR, CORR, W>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
     }
   }
   int p_waited = p_first - 1;
@@ -379,7 +384,7 @@ __global__ void __launch_bounds__(GeoF2<false, false>::THREADS, GeoF2<false, fal
     if (tid == 0 && p > z0 - 1 && p_next <= p_last) {
       const int q = p_next - p_first;
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_plane_face2<T, PAIR, CORR>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
+      issue_plane_face2<T, PAIR, CORR, W>(a, smem + (q % NS) * G::STAGE, smem_u32(&bars[q % NS]), p_next, x0, y0, b);
       ++p_next;
     }
     mine = wait_plane(p + 1, a.wait_budget);

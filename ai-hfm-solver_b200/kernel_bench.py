@@ -6,7 +6,8 @@
 Kernels: ``smooth`` (one weighted-Jacobi sweep), ``resid`` (A phi - b), ``restrict`` (fused
 residual + restriction), ``correct`` (fused prolongation + correction + sweep), ``apply27``
 (27-point conv), ``transfer-r`` / ``transfer-p`` (standalone restriction / prolongation),
-``ns-step`` (time steps of the obstacle flow at --shape, default 64,128,128: 24 boxes, 7-point
+``smooth2`` (face7: coarse correction and two sweeps in one pass), ``ns-step`` (time steps
+of the obstacle flow at --shape, default 64,128,128: 24 boxes, 7-point
 diffusion, F-cycle pressure solve to 1e-5; --reps steps in one timed region, the target of a
 launch list).
 Forms: ``sigma7`` (per-cell conductivities), ``face7`` (stored faces; 16-bit storage),
@@ -113,6 +114,12 @@ def main():
                              P(out), B, Z, Y, X, 2.0 / 3.0, 0, stream)) if typed else \
              (lambda: L.call("hfm_prolong_correct_smooth", C.byref(st), P(x), P(wc), P(b), P(out),
                              B, Z, Y, X, 2.0 / 3.0, 0, stream))
+        nbytes = 3 * field + field / 8 + coef_bytes
+    elif a.kernel == "smooth2":
+        if a.form != "face7":
+            raise SystemExit("smooth2 (two sweeps per pass) is a face7 kernel")
+        fn = lambda: L.call("hfm_face7_smooth2_typed", C.byref(st), code, P(x), P(wc), P(b), P(out),
+                            B, Z, Y, X, 2.0 / 3.0, stream)
         nbytes = 3 * field + field / 8 + coef_bytes
     elif a.kernel == "apply27":
         w27 = W.pressure27().reshape(27).copy()

@@ -1,7 +1,9 @@
 """Two Jacobi sweeps per pass on FACE7 levels (temporal blocking) against one sweep per pass.
 
 hfm_face7_smooth2_typed equals the two one-sweep entry points called in turn, bit for bit,
-with and without the coarse correction, on grids with partial tiles and several z chunks.
+with and without the coarse correction, on grids with partial tiles and several z chunks:
+tiles 64 wide (X <= 64), 128 wide (64 < X <= 128, one tile per row) and 64 wide with the
+first sweep's ring columns computed cell by cell inside the grid (X > 128).
 
 The two-sweep kernel recomputes the first sweep on a one-cell ring around its tile, in the
 operation order of the tiles that own those cells, and stores it rounded to the storage type
@@ -60,7 +62,8 @@ def _face_op(hfm, T, dtype, sig, B, Z, Y, X):
 @pytest.mark.parametrize("dtype", ["bf16", "f16"])
 @pytest.mark.parametrize("shape,corr", [((2, 10, 20, 72), False), ((1, 12, 34, 128), True),
                                         ((3, 6, 16, 64), True), ((2, 4, 16, 48), True),
-                                        ((1, 40, 48, 112), True)])
+                                        ((1, 40, 48, 112), True), ((1, 6, 16, 192), True),
+                                        ((2, 8, 24, 136), False)])
 def test_smooth2_entry_point_equals_two_sweeps(hfm, T, dtype, shape, corr):
     """hfm_face7_smooth2_typed against hfm_prolong_correct_smooth_typed (or
     hfm_op_jacobi_typed) followed by hfm_op_jacobi_typed: the same bits."""
