@@ -69,13 +69,46 @@ __device__ __forceinline__ float sub_apply(const SubLevel<T> &L, const float *ph
          ayp * (pc - P(z, y + 1, x)) + azm * (pc - P(z - 1, y, x)) + azp * (pc - P(z + 1, y, x));
 }
 
+// Coordinates of the cells a thread visits in a block-strided loop over a Z x Y x X grid: the
+// first from one division, the next ones by adding the stride's own coordinates with carries
+// (dx < X, dy < Y, so at most one carry each) instead of dividing per cell.
+struct Walk {
+  int z, y, x, dz, dy, dx;
+  __device__ Walk(int i, int stride, int Y, int X) {
+    x = i % X;
+    const int t = i / X;
+    y = t % Y;
+    z = t / Y;
+    dx = stride % X;
+    const int u = stride / X;
+    dy = u % Y;
+    dz = u / Y;
+  }
+  __device__ void step(int Y, int X) {
+    x += dx;
+    int cy = 0;
+    if (x >= X) {
+      x -= X;
+      cy = 1;
+    }
+    y += dy + cy;
+    int cz = 0;
+    if (y >= Y) {
+      y -= Y;
+      cz = 1;
+    }
+    z += dz + cz;
+  }
+};
+
 // out = phi' + om (f - A phi') / diag with phi' = in - P(cor) (in / cor may be null)
 template <int KIND, class T>
 __device__ void sub_sweep(const SubLevel<T> &L, const float *in, const float *cor,
                           const SubLevel<T> *Lc, const float *f, float *out, float om,
                           const T *S) {
-  for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
-    const int x = i % L.X, t = i / L.X, y = t % L.Y, z = t / L.Y;
+  Walk w(threadIdx.x, blockDim.x, L.Y, L.X);
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x, w.step(L.Y, L.X)) {
+    const int x = w.x, y = w.y, z = w.z;
     float dg;
     const float ax = sub_apply<KIND, T>(L, in, cor, Lc, S, z, y, x, &dg);
     float pc = in ? in[i] : 0.f;
@@ -89,8 +122,9 @@ __device__ void sub_sweep(const SubLevel<T> &L, const float *in, const float *co
 template <int KIND, class T>
 __device__ void sub_resid_restrict(const SubLevel<T> &L, const float *ph, const float *f,
                                    const SubLevel<T> &Lc, float *fc, const T *S) {
-  for (int j = threadIdx.x; j < Lc.n; j += blockDim.x) {
-    const int xc = j % Lc.X, t = j / Lc.X, yc = t % Lc.Y, zc = t / Lc.Y;
+  Walk w(threadIdx.x, blockDim.x, Lc.Y, Lc.X);
+  for (int j = threadIdx.x; j < Lc.n; j += blockDim.x, w.step(Lc.Y, Lc.X)) {
+    const int xc = w.x, yc = w.y, zc = w.z;
     float sum = 0.f;
 #pragma unroll
     for (int a = 0; a < 2; ++a)
@@ -156,15 +190,51 @@ __device__ void subcycle_body(const SubArgs<T> &a, int64_t inst, unsigned char *
     zero[l] = a.nu_pre == 0;
     sub_resid_restrict<KIND, T>(L, zero[l] ? nullptr : buf[c], f, a.lv[l + 1], F + a.lv[l + 1].o_rhs, S);
   }
-  // coarsest: coarse_sweeps sweeps from zero
+  // coarsest: coarse_sweeps sweeps from zero; a level of at most 64 cells (4^3, 3^3) on one
+  // warp, two cells a lane with their coordinates computed once, __syncwarp() between the
+  // sweeps instead of a block barrier (the per-cell arithmetic is sub_sweep's)
   {
     const SubLevel<T> &L = a.lv[nl - 1];
     float *buf[2] = {F + L.o_phi, F + L.o_tmp};
     int c = 0;
-    for (int k = 0; k < a.coarse_sweeps; ++k) {
-      sub_sweep<KIND, T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1],
-                   a.coarse_omega, S);
-      c ^= 1;
+    if (L.n <= 64 && a.coarse_sweeps > 0) {
+      if (threadIdx.x < 32) {
+        const float *f = F + L.o_rhs;
+        int zz[2], yy[2], xx[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int i = threadIdx.x + 32 * q;
+          xx[q] = i % L.X;
+          const int t = i / L.X;
+          yy[q] = t % L.Y;
+          zz[q] = t / L.Y;
+        }
+        for (int k = 0; k < a.coarse_sweeps; ++k) {
+          const float *in = k == 0 ? nullptr : buf[c];
+          float *out = buf[c ^ 1];
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const int i = threadIdx.x + 32 * q;
+            if (i < L.n) {
+              float dg;
+              const float ax = sub_apply<KIND, T>(L, in, nullptr, nullptr, S, zz[q], yy[q], xx[q], &dg);
+              const float pc = in ? in[i] : 0.f;
+              out[i] = pc + a.coarse_omega * __fdividef(f[i] - ax, dg);
+            }
+          }
+          __syncwarp();
+          c ^= 1;
+        }
+      } else {
+        c = a.coarse_sweeps & 1;
+      }
+      __syncthreads();
+    } else {
+      for (int k = 0; k < a.coarse_sweeps; ++k) {
+        sub_sweep<KIND, T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1],
+                           a.coarse_omega, S);
+        c ^= 1;
+      }
     }
     if (a.coarse_sweeps == 0) {
       for (int i = threadIdx.x; i < L.n; i += blockDim.x) buf[0][i] = 0.f;
