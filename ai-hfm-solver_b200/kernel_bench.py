@@ -6,7 +6,8 @@
 Kernels: ``smooth`` (one weighted-Jacobi sweep), ``resid`` (A phi - b), ``restrict`` (fused
 residual + restriction), ``correct`` (fused prolongation + correction + sweep), ``apply27``
 (27-point conv), ``transfer-r`` / ``transfer-p`` (standalone restriction / prolongation),
-``smooth2`` (face7: coarse correction and two sweeps in one pass), ``ns-step`` (time steps
+``smooth2`` (face7: coarse correction and two sweeps in one pass), ``mg-iter`` (bf16
+refinement + PCG iterations on a handle of --batch slots of --n^3), ``ns-step`` (time steps
 of the obstacle flow at --shape, default 64,128,128: 24 boxes, 7-point
 diffusion, F-cycle pressure solve to 1e-5; --reps steps in one timed region, the target of a
 launch list).
@@ -44,6 +45,8 @@ def main():
     ops, W, L = hfm.ops, hfm.weights, hfm._lib
     if a.kernel == "ns-step":
         return ns_step(hfm, torch, a)
+    if a.kernel == "mg-iter":
+        return mg_iter(hfm, torch, a)
     Z, Y, X = (tuple(int(v) for v in a.shape.split(",")) if a.shape else (a.n, a.n, a.n))
     B = a.batch
     n = Z * Y * X
@@ -150,6 +153,38 @@ def main():
                       "ms_per_launch": ms, "bytes_per_launch": nbytes,
                       "bytes_per_cell": nbytes / (B * n),
                       "gbs": nbytes / (ms / 1e3) / 1e9 if ms > 0 else None}))
+
+
+def mg_iter(hfm, torch, a):
+    """Float64 refinement around bf16 PCG-V(2,2) on a handle of --batch slots of --n^3 (the
+    served 128^3 bucket by default: 64 slots), --reps iterations in one timed region after
+    --warmup: the target of a launch list of the CG kernels (q = A p with p . q, k_cg_p,
+    k_cg_xr, the float64 outer residual) next to the cycle's kernels."""
+    M, L = hfm.multigrid, hfm._lib
+    n, B = a.n, a.batch
+    shape = (n, n, n)
+    sig = torch.exp(torch.randn((3, B) + shape, device="cuda",
+                                generator=torch.Generator(device="cuda").manual_seed(0)))
+    f = torch.randn((B,) + shape, device="cuda", dtype=torch.float64,
+                    generator=torch.Generator(device="cuda").manual_seed(1))
+    cfg = M.SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-300, max_cycles=100000,
+                         inner_tol=1e-3)
+    with M.Multigrid(shape, L.OP_SIGMA7, cfg, slots=B) as h:
+        h.set_operator(hfm.ops.Sigma7(sig[0], sig[1], sig[2]))
+        del sig
+        for s in range(B):
+            h.load_f64(s, f[s])
+        h.run(a.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.cuda.nvtx.range_push("timed")  # lets a profiler select the timed iterations
+        h.run(a.reps)
+        torch.cuda.nvtx.range_pop()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.reps
+    print(json.dumps({"kernel": "mg-iter", "shape": [B, n, n, n], "ms_per_iteration": ms}))
 
 
 def ns_step(hfm, torch, a):
