@@ -1345,8 +1345,12 @@ class Engine : public EngineBase {
       HFM_CHECK_LAUNCH("k_dot_partials");
       nblk_rz = vb;
     }
-    k_cg_p<T><<<ib, 256, 0, s>>>(z, p, it, m_->state, rz_part, nblk_rz, m_->scal, m_->active,
-                                 scaled, m_->gscale);
+    // k_cg_p writes no per-chunk partials, so it takes chunks four times longer: every chunk
+    // re-sums the slot's r . z partials (three block barriers), which at 4096 elements held
+    // it near 0.7 of the copy bandwidth
+    const Items itp{B, std::max(1, it.CH / 4), nf};
+    k_cg_p<T><<<item_blocks(B, itp.CH), 256, 0, s>>>(z, p, itp, m_->state, rz_part, nblk_rz,
+                                                     m_->scal, m_->active, scaled, m_->gscale);
     HFM_CHECK_LAUNCH("k_cg_p");
     // q = A p with the partial sums of p . q in the same pass (float32 operator on the fine
     // level), into a partials buffer of their own
