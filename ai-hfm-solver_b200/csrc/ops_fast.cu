@@ -9,6 +9,9 @@
 //   * y neighbours are vector loads served mostly by L1 (the rows belong to the same block).
 // Modes: SMOOTH (weighted Jacobi), RESID (A phi - b, optional norm partials), RESTRICT
 // (residual of R = 2 rows x 2 planes x 2 columns averaged into the coarse grid).
+#include <map>
+#include <mutex>
+
 #include "hfm_internal.cuh"
 
 namespace hfm {
@@ -443,15 +446,32 @@ __global__ void __launch_bounds__(kFastThreads)
   }
 }
 
-// Grid shape: (plane tiles, z chunks, instances); z chunks sized so that the launch has
-// about eight blocks per SM, and at least 4 planes each (even for the restriction).
+// Resident blocks per SM of a kernel (its registers decide: 2-3 blocks of 256 threads),
+// looked up once per kernel.
+int resident_blocks(const void *kernel) {
+  static std::mutex mu;
+  static std::map<const void *, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kFastThreads, 0) != cudaSuccess || nb < 1)
+    nb = 2;
+  cache[kernel] = nb;
+  return nb;
+}
+
+// Grid shape: (plane tiles, z chunks, instances); z chunks sized so that the launch fills the
+// GPU's resident blocks once (a second, partly filled wave doubled the time of the small
+// levels: 64 instances of 32^3 made 512 blocks against 444 resident), at least 4 planes each
+// (even for the restriction).
 template <class T>
-dim3 fast_grid(FastArgs<T> &a, int B, int rows, bool even_chunks) {
+dim3 fast_grid(FastArgs<T> &a, int B, int rows, bool even_chunks, int per_sm) {
   const int nvx = a.X >> 2;
   const int64_t vecs = (int64_t)((a.Y + rows - 1) / rows) * nvx;
   const int tiles = (int)((vecs + kFastThreads - 1) / kFastThreads);
-  const int64_t target = (int64_t)sm_count() * 8;
-  int64_t chunks = (target + (int64_t)tiles * B - 1) / ((int64_t)tiles * B);
+  const int64_t target = (int64_t)sm_count() * per_sm;
+  int64_t chunks = std::max<int64_t>(1, target / ((int64_t)tiles * B));
   int zc = (int)((a.Z + chunks - 1) / chunks);
   if (zc < 4) zc = 4;
   if (even_chunks && (zc & 1)) ++zc;
@@ -503,9 +523,13 @@ int fast_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const
   if (phi.base && phi.base_stride != stride) return fail(HFM_ERR_BAD_ARG, "fast path: stride mismatch");
   const int corr = phi.corr ? (phi.corr_coarse ? C_COARSE : C_SAME) : C_NONE;
   const int rows = (mode == M_RESTRICT) ? 2 : 1;
-  dim3 grid = fast_grid<T>(a, B, rows, mode == M_RESTRICT);
-  if (nblk_out) *nblk_out = grid.x * grid.y;
-#define HFM_FAST_GO(KER) KER<<<grid, kFastThreads, 0, s>>>(a)
+#define HFM_FAST_GO(KER)                                                                       \
+  do {                                                                                         \
+    const dim3 grid = fast_grid<T>(a, B, rows, mode == M_RESTRICT,                             \
+                                   resident_blocks((const void *)KER));                        \
+    if (nblk_out) *nblk_out = grid.x * grid.y;                                                 \
+    KER<<<grid, kFastThreads, 0, s>>>(a);                                                      \
+  } while (0)
   // dispatch
   if (kind == HFM_OP_K27) {
     if (mode == M_SMOOTH) {
