@@ -7,7 +7,8 @@ Kernels: ``smooth`` (one weighted-Jacobi sweep), ``resid`` (A phi - b), ``restri
 residual + restriction), ``correct`` (fused prolongation + correction + sweep), ``apply27``
 (27-point conv), ``transfer-r`` / ``transfer-p`` (standalone restriction / prolongation),
 ``smooth2`` (face7: coarse correction and two sweeps in one pass), ``mg-iter`` (bf16
-refinement + PCG iterations on a handle of --batch slots of --n^3), ``ns-step`` (time steps
+refinement + PCG iterations on a handle of --batch slots of --n^3), ``kolmogorov-step``
+(time steps of the 2D Kolmogorov flow at --n^2), ``ns-step`` (time steps
 of the obstacle flow at --shape, default 64,128,128: 24 boxes, 7-point
 diffusion, F-cycle pressure solve to 1e-5; --reps steps in one timed region, the target of a
 launch list).
@@ -47,6 +48,8 @@ def main():
         return ns_step(hfm, torch, a)
     if a.kernel == "mg-iter":
         return mg_iter(hfm, torch, a)
+    if a.kernel == "kolmogorov-step":
+        return kolmogorov_step(hfm, torch, a)
     Z, Y, X = (tuple(int(v) for v in a.shape.split(",")) if a.shape else (a.n, a.n, a.n))
     B = a.batch
     n = Z * Y * X
@@ -185,6 +188,25 @@ def mg_iter(hfm, torch, a):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / a.reps
     print(json.dumps({"kernel": "mg-iter", "shape": [B, n, n, n], "ms_per_iteration": ms}))
+
+
+def kolmogorov_step(hfm, torch, a):
+    """Time steps of the doubly periodic Kolmogorov flow at --n^2 (the 2D configuration:
+    nu 1/40, sin(4y) forcing, dt 1e-3, three pressure V-cycles per step), --reps steps in
+    one timed region (NVTX range "timed")."""
+    kf = hfm.kolmogorov.KolmogorovFlow(n=a.n, dt=1e-3, cycles=3, seed=0)
+    for _ in range(a.warmup):
+        kf.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    torch.cuda.nvtx.range_push("timed")
+    for _ in range(a.reps):
+        kf.step()
+    torch.cuda.nvtx.range_pop()
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel": "kolmogorov-step", "n": a.n, "ms_per_step": e0.elapsed_time(e1) / a.reps}))
 
 
 def ns_step(hfm, torch, a):

@@ -66,6 +66,9 @@ def parse():
                    help="16-bit cycles keep the conductivity form on the plane-marching levels")
     p.add_argument("--persistent", action="store_true",
                    help="the small end of the V-cycle as one persistent kernel")
+    p.add_argument("--slots", type=int, default=64, help="slots per bucket (before admission by footprint)")
+    p.add_argument("--cycles-per-tick", type=int, default=4,
+                   help="refinement/PCG iterations per bucket launch")
     p.add_argument("--temporal", action="store_true",
                    help="two Jacobi sweeps per pass on the face-form levels")
     p.add_argument("--quick", action="store_true",
@@ -447,7 +450,8 @@ def run_serve(args, pkg, torch, rank, world, local):
                          inner_tol=1e-3, nu_pre=args.nu, nu_post=args.nu,
                          faces=not args.no_faces, persistent=args.persistent,
                          temporal=args.temporal)
-    server = sv.SolveServer(cfg=cfg, slots=64, budget_bytes=120e9, cycles_per_tick=4)
+    server = sv.SolveServer(cfg=cfg, slots=args.slots, budget_bytes=120e9,
+                            cycles_per_tick=args.cycles_per_tick)
 
     def barrier():
         if world > 1:
