@@ -58,8 +58,11 @@ template <class T, bool SIG = true, bool CC = true, bool DS = false> struct Geo 
   static constexpr int VEC = 16 / (int)sizeof(T);
   static constexpr int TPR = TX / VEC;
   static constexpr int THREADS = TPR * TY;
-  static constexpr int NS = sizeof(T) == 4 ? 5 : 4;    // pipeline stages
-  static constexpr int MINB = sizeof(T) == 4 ? 3 : 4;  // resident blocks per SM
+  // 4 stages and 4 resident blocks per SM for both: float32 with 5 stages fitted 3 blocks
+  // (12 warps per SM), and ncu showed the sweep latency-bound there (issue slots 42 % busy,
+  // shared-memory and dependency stalls), not bandwidth-bound
+  static constexpr int NS = 4;    // pipeline stages
+  static constexpr int MINB = 4;  // resident blocks per SM
   static constexpr int HX = 16 / (int)sizeof(T);
   static constexpr int PW = TX + 2 * HX;           // phi / sx tile width
   static constexpr int CW = TX / 2 + 2 * HX;       // coarse tile width
@@ -591,15 +594,16 @@ int go_face(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
   return HFM_OK;
 }
 
-// Grid (plane tiles, z chunks, instances): z chunks sized for about 3 resident blocks per SM
-// and four waves, at least 2 planes each.  (Eight waves, which shrink the partly filled last
-// wave, measured slower: every chunk re-reads its two halo planes and refills its pipeline.)
+// Grid (plane tiles, z chunks, instances): z chunks sized for about four waves (of 4 resident
+// blocks per SM for float32, 3 for 16-bit storage, the sizing the 16-bit kernels were tuned
+// with), at least 2 planes each.  (Eight waves, which shrink the partly filled last wave,
+// measured slower: every chunk re-reads its two halo planes and refills its pipeline.)
 template <class T>
 dim3 tma_grid(TmaArgs<T> &a, Grid3 g, int B) {
   constexpr int TY = Geo<T>::TY;
   a.tiles_x = (g.X + TX - 1) / TX;
   const int tiles = a.tiles_x * ((g.Y + TY - 1) / TY);
-  const int64_t slots = (int64_t)sm_count() * 3 * 4;
+  const int64_t slots = (int64_t)sm_count() * (sizeof(T) == 4 ? 4 : 3) * 4;
   int64_t chunks = (slots + (int64_t)tiles * B - 1) / ((int64_t)tiles * B);
   int zc = (int)((g.Z + chunks - 1) / chunks);
   if (zc < 2) zc = 2;
