@@ -6,7 +6,8 @@
 Kernels: ``smooth`` (one weighted-Jacobi sweep), ``resid`` (A phi - b), ``restrict`` (fused
 residual + restriction), ``correct`` (fused prolongation + correction + sweep), ``apply27``
 (27-point conv), ``transfer-r`` / ``transfer-p`` (standalone restriction / prolongation),
-``smooth2`` (face7: coarse correction and two sweeps in one pass), ``mg-iter`` (bf16
+``smooth2`` (face7: coarse correction and two sweeps in one pass), ``served-shares``
+(kernel-time shares of one pass over the served stream of --batch requests), ``mg-iter`` (bf16
 refinement + PCG iterations on a handle of --batch slots of --n^3), ``kolmogorov-step``
 (time steps of the 2D Kolmogorov flow at --n^2), ``ns-step`` (time steps
 of the obstacle flow at --shape, default 64,128,128: 24 boxes, 7-point
@@ -50,6 +51,8 @@ def main():
         return mg_iter(hfm, torch, a)
     if a.kernel == "kolmogorov-step":
         return kolmogorov_step(hfm, torch, a)
+    if a.kernel == "served-shares":
+        return served_shares(hfm, torch, a)
     Z, Y, X = (tuple(int(v) for v in a.shape.split(",")) if a.shape else (a.n, a.n, a.n))
     B = a.batch
     n = Z * Y * X
@@ -188,6 +191,43 @@ def mg_iter(hfm, torch, a):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / a.reps
     print(json.dumps({"kernel": "mg-iter", "shape": [B, n, n, n], "ms_per_iteration": ms}))
+
+
+def served_shares(hfm, torch, a):
+    """Kernel-time shares of one pass over the served stream (--batch requests, the
+    benchmark's stream and solver settings), from the CUDA activity trace of torch's
+    profiler: every kernel of the pass, aggregated by name.  The pass runs once unprofiled
+    first (graph capture, warm-up).  Times under a tracer are for shares only."""
+    from torch.profiler import profile, ProfilerActivity
+    sv, M = hfm.serving, hfm.multigrid
+    reqs = sv.make_stream(count=a.batch, rate=2000.0, seed=0, device=torch.device("cuda"))
+    cfg = M.SolverConfig(cycle="V", accel="ir", storage="bf16", tol=1e-6, max_cycles=600,
+                         inner_tol=1e-3)
+    server = sv.SolveServer(cfg=cfg, slots=64, budget_bytes=120e9, cycles_per_tick=4)
+    try:
+        server.serve(reqs, realtime=True)
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            server.serve(reqs, realtime=True)
+            torch.cuda.synchronize()
+    finally:
+        server.close()
+    tot, cnt = {}, {}
+    for e in prof.events():
+        if getattr(e.device_type, "name", "") != "CUDA" or e.name.startswith(("Memcpy", "Memset")):
+            continue
+        name = e.name.replace("(anonymous namespace)::", "").replace("hfm::", "")
+        name = name.replace("void ", "").split("(")[0]
+        t = getattr(e, "device_time_total", None)
+        if t is None:
+            t = getattr(e, "cuda_time_total", 0.0)
+        tot[name] = tot.get(name, 0.0) + t
+        cnt[name] = cnt.get(name, 0) + 1
+    T = sum(tot.values())
+    rows = sorted(tot.items(), key=lambda kv: -kv[1])
+    print(json.dumps({"kernel": "served-shares", "requests": a.batch, "kernel_ms": T / 1e3,
+                      "kernels": [{"name": k, "launches": cnt[k], "ms": v / 1e3,
+                                   "share": v / T} for k, v in rows]}))
 
 
 def kolmogorov_step(hfm, torch, a):
