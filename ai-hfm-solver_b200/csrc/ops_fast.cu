@@ -180,7 +180,7 @@ __device__ __forceinline__ double block_reduce(double v) {
 // 7-point forms (CONST7, SIGMA7).  R rows per thread.
 // ---------------------------------------------------------------------------------------
 template <int KIND, class T, int MODE, int CORR, int R>
-__global__ void __launch_bounds__(kFastThreads)
+__global__ void __launch_bounds__(kFastThreads, R == 1 ? 4 : 2)
     k_fast7(FastArgs<T> a) {
   const int64_t inst = blockIdx.z;
   if (a.active && !a.active[inst]) return;
