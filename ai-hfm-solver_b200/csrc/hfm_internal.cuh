@@ -286,7 +286,7 @@ template <class T> struct SubLevel {
   float k[27];               // CONST7 (k[0..2] = kz, ky, kx) / K27 weights of this level
   const T *sx, *sy, *sz;     // the level's conductivities, instance stride n
   int o_phi, o_tmp, o_rhs;   // float offsets of the level's fields in shared memory
-  int o_sig;                 // element offset of its conductivities in the T region
+  int o_face;                // float offset of its face arrays and diagonal (SIGMA7)
 };
 template <class T> struct SubArgs {
   SubLevel<T> lv[kMaxSubLevels];
@@ -296,9 +296,8 @@ template <class T> struct SubArgs {
   const int *active;
   float omega, coarse_omega;
   int nu_pre, nu_post, coarse_sweeps;
-  int sig_byte_offset;
 };
-size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size, bool sigma);
+size_t subcycle_smem_bytes(const Grid3 *g, int nlev, bool sigma);
 template <class T> int launch_subcycle(int kind, SubArgs<T> a, int B, cudaStream_t s);
 
 // The small end of a V-cycle as one persistent kernel (subcycle.cu): a level l1 that the

@@ -1004,10 +1004,9 @@ class Engine : public EngineBase {
     int l0 = m_->L - 1;
     while (l0 - 1 >= 1 && n(l0 - 1) <= 4096 && m_->L - (l0 - 1) <= kMaxSubLevels) --l0;
     if (l0 >= m_->L - 1) return -1;
-    int ns[kMaxSubLevels];
-    for (int l = l0; l < m_->L; ++l) ns[l - l0] = (int)n(l);
-    if (subcycle_smem_bytes(ns, m_->L - l0, (int)sizeof(T), k == HFM_OP_SIGMA7) > kSubcycleMaxSmem)
-      return -1;
+    Grid3 gs[kMaxSubLevels];
+    for (int l = l0; l < m_->L; ++l) gs[l - l0] = g(l);
+    if (subcycle_smem_bytes(gs, m_->L - l0, k == HFM_OP_SIGMA7) > kSubcycleMaxSmem) return -1;
     return l0;
   }
 

@@ -23,17 +23,29 @@ namespace {
 
 constexpr int kSubThreads = 512;
 
+// Shared-memory layout of one level (floats): phi and tmp with a one-cell ghost layer on every
+// side, kept zero ((Z+2)(Y+2)(X+2) each), so a stencil reads its neighbours without bounds
+// checks; rhs (Z Y X); for SIGMA7 the level's face coefficients Fx [Z][Y][X+1], Fy
+// [Z][Y+1][X], Fz [Z+1][Y][X] (c_d (s_i + s_j) / 2, wall faces c_d s_i) and the diagonal
+// (Z Y X), formed once per launch from the conductivities in global memory.
+__host__ __device__ __forceinline__ int sub_padded(int Z, int Y, int X) { return (Z + 2) * (Y + 2) * (X + 2); }
+__host__ __device__ __forceinline__ int sub_faces(int Z, int Y, int X) {
+  return Z * Y * (X + 1) + Z * (Y + 1) * X + (Z + 1) * Y * X;
+}
+
+// Index of cell (z, y, x) (each may be -1 .. extent) in a padded field.
+__device__ __forceinline__ int pix(int z, int y, int x, int Y, int X) {
+  return ((z + 1) * (Y + 2) + (y + 1)) * (X + 2) + (x + 1);
+}
+
+// A phi at cell (z, y, x), whose padded index is ip, with its diagonal.  ph is a padded field
+// (ghosts zero); the face coefficients (SIGMA7) and diagonals come from the level's shared
+// arrays.  The products and sums are those the conductivity form evaluates.
 template <int KIND, class T>
-__device__ __forceinline__ float sub_apply(const SubLevel<T> &L, const float *ph, const float *cor,
-                                           const SubLevel<T> *Lc, const T *S, int z, int y, int x,
-                                           float *diag) {
+__device__ __forceinline__ float sub_apply(const SubLevel<T> &L, const float *ph, const float *Fc,
+                                           int z, int y, int x, int ip, int i, float *diag) {
   const int X = L.X, Y = L.Y, Z = L.Z;
-  auto P = [&](int zz, int yy, int xx) -> float {
-    if (zz < 0 || zz >= Z || yy < 0 || yy >= Y || xx < 0 || xx >= X) return 0.f;
-    float v = ph ? ph[(zz * Y + yy) * X + xx] : 0.f;
-    if (cor) v -= cor[((zz >> 1) * Lc->Y + (yy >> 1)) * Lc->X + (xx >> 1)];
-    return v;
-  };
+  const int PX = X + 2, PXY = (X + 2) * (Y + 2);
   if (KIND == HFM_OP_K27) {
     float acc = 0.f;
 #pragma unroll
@@ -43,7 +55,7 @@ __device__ __forceinline__ float sub_apply(const SubLevel<T> &L, const float *ph
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const float wgt = L.k[9 * a + 3 * b + c];
-          if (wgt != 0.f) acc += wgt * P(z + a - 1, y + b - 1, x + c - 1);
+          if (wgt != 0.f) acc += wgt * ph[ip + (a - 1) * PXY + (b - 1) * PX + (c - 1)];
         }
     *diag = L.k[13];
     return acc;
@@ -51,22 +63,18 @@ __device__ __forceinline__ float sub_apply(const SubLevel<T> &L, const float *ph
   if (KIND == HFM_OP_CONST7) {
     const float kz = L.k[0], ky = L.k[1], kx = L.k[2], d = 2.f * (kz + ky + kx);
     *diag = d;
-    return d * P(z, y, x) - kz * (P(z - 1, y, x) + P(z + 1, y, x)) -
-           ky * (P(z, y - 1, x) + P(z, y + 1, x)) - kx * (P(z, y, x - 1) + P(z, y, x + 1));
+    return d * ph[ip] - kz * (ph[ip - PXY] + ph[ip + PXY]) - ky * (ph[ip - PX] + ph[ip + PX]) -
+           kx * (ph[ip - 1] + ph[ip + 1]);
   }
-  const T *sx = S + L.o_sig, *sy = sx + L.n, *sz = sy + L.n;
-  const int i = (z * Y + y) * X + x;
-  const float vx = St<T>::to(sx[i]), vy = St<T>::to(sy[i]), vz = St<T>::to(sz[i]);
-  const float axm = L.cx * (x > 0 ? 0.5f * (vx + St<T>::to(sx[i - 1])) : vx);
-  const float axp = L.cx * (x < X - 1 ? 0.5f * (vx + St<T>::to(sx[i + 1])) : vx);
-  const float aym = L.cy * (y > 0 ? 0.5f * (vy + St<T>::to(sy[i - X])) : vy);
-  const float ayp = L.cy * (y < Y - 1 ? 0.5f * (vy + St<T>::to(sy[i + X])) : vy);
-  const float azm = L.cz * (z > 0 ? 0.5f * (vz + St<T>::to(sz[i - X * Y])) : vz);
-  const float azp = L.cz * (z < Z - 1 ? 0.5f * (vz + St<T>::to(sz[i + X * Y])) : vz);
-  const float pc = P(z, y, x);
-  *diag = axm + axp + aym + ayp + azm + azp;
-  return axm * (pc - P(z, y, x - 1)) + axp * (pc - P(z, y, x + 1)) + aym * (pc - P(z, y - 1, x)) +
-         ayp * (pc - P(z, y + 1, x)) + azm * (pc - P(z - 1, y, x)) + azp * (pc - P(z + 1, y, x));
+  const float *fx = Fc, *fy = fx + Z * Y * (X + 1), *fz = fy + Z * (Y + 1) * X, *dg = fz + (Z + 1) * Y * X;
+  const int ixf = (z * Y + y) * (X + 1) + x, iyf = (z * (Y + 1) + y) * X + x;
+  const float axm = fx[ixf], axp = fx[ixf + 1];
+  const float aym = fy[iyf], ayp = fy[iyf + X];
+  const float azm = fz[i], azp = fz[i + X * Y];
+  const float pc = ph[ip];
+  *diag = dg[i];
+  return axm * (pc - ph[ip - 1]) + axp * (pc - ph[ip + 1]) + aym * (pc - ph[ip - PX]) +
+         ayp * (pc - ph[ip + PX]) + azm * (pc - ph[ip - PXY]) + azp * (pc - ph[ip + PXY]);
 }
 
 // Coordinates of the cells a thread visits in a block-strided loop over a Z x Y x X grid: the
@@ -101,27 +109,44 @@ struct Walk {
   }
 };
 
-// out = phi' + om (f - A phi') / diag with phi' = in - P(cor) (in / cor may be null)
+// out = in + om (f - A in) / diag over the level's cells (in may be null: a zero iterate;
+// in and out are padded fields, only out's interior is written)
 template <int KIND, class T>
-__device__ void sub_sweep(const SubLevel<T> &L, const float *in, const float *cor,
-                          const SubLevel<T> *Lc, const float *f, float *out, float om,
-                          const T *S) {
+__device__ void sub_sweep(const SubLevel<T> &L, const float *in, const float *Fc, const float *f,
+                          float *out, float om, const float *zero_pad) {
+  // a zero iterate: A in = 0 and the diagonal from zero_pad's call (a zero-filled field)
+  const float *ph = in ? in : zero_pad;
   Walk w(threadIdx.x, blockDim.x, L.Y, L.X);
   for (int i = threadIdx.x; i < L.n; i += blockDim.x, w.step(L.Y, L.X)) {
-    const int x = w.x, y = w.y, z = w.z;
+    const int ip = pix(w.z, w.y, w.x, L.Y, L.X);
     float dg;
-    const float ax = sub_apply<KIND, T>(L, in, cor, Lc, S, z, y, x, &dg);
-    float pc = in ? in[i] : 0.f;
-    if (cor) pc -= cor[((z >> 1) * Lc->Y + (y >> 1)) * Lc->X + (x >> 1)];
-    out[i] = pc + om * __fdividef(f[i] - ax, dg);
+    float ax = sub_apply<KIND, T>(L, ph, Fc, w.z, w.y, w.x, ip, i, &dg);
+    if (!in) ax = 0.f;
+    const float pc = in ? in[ip] : 0.f;
+    out[ip] = pc + om * __fdividef(f[i] - ax, dg);
   }
   __syncthreads();
 }
 
-// fc = R(A phi - f): 0.125 times the sum over each coarse cell's eight fine residuals
+// phi -= P(coarse) on the level's interior (nearest prolongation; phi identically zero when
+// `zero`: phi = -P(coarse)).  Both fields padded.
+template <class T>
+__device__ void sub_correct(const SubLevel<T> &L, float *ph, const SubLevel<T> &Lc,
+                            const float *coarse, bool zero) {
+  Walk w(threadIdx.x, blockDim.x, L.Y, L.X);
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x, w.step(L.Y, L.X)) {
+    const int ip = pix(w.z, w.y, w.x, L.Y, L.X);
+    const float c = coarse[pix(w.z >> 1, w.y >> 1, w.x >> 1, Lc.Y, Lc.X)];
+    ph[ip] = zero ? -c : ph[ip] - c;
+  }
+  __syncthreads();
+}
+
+// fc = R(A phi - f): 0.125 times the sum over each coarse cell's eight fine residuals (ph
+// padded, or null for a zero iterate)
 template <int KIND, class T>
-__device__ void sub_resid_restrict(const SubLevel<T> &L, const float *ph, const float *f,
-                                   const SubLevel<T> &Lc, float *fc, const T *S) {
+__device__ void sub_resid_restrict(const SubLevel<T> &L, const float *ph, const float *Fc,
+                                   const float *f, const SubLevel<T> &Lc, float *fc) {
   Walk w(threadIdx.x, blockDim.x, Lc.Y, Lc.X);
   for (int j = threadIdx.x; j < Lc.n; j += blockDim.x, w.step(Lc.Y, Lc.X)) {
     const int xc = w.x, yc = w.y, zc = w.z;
@@ -133,8 +158,10 @@ __device__ void sub_resid_restrict(const SubLevel<T> &L, const float *ph, const 
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
           const int z = 2 * zc + a, y = 2 * yc + b, x = 2 * xc + c;
+          const int i = (z * L.Y + y) * L.X + x;
           float dg;
-          sum += sub_apply<KIND, T>(L, ph, nullptr, nullptr, S, z, y, x, &dg) - f[(z * L.Y + y) * L.X + x];
+          const float ax = ph ? sub_apply<KIND, T>(L, ph, Fc, z, y, x, pix(z, y, x, L.Y, L.X), i, &dg) : 0.f;
+          sum += ax - f[i];
         }
     fc[j] = 0.125f * sum;
   }
@@ -152,21 +179,52 @@ template <> __device__ __forceinline__ __half ld_l2<__half>(const __half *p) {
   return __ushort_as_half(__ldcg(reinterpret_cast<const unsigned short *>(p)));
 }
 
+// The face coefficients and diagonals of a SIGMA7 level of instance `inst` into its shared
+// arrays, from the conductivities in global memory, as the conductivity form forms them.
+template <class T>
+__device__ void sub_faces_init(const SubLevel<T> &L, int64_t inst, float *Fc) {
+  const int X = L.X, Y = L.Y, Z = L.Z;
+  const int64_t g = inst * (int64_t)L.n;
+  const T *sx = L.sx + g, *sy = L.sy + g, *sz = L.sz + g;
+  float *fx = Fc, *fy = fx + Z * Y * (X + 1), *fz = fy + Z * (Y + 1) * X;
+  const int nx = Z * Y * (X + 1), ny = Z * (Y + 1) * X, nz = (Z + 1) * Y * X;
+  for (int k = threadIdx.x; k < nx; k += blockDim.x) {
+    const int i = k % (X + 1), row = k / (X + 1);
+    const float a = i > 0 ? St<T>::to(sx[row * X + i - 1]) : 0.f, b = i < X ? St<T>::to(sx[row * X + i]) : 0.f;
+    fx[k] = L.cx * (i == 0 ? b : (i == X ? a : 0.5f * (b + a)));
+  }
+  for (int k = threadIdx.x; k < ny; k += blockDim.x) {
+    const int x = k % X, t = k / X, j = t % (Y + 1), z = t / (Y + 1);
+    const int c0 = (z * Y + j) * X + x;
+    const float a = j > 0 ? St<T>::to(sy[c0 - X]) : 0.f, b = j < Y ? St<T>::to(sy[c0]) : 0.f;
+    fy[k] = L.cy * (j == 0 ? b : (j == Y ? a : 0.5f * (b + a)));
+  }
+  for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+    const int yx = k % (Y * X), kz = k / (Y * X);
+    const float a = kz > 0 ? St<T>::to(sz[(kz - 1) * Y * X + yx]) : 0.f, b = kz < Z ? St<T>::to(sz[kz * Y * X + yx]) : 0.f;
+    fz[k] = L.cz * (kz == 0 ? b : (kz == Z ? a : 0.5f * (b + a)));
+  }
+  __syncthreads();
+  float *dg = fz + nz;
+  Walk w(threadIdx.x, blockDim.x, Y, X);
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x, w.step(Y, X)) {
+    const int ixf = (w.z * Y + w.y) * (X + 1) + w.x, iyf = (w.z * (Y + 1) + w.y) * X + w.x;
+    dg[i] = fx[ixf] + fx[ixf + 1] + fy[iyf] + fy[iyf + X] + fz[i] + fz[i + X * Y];
+  }
+}
+
 // The coarse-end V-cycle of one instance with the block's shared memory `sub_smem`.  COH:
 // the right-hand side was written by other blocks of the same launch (read through L2).
 template <int KIND, class T, bool COH>
 __device__ void subcycle_body(const SubArgs<T> &a, int64_t inst, unsigned char *sub_smem) {
   float *F = reinterpret_cast<float *>(sub_smem);
-  T *S = reinterpret_cast<T *>(sub_smem + a.sig_byte_offset);
   const int nl = a.nlev;
-  for (int l = 0; l < nl && KIND == HFM_OP_SIGMA7; ++l) {
+  // zero every padded field (ghosts stay zero: sweeps write interiors only), faces, rhs
+  for (int l = 0; l < nl; ++l) {
     const SubLevel<T> &L = a.lv[l];
-    const int64_t g = inst * (int64_t)L.n;
-    for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
-      S[L.o_sig + i] = L.sx[g + i];
-      S[L.o_sig + L.n + i] = L.sy[g + i];
-      S[L.o_sig + 2 * L.n + i] = L.sz[g + i];
-    }
+    const int np = 2 * sub_padded(L.Z, L.Y, L.X);
+    for (int i = threadIdx.x; i < np; i += blockDim.x) F[L.o_phi + i] = 0.f;
+    if (KIND == HFM_OP_SIGMA7) sub_faces_init<T>(L, inst, F + L.o_face);
   }
   for (int i = threadIdx.x; i < a.lv[0].n; i += blockDim.x) {
     const T *src = a.rhs + inst * (int64_t)a.lv[0].n + i;
@@ -180,27 +238,28 @@ __device__ void subcycle_body(const SubArgs<T> &a, int64_t inst, unsigned char *
   for (int l = 0; l < nl - 1; ++l) {
     const SubLevel<T> &L = a.lv[l];
     float *buf[2] = {F + L.o_phi, F + L.o_tmp};
-    const float *f = F + L.o_rhs;
+    const float *f = F + L.o_rhs, *Fc = F + L.o_face;
     int c = 0;
     for (int k = 0; k < a.nu_pre; ++k) {
-      sub_sweep<KIND, T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, f, buf[c ^ 1], a.omega, S);
+      sub_sweep<KIND, T>(L, k == 0 ? nullptr : buf[c], Fc, f, buf[c ^ 1], a.omega, buf[c]);
       c ^= 1;
     }
     cur[l] = c;
     zero[l] = a.nu_pre == 0;
-    sub_resid_restrict<KIND, T>(L, zero[l] ? nullptr : buf[c], f, a.lv[l + 1], F + a.lv[l + 1].o_rhs, S);
+    sub_resid_restrict<KIND, T>(L, zero[l] ? nullptr : buf[c], Fc, f, a.lv[l + 1], F + a.lv[l + 1].o_rhs);
   }
   // coarsest: coarse_sweeps sweeps from zero; a level of at most 64 cells (4^3, 3^3) on one
-  // warp, two cells a lane with their coordinates computed once, __syncwarp() between the
+  // warp, two cells a lane with their indices computed once, __syncwarp() between the
   // sweeps instead of a block barrier (the per-cell arithmetic is sub_sweep's)
   {
     const SubLevel<T> &L = a.lv[nl - 1];
     float *buf[2] = {F + L.o_phi, F + L.o_tmp};
+    const float *Fc = F + L.o_face;
     int c = 0;
     if (L.n <= 64 && a.coarse_sweeps > 0) {
       if (threadIdx.x < 32) {
         const float *f = F + L.o_rhs;
-        int zz[2], yy[2], xx[2];
+        int zz[2], yy[2], xx[2], ipp[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
           const int i = threadIdx.x + 32 * q;
@@ -208,6 +267,7 @@ __device__ void subcycle_body(const SubArgs<T> &a, int64_t inst, unsigned char *
           const int t = i / L.X;
           yy[q] = t % L.Y;
           zz[q] = t / L.Y;
+          ipp[q] = pix(zz[q], yy[q], xx[q], L.Y, L.X);
         }
         for (int k = 0; k < a.coarse_sweeps; ++k) {
           const float *in = k == 0 ? nullptr : buf[c];
@@ -217,9 +277,10 @@ __device__ void subcycle_body(const SubArgs<T> &a, int64_t inst, unsigned char *
             const int i = threadIdx.x + 32 * q;
             if (i < L.n) {
               float dg;
-              const float ax = sub_apply<KIND, T>(L, in, nullptr, nullptr, S, zz[q], yy[q], xx[q], &dg);
-              const float pc = in ? in[i] : 0.f;
-              out[i] = pc + a.coarse_omega * __fdividef(f[i] - ax, dg);
+              const float ax = sub_apply<KIND, T>(L, in ? in : buf[c], Fc, zz[q], yy[q], xx[q], ipp[q], i, &dg);
+              const float axv = in ? ax : 0.f;
+              const float pc = in ? in[ipp[q]] : 0.f;
+              out[ipp[q]] = pc + a.coarse_omega * __fdividef(f[i] - axv, dg);
             }
           }
           __syncwarp();
@@ -231,36 +292,34 @@ __device__ void subcycle_body(const SubArgs<T> &a, int64_t inst, unsigned char *
       __syncthreads();
     } else {
       for (int k = 0; k < a.coarse_sweeps; ++k) {
-        sub_sweep<KIND, T>(L, k == 0 ? nullptr : buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1],
-                           a.coarse_omega, S);
+        sub_sweep<KIND, T>(L, k == 0 ? nullptr : buf[c], Fc, F + L.o_rhs, buf[c ^ 1], a.coarse_omega, buf[c]);
         c ^= 1;
       }
     }
-    if (a.coarse_sweeps == 0) {
-      for (int i = threadIdx.x; i < L.n; i += blockDim.x) buf[0][i] = 0.f;
-      __syncthreads();
-    }
     cur[nl - 1] = c;
   }
-  // up: prolongation + correction with the first post-sweep, then the other post-sweeps
+  // up: prolongation + correction (in place), then the post-sweeps
   const int post = a.nu_post > 0 ? a.nu_post : 1;
   for (int l = nl - 2; l >= 0; --l) {
     const SubLevel<T> &L = a.lv[l];
     const SubLevel<T> &Lc = a.lv[l + 1];
     float *buf[2] = {F + L.o_phi, F + L.o_tmp};
     const float *coarse = F + (cur[l + 1] ? Lc.o_tmp : Lc.o_phi);
+    const float *Fc = F + L.o_face;
     int c = cur[l];
+    sub_correct<T>(L, buf[c], Lc, coarse, zero[l]);
     for (int k = 0; k < post; ++k) {
       const float om = a.nu_post == 0 ? 0.f : a.omega;
-      if (k == 0) sub_sweep<KIND, T>(L, zero[l] ? nullptr : buf[c], coarse, &Lc, F + L.o_rhs, buf[c ^ 1], om, S);
-      else sub_sweep<KIND, T>(L, buf[c], nullptr, nullptr, F + L.o_rhs, buf[c ^ 1], om, S);
+      sub_sweep<KIND, T>(L, buf[c], Fc, F + L.o_rhs, buf[c ^ 1], om, buf[c]);
       c ^= 1;
     }
     cur[l] = c;
   }
-  const float *res = F + (cur[0] ? a.lv[0].o_tmp : a.lv[0].o_phi);
-  for (int i = threadIdx.x; i < a.lv[0].n; i += blockDim.x)
-    a.out[inst * (int64_t)a.lv[0].n + i] = St<T>::from(res[i]);
+  const SubLevel<T> &L0 = a.lv[0];
+  const float *res = F + (cur[0] ? L0.o_tmp : L0.o_phi);
+  Walk w(threadIdx.x, blockDim.x, L0.Y, L0.X);
+  for (int i = threadIdx.x; i < L0.n; i += blockDim.x, w.step(L0.Y, L0.X))
+    a.out[inst * (int64_t)L0.n + i] = St<T>::from(res[pix(w.z, w.y, w.x, L0.Y, L0.X)]);
 }
 
 template <int KIND, class T>
@@ -273,14 +332,14 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(const __grid_constant_
 
 }  // namespace
 
-size_t subcycle_smem_bytes(const int *n, int nlev, int elem_size, bool sigma) {
-  size_t f = 0, sg = 0;
+size_t subcycle_smem_bytes(const Grid3 *g, int nlev, bool sigma) {
+  size_t f = 0;
   for (int l = 0; l < nlev; ++l) {
-    f += (size_t)3 * n[l];
-    if (sigma) sg += (size_t)3 * n[l];
+    const int Z = g[l].Z, Y = g[l].Y, X = g[l].X, n = Z * Y * X;
+    f += (size_t)2 * sub_padded(Z, Y, X) + n;
+    if (sigma) f += (size_t)sub_faces(Z, Y, X) + n;
   }
-  const size_t fbytes = ((f * 4 + 15) / 16) * 16;
-  return fbytes + sg * (size_t)elem_size;
+  return ((f * 4 + 15) / 16) * 16;
 }
 
 template <int KIND, class T>
@@ -293,25 +352,23 @@ int go_subcycle(const SubArgs<T> &a, int B, size_t smem, cudaStream_t s) {
   return HFM_OK;
 }
 
-// Shared-memory layout of the coarse-end cycle: float fields of every level, then (SIGMA7)
-// the conductivities.  Returns the bytes, 0 if they exceed the limit.
+// Shared-memory layout of the coarse-end cycle, level after level: phi and tmp (padded), rhs,
+// and for SIGMA7 the face arrays and the diagonal.  Returns the bytes, 0 if they exceed the
+// limit.
 template <class T> size_t layout_sub(int kind, SubArgs<T> &a) {
-  int n[kMaxSubLevels];
-  for (int l = 0; l < a.nlev; ++l) n[l] = a.lv[l].n;
+  Grid3 g[kMaxSubLevels];
   int off = 0;
   for (int l = 0; l < a.nlev; ++l) {
-    a.lv[l].o_phi = off;
-    a.lv[l].o_tmp = off + n[l];
-    a.lv[l].o_rhs = off + 2 * n[l];
-    off += 3 * n[l];
+    SubLevel<T> &L = a.lv[l];
+    g[l] = Grid3{L.Z, L.Y, L.X};
+    const int np = sub_padded(L.Z, L.Y, L.X);
+    L.o_phi = off;
+    L.o_tmp = off + np;
+    L.o_rhs = off + 2 * np;
+    L.o_face = L.o_rhs + L.n;
+    off = L.o_face + (kind == HFM_OP_SIGMA7 ? sub_faces(L.Z, L.Y, L.X) + L.n : 0);
   }
-  a.sig_byte_offset = ((off * 4 + 15) / 16) * 16;
-  int soff = 0;
-  for (int l = 0; l < a.nlev; ++l) {
-    a.lv[l].o_sig = soff;
-    soff += 3 * n[l];
-  }
-  const size_t smem = subcycle_smem_bytes(n, a.nlev, (int)sizeof(T), kind == HFM_OP_SIGMA7);
+  const size_t smem = subcycle_smem_bytes(g, a.nlev, kind == HFM_OP_SIGMA7);
   return smem > kSubcycleMaxSmem ? 0 : smem;
 }
 
@@ -510,24 +567,8 @@ template int launch_small<__half>(int, SmallArgs<__half>, int, cudaStream_t);
 
 template <class T>
 int launch_subcycle(int kind, SubArgs<T> a, int B, cudaStream_t s) {
-  int n[kMaxSubLevels];
-  for (int l = 0; l < a.nlev; ++l) n[l] = a.lv[l].n;
-  // shared-memory layout: float fields of every level, then (SIGMA7) the conductivities
-  int off = 0;
-  for (int l = 0; l < a.nlev; ++l) {
-    a.lv[l].o_phi = off;
-    a.lv[l].o_tmp = off + n[l];
-    a.lv[l].o_rhs = off + 2 * n[l];
-    off += 3 * n[l];
-  }
-  a.sig_byte_offset = ((off * 4 + 15) / 16) * 16;
-  int soff = 0;
-  for (int l = 0; l < a.nlev; ++l) {
-    a.lv[l].o_sig = soff;
-    soff += 3 * n[l];
-  }
-  const size_t smem = subcycle_smem_bytes(n, a.nlev, (int)sizeof(T), kind == HFM_OP_SIGMA7);
-  if (smem > kSubcycleMaxSmem) return fail(HFM_ERR_BAD_ARG, "subcycle: levels exceed shared memory");
+  const size_t smem = layout_sub<T>(kind, a);
+  if (!smem) return fail(HFM_ERR_BAD_ARG, "subcycle: levels exceed shared memory");
   switch (kind) {
     case HFM_OP_SIGMA7: return go_subcycle<HFM_OP_SIGMA7, T>(a, B, smem, s);
     case HFM_OP_CONST7: return go_subcycle<HFM_OP_CONST7, T>(a, B, smem, s);
