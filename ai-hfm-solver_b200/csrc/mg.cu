@@ -839,10 +839,15 @@ struct Level {
 };
 
 // A level of a handle holds FACE7 arrays: 16-bit SIGMA7 storage, the option not set, and a
-// grid the face plane-marching kernel takes.
+// grid the face plane-marching kernel takes, or a level of more than 4096 cells the
+// register-queue kernels take (the levels between the plane-marching ones and the fused
+// coarse cycle, which forms its own faces in shared memory).
 static bool face_level(const hfm_mg_config &c, Grid3 g) {
-  return c.op_kind == HFM_OP_SIGMA7 && (c.storage == HFM_BF16 || c.storage == HFM_F16) &&
-         !(c.options & HFM_OPT_NO_FACES) && tma_eligible(HFM_OP_FACE7, g, FAST_SMOOTH, nullptr, 0, 2);
+  if (c.op_kind != HFM_OP_SIGMA7 || (c.storage != HFM_BF16 && c.storage != HFM_F16) ||
+      (c.options & HFM_OPT_NO_FACES))
+    return false;
+  return tma_eligible(HFM_OP_FACE7, g, FAST_SMOOTH, nullptr, 0, 2) ||
+         (fast_eligible(HFM_OP_FACE7, g, false) && g.n() > 4096);
 }
 
 class EngineBase {

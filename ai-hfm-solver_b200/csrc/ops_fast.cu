@@ -209,9 +209,15 @@ __global__ void __launch_bounds__(kFastThreads, R == 1 ? 4 : 2)
     cz = a.op.c[0] * s;
     cy = a.op.c[1] * s;
     cx = a.op.c[2] * s;
-    sx = (const T *)a.op.coef[0] + inst * a.op.coef_stride;
-    sy = (const T *)a.op.coef[1] + inst * a.op.coef_stride;
-    sz = (const T *)a.op.coef[2] + inst * a.op.coef_stride;
+    if (KIND == HFM_OP_FACE7) {  // instance strides follow from the extents
+      sx = (const T *)a.op.coef[0] + inst * face7_nx(Z, Y, X);
+      sy = (const T *)a.op.coef[1] + inst * face7_ny(Z, Y, X);
+      sz = (const T *)a.op.coef[2] + inst * face7_nz(Z, Y, X);
+    } else {
+      sx = (const T *)a.op.coef[0] + inst * a.op.coef_stride;
+      sy = (const T *)a.op.coef[1] + inst * a.op.coef_stride;
+      sz = (const T *)a.op.coef[2] + inst * a.op.coef_stride;
+    }
   }
 
   // per-row z queue: phi' at z-1, z, z+1; for SIGMA7 also sigma_z at z and the z- face
@@ -235,6 +241,12 @@ __global__ void __launch_bounds__(kFastThreads, R == 1 ? 4 : 2)
 #pragma unroll
         for (int e = 0; e < 4; ++e) azlo[r].v[e] = cz * szc[r].v[e];
       }
+    } else if (KIND == HFM_OP_FACE7) {
+      // the z face below plane z0 (wall faces included in the array), times the scale
+      const float s = a.op.scale;
+      const F4 fz = rin[r] ? ld4<T>(sz + (int64_t)z0 * plane + (int64_t)yr[r] * X + x0) : F4{{0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) azlo[r].v[e] = s * fz.v[e];
     }
   }
   double acc = 0.0;
@@ -262,6 +274,32 @@ __global__ void __launch_bounds__(kFastThreads, R == 1 ? 4 : 2)
                     ky * (pym.v[e] + pyp.v[e]) - kx * (xm + xp);
           dg.v[e] = dconst;
         }
+      } else if (KIND == HFM_OP_FACE7) {
+        // stored faces (scale applied here): the x faces of the 4 cells and the one right of
+        // the last, the y faces below and above, the z face above (the one below is carried)
+        const float s = a.op.scale;
+        const int64_t rx = ((int64_t)z * Y + y) * (X + 8) + x0;
+        const int64_t ry = ((int64_t)z * (Y + 1) + y) * X + x0;
+        const F4 zero4{{0.f, 0.f, 0.f, 0.f}};
+        const F4 fx = in ? ld4<T>(sx + rx) : zero4;
+        const float fx4 = in ? St<T>::ld(sx + rx + 4) : 0.f;
+        const F4 fyl = in ? ld4<T>(sy + ry) : zero4;
+        const F4 fyh = in ? ld4<T>(sy + ry + X) : zero4;
+        const F4 fzh = in ? ld4<T>(sz + off + plane) : zero4;
+        F4 azhi;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float axm = s * fx.v[e], axp = s * (e == 3 ? fx4 : fx.v[e + 1]);
+          const float aym = s * fyl.v[e], ayp = s * fyh.v[e];
+          azhi.v[e] = s * fzh.v[e];
+          const float xm = e == 0 ? pl : pc[r].v[e - 1];
+          const float xp = e == 3 ? pr : pc[r].v[e + 1];
+          const float p = pc[r].v[e];
+          Ax.v[e] = axm * (p - xm) + axp * (p - xp) + aym * (p - pym.v[e]) + ayp * (p - pyp.v[e]) +
+                    azlo[r].v[e] * (p - pm[r].v[e]) + azhi.v[e] * (p - pp[r].v[e]);
+          dg.v[e] = ((axm + axp) + (aym + ayp)) + (azlo[r].v[e] + azhi.v[e]);
+        }
+        azlo[r] = azhi;
       } else {
         F4 sxc = in ? ld4<T>(sx + off) : F4{{1.f, 1.f, 1.f, 1.f}};
         float sxl, sxr;
@@ -483,7 +521,8 @@ dim3 fast_grid(FastArgs<T> &a, int B, int rows, bool even_chunks, int per_sm) {
 }  // namespace
 
 bool fast_eligible(int kind, Grid3 g, bool restrict_mode) {
-  if (kind != HFM_OP_CONST7 && kind != HFM_OP_SIGMA7 && kind != HFM_OP_K27) return false;
+  if (kind != HFM_OP_CONST7 && kind != HFM_OP_SIGMA7 && kind != HFM_OP_K27 && kind != HFM_OP_FACE7)
+    return false;
   if ((g.X & 3) || g.X < 4) return false;
   if (restrict_mode) {
     if (kind == HFM_OP_K27) return false;
@@ -555,6 +594,8 @@ int fast_launch(int kind, int mode, const DevOp &op, const PhiSrc<T> &phi, const
   }
     if (kind == HFM_OP_CONST7) {
       HFM_FAST7(HFM_OP_CONST7)
+    } else if (kind == HFM_OP_FACE7) {
+      HFM_FAST7(HFM_OP_FACE7)
     } else {
       HFM_FAST7(HFM_OP_SIGMA7)
     }

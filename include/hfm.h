@@ -465,9 +465,10 @@ typedef struct {
  * sweeps its 2^3 level twice; Anisotropic_3d_Multigrid_7point.ipynb:424-432 once) */
 #define HFM_OPT_SAWTOOTH_COARSE_SWEEPS 4
 /* options: 16-bit SIGMA7 handles keep the per-cell conductivities on every level (by default
- * the levels the plane-marching kernels take - X >= 48, Y >= 16 - also hold the FACE7 face
- * arrays of their operator, formed from float32 conductivities on the fine level, and run
- * the face kernels there: each face rounded once to the storage type instead of forming
+ * the levels the plane-marching kernels take - X >= 48, Y >= 16 - and the levels of more
+ * than 4096 cells the register-queue kernels take (X a multiple of 4) also hold the FACE7
+ * face arrays of their operator, formed from float32 conductivities on the fine level, and
+ * run the face kernels there: each face rounded once to the storage type instead of forming
  * faces from rounded conductivities) */
 #define HFM_OPT_NO_FACES 8
 /* options: run the small end of a V-cycle - the level above the fused coarse cycle when the

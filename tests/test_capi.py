@@ -142,9 +142,11 @@ def test_face7_host_calls(lib, pkg):
     with_faces = lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1)
     cfg.options = L.OPT_NO_FACES
     without = lib.hfm_mg_footprint_bytes(C.byref(cfg), 128, 128, 128, 1)
-    # faces on the 128^3 and 64^3 levels (X >= 48): 3 arrays of about n cells, 2 bytes each
+    # faces on the 128^3 and 64^3 levels (plane-marching kernels, X >= 48) and the 32^3 level
+    # (register-queue kernels, more than 4096 cells): 3 arrays of about n cells, 2 bytes each
     extra = 2 * (128 * 128 * 136 + 128 * 129 * 128 + 129 * 128 * 128 +
-                 64 * 64 * 72 + 64 * 65 * 64 + 65 * 64 * 64)
+                 64 * 64 * 72 + 64 * 65 * 64 + 65 * 64 * 64 +
+                 32 * 32 * 40 + 32 * 33 * 32 + 33 * 32 * 32)
     assert with_faces - without == extra
     cfg.options = 0
     cfg.storage = L.F32
