@@ -594,21 +594,30 @@ int go_face(const TmaArgs<T> &a, dim3 grid, cudaStream_t s) {
   return HFM_OK;
 }
 
-// Grid (plane tiles, z chunks, instances): z chunks sized for about four waves (of 4 resident
-// blocks per SM for float32, 3 for 16-bit storage, the sizing the 16-bit kernels were tuned
-// with), at least 2 planes each.  (Eight waves, which shrink the partly filled last wave,
-// measured slower: every chunk re-reads its two halo planes and refills its pipeline.)
+// Grid (plane tiles, z chunks, instances).  The z chunk length (even, at least 2) minimises
+// (rounds of resident blocks) x (planes a block marches + 2 for its two halo planes and the
+// pipeline fill): a last round that is only partly filled costs a whole round, and every
+// chunk re-reads its halo planes.  (A fixed four waves left the 64^3 levels of 64 instances
+// at 3.03 waves - a fourth round for 3 % of the blocks.)
 template <class T>
 dim3 tma_grid(TmaArgs<T> &a, Grid3 g, int B) {
   constexpr int TY = Geo<T>::TY;
   a.tiles_x = (g.X + TX - 1) / TX;
   const int tiles = a.tiles_x * ((g.Y + TY - 1) / TY);
-  const int64_t slots = (int64_t)sm_count() * (sizeof(T) == 4 ? 4 : 3) * 4;
-  int64_t chunks = (slots + (int64_t)tiles * B - 1) / ((int64_t)tiles * B);
-  int zc = (int)((g.Z + chunks - 1) / chunks);
-  if (zc < 2) zc = 2;
-  if (zc & 1) ++zc;
-  if (zc > g.Z) zc = g.Z;
+  const int64_t per = (int64_t)tiles * B;
+  const int64_t cap = (int64_t)sm_count() * Geo<T>::MINB;
+  int zc = g.Z;
+  int64_t best = -1;
+  for (int c = 2; c < g.Z + 2; c += 2) {
+    const int zcc = c > g.Z ? g.Z : c;
+    const int64_t chunks = (g.Z + zcc - 1) / zcc;
+    const int64_t cost = ((per * chunks + cap - 1) / cap) * (zcc + 2);
+    if (best < 0 || cost <= best) {
+      best = cost;
+      zc = zcc;
+    }
+    if (zcc == g.Z) break;
+  }
   a.zc = zc;
   return dim3(tiles, (g.Z + zc - 1) / zc, B);
 }
