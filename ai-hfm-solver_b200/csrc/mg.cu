@@ -290,14 +290,6 @@ __global__ void k_ir_update(double *__restrict__ x64, const float *__restrict__ 
   HFM_END_ITEMS
 }
 
-// A new inner solve starts from x_in = 0.
-__global__ void k_ir_start_inner(float *__restrict__ xin, Items it, const SlotState *st,
-                                 const int *active) {
-  HFM_FOR_ITEMS(it, active[slot] && st[slot].inner_cycles == 0)
-  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) xin[base + i] = 0.f;
-  HFM_END_ITEMS
-}
-
 // float64 outer residual r = b - A x (sigma / kernel read as float32), written as the float32
 // right-hand side of the next inner solve (and, when `rstore` is given, as the 16-bit copy the
 // inner cycle reads), with partial sums of r^2.
@@ -743,20 +735,24 @@ __global__ void k_cg_p(const TZ *__restrict__ z, float *__restrict__ p, Items it
 // x += alpha p, r -= alpha q, partial sums of r^2; with `rstore` also the storage-type copy of
 // the new r that the next iteration's cycle reads (bf16 refinement: no separate conversion).
 // alpha = rz_new / p.q, with p.q summed here from the slot's nblk_pq partials of the operator
-// pass (a buffer of its own: this kernel writes its r^2 partials into `partials`).
+// pass (a buffer of its own: this kernel writes its r^2 partials into `partials`).  With
+// `fresh` (refinement) the first iteration of an inner solve starts from x = 0: x = alpha p,
+// x not read (no separate zeroing pass).
 template <class T>
 __global__ void k_cg_xr(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
                         const float *__restrict__ q, T *__restrict__ rstore, Items it,
                         const double *__restrict__ pq_part, int nblk_pq,
-                        const double *__restrict__ rz_new, double *partials, const int *active) {
+                        const double *__restrict__ rz_new, double *partials, const int *active,
+                        const SlotState *st, int fresh) {
   HFM_FOR_ITEMS(it, active[slot])
   const double pq = slot_sum(pq_part + (int64_t)slot * nblk_pq, nblk_pq);
   const float alpha = (pq != 0.0) ? (float)(rz_new[slot] / pq) : 0.f;
+  const bool zx = fresh && st[slot].inner_cycles == 0;
   double acc = 0.0;
   if (v4) {
     for (int64_t i = lo + 4 * threadIdx.x; i < hi; i += 4 * blockDim.x) {
       const int64_t k = base + i;
-      float4 xv = ld4v<float>(x + k), rv = ld4v<float>(r + k);
+      float4 xv = zx ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4v<float>(x + k), rv = ld4v<float>(r + k);
       const float4 pv = ld4v<float>(p + k), qv = ld4v<float>(q + k);
       xv.x += alpha * pv.x; xv.y += alpha * pv.y; xv.z += alpha * pv.z; xv.w += alpha * pv.w;
       rv.x -= alpha * qv.x; rv.y -= alpha * qv.y; rv.z -= alpha * qv.z; rv.w -= alpha * qv.w;
@@ -768,7 +764,7 @@ __global__ void k_cg_xr(float *__restrict__ x, float *__restrict__ r, const floa
   } else {
     for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
       const int64_t k = base + i;
-      x[k] += alpha * p[k];
+      x[k] = (zx ? 0.f : x[k]) + alpha * p[k];
       const float rv = r[k] - alpha * q[k];
       r[k] = rv;
       if (rstore) rstore[k] = St<T>::from(rv);
@@ -1328,8 +1324,6 @@ class Engine : public EngineBase {
     k_check_outer<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
                                     m_->cfg.tol, m_->cfg.max_cycles, m_->wait_fail);
     HFM_CHECK_LAUNCH("k_check_outer");
-    k_ir_start_inner<<<ib, 256, 0, s>>>(m_->cg[0], it, m_->state, m_->active);
-    HFM_CHECK_LAUNCH("k_ir_start_inner");
     return HFM_OK;
   }
 
@@ -1384,7 +1378,8 @@ class Engine : public EngineBase {
       return st;
     // x += alpha p ; r -= alpha q ; ||r||  (alpha from rz_new and the p . q partials)
     k_cg_xr<T><<<ib, 256, 0, s>>>(x, r, p, q, fused_rhs() ? rhs(0) : nullptr, it, m_->partials2,
-                                  nblk_pq, m_->scal, m_->partials, m_->active);
+                                  nblk_pq, m_->scal, m_->partials, m_->active, m_->state,
+                                  ir ? 1 : 0);
     HFM_CHECK_LAUNCH("k_cg_xr");
     if (!ir) return check(vb, 0, s, m_->scal);
     k_check_inner<<<B, 256, 0, s>>>(m_->partials, vb, m_->state, m_->active, m_->outer,
