@@ -146,6 +146,7 @@ SIGNATURES = {
     "hfm_outer_residual2d": (I, [P, P, P, I, P, I, I, I, U, P, P, P]),
     "hfm_update2d": (I, [P, I, P, F, I64, P]),
     "hfm_coarse_jacobi2d": (I, [I, P, P, P, I, I, I, F, I, U, P]),
+    "hfm_subcycle2d": (I, [I, P, P, P, I, I, I, I, F, I, I, I, U, P]),
     "hfm_mean_subtract2d": (I, [P, I, I64, P]),
     "hfm_kolmogorov_stage": (I, [P, P, P, P, P, P, I, I, F, F, F, F, F, F, P]),
     "hfm_kolmogorov_divergence": (I, [P, P, P, I, I, F, F, P]),

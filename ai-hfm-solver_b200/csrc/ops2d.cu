@@ -213,6 +213,142 @@ __global__ void __launch_bounds__(kT2) k2_coarse_jacobi(W9 w, const T *__restric
   for (int i = threadIdx.x; i < n; i += blockDim.x) out[b * n + i] = St<T>::from(a[i]);
 }
 
+// ------------------------------------------------------------------ fused coarse cycle
+// The V-cycle of the levels of at most 4096 cells (64^2 .. 4^2 of a 512^2 grid) in one
+// launch: one 1024-thread block per instance, every field of those levels in shared memory
+// (float32), sweeps separated by __syncthreads().  The steps and their arithmetic are those
+// of the per-level kernels (Multigrid2D._cycle): nu_pre sweeps from zero, residual + 2 x 2
+// averaging restriction (0.25 x the sum), recursion, `sweeps` sweeps from zero on the
+// coarsest level, then the nearest-prolongation correction phi - P w and nu_post sweeps;
+// iterates stay in float32 between sweeps (the per-level path stores them in the storage
+// type, so float32 storage gives the same bits).
+constexpr int kSub2Levels = 8;
+constexpr int kSub2Threads = 1024;
+struct Sub2Args {
+  W9 w[kSub2Levels];
+  int Y[kSub2Levels], X[kSub2Levels];
+  int nlev, periodic, nu_pre, nu_post, coarse_sweeps;
+  float omega;
+};
+
+__device__ __forceinline__ float apply9(const W9 &w, const float *ph, int y, int x, int Y, int X,
+                                        int periodic, float *centre) {
+  float acc = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      int yy = y + a - 1, xx = x + c - 1;
+      float v;
+      if (periodic) {
+        yy = yy < 0 ? yy + Y : (yy >= Y ? yy - Y : yy);
+        xx = xx < 0 ? xx + X : (xx >= X ? xx - X : xx);
+        v = ph[yy * X + xx];
+      } else {
+        v = (yy < 0 || yy >= Y || xx < 0 || xx >= X) ? 0.f : ph[yy * X + xx];
+      }
+      if (a == 1 && c == 1) *centre = v;
+      acc += w.w[3 * a + c] * v;
+    }
+  return acc;
+}
+
+// out = in + omega (f - A in) / w[4] on level (Y, X); in == nullptr: a zero iterate
+__device__ void sub2_sweep(const W9 &w, const float *in, const float *f, float *out, int Y, int X,
+                           int periodic, float omega) {
+  const int n = Y * X;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    float pc = 0.f, ax = 0.f;
+    if (in) ax = apply9(w, in, i / X, i % X, Y, X, periodic, &pc);
+    out[i] = pc + omega * (f[i] - ax) / w.w[4];
+  }
+  __syncthreads();
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSub2Threads) k2_subcycle(const __grid_constant__ Sub2Args a,
+                                                            const T *__restrict__ rhs,
+                                                            T *__restrict__ out) {
+  extern __shared__ float sm2[];
+  const int64_t b = blockIdx.x;
+  const int nl = a.nlev;
+  int off[kSub2Levels];
+  int o = 0;
+  for (int l = 0; l < nl; ++l) {
+    off[l] = o;
+    o += 3 * a.Y[l] * a.X[l];
+  }
+  // level l: phi at off, tmp at off + n, rhs at off + 2 n
+  const int n0 = a.Y[0] * a.X[0];
+  for (int i = threadIdx.x; i < n0; i += blockDim.x) sm2[off[0] + 2 * n0 + i] = St<T>::to(rhs[b * n0 + i]);
+  __syncthreads();
+  int cur[kSub2Levels];
+  for (int l = 0; l < nl - 1; ++l) {
+    const int Y = a.Y[l], X = a.X[l], n = Y * X;
+    float *buf[2] = {sm2 + off[l], sm2 + off[l] + n};
+    const float *f = sm2 + off[l] + 2 * n;
+    int c = 0;
+    sub2_sweep(a.w[l], nullptr, f, buf[0], Y, X, a.periodic, a.omega);
+    for (int k = 1; k < a.nu_pre; ++k) {
+      sub2_sweep(a.w[l], buf[c], f, buf[c ^ 1], Y, X, a.periodic, a.omega);
+      c ^= 1;
+    }
+    cur[l] = c;
+    // coarse rhs = 0.25 * sum over the 2 x 2 fine cells of (A phi - f)
+    const int Yc = a.Y[l + 1], Xc = a.X[l + 1];
+    float *fc = sm2 + off[l + 1] + 2 * Yc * Xc;
+    for (int j = threadIdx.x; j < Yc * Xc; j += blockDim.x) {
+      const int yc = j / Xc, xc = j % Xc;
+      float sum = 0.f;
+#pragma unroll
+      for (int p = 0; p < 2; ++p)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int y = 2 * yc + p, x = 2 * xc + q;
+          float pc;
+          const float v = apply9(a.w[l], buf[c], y, x, Y, X, a.periodic, &pc) - f[y * X + x];
+          sum += v;
+        }
+      fc[j] = 0.25f * sum;
+    }
+    __syncthreads();
+  }
+  {
+    const int l = nl - 1, Y = a.Y[l], X = a.X[l], n = Y * X;
+    float *buf[2] = {sm2 + off[l], sm2 + off[l] + n};
+    const float *f = sm2 + off[l] + 2 * n;
+    int c = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) buf[0][i] = 0.f;
+    __syncthreads();
+    for (int k = 0; k < a.coarse_sweeps; ++k) {
+      sub2_sweep(a.w[l], buf[c], f, buf[c ^ 1], Y, X, a.periodic, a.omega);
+      c ^= 1;
+    }
+    cur[l] = c;
+  }
+  for (int l = nl - 2; l >= 0; --l) {
+    const int Y = a.Y[l], X = a.X[l], n = Y * X, Xc = a.X[l + 1];
+    float *buf[2] = {sm2 + off[l], sm2 + off[l] + n};
+    const float *f = sm2 + off[l] + 2 * n;
+    const float *wc = sm2 + off[l + 1] + cur[l + 1] * a.Y[l + 1] * Xc;
+    int c = cur[l];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int y = i / X, x = i % X;
+      buf[c][i] = buf[c][i] + -1.f * wc[(y >> 1) * Xc + (x >> 1)];
+    }
+    __syncthreads();
+    sub2_sweep(a.w[l], buf[c], f, buf[c ^ 1], Y, X, a.periodic, a.nu_post ? a.omega : 0.f);
+    c ^= 1;
+    for (int k = 1; k < a.nu_post; ++k) {
+      sub2_sweep(a.w[l], buf[c], f, buf[c ^ 1], Y, X, a.periodic, a.omega);
+      c ^= 1;
+    }
+    cur[l] = c;
+  }
+  const float *res = sm2 + off[0] + cur[0] * n0;
+  for (int i = threadIdx.x; i < n0; i += blockDim.x) out[b * n0 + i] = St<T>::from(res[i]);
+}
+
 // Subtract each instance's mean (the constant null space of a periodic operator).  One
 // thread-block cluster of kMeanCluster blocks per instance: each block sums its contiguous
 // share in a fixed order (thread-strided, warp tree, warps in order), the blocks read the
@@ -487,6 +623,44 @@ int hfm_coarse_jacobi2d(int dtype, const float *w9_host, const void *rhs, void *
                      w9_of(w9_host), (const T *)rhs, (T *)out, Y, X, omega, sweeps,
                      (flags & HFM_FLAG_PERIODIC) ? 1 : 0)));
   HFM_CHECK_LAUNCH("k2_coarse_jacobi");
+  return HFM_OK;
+}
+
+int hfm_subcycle2d(int dtype, const float *w9_levels, const void *rhs, void *out, int B, int Y, int X,
+                   int nlev, float omega, int nu_pre, int nu_post, int coarse_sweeps, unsigned flags,
+                   hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Y, X)) || (st = check_dtype2(dtype))) return st;
+  if (!w9_levels || !rhs || !out || nlev < 1 || nlev > kSub2Levels || nu_pre < 1 || nu_post < 0 ||
+      coarse_sweeps < 0)
+    return fail(HFM_ERR_BAD_ARG, "hfm_subcycle2d: bad argument");
+  if ((int64_t)Y * X > 4096) return fail(HFM_ERR_BAD_ARG, "hfm_subcycle2d: at most 4096 cells on the first level");
+  Sub2Args a;
+  a.nlev = nlev;
+  a.periodic = (flags & HFM_FLAG_PERIODIC) ? 1 : 0;
+  a.nu_pre = nu_pre;
+  a.nu_post = nu_post;
+  a.coarse_sweeps = coarse_sweeps;
+  a.omega = omega;
+  size_t smem = 0;
+  for (int l = 0; l < nlev; ++l) {
+    a.Y[l] = l ? a.Y[l - 1] / 2 : Y;
+    a.X[l] = l ? a.X[l - 1] / 2 : X;
+    if (a.Y[l] < 1 || a.X[l] < 1) return fail(HFM_ERR_BAD_ARG, "hfm_subcycle2d: too many levels");
+    if (l + 1 < nlev && ((a.Y[l] & 1) || (a.X[l] & 1)))
+      return fail(HFM_ERR_BAD_ARG, "hfm_subcycle2d: odd extent above the coarsest level");
+    if (w9_levels[9 * l + 4] == 0.f) return fail(HFM_ERR_BAD_ARG, "hfm_subcycle2d: zero diagonal weight");
+    a.w[l] = w9_of(w9_levels + 9 * l);
+    smem += (size_t)3 * a.Y[l] * a.X[l] * sizeof(float);
+  }
+  for (int l = nlev; l < kSub2Levels; ++l) a.Y[l] = a.X[l] = 0;
+  HFM2_DT(dtype, {
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        k2_subcycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 4096 * 2 * (int)sizeof(float));
+    if (attr != cudaSuccess) return fail(HFM_ERR_CUDA, "hfm_subcycle2d: shared memory attribute");
+    k2_subcycle<T><<<B, kSub2Threads, smem, (cudaStream_t)stream>>>(a, (const T *)rhs, (T *)out);
+  });
+  HFM_CHECK_LAUNCH("k2_subcycle");
   return HFM_OK;
 }
 

@@ -40,6 +40,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--dtype", default="f32", choices=["f32", "bf16", "f16"],
                     help="storage of fields and coefficients")
+    ap.add_argument("--per-level", action="store_true",
+                    help="kolmogorov-step: one launch per coarse-level step instead of the fused "
+                         "coarse cycle")
     a = ap.parse_args()
     import torch
     import __graft_entry__ as ge
@@ -235,6 +238,8 @@ def kolmogorov_step(hfm, torch, a):
     nu 1/40, sin(4y) forcing, dt 1e-3, three pressure V-cycles per step), --reps steps in
     one timed region (NVTX range "timed")."""
     kf = hfm.kolmogorov.KolmogorovFlow(n=a.n, dt=1e-3, cycles=3, seed=0)
+    if a.per_level:
+        kf.mg.fused_coarse = False
     for _ in range(a.warmup):
         kf.step()
     torch.cuda.synchronize()
@@ -246,7 +251,8 @@ def kolmogorov_step(hfm, torch, a):
     torch.cuda.nvtx.range_pop()
     e1.record()
     torch.cuda.synchronize()
-    print(json.dumps({"kernel": "kolmogorov-step", "n": a.n, "ms_per_step": e0.elapsed_time(e1) / a.reps}))
+    print(json.dumps({"kernel": "kolmogorov-step", "n": a.n, "fused_coarse": kf.mg.fused_coarse,
+                      "ms_per_step": e0.elapsed_time(e1) / a.reps}))
 
 
 def ns_step(hfm, torch, a):

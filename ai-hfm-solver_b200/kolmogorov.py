@@ -60,7 +60,8 @@ def laplace5(h):
 
 class Multigrid2D:
     def __init__(self, shape, w9, storage="f32", periodic=True, nu_pre=2, nu_post=2, omega=0.8,
-                 coarse_scale=0.25, min_edge=4, coarse_sweeps=32, slots=1, device="cuda"):
+                 coarse_scale=0.25, min_edge=4, coarse_sweeps=32, slots=1, device="cuda",
+                 fused_coarse=True):
         if storage not in _DT:
             raise ValueError("storage must be f32 or bf16")
         if nu_pre < 1:
@@ -77,6 +78,13 @@ class Multigrid2D:
         self.coarse_sweeps = coarse_sweeps
         w = np.asarray(w9, np.float64).reshape(3, 3)
         self.ws = [_w9(w * coarse_scale ** l) for l in range(self.L)]
+        # levels of at most 4096 cells run as one fused launch (hfm_subcycle2d) when enabled
+        self.l_sub = next((l for l, s in enumerate(self.shapes) if s[0] * s[1] <= 4096), self.L)
+        self.fused_coarse = bool(fused_coarse) and self.L - self.l_sub <= 8 and all(
+            s[0] % 2 == 0 and s[1] % 2 == 0 for s in self.shapes[self.l_sub:-1])
+        if self.fused_coarse:
+            self.ws_sub = (C.c_float * (9 * (self.L - self.l_sub)))(
+                *[v for l in range(self.l_sub, self.L) for v in self.ws[l]])
         mk = lambda s, dt: torch.zeros((slots,) + s, dtype=dt, device=device)
         self.w = [mk(s, self.tdt) for s in self.shapes]
         self.tmp = [mk(s, self.tdt) for s in self.shapes]
@@ -92,6 +100,11 @@ class Multigrid2D:
     def _cycle(self, l):
         """Approximate solution of A w = rhs[l] from w = 0; returns the tensor holding it."""
         Y, X = self.shapes[l]
+        if self.fused_coarse and l == self.l_sub:
+            L.call("hfm_subcycle2d", self.code, self.ws_sub, _p(self.rhs[l]), _p(self.w[l]),
+                   self.slots, Y, X, self.L - l, self.omega, self.nu_pre, self.nu_post,
+                   self.coarse_sweeps, self.flags, _stream())
+            return self.w[l]
         if l == self.L - 1:
             L.call("hfm_coarse_jacobi2d", self.code, self.ws[l], _p(self.rhs[l]), _p(self.w[l]),
                    self.slots, Y, X, self.omega, self.coarse_sweeps, self.flags, _stream())

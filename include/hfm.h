@@ -400,6 +400,18 @@ int hfm_update2d(float *p, int dtype, const void *w, float sign, int64_t n, hfm_
  * shared memory (the coarsest level of a cycle). */
 int hfm_coarse_jacobi2d(int dtype, const float *w9_host, const void *rhs, void *out, int B, int Y,
                         int X, float omega, int sweeps, unsigned flags, hfm_stream_t stream);
+/* The V-cycle of the coarse levels in one launch, one 1024-thread block per instance with
+ * every field in shared memory (float32 between sweeps): from rhs on a first level of at most
+ * 4096 cells (Y x X, each coarser level Y/2 x X/2, extents even above the coarsest), nlev <= 8
+ * levels with weights w9_levels[9 l .. 9 l + 8], nu_pre >= 1 weighted-Jacobi sweeps from
+ * zero, residual and 2 x 2 averaging restriction, coarse_sweeps sweeps from zero on the
+ * coarsest level, nearest-prolongation correction phi - P w and nu_post sweeps.  The steps of
+ * the per-level entry points above (hfm_jacobi2d, hfm_residual_restrict2d,
+ * hfm_coarse_jacobi2d) in the same order and arithmetic: float32 storage gives their bits;
+ * bf16 storage rounds only rhs on load and the result on store. */
+int hfm_subcycle2d(int dtype, const float *w9_levels, const void *rhs, void *out, int B, int Y, int X,
+                   int nlev, float omega, int nu_pre, int nu_post, int coarse_sweeps, unsigned flags,
+                   hfm_stream_t stream);
 /* Subtract each instance's mean from p (B instances of n values): the constant null space of
  * a periodic pressure operator. */
 int hfm_mean_subtract2d(float *p, int B, int64_t n, hfm_stream_t stream);

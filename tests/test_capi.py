@@ -183,6 +183,26 @@ def test_face7_smooth2_validates_without_gpu(lib, pkg):
     assert b"aligned" in lib.hfm_last_error()
 
 
+def test_subcycle2d_validates_without_gpu(lib, pkg):
+    """The fused 2D coarse cycle rejects first levels above 4096 cells, more than 8 levels, odd
+    extents above the coarsest level, nu_pre < 1 and zero diagonal weights on the host."""
+    L = pkg._lib
+    w = (C.c_float * 72)(*([0, -1, 0, -1, 4, -1, 0, -1, 0] * 8))
+    buf = (C.c_float * 16)()
+    p = C.c_void_p(C.addressof(buf))
+    f = lambda *a: lib.hfm_subcycle2d(L.F32, w, p, p, *a)
+    assert f(1, 128, 64, 2, 0.8, 2, 2, 8, L.FLAG_PERIODIC, None) == L.ERR_BAD_ARG    # 8192 cells
+    assert f(1, 64, 64, 9, 0.8, 2, 2, 8, L.FLAG_PERIODIC, None) == L.ERR_BAD_ARG     # 9 levels
+    assert f(1, 64, 64, 8, 0.8, 2, 2, 8, L.FLAG_PERIODIC, None) == L.ERR_BAD_ARG     # 64 -> 0
+    assert f(1, 12, 20, 4, 0.8, 2, 2, 8, L.FLAG_PERIODIC, None) == L.ERR_BAD_ARG     # 3 x 5 above 1 x 2
+    assert b"odd" in lib.hfm_last_error()
+    assert f(1, 64, 64, 3, 0.8, 0, 2, 8, L.FLAG_PERIODIC, None) == L.ERR_BAD_ARG     # nu_pre 0
+    assert lib.hfm_subcycle2d(L.BF16, w, None, p, 1, 64, 64, 3, 0.8, 2, 2, 8, 0, None) == L.ERR_BAD_ARG
+    w[9 + 4] = 0.0
+    assert f(1, 64, 64, 3, 0.8, 2, 2, 8, L.FLAG_PERIODIC, None) == L.ERR_BAD_ARG
+    assert b"diagonal" in lib.hfm_last_error()
+
+
 def test_serve_config_and_validation_without_gpu(lib, pkg):
     """hfm_serve_*: the default configuration and the host-side checks that run before any
     device allocation."""

@@ -125,6 +125,39 @@ def test_periodic_pressure_cycles(hfm, T, storage):
     assert abs(float(p.double().mean())) < 1e-6
 
 
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("shape,slots,nu", [((512, 512), 1, (2, 2)), ((64, 64), 2, (2, 2)),
+                                            ((128, 96), 3, (1, 0)), ((256, 64), 1, (3, 1))])
+def test_fused_coarse_cycle_same_bits(hfm, T, periodic, shape, slots, nu):
+    """Outer iterations with the levels of at most 4096 cells in one launch (hfm_subcycle2d)
+    give the bits of the per-level launches in float32 storage, and agree to bf16 rounding in
+    bf16 storage (the fused launch keeps those levels in float32)."""
+    KM = hfm.kolmogorov
+    Y, X = shape
+    rng = np.random.default_rng(Y + X + slots)
+    w = KM.laplace5(2 * np.pi / X)
+    if not periodic:
+        w[1, 1] *= 1.1  # diagonally dominant
+    f = rng.standard_normal((slots, Y, X)).astype(np.float32)
+    if periodic:
+        f -= f.mean(axis=(1, 2), keepdims=True)
+    fd = T.from_numpy(f).cuda()
+    out = {}
+    for storage in ("f32", "bf16"):
+        for fused in (True, False):
+            mg = KM.Multigrid2D(shape, w, storage=storage, periodic=periodic, nu_pre=nu[0],
+                                nu_post=nu[1], slots=slots, fused_coarse=fused)
+            assert mg.fused_coarse == fused
+            p = T.zeros((slots, Y, X), device="cuda")
+            for _ in range(3):
+                mg.iterate(p, fd)
+            out[storage, fused] = p.cpu().numpy()
+    assert np.isfinite(out["f32", True]).all()
+    np.testing.assert_array_equal(out["f32", True], out["f32", False])
+    close(out["bf16", True], out["f32", False], 2e-2)
+    close(out["bf16", True], out["bf16", False], 2e-2)
+
+
 def test_kolmogorov_step_matches_oracle(hfm, T):
     KM = hfm.kolmogorov
     n = 64
