@@ -216,7 +216,8 @@ __global__ void __launch_bounds__(kT2) k2_coarse_jacobi(W9 w, const T *__restric
 // ------------------------------------------------------------------ fused coarse cycle
 // The V-cycle of the levels of at most 4096 cells (64^2 .. 4^2 of a 512^2 grid) in one
 // launch: one 1024-thread block per instance, every field of those levels in shared memory
-// (float32), sweeps separated by __syncthreads().  The steps and their arithmetic are those
+// (float32), sweeps separated by __syncthreads(); a coarsest level of at most 32 cells runs on
+// one warp with its iterate in registers (shuffles, no barriers).  The steps and their arithmetic are those
 // of the per-level kernels (Multigrid2D._cycle): nu_pre sweeps from zero, residual + 2 x 2
 // averaging restriction (0.25 x the sum), recursion, `sweeps` sweeps from zero on the
 // coarsest level, then the nearest-prolongation correction phi - P w and nu_post sweeps;
@@ -231,39 +232,185 @@ struct Sub2Args {
   float omega;
 };
 
+// Cells t, t + nt, t + 2 nt, ... of a Y x X level with (y, x) advanced without a division.
+template <class F>
+__device__ __forceinline__ void walk2(int Y, int X, int t, int nt, F &&f) {
+  int y = t / X, x = t - y * X;
+  const int sy = nt / X, sx = nt - sy * X;
+  for (int i = t; i < Y * X; i += nt) {
+    f(i, y, x);
+    x += sx;
+    y += sy;
+    if (x >= X) {
+      x -= X;
+      ++y;
+    }
+  }
+}
+
+// A phi at (y, x) in the operation order of conv9 (rows, then columns); zero or periodic padding
 __device__ __forceinline__ float apply9(const W9 &w, const float *ph, int y, int x, int Y, int X,
                                         int periodic, float *centre) {
+  int r[3] = {y - 1, y, y + 1}, c[3] = {x - 1, x, x + 1};
+  bool vr[3] = {true, true, true}, vc[3] = {true, true, true};
+  if (periodic) {
+    r[0] = r[0] < 0 ? Y - 1 : r[0];
+    r[2] = r[2] >= Y ? 0 : r[2];
+    c[0] = c[0] < 0 ? X - 1 : c[0];
+    c[2] = c[2] >= X ? 0 : c[2];
+  } else {
+    vr[0] = r[0] >= 0;
+    vr[2] = r[2] < Y;
+    vc[0] = c[0] >= 0;
+    vc[2] = c[2] < X;
+  }
   float acc = 0.f;
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      int yy = y + a - 1, xx = x + c - 1;
-      float v;
-      if (periodic) {
-        yy = yy < 0 ? yy + Y : (yy >= Y ? yy - Y : yy);
-        xx = xx < 0 ? xx + X : (xx >= X ? xx - X : xx);
-        v = ph[yy * X + xx];
-      } else {
-        v = (yy < 0 || yy >= Y || xx < 0 || xx >= X) ? 0.f : ph[yy * X + xx];
-      }
-      if (a == 1 && c == 1) *centre = v;
-      acc += w.w[3 * a + c] * v;
+    for (int b = 0; b < 3; ++b) {
+      const float v = (vr[a] && vc[b]) ? ph[r[a] * X + c[b]] : 0.f;
+      if (a == 1 && b == 1) *centre = v;
+      acc += w.w[3 * a + b] * v;
     }
   return acc;
 }
 
-// out = in + omega (f - A in) / w[4] on level (Y, X); in == nullptr: a zero iterate
-__device__ void sub2_sweep(const W9 &w, const float *in, const float *f, float *out, int Y, int X,
-                           int periodic, float omega) {
-  const int n = Y * X;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+// out = in + omega (f - A in) / w[4] on level (Y, X), the whole block; in == nullptr: a zero
+// iterate
+__device__ void sub2_sweep(const W9 &w, const float *__restrict__ in, const float *__restrict__ f,
+                           float *__restrict__ out, int Y, int X, int periodic, float omega) {
+  walk2(Y, X, threadIdx.x, blockDim.x, [&](int i, int y, int x) {
     float pc = 0.f, ax = 0.f;
-    if (in) ax = apply9(w, in, i / X, i % X, Y, X, periodic, &pc);
+    if (in) ax = apply9(w, in, y, x, Y, X, periodic, &pc);
     out[i] = pc + omega * (f[i] - ax) / w.w[4];
-  }
+  });
   __syncthreads();
 }
+
+// `sweeps` sweeps from zero on a level of at most 32 cells by warp 0, one cell per lane in a
+// register and the neighbours by shuffles; the same operation order as apply9 / sub2_sweep.
+// Lanes outside the level carry zeros.  Returns this lane's value.
+__device__ float sub2_coarsest_warp(const W9 &w9, const float *__restrict__ f, int Y, int X,
+                                    int periodic, float omega, int sweeps) {
+  const int lane = threadIdx.x, n = Y * X;
+  const bool live = lane < n;
+  const int y = live ? lane / X : 0, x = live ? lane - (lane / X) * X : 0;
+  int r[3] = {y - 1, y, y + 1}, c[3] = {x - 1, x, x + 1};
+  unsigned ok = 0x1ff;  // bit 3a + b: neighbour (a, b) inside the grid
+  if (periodic) {
+    r[0] = r[0] < 0 ? Y - 1 : r[0];
+    r[2] = r[2] >= Y ? 0 : r[2];
+    c[0] = c[0] < 0 ? X - 1 : c[0];
+    c[2] = c[2] >= X ? 0 : c[2];
+  } else {
+    if (r[0] < 0) ok &= ~0x007u;
+    if (r[2] >= Y) ok &= ~0x1c0u;
+    if (c[0] < 0) ok &= ~0x049u;
+    if (c[2] >= X) ok &= ~0x124u;
+  }
+  if (!live) ok = 0;
+  int src[9];
+  float w[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    src[k] = (ok >> k) & 1 ? r[k / 3] * X + c[k % 3] : lane;
+    w[k] = w9.w[k];
+  }
+  const float fv = live ? f[lane] : 0.f;
+  float ph = 0.f;
+  for (int s = 0; s < sweeps; ++s) {
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float v = __shfl_sync(0xffffffffu, ph, src[k]);
+      acc += w[k] * ((ok >> k) & 1 ? v : 0.f);
+    }
+    const float nv = ph + omega * (fv - acc) / w[4];
+    ph = live ? nv : 0.f;
+  }
+  return ph;
+}
+
+// Shared-memory layout of level l: phi at off[l], tmp at off[l] + n, rhs at off[l] + 2 n.
+struct Sub2Walk {
+  const Sub2Args &a;
+  float *sm;
+  int off[kSub2Levels];
+  int cur[kSub2Levels];  // which of phi / tmp holds level l's iterate
+  __device__ float *buf(int l, int k) const { return sm + off[l] + k * a.Y[l] * a.X[l]; }
+  __device__ float *rhs(int l) const { return sm + off[l] + 2 * a.Y[l] * a.X[l]; }
+
+  // pre-sweeps from zero, then the coarse rhs 0.25 * sum over the 2 x 2 cells of (A phi - f)
+  __device__ void down(int l) {
+    const int Y = a.Y[l], X = a.X[l];
+    const float *f = rhs(l);
+    int c = 0;
+    sub2_sweep(a.w[l], nullptr, f, buf(l, 0), Y, X, a.periodic, a.omega);
+    for (int k = 1; k < a.nu_pre; ++k) {
+      sub2_sweep(a.w[l], buf(l, c), f, buf(l, c ^ 1), Y, X, a.periodic, a.omega);
+      c ^= 1;
+    }
+    cur[l] = c;
+    const float *ph = buf(l, c);
+    float *fc = rhs(l + 1);
+    walk2(a.Y[l + 1], a.X[l + 1], threadIdx.x, blockDim.x, [&](int j, int yc, int xc) {
+      float sum = 0.f;
+#pragma unroll
+      for (int p = 0; p < 2; ++p)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int y = 2 * yc + p, x = 2 * xc + q;
+          float pc;
+          sum += apply9(a.w[l], ph, y, x, Y, X, a.periodic, &pc) - f[y * X + x];
+        }
+      fc[j] = 0.25f * sum;
+    });
+    __syncthreads();
+  }
+
+  // coarse_sweeps sweeps from zero on the coarsest level; the result in buf(l, cur[l])
+  __device__ void coarsest(int l) {
+    const int Y = a.Y[l], X = a.X[l], n = Y * X;
+    if (n <= 32) {
+      if (threadIdx.x < 32) {
+        const float v = sub2_coarsest_warp(a.w[l], rhs(l), Y, X, a.periodic, a.omega, a.coarse_sweeps);
+        if (threadIdx.x < n) buf(l, 0)[threadIdx.x] = v;
+      }
+      __syncthreads();
+      cur[l] = 0;
+      return;
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) buf(l, 0)[i] = 0.f;
+    __syncthreads();
+    int c = 0;
+    for (int k = 0; k < a.coarse_sweeps; ++k) {
+      sub2_sweep(a.w[l], buf(l, c), rhs(l), buf(l, c ^ 1), Y, X, a.periodic, a.omega);
+      c ^= 1;
+    }
+    cur[l] = c;
+  }
+
+  // phi - P w (nearest prolongation of level l + 1), then the post-sweeps
+  __device__ void up(int l) {
+    const int Y = a.Y[l], X = a.X[l], Xc = a.X[l + 1];
+    const float *f = rhs(l);
+    const float *wc = buf(l + 1, cur[l + 1]);
+    int c = cur[l];
+    float *ph = buf(l, c);
+    walk2(Y, X, threadIdx.x, blockDim.x, [&](int i, int y, int x) {
+      ph[i] = ph[i] - wc[(y >> 1) * Xc + (x >> 1)];
+    });
+    __syncthreads();
+    sub2_sweep(a.w[l], buf(l, c), f, buf(l, c ^ 1), Y, X, a.periodic, a.nu_post ? a.omega : 0.f);
+    c ^= 1;
+    for (int k = 1; k < a.nu_post; ++k) {
+      sub2_sweep(a.w[l], buf(l, c), f, buf(l, c ^ 1), Y, X, a.periodic, a.omega);
+      c ^= 1;
+    }
+    cur[l] = c;
+  }
+};
 
 template <class T>
 __global__ void __launch_bounds__(kSub2Threads) k2_subcycle(const __grid_constant__ Sub2Args a,
@@ -272,80 +419,19 @@ __global__ void __launch_bounds__(kSub2Threads) k2_subcycle(const __grid_constan
   extern __shared__ float sm2[];
   const int64_t b = blockIdx.x;
   const int nl = a.nlev;
-  int off[kSub2Levels];
+  Sub2Walk s{a, sm2};
   int o = 0;
   for (int l = 0; l < nl; ++l) {
-    off[l] = o;
+    s.off[l] = o;
     o += 3 * a.Y[l] * a.X[l];
   }
-  // level l: phi at off, tmp at off + n, rhs at off + 2 n
   const int n0 = a.Y[0] * a.X[0];
-  for (int i = threadIdx.x; i < n0; i += blockDim.x) sm2[off[0] + 2 * n0 + i] = St<T>::to(rhs[b * n0 + i]);
+  for (int i = threadIdx.x; i < n0; i += blockDim.x) s.rhs(0)[i] = St<T>::to(rhs[b * n0 + i]);
   __syncthreads();
-  int cur[kSub2Levels];
-  for (int l = 0; l < nl - 1; ++l) {
-    const int Y = a.Y[l], X = a.X[l], n = Y * X;
-    float *buf[2] = {sm2 + off[l], sm2 + off[l] + n};
-    const float *f = sm2 + off[l] + 2 * n;
-    int c = 0;
-    sub2_sweep(a.w[l], nullptr, f, buf[0], Y, X, a.periodic, a.omega);
-    for (int k = 1; k < a.nu_pre; ++k) {
-      sub2_sweep(a.w[l], buf[c], f, buf[c ^ 1], Y, X, a.periodic, a.omega);
-      c ^= 1;
-    }
-    cur[l] = c;
-    // coarse rhs = 0.25 * sum over the 2 x 2 fine cells of (A phi - f)
-    const int Yc = a.Y[l + 1], Xc = a.X[l + 1];
-    float *fc = sm2 + off[l + 1] + 2 * Yc * Xc;
-    for (int j = threadIdx.x; j < Yc * Xc; j += blockDim.x) {
-      const int yc = j / Xc, xc = j % Xc;
-      float sum = 0.f;
-#pragma unroll
-      for (int p = 0; p < 2; ++p)
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int y = 2 * yc + p, x = 2 * xc + q;
-          float pc;
-          const float v = apply9(a.w[l], buf[c], y, x, Y, X, a.periodic, &pc) - f[y * X + x];
-          sum += v;
-        }
-      fc[j] = 0.25f * sum;
-    }
-    __syncthreads();
-  }
-  {
-    const int l = nl - 1, Y = a.Y[l], X = a.X[l], n = Y * X;
-    float *buf[2] = {sm2 + off[l], sm2 + off[l] + n};
-    const float *f = sm2 + off[l] + 2 * n;
-    int c = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) buf[0][i] = 0.f;
-    __syncthreads();
-    for (int k = 0; k < a.coarse_sweeps; ++k) {
-      sub2_sweep(a.w[l], buf[c], f, buf[c ^ 1], Y, X, a.periodic, a.omega);
-      c ^= 1;
-    }
-    cur[l] = c;
-  }
-  for (int l = nl - 2; l >= 0; --l) {
-    const int Y = a.Y[l], X = a.X[l], n = Y * X, Xc = a.X[l + 1];
-    float *buf[2] = {sm2 + off[l], sm2 + off[l] + n};
-    const float *f = sm2 + off[l] + 2 * n;
-    const float *wc = sm2 + off[l + 1] + cur[l + 1] * a.Y[l + 1] * Xc;
-    int c = cur[l];
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const int y = i / X, x = i % X;
-      buf[c][i] = buf[c][i] + -1.f * wc[(y >> 1) * Xc + (x >> 1)];
-    }
-    __syncthreads();
-    sub2_sweep(a.w[l], buf[c], f, buf[c ^ 1], Y, X, a.periodic, a.nu_post ? a.omega : 0.f);
-    c ^= 1;
-    for (int k = 1; k < a.nu_post; ++k) {
-      sub2_sweep(a.w[l], buf[c], f, buf[c ^ 1], Y, X, a.periodic, a.omega);
-      c ^= 1;
-    }
-    cur[l] = c;
-  }
-  const float *res = sm2 + off[0] + cur[0] * n0;
+  for (int l = 0; l < nl - 1; ++l) s.down(l);
+  s.coarsest(nl - 1);
+  for (int l = nl - 2; l >= 0; --l) s.up(l);
+  const float *res = s.buf(0, s.cur[0]);
   for (int i = threadIdx.x; i < n0; i += blockDim.x) out[b * n0 + i] = St<T>::from(res[i]);
 }
 

@@ -9,7 +9,8 @@ residual + restriction), ``correct`` (fused prolongation + correction + sweep), 
 ``smooth2`` (face7: coarse correction and two sweeps in one pass), ``served-shares``
 (kernel-time shares of one pass over the served stream of --batch requests), ``mg-iter`` (bf16
 refinement + PCG iterations on a handle of --batch slots of --n^3), ``kolmogorov-step``
-(time steps of the 2D Kolmogorov flow at --n^2), ``ns-step`` (time steps
+(time steps of the 2D Kolmogorov flow at --n^2), ``subcycle2d`` (the fused 2D coarse cycle
+from --n^2 down to 4^2, periodic 5-point operator, --batch instances), ``ns-step`` (time steps
 of the obstacle flow at --shape, default 64,128,128: 24 boxes, 7-point
 diffusion, F-cycle pressure solve to 1e-5; --reps steps in one timed region, the target of a
 launch list).
@@ -54,6 +55,8 @@ def main():
         return mg_iter(hfm, torch, a)
     if a.kernel == "kolmogorov-step":
         return kolmogorov_step(hfm, torch, a)
+    if a.kernel == "subcycle2d":
+        return subcycle2d(hfm, torch, a)
     if a.kernel == "served-shares":
         return served_shares(hfm, torch, a)
     Z, Y, X = (tuple(int(v) for v in a.shape.split(",")) if a.shape else (a.n, a.n, a.n))
@@ -253,6 +256,32 @@ def kolmogorov_step(hfm, torch, a):
     torch.cuda.synchronize()
     print(json.dumps({"kernel": "kolmogorov-step", "n": a.n, "fused_coarse": kf.mg.fused_coarse,
                       "ms_per_step": e0.elapsed_time(e1) / a.reps}))
+
+
+def subcycle2d(hfm, torch, a):
+    """hfm_subcycle2d alone: V(2,2) from --n^2 down to 4^2 with 32 coarsest sweeps, --batch
+    instances (one block each), --reps launches in one timed region."""
+    KM, L = hfm.kolmogorov, hfm._lib
+    mg = KM.Multigrid2D((a.n, a.n), KM.laplace5(2 * 3.141592653589793 / a.n), slots=a.batch)
+    assert mg.fused_coarse and mg.l_sub == 0
+    g = torch.Generator(device="cuda").manual_seed(0)
+    rhs = torch.randn((a.batch, a.n, a.n), device="cuda", generator=g)
+    out = torch.empty_like(rhs)
+    st = hfm.ops._stream()
+    P = lambda t: C.c_void_p(t.data_ptr())
+    go = lambda: L.call("hfm_subcycle2d", L.F32, mg.ws_sub, P(rhs), P(out), a.batch, a.n, a.n, mg.L,
+                        mg.omega, mg.nu_pre, mg.nu_post, mg.coarse_sweeps, mg.flags, st)
+    for _ in range(a.warmup):
+        go()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        go()
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel": "subcycle2d", "n": a.n, "batch": a.batch, "levels": mg.L,
+                      "us_per_launch": 1e3 * e0.elapsed_time(e1) / a.reps}))
 
 
 def ns_step(hfm, torch, a):
