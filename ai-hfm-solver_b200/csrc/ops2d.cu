@@ -229,18 +229,31 @@ struct Sub2Args {
   W9 w[kSub2Levels];
   int Y[kSub2Levels], X[kSub2Levels];
   int nlev, periodic, nu_pre, nu_post, coarse_sweeps;
+  int smem_floats;  // shared memory of all levels, in floats
   float omega;
 };
 
-// Cells t, t + nt, t + 2 nt, ... of a Y x X level with (y, x) advanced without a division.
+// This thread's first cell of a Y x X level and the step between its cells, for walks by
+// the whole block (thread t visits cells t, t + nt, ...; one division per level visit).
+struct Walk2 {
+  int y0, x0, sy, sx;
+};
+__device__ __forceinline__ Walk2 walk2_of(int X) {
+  Walk2 w;
+  const int t = threadIdx.x, nt = blockDim.x;
+  w.y0 = t / X;
+  w.x0 = t - w.y0 * X;
+  w.sy = nt / X;
+  w.sx = nt - w.sy * X;
+  return w;
+}
 template <class F>
-__device__ __forceinline__ void walk2(int Y, int X, int t, int nt, F &&f) {
-  int y = t / X, x = t - y * X;
-  const int sy = nt / X, sx = nt - sy * X;
-  for (int i = t; i < Y * X; i += nt) {
-    f(i, y, x);
-    x += sx;
-    y += sy;
+__device__ __forceinline__ void walk2(const Walk2 &w, int Y, int X, F &&f) {
+  int y = w.y0, x = w.x0;
+  while (y < Y) {
+    f(y * X + x, y, x);
+    x += w.sx;
+    y += w.sy;
     if (x >= X) {
       x -= X;
       ++y;
@@ -248,42 +261,57 @@ __device__ __forceinline__ void walk2(int Y, int X, int t, int nt, F &&f) {
   }
 }
 
-// A phi at (y, x) in the operation order of conv9 (rows, then columns); zero or periodic padding
-__device__ __forceinline__ float apply9(const W9 &w, const float *ph, int y, int x, int Y, int X,
-                                        int periodic, float *centre) {
-  int r[3] = {y - 1, y, y + 1}, c[3] = {x - 1, x, x + 1};
-  bool vr[3] = {true, true, true}, vc[3] = {true, true, true};
-  if (periodic) {
-    r[0] = r[0] < 0 ? Y - 1 : r[0];
-    r[2] = r[2] >= Y ? 0 : r[2];
-    c[0] = c[0] < 0 ? X - 1 : c[0];
-    c[2] = c[2] >= X ? 0 : c[2];
-  } else {
-    vr[0] = r[0] >= 0;
-    vr[2] = r[2] < Y;
-    vc[0] = c[0] >= 0;
-    vc[2] = c[2] < X;
-  }
+// The iterates of a level live in (Y + 2) x (X + 2) fields (row pitch P = X + 2): the cells
+// inside and a one-cell ring that holds zeros (zero padding) or the periodic images of the
+// opposite edge, so that a stencil reads nine fixed offsets.  A phi at a cell, in the order
+// of conv9 (rows, then columns).
+__device__ __forceinline__ float stencil9(const W9 &w, const float *c, int P, float *centre) {
+  const float *u = c - P, *d = c + P;
   float acc = 0.f;
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      const float v = (vr[a] && vc[b]) ? ph[r[a] * X + c[b]] : 0.f;
-      if (a == 1 && b == 1) *centre = v;
-      acc += w.w[3 * a + b] * v;
-    }
+  acc += w.w[0] * u[-1];
+  acc += w.w[1] * u[0];
+  acc += w.w[2] * u[1];
+  acc += w.w[3] * c[-1];
+  acc += w.w[4] * c[0];
+  acc += w.w[5] * c[1];
+  acc += w.w[6] * d[-1];
+  acc += w.w[7] * d[0];
+  acc += w.w[8] * d[1];
+  *centre = c[0];
   return acc;
+}
+
+// fld(y, x) = v, and on a periodic level also every ring cell that is an image of (y, x)
+__device__ __forceinline__ void put2(float *fld, int P, int Y, int X, int y, int x, float v,
+                                     int periodic) {
+  float *c = fld + (y + 1) * P + x + 1;
+  *c = v;
+  if (!periodic) return;
+  const bool t0 = y == 0, t1 = y == Y - 1;
+  if (t0) c[Y * P] = v;
+  if (t1) c[-Y * P] = v;
+  if (x == 0) {
+    c[X] = v;
+    if (t0) c[Y * P + X] = v;
+    if (t1) c[-Y * P + X] = v;
+  }
+  if (x == X - 1) {
+    c[-X] = v;
+    if (t0) c[Y * P - X] = v;
+    if (t1) c[-Y * P - X] = v;
+  }
 }
 
 // out = in + omega (f - A in) / w[4] on level (Y, X), the whole block; in == nullptr: a zero
 // iterate
-__device__ void sub2_sweep(const W9 &w, const float *__restrict__ in, const float *__restrict__ f,
-                           float *__restrict__ out, int Y, int X, int periodic, float omega) {
-  walk2(Y, X, threadIdx.x, blockDim.x, [&](int i, int y, int x) {
+__device__ __forceinline__ void sub2_sweep(const W9 &w, const float *__restrict__ in, const float *__restrict__ f,
+                           float *__restrict__ out, int Y, int X, const Walk2 &wk, int periodic,
+                           float omega) {
+  const int P = X + 2;
+  walk2(wk, Y, X, [&](int i, int y, int x) {
     float pc = 0.f, ax = 0.f;
-    if (in) ax = apply9(w, in, y, x, Y, X, periodic, &pc);
-    out[i] = pc + omega * (f[i] - ax) / w.w[4];
+    if (in) ax = stencil9(w, in + (y + 1) * P + x + 1, P, &pc);
+    put2(out, P, Y, X, y, x, pc + omega * (f[i] - ax) / w.w[4], periodic);
   });
   __syncthreads();
 }
@@ -291,7 +319,7 @@ __device__ void sub2_sweep(const W9 &w, const float *__restrict__ in, const floa
 // `sweeps` sweeps from zero on a level of at most 32 cells by warp 0, one cell per lane in a
 // register and the neighbours by shuffles; the same operation order as apply9 / sub2_sweep.
 // Lanes outside the level carry zeros.  Returns this lane's value.
-__device__ float sub2_coarsest_warp(const W9 &w9, const float *__restrict__ f, int Y, int X,
+__device__ __forceinline__ float sub2_coarsest_warp(const W9 &w9, const float *__restrict__ f, int Y, int X,
                                     int periodic, float omega, int sweeps) {
   const int lane = threadIdx.x, n = Y * X;
   const bool live = lane < n;
@@ -332,108 +360,149 @@ __device__ float sub2_coarsest_warp(const W9 &w9, const float *__restrict__ f, i
   return ph;
 }
 
-// Shared-memory layout of level l: phi at off[l], tmp at off[l] + n, rhs at off[l] + 2 n.
-struct Sub2Walk {
-  const Sub2Args &a;
-  float *sm;
-  int off[kSub2Levels];
-  int cur[kSub2Levels];  // which of phi / tmp holds level l's iterate
-  __device__ float *buf(int l, int k) const { return sm + off[l] + k * a.Y[l] * a.X[l]; }
-  __device__ float *rhs(int l) const { return sm + off[l] + 2 * a.Y[l] * a.X[l]; }
-
-  // pre-sweeps from zero, then the coarse rhs 0.25 * sum over the 2 x 2 cells of (A phi - f)
-  __device__ void down(int l) {
-    const int Y = a.Y[l], X = a.X[l];
-    const float *f = rhs(l);
-    int c = 0;
-    sub2_sweep(a.w[l], nullptr, f, buf(l, 0), Y, X, a.periodic, a.omega);
-    for (int k = 1; k < a.nu_pre; ++k) {
-      sub2_sweep(a.w[l], buf(l, c), f, buf(l, c ^ 1), Y, X, a.periodic, a.omega);
-      c ^= 1;
-    }
-    cur[l] = c;
-    const float *ph = buf(l, c);
-    float *fc = rhs(l + 1);
-    walk2(a.Y[l + 1], a.X[l + 1], threadIdx.x, blockDim.x, [&](int j, int yc, int xc) {
-      float sum = 0.f;
-#pragma unroll
-      for (int p = 0; p < 2; ++p)
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int y = 2 * yc + p, x = 2 * xc + q;
-          float pc;
-          sum += apply9(a.w[l], ph, y, x, Y, X, a.periodic, &pc) - f[y * X + x];
-        }
-      fc[j] = 0.25f * sum;
-    });
-    __syncthreads();
-  }
-
-  // coarse_sweeps sweeps from zero on the coarsest level; the result in buf(l, cur[l])
-  __device__ void coarsest(int l) {
-    const int Y = a.Y[l], X = a.X[l], n = Y * X;
-    if (n <= 32) {
-      if (threadIdx.x < 32) {
-        const float v = sub2_coarsest_warp(a.w[l], rhs(l), Y, X, a.periodic, a.omega, a.coarse_sweeps);
-        if (threadIdx.x < n) buf(l, 0)[threadIdx.x] = v;
-      }
-      __syncthreads();
-      cur[l] = 0;
-      return;
-    }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) buf(l, 0)[i] = 0.f;
-    __syncthreads();
-    int c = 0;
-    for (int k = 0; k < a.coarse_sweeps; ++k) {
-      sub2_sweep(a.w[l], buf(l, c), rhs(l), buf(l, c ^ 1), Y, X, a.periodic, a.omega);
-      c ^= 1;
-    }
-    cur[l] = c;
-  }
-
-  // phi - P w (nearest prolongation of level l + 1), then the post-sweeps
-  __device__ void up(int l) {
-    const int Y = a.Y[l], X = a.X[l], Xc = a.X[l + 1];
-    const float *f = rhs(l);
-    const float *wc = buf(l + 1, cur[l + 1]);
-    int c = cur[l];
-    float *ph = buf(l, c);
-    walk2(Y, X, threadIdx.x, blockDim.x, [&](int i, int y, int x) {
-      ph[i] = ph[i] - wc[(y >> 1) * Xc + (x >> 1)];
-    });
-    __syncthreads();
-    sub2_sweep(a.w[l], buf(l, c), f, buf(l, c ^ 1), Y, X, a.periodic, a.nu_post ? a.omega : 0.f);
-    c ^= 1;
-    for (int k = 1; k < a.nu_post; ++k) {
-      sub2_sweep(a.w[l], buf(l, c), f, buf(l, c ^ 1), Y, X, a.periodic, a.omega);
-      c ^= 1;
-    }
-    cur[l] = c;
-  }
+// One level of the fused cycle: extents, row pitch of the padded iterates P = X + 2, their
+// size np = (Y + 2) P, the level's offset in shared memory (two iterates, then the rhs of
+// Y X floats) and its weights, held in registers while the level runs.
+struct Lv2 {
+  int Y, X, P, np, off;
+  W9 w;
 };
+
+// pre-sweeps from zero, then the coarse rhs 0.25 * sum over the 2 x 2 cells of (A phi - f);
+// the iterate ends in buffer (nu_pre - 1) & 1
+__device__ __forceinline__ void sub2_down(float *sm, const Lv2 &L, const Lv2 &Lc,
+                                          const Sub2Args &a) {
+  float *const b0 = sm + L.off, *const b1 = b0 + L.np;
+  auto buf = [&](int k) { return k ? b1 : b0; };  // selects: no local-memory array
+  const float *f = sm + L.off + 2 * L.np;
+  const Walk2 wk = walk2_of(L.X);
+  int c = 0;
+  sub2_sweep(L.w, nullptr, f, buf(0), L.Y, L.X, wk, a.periodic, a.omega);
+  for (int k = 1; k < a.nu_pre; ++k) {
+    sub2_sweep(L.w, buf(c), f, buf(c ^ 1), L.Y, L.X, wk, a.periodic, a.omega);
+    c ^= 1;
+  }
+  const float *ph = buf(c);
+  float *fc = sm + Lc.off + 2 * Lc.np;
+  const int P = L.P, X = L.X;
+  walk2(walk2_of(Lc.X), Lc.Y, Lc.X, [&](int j, int yc, int xc) {
+    float sum = 0.f;
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int y = 2 * yc + p, x = 2 * xc + q;
+        float pc;
+        sum += stencil9(L.w, ph + (y + 1) * P + x + 1, P, &pc) - f[y * X + x];
+      }
+    fc[j] = 0.25f * sum;
+  });
+  __syncthreads();
+}
+
+// coarse_sweeps sweeps from zero on the coarsest level; returns the buffer holding the result
+__device__ __forceinline__ int sub2_coarsest(float *sm, const Lv2 &L, const Sub2Args &a) {
+  float *const b0 = sm + L.off, *const b1 = b0 + L.np;
+  auto buf = [&](int k) { return k ? b1 : b0; };  // selects: no local-memory array
+  const float *f = sm + L.off + 2 * L.np;
+  const int n = L.Y * L.X;
+  if (n <= 32) {
+    if (threadIdx.x < 32) {
+      const float v = sub2_coarsest_warp(L.w, f, L.Y, L.X, a.periodic, a.omega, a.coarse_sweeps);
+      const int y = threadIdx.x / L.X, x = threadIdx.x - y * L.X;
+      if (threadIdx.x < n) buf(0)[(y + 1) * L.P + x + 1] = v;
+    }
+    __syncthreads();
+    return 0;
+  }
+  // buf(0) holds zeros (shared memory is cleared at the start)
+  const Walk2 wk = walk2_of(L.X);
+  int c = 0;
+  for (int k = 0; k < a.coarse_sweeps; ++k) {
+    sub2_sweep(L.w, buf(c), f, buf(c ^ 1), L.Y, L.X, wk, a.periodic, a.omega);
+    c ^= 1;
+  }
+  return c;
+}
+
+// phi - P w (nearest prolongation of the coarser level's result wc), then the post-sweeps;
+// the iterate starts in buffer c and the result's buffer is returned
+__device__ __forceinline__ int sub2_up(float *sm, const Lv2 &L, const Lv2 &Lc, int c, int cc,
+                                       const Sub2Args &a) {
+  float *const b0 = sm + L.off, *const b1 = b0 + L.np;
+  auto buf = [&](int k) { return k ? b1 : b0; };  // selects: no local-memory array
+  const float *f = sm + L.off + 2 * L.np;
+  const float *wc = sm + Lc.off + cc * Lc.np;
+  const Walk2 wk = walk2_of(L.X);
+  const int P = L.P, Pc = Lc.P;
+  float *ph = buf(c);
+  walk2(wk, L.Y, L.X, [&](int, int y, int x) {
+    const float v = ph[(y + 1) * P + x + 1] - wc[((y >> 1) + 1) * Pc + (x >> 1) + 1];
+    put2(ph, P, L.Y, L.X, y, x, v, a.periodic);
+  });
+  __syncthreads();
+  sub2_sweep(L.w, buf(c), f, buf(c ^ 1), L.Y, L.X, wk, a.periodic, a.nu_post ? a.omega : 0.f);
+  c ^= 1;
+  for (int k = 1; k < a.nu_post; ++k) {
+    sub2_sweep(L.w, buf(c), f, buf(c ^ 1), L.Y, L.X, wk, a.periodic, a.omega);
+    c ^= 1;
+  }
+  return c;
+}
 
 template <class T>
 __global__ void __launch_bounds__(kSub2Threads) k2_subcycle(const __grid_constant__ Sub2Args a,
                                                             const T *__restrict__ rhs,
                                                             T *__restrict__ out) {
   extern __shared__ float sm2[];
-  const int64_t b = blockIdx.x;
+  __shared__ Lv2 lv[kSub2Levels];
   const int nl = a.nlev;
-  Sub2Walk s{a, sm2};
-  int o = 0;
-  for (int l = 0; l < nl; ++l) {
-    s.off[l] = o;
-    o += 3 * a.Y[l] * a.X[l];
+  if (threadIdx.x < nl) {
+    const int l = threadIdx.x;
+    int o = 0;
+    for (int k = 0; k < l; ++k) o += 2 * (a.Y[k] + 2) * (a.X[k] + 2) + a.Y[k] * a.X[k];
+    Lv2 L;
+    L.Y = a.Y[l];
+    L.X = a.X[l];
+    L.P = L.X + 2;
+    L.np = (L.Y + 2) * L.P;
+    L.off = o;
+    L.w = a.w[l];
+    lv[l] = L;
   }
-  const int n0 = a.Y[0] * a.X[0];
-  for (int i = threadIdx.x; i < n0; i += blockDim.x) s.rhs(0)[i] = St<T>::to(rhs[b * n0 + i]);
+  for (int i = threadIdx.x; i < a.smem_floats; i += blockDim.x) sm2[i] = 0.f;
+  const int64_t b = blockIdx.x;
+  const int Y0 = a.Y[0], X0 = a.X[0], n0 = Y0 * X0, P0 = X0 + 2;
+  float *f0 = sm2 + 2 * (Y0 + 2) * P0;
+  for (int i = threadIdx.x; i < n0; i += blockDim.x) f0[i] = St<T>::to(rhs[b * n0 + i]);
   __syncthreads();
-  for (int l = 0; l < nl - 1; ++l) s.down(l);
-  s.coarsest(nl - 1);
-  for (int l = nl - 2; l >= 0; --l) s.up(l);
-  const float *res = s.buf(0, s.cur[0]);
-  for (int i = threadIdx.x; i < n0; i += blockDim.x) out[b * n0 + i] = St<T>::from(res[i]);
+  for (int l = 0; l < nl - 1; ++l) {
+    const Lv2 L = lv[l], Lc = lv[l + 1];
+    sub2_down(sm2, L, Lc, a);
+  }
+  const int cd = (a.nu_pre - 1) & 1;  // a level's iterate after its pre-sweeps
+  int cc;
+  {
+    const Lv2 L = lv[nl - 1];
+    cc = sub2_coarsest(sm2, L, a);
+  }
+  for (int l = nl - 2; l >= 0; --l) {
+    const Lv2 L = lv[l], Lc = lv[l + 1];
+    cc = sub2_up(sm2, L, Lc, cd, cc, a);
+  }
+  const float *res = sm2 + cc * (Y0 + 2) * P0;
+  walk2(walk2_of(X0), Y0, X0, [&](int i, int y, int x) {
+    out[b * n0 + i] = St<T>::from(res[(y + 1) * P0 + x + 1]);
+  });
 }
+
+// Shared-memory bytes of k2_subcycle for nlev levels from Y x X (each coarser level halved)
+size_t sub2_smem_bytes(int Y, int X, int nlev) {
+  size_t n = 0;
+  for (int l = 0; l < nlev; ++l, Y /= 2, X /= 2) n += (size_t)2 * (Y + 2) * (X + 2) + (size_t)Y * X;
+  return n * sizeof(float);
+}
+constexpr size_t kSub2MaxSmem = 200 * 1024;
 
 // Subtract each instance's mean (the constant null space of a periodic operator).  One
 // thread-block cluster of kMeanCluster blocks per instance: each block sums its contiguous
@@ -728,7 +797,6 @@ int hfm_subcycle2d(int dtype, const float *w9_levels, const void *rhs, void *out
   a.nu_post = nu_post;
   a.coarse_sweeps = coarse_sweeps;
   a.omega = omega;
-  size_t smem = 0;
   for (int l = 0; l < nlev; ++l) {
     a.Y[l] = l ? a.Y[l - 1] / 2 : Y;
     a.X[l] = l ? a.X[l - 1] / 2 : X;
@@ -737,13 +805,15 @@ int hfm_subcycle2d(int dtype, const float *w9_levels, const void *rhs, void *out
       return fail(HFM_ERR_BAD_ARG, "hfm_subcycle2d: odd extent above the coarsest level");
     if (w9_levels[9 * l + 4] == 0.f) return fail(HFM_ERR_BAD_ARG, "hfm_subcycle2d: zero diagonal weight");
     a.w[l] = w9_of(w9_levels + 9 * l);
-    smem += (size_t)3 * a.Y[l] * a.X[l] * sizeof(float);
   }
   for (int l = nlev; l < kSub2Levels; ++l) a.Y[l] = a.X[l] = 0;
+  const size_t smem = sub2_smem_bytes(Y, X, nlev);
+  if (smem > kSub2MaxSmem) return fail(HFM_ERR_UNSUPPORTED, "hfm_subcycle2d: levels exceed shared memory");
+  a.smem_floats = (int)(smem / sizeof(float));
   HFM2_DT(dtype, {
-    static const cudaError_t attr = cudaFuncSetAttribute(
-        k2_subcycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 4096 * 2 * (int)sizeof(float));
-    if (attr != cudaSuccess) return fail(HFM_ERR_CUDA, "hfm_subcycle2d: shared memory attribute");
+    if ((st = set_max_dynamic_smem((const void *)k2_subcycle<T>, (int)kSub2MaxSmem,
+                                   "cudaFuncSetAttribute(k2_subcycle)")))
+      return st;
     k2_subcycle<T><<<B, kSub2Threads, smem, (cudaStream_t)stream>>>(a, (const T *)rhs, (T *)out);
   });
   HFM_CHECK_LAUNCH("k2_subcycle");
