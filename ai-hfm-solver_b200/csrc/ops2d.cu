@@ -471,6 +471,7 @@ __global__ void __launch_bounds__(kSub2Threads) k2_subcycle(const __grid_constan
     lv[l] = L;
   }
   for (int i = threadIdx.x; i < a.smem_floats; i += blockDim.x) sm2[i] = 0.f;
+  __syncthreads();  // the zeros land before the rhs below
   const int64_t b = blockIdx.x;
   const int Y0 = a.Y[0], X0 = a.X[0], n0 = Y0 * X0, P0 = X0 + 2;
   float *f0 = sm2 + 2 * (Y0 + 2) * P0;
