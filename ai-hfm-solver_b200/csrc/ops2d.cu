@@ -241,10 +241,18 @@ struct Walk2 {
 __device__ __forceinline__ Walk2 walk2_of(int X) {
   Walk2 w;
   const int t = threadIdx.x, nt = blockDim.x;
-  w.y0 = t / X;
-  w.x0 = t - w.y0 * X;
-  w.sy = nt / X;
-  w.sx = nt - w.sy * X;
+  if ((X & (X - 1)) == 0) {  // a power of two: shifts and masks
+    const int s = __ffs(X) - 1;
+    w.y0 = t >> s;
+    w.x0 = t & (X - 1);
+    w.sy = nt >> s;
+    w.sx = nt & (X - 1);
+  } else {
+    w.y0 = t / X;
+    w.x0 = t - w.y0 * X;
+    w.sy = nt / X;
+    w.sx = nt - w.sy * X;
+  }
   return w;
 }
 template <class F>
