@@ -18,6 +18,7 @@ F32, BF16, F16, F64 = range(4)
 OP_CONST7, OP_SIGMA7, OP_DIR7, OP_K27, OP_FACE7 = range(5)
 # flags
 FLAG_ZERO_XEND, FLAG_TOP_COPY, FLAG_ZERO_GUESS, FLAG_PERIODIC, FLAG_SAME_LEVEL_CORR = 1, 2, 4, 8, 16
+FLAG_TWO_SWEEPS = 32
 # hfm_cycle / hfm_accel
 CYCLE_SAWTOOTH, CYCLE_V, CYCLE_F = range(3)
 ACCEL_NONE, ACCEL_CG, ACCEL_IR = range(3)

@@ -45,8 +45,29 @@ template <class T> struct Src2 {
   }
 };
 
-template <class T>
-__device__ __forceinline__ float conv9(const W9 &w, const Src2<T> &s, int64_t b, int y, int x,
+// The first Jacobi sweep from a zero iterate at (y, x), as hfm_jacobi2d stores it: 0 + omega
+// f / w[4] rounded to T (0 outside a zero-padded grid); the source of the second sweep of a
+// fused pair.
+template <class T> struct Sweep1Src {
+  const T *f;
+  float omega, diag;
+  int64_t stride;
+  int Y, X;
+  int periodic;
+  __device__ __forceinline__ float operator()(int64_t b, int y, int x) const {
+    if (periodic) {
+      y = y < 0 ? y + Y : (y >= Y ? y - Y : y);
+      x = x < 0 ? x + X : (x >= X ? x - X : x);
+    } else if (y < 0 || y >= Y || x < 0 || x >= X) {
+      return 0.f;
+    }
+    const float fv = St<T>::ld(f + b * stride + (int64_t)y * X + x);
+    return St<T>::to(St<T>::from(0.f + omega * fv / diag));
+  }
+};
+
+template <class S>
+__device__ __forceinline__ float conv9(const W9 &w, const S &s, int64_t b, int y, int x,
                                        float *centre) {
   float acc = 0.f;
 #pragma unroll
@@ -70,13 +91,30 @@ __global__ void __launch_bounds__(kT2) k2_stencil(W9 w, Src2<T> s, const T *__re
        i += (int64_t)gridDim.x * blockDim.x) {
     const int y = (int)(i / s.X), x = (int)(i % s.X);
     float pc;
-    const float ax = conv9<T>(w, s, b, y, x, &pc);
+    const float ax = conv9(w, s, b, y, x, &pc);
     const float fv = f ? St<T>::ld(f + b * s.stride + i) : 0.f;
     float r;
     if (MODE == 0) r = ax;
     else if (MODE == 1) r = ax - fv;
     else r = pc + omega * (fv - ax) / w.w[4];
     out[b * s.stride + i] = St<T>::from(r);
+  }
+}
+
+// Two Jacobi sweeps from a zero iterate in one pass: out = phi1 + omega (f - A phi1) / w[4]
+// with phi1 the first sweep (Sweep1Src), recomputed at each neighbour; the bits of two
+// hfm_jacobi2d launches.
+template <class T>
+__global__ void __launch_bounds__(kT2) k2_two_sweeps(W9 w, Sweep1Src<T> s, T *__restrict__ out) {
+  const int64_t b = blockIdx.y;
+  const int64_t n = (int64_t)s.Y * s.X;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / s.X), x = (int)(i % s.X);
+    float pc;
+    const float ax = conv9(w, s, b, y, x, &pc);
+    const float fv = St<T>::ld(s.f + b * s.stride + i);
+    out[b * s.stride + i] = St<T>::from(pc + s.omega * (fv - ax) / w.w[4]);
   }
 }
 
@@ -98,7 +136,7 @@ __global__ void __launch_bounds__(kT2) k2_resid_restrict(W9 w, Src2<TI> s, const
       for (int c = 0; c < 2; ++c) {
         const int y = 2 * yc + a, x = 2 * xc + c;
         float pc;
-        float v = conv9<TI>(w, s, b, y, x, &pc);
+        float v = conv9(w, s, b, y, x, &pc);
         if (f) v -= St<TI>::ld(f + b * s.stride + (int64_t)y * s.X + x);
         sum += v;
       }
@@ -119,7 +157,7 @@ __global__ void __launch_bounds__(kT2) k2_outer_resid(W9 w, Src2<float> s, const
        i += (int64_t)gridDim.x * blockDim.x) {
     const int y = (int)(i / s.X), x = (int)(i % s.X);
     float pc;
-    const float v = conv9<float>(w, s, b, y, x, &pc) - f[b * s.stride + i];
+    const float v = conv9(w, s, b, y, x, &pc) - f[b * s.stride + i];
     r[b * s.stride + i] = St<TO>::from(v);
     acc += (double)v * v;
   }
@@ -714,6 +752,24 @@ int hfm_jacobi2d(int dtype, const float *w9_host, const void *base, const void *
   if (coarse && !(flags & HFM_FLAG_SAME_LEVEL_CORR) && ((Y | X) & 1))
     return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: coarse correction needs even extents");
   const int64_t n = (int64_t)Y * X;
+  if (flags & HFM_FLAG_TWO_SWEEPS) {
+    if (base || coarse || !rhs || rhs == out)
+      return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: two sweeps start from zero (base, coarse NULL) "
+                                   "and need an rhs apart from out");
+    HFM2_DT(dtype, {
+      Sweep1Src<T> s;
+      s.f = (const T *)rhs;
+      s.omega = omega;
+      s.diag = w9_host[4];
+      s.stride = n;
+      s.Y = Y;
+      s.X = X;
+      s.periodic = (flags & HFM_FLAG_PERIODIC) ? 1 : 0;
+      k2_two_sweeps<T><<<dim3(blocks2(n, B), B), kT2, 0, (cudaStream_t)stream>>>(w9_of(w9_host), s, (T *)out);
+    });
+    HFM_CHECK_LAUNCH("k2_two_sweeps");
+    return HFM_OK;
+  }
   HFM2_DT(dtype, (k2_stencil<T, 2><<<dim3(blocks2(n, B), B), kT2, 0, (cudaStream_t)stream>>>(
                      w9_of(w9_host), src2<T>(base, coarse, coarse_sign, Y, X, flags),
                      (const T *)rhs, (T *)out, omega)));

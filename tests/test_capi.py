@@ -203,6 +203,22 @@ def test_subcycle2d_validates_without_gpu(lib, pkg):
     assert b"diagonal" in lib.hfm_last_error()
 
 
+def test_two_sweeps_flag_validates_without_gpu(lib, pkg):
+    """HFM_FLAG_TWO_SWEEPS starts from zero: a base or coarse field, a missing rhs or an rhs
+    that is the output are refused on the host."""
+    L = pkg._lib
+    w = (C.c_float * 9)(0, -1, 0, -1, 4, -1, 0, -1, 0)
+    b1, b2 = (C.c_float * 64)(), (C.c_float * 64)()
+    p, q = C.c_void_p(C.addressof(b1)), C.c_void_p(C.addressof(b2))
+    f = lambda base, coarse, rhs, out: lib.hfm_jacobi2d(L.F32, w, base, coarse, 0.0, rhs, out, 1, 8,
+                                                        8, 0.8, L.FLAG_TWO_SWEEPS, None)
+    assert f(p, None, p, q) == L.ERR_BAD_ARG
+    assert f(None, p, p, q) == L.ERR_BAD_ARG
+    assert f(None, None, None, q) == L.ERR_BAD_ARG
+    assert f(None, None, q, q) == L.ERR_BAD_ARG
+    assert b"two sweeps" in lib.hfm_last_error()
+
+
 def test_serve_config_and_validation_without_gpu(lib, pkg):
     """hfm_serve_*: the default configuration and the host-side checks that run before any
     device allocation."""

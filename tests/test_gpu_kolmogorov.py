@@ -125,6 +125,59 @@ def test_periodic_pressure_cycles(hfm, T, storage):
     assert abs(float(p.double().mean())) < 1e-6
 
 
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("shape", [(1, 17, 23), (3, 64, 48), (2, 512, 512)])
+def test_two_sweeps_from_zero_same_bits(hfm, T, storage, periodic, shape):
+    """hfm_jacobi2d with HFM_FLAG_TWO_SWEEPS equals two hfm_jacobi2d calls from zero, bit for
+    bit, in float32 and bf16 storage (the first sweep rounded to the storage type)."""
+    L = hfm._lib
+    KM = hfm.kolmogorov
+    code, tdt = KM._DT[storage]
+    rng = np.random.default_rng(sum(shape))
+    w = rng.standard_normal((3, 3))
+    w[1, 1] = 2.0 + np.abs(w).sum()
+    f = T.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda().to(tdt)
+    B, Y, X = shape
+    fl = L.FLAG_PERIODIC if periodic else 0
+    P = lambda t: C.c_void_p(t.data_ptr())
+    st = hfm.ops._stream()
+    one, two, fused = T.empty_like(f), T.empty_like(f), T.empty_like(f)
+    L.call("hfm_jacobi2d", code, _w9(w), None, None, 0.0, P(f), P(one), B, Y, X, 0.8, fl, st)
+    L.call("hfm_jacobi2d", code, _w9(w), P(one), None, 0.0, P(f), P(two), B, Y, X, 0.8, fl, st)
+    L.call("hfm_jacobi2d", code, _w9(w), None, None, 0.0, P(f), P(fused), B, Y, X, 0.8,
+           fl | L.FLAG_TWO_SWEEPS, st)
+    T.cuda.synchronize()
+    a, r = fused.float().cpu().numpy(), two.float().cpu().numpy()
+    assert np.isfinite(a).all()
+    np.testing.assert_array_equal(a, r)
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_fused_pre_sweeps_cycle_same_bits(hfm, T, storage, periodic):
+    """Outer iterations with and without the fused first two pre-sweeps: the same bits."""
+    KM = hfm.kolmogorov
+    Y, X, slots = 256, 192, 2
+    rng = np.random.default_rng(7)
+    w = KM.laplace5(2 * np.pi / X)
+    if not periodic:
+        w[1, 1] *= 1.1
+    f = rng.standard_normal((slots, Y, X)).astype(np.float32)
+    f -= f.mean(axis=(1, 2), keepdims=True)
+    fd = T.from_numpy(f).cuda()
+    out = {}
+    for fused in (True, False):
+        mg = KM.Multigrid2D((Y, X), w, storage=storage, periodic=periodic, nu_pre=3, slots=slots,
+                            fused_pre=fused)
+        p = T.zeros((slots, Y, X), device="cuda")
+        for _ in range(3):
+            mg.iterate(p, fd)
+        out[fused] = p.cpu().numpy()
+    assert np.isfinite(out[True]).all()
+    np.testing.assert_array_equal(out[True], out[False])
+
+
 @pytest.mark.parametrize("periodic", [True, False])
 @pytest.mark.parametrize("shape,slots,nu", [((512, 512), 1, (2, 2)), ((64, 64), 2, (2, 2)),
                                             ((128, 96), 3, (1, 0)), ((256, 64), 1, (3, 1))])
