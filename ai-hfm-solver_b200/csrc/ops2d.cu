@@ -118,6 +118,53 @@ __global__ void __launch_bounds__(kT2) k2_two_sweeps(W9 w, Sweep1Src<T> s, T *__
   }
 }
 
+// Two Jacobi sweeps in one pass from phi = base + sign P(coarse) (Src2): a 32 x 8 tile of
+// the first sweep and its one-cell ring in shared memory (each value computed as the
+// one-sweep launch computes it and rounded to T as it stores it), then the second sweep from
+// there; the bits of two hfm_jacobi2d launches.
+constexpr int kTwoTX = 32, kTwoTY = 8;
+static_assert(kTwoTX * kTwoTY == kT2, "one thread per output cell of a tile");
+template <class T>
+__global__ void __launch_bounds__(kT2) k2_two_sweeps_tile(W9 w, Src2<T> s, const T *__restrict__ f,
+                                                          T *__restrict__ out, float omega) {
+  __shared__ float mid[kTwoTY + 2][kTwoTX + 2];
+  const int64_t b = blockIdx.z;
+  const int x0 = blockIdx.x * kTwoTX, y0 = blockIdx.y * kTwoTY;
+  for (int k = threadIdx.x; k < (kTwoTY + 2) * (kTwoTX + 2); k += blockDim.x) {
+    const int ty = k / (kTwoTX + 2), tx = k - ty * (kTwoTX + 2);
+    int y = y0 + ty - 1, x = x0 + tx - 1;  // -1 <= y <= y0 + kTwoTY, likewise x
+    float v = 0.f;
+    // cells past row Y / column X neighbour no cell of the grid: left at 0
+    bool live = y <= s.Y && x <= s.X;
+    if (s.periodic) {
+      y = y < 0 ? y + s.Y : (y >= s.Y ? y - s.Y : y);
+      x = x < 0 ? x + s.X : (x >= s.X ? x - s.X : x);
+    } else {
+      live = live && y >= 0 && y < s.Y && x >= 0 && x < s.X;
+    }
+    if (live) {
+      float pc;
+      const float ax = conv9(w, s, b, y, x, &pc);
+      const float fv = St<T>::ld(f + b * s.stride + (int64_t)y * s.X + x);
+      v = St<T>::to(St<T>::from(pc + omega * (fv - ax) / w.w[4]));
+    }
+    mid[ty][tx] = v;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x % kTwoTX, ty = threadIdx.x / kTwoTX;
+  const int y = y0 + ty, x = x0 + tx;
+  if (y < s.Y && x < s.X) {
+    float acc = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc += w.w[3 * a + c] * mid[ty + a][tx + c];
+    const float pc = mid[ty + 1][tx + 1];
+    const int64_t i = b * s.stride + (int64_t)y * s.X + x;
+    out[i] = St<T>::from(pc + omega * (St<T>::ld(f + i) - acc) / w.w[4]);
+  }
+}
+
 // Coarse cell (yc, xc) = 0.25 * sum over its 2x2 fine cells of (A phi - f); float32 phi and f
 // may be read while the coarse output is stored in T (TI = input storage).
 template <class TI, class TO>
@@ -753,9 +800,17 @@ int hfm_jacobi2d(int dtype, const float *w9_host, const void *base, const void *
     return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: coarse correction needs even extents");
   const int64_t n = (int64_t)Y * X;
   if (flags & HFM_FLAG_TWO_SWEEPS) {
-    if (base || coarse || !rhs || rhs == out)
-      return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: two sweeps start from zero (base, coarse NULL) "
-                                   "and need an rhs apart from out");
+    if (!rhs || rhs == out)
+      return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: two sweeps need an rhs apart from out");
+    if (base || coarse) {
+      const dim3 grid((X + kTwoTX - 1) / kTwoTX, (Y + kTwoTY - 1) / kTwoTY, B);
+      if (grid.y > 65535) return fail(HFM_ERR_BAD_ARG, "hfm_jacobi2d: two sweeps: Y too large");
+      HFM2_DT(dtype, (k2_two_sweeps_tile<T><<<grid, kT2, 0, (cudaStream_t)stream>>>(
+                         w9_of(w9_host), src2<T>(base, coarse, coarse_sign, Y, X, flags),
+                         (const T *)rhs, (T *)out, omega)));
+      HFM_CHECK_LAUNCH("k2_two_sweeps_tile");
+      return HFM_OK;
+    }
     HFM2_DT(dtype, {
       Sweep1Src<T> s;
       s.f = (const T *)rhs;

@@ -43,7 +43,7 @@ def main():
                     help="storage of fields and coefficients")
     ap.add_argument("--per-level", action="store_true",
                     help="kolmogorov-step: one launch per level step (no fused coarse cycle, no "
-                         "fused first two pre-sweeps)")
+                         "fused pairs of sweeps)")
     a = ap.parse_args()
     import torch
     import __graft_entry__ as ge
@@ -242,7 +242,7 @@ def kolmogorov_step(hfm, torch, a):
     one timed region (NVTX range "timed")."""
     kf = hfm.kolmogorov.KolmogorovFlow(n=a.n, dt=1e-3, cycles=3, seed=0)
     if a.per_level:
-        kf.mg.fused_coarse = kf.mg.fused_pre = False
+        kf.mg.fused_coarse = kf.mg.fused_pairs = False
     for _ in range(a.warmup):
         kf.step()
     torch.cuda.synchronize()
@@ -255,7 +255,7 @@ def kolmogorov_step(hfm, torch, a):
     e1.record()
     torch.cuda.synchronize()
     print(json.dumps({"kernel": "kolmogorov-step", "n": a.n, "fused_coarse": kf.mg.fused_coarse,
-                      "fused_pre": kf.mg.fused_pre,
+                      "fused_pairs": kf.mg.fused_pairs,
                       "ms_per_step": e0.elapsed_time(e1) / a.reps}))
 
 

@@ -61,7 +61,7 @@ def laplace5(h):
 class Multigrid2D:
     def __init__(self, shape, w9, storage="f32", periodic=True, nu_pre=2, nu_post=2, omega=0.8,
                  coarse_scale=0.25, min_edge=4, coarse_sweeps=32, slots=1, device="cuda",
-                 fused_coarse=True, fused_pre=True):
+                 fused_coarse=True, fused_pairs=True):
         if storage not in _DT:
             raise ValueError("storage must be f32 or bf16")
         if nu_pre < 1:
@@ -76,8 +76,9 @@ class Multigrid2D:
         self.flags = L.FLAG_PERIODIC if periodic else 0
         self.nu_pre, self.nu_post, self.omega = nu_pre, nu_post, float(omega)
         self.coarse_sweeps = coarse_sweeps
-        # the first two pre-sweeps from zero in one launch (HFM_FLAG_TWO_SWEEPS) when enabled
-        self.fused_pre = bool(fused_pre)
+        # pairs of sweeps in one launch (HFM_FLAG_TWO_SWEEPS) when enabled: the first two
+        # pre-sweeps from zero, and the correction + sweep with the next post-sweep
+        self.fused_pairs = bool(fused_pairs)
         w = np.asarray(w9, np.float64).reshape(3, 3)
         self.ws = [_w9(w * coarse_scale ** l) for l in range(self.L)]
         # levels of at most 4096 cells run as one fused launch (hfm_subcycle2d) when enabled
@@ -113,7 +114,7 @@ class Multigrid2D:
             return self.w[l]
         cur, oth = self.w[l], self.tmp[l]
         done = 1
-        if self.fused_pre and self.nu_pre >= 2:
+        if self.fused_pairs and self.nu_pre >= 2:
             L.call("hfm_jacobi2d", self.code, self.ws[l], None, None, 0.0, _p(self.rhs[l]), _p(oth),
                    self.slots, Y, X, self.omega, self.flags | L.FLAG_TWO_SWEEPS, _stream())
             cur, oth = oth, cur
@@ -126,10 +127,17 @@ class Multigrid2D:
         L.call("hfm_residual_restrict2d", self.code, self.ws[l], _p(cur), _p(self.rhs[l]),
                _p(self.rhs[l + 1]), self.slots, Y, X, self.flags, _stream())
         wc = self._cycle(l + 1)
-        # prolongation + correction w -= P w_c fused with the first post-sweep
-        self._jacobi(l, cur, wc, -1.0, self.rhs[l], oth, self.omega if self.nu_post else 0.0)
-        cur, oth = oth, cur
-        for _ in range(self.nu_post - 1):
+        # prolongation + correction w -= P w_c fused with the first post-sweep (and the second)
+        if self.fused_pairs and self.nu_post >= 2:
+            L.call("hfm_jacobi2d", self.code, self.ws[l], _p(cur), _p(wc), -1.0, _p(self.rhs[l]),
+                   _p(oth), self.slots, Y, X, self.omega, self.flags | L.FLAG_TWO_SWEEPS, _stream())
+            cur, oth = oth, cur
+            done = 2
+        else:
+            self._jacobi(l, cur, wc, -1.0, self.rhs[l], oth, self.omega if self.nu_post else 0.0)
+            cur, oth = oth, cur
+            done = 1
+        for _ in range(self.nu_post - done):
             self._jacobi(l, cur, None, 0.0, self.rhs[l], oth, self.omega)
             cur, oth = oth, cur
         return cur

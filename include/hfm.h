@@ -59,8 +59,8 @@ typedef enum {
 #define HFM_FLAG_ZERO_GUESS 4u /* the input phi is identically zero (not read) */
 #define HFM_FLAG_PERIODIC 8u   /* 2D operators: wrap around instead of zero padding */
 #define HFM_FLAG_SAME_LEVEL_CORR 16u /* hfm_jacobi2d: `coarse` is on the same grid (no upsampling) */
-#define HFM_FLAG_TWO_SWEEPS 32u /* hfm_jacobi2d: two sweeps from a zero iterate (base, coarse NULL)
-                                   in one pass, the bits of two calls */
+#define HFM_FLAG_TWO_SWEEPS 32u /* hfm_jacobi2d: two sweeps (the first from base + sign P(coarse),
+                                   the second plain) in one pass, the bits of two calls */
 
 /* Operator descriptor (plain data, copied by value into each launch).
  *   CONST7: k[0..2] = (kz, ky, kx) = (Dz/dz^2, Dy/dy^2, Dx/dx^2); diagonal 2(kz+ky+kx).

@@ -204,16 +204,17 @@ def test_subcycle2d_validates_without_gpu(lib, pkg):
 
 
 def test_two_sweeps_flag_validates_without_gpu(lib, pkg):
-    """HFM_FLAG_TWO_SWEEPS starts from zero: a base or coarse field, a missing rhs or an rhs
-    that is the output are refused on the host."""
+    """HFM_FLAG_TWO_SWEEPS: a missing rhs, an rhs or a base that is the output and a coarse
+    correction on odd extents are refused on the host."""
     L = pkg._lib
     w = (C.c_float * 9)(0, -1, 0, -1, 4, -1, 0, -1, 0)
     b1, b2 = (C.c_float * 64)(), (C.c_float * 64)()
     p, q = C.c_void_p(C.addressof(b1)), C.c_void_p(C.addressof(b2))
     f = lambda base, coarse, rhs, out: lib.hfm_jacobi2d(L.F32, w, base, coarse, 0.0, rhs, out, 1, 8,
                                                         8, 0.8, L.FLAG_TWO_SWEEPS, None)
-    assert f(p, None, p, q) == L.ERR_BAD_ARG
-    assert f(None, p, p, q) == L.ERR_BAD_ARG
+    assert f(q, None, p, q) == L.ERR_BAD_ARG                                   # base == out
+    assert lib.hfm_jacobi2d(L.F32, w, p, p, -1.0, p, q, 1, 7, 8, 0.8, L.FLAG_TWO_SWEEPS,
+                            None) == L.ERR_BAD_ARG                            # odd Y, coarse
     assert f(None, None, None, q) == L.ERR_BAD_ARG
     assert f(None, None, q, q) == L.ERR_BAD_ARG
     assert b"two sweeps" in lib.hfm_last_error()

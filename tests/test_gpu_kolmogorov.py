@@ -155,8 +155,42 @@ def test_two_sweeps_from_zero_same_bits(hfm, T, storage, periodic, shape):
 
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
 @pytest.mark.parametrize("periodic", [True, False])
-def test_fused_pre_sweeps_cycle_same_bits(hfm, T, storage, periodic):
-    """Outer iterations with and without the fused first two pre-sweeps: the same bits."""
+@pytest.mark.parametrize("shape", [(17, 23), (1, 9), (40, 72)])
+def test_two_sweeps_with_correction_same_bits(hfm, T, storage, periodic, shape):
+    """hfm_jacobi2d with HFM_FLAG_TWO_SWEEPS from base - P(coarse) (or base alone) equals the
+    correction + sweep launch followed by a plain sweep, bit for bit; partial tiles in x and
+    y and a one-row grid."""
+    L = hfm._lib
+    KM = hfm.kolmogorov
+    code, tdt = KM._DT[storage]
+    Y, X = shape
+    corr = Y % 2 == 0 and X % 2 == 0
+    B = 2
+    rng = np.random.default_rng(Y * X)
+    w = rng.standard_normal((3, 3))
+    w[1, 1] = 2.0 + np.abs(w).sum()
+    rnd = lambda s: T.from_numpy(rng.standard_normal(s).astype(np.float32)).cuda().to(tdt)
+    f, base = rnd((B, Y, X)), rnd((B, Y, X))
+    wc = rnd((B, Y // 2, X // 2)) if corr else None
+    fl = L.FLAG_PERIODIC if periodic else 0
+    P = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+    st = hfm.ops._stream()
+    one, two, fused = T.empty_like(f), T.empty_like(f), T.empty_like(f)
+    L.call("hfm_jacobi2d", code, _w9(w), P(base), P(wc), -1.0, P(f), P(one), B, Y, X, 0.8, fl, st)
+    L.call("hfm_jacobi2d", code, _w9(w), P(one), None, 0.0, P(f), P(two), B, Y, X, 0.8, fl, st)
+    L.call("hfm_jacobi2d", code, _w9(w), P(base), P(wc), -1.0, P(f), P(fused), B, Y, X, 0.8,
+           fl | L.FLAG_TWO_SWEEPS, st)
+    T.cuda.synchronize()
+    a, r = fused.float().cpu().numpy(), two.float().cpu().numpy()
+    assert np.isfinite(a).all()
+    np.testing.assert_array_equal(a, r)
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("nu", [(2, 2), (3, 3)])
+def test_fused_pairs_cycle_same_bits(hfm, T, storage, periodic, nu):
+    """Outer iterations with and without the fused pairs of sweeps: the same bits."""
     KM = hfm.kolmogorov
     Y, X, slots = 256, 192, 2
     rng = np.random.default_rng(7)
@@ -168,8 +202,8 @@ def test_fused_pre_sweeps_cycle_same_bits(hfm, T, storage, periodic):
     fd = T.from_numpy(f).cuda()
     out = {}
     for fused in (True, False):
-        mg = KM.Multigrid2D((Y, X), w, storage=storage, periodic=periodic, nu_pre=3, slots=slots,
-                            fused_pre=fused)
+        mg = KM.Multigrid2D((Y, X), w, storage=storage, periodic=periodic, nu_pre=nu[0],
+                            nu_post=nu[1], slots=slots, fused_pairs=fused)
         p = T.zeros((slots, Y, X), device="cuda")
         for _ in range(3):
             mg.iterate(p, fd)
