@@ -410,7 +410,9 @@ int hfm_coarse_jacobi2d(int dtype, const float *w9_host, const void *rhs, void *
  * coarsest level, nearest-prolongation correction phi - P w and nu_post sweeps.  The steps of
  * the per-level entry points above (hfm_jacobi2d, hfm_residual_restrict2d,
  * hfm_coarse_jacobi2d) in the same order and arithmetic: float32 storage gives their bits;
- * bf16 storage rounds only rhs on load and the result on store. */
+ * bf16 storage rounds only rhs on load and the result on store.  Levels needing more than
+ * 200 KB of shared memory (two padded iterates and the rhs per level) return
+ * HFM_ERR_UNSUPPORTED. */
 int hfm_subcycle2d(int dtype, const float *w9_levels, const void *rhs, void *out, int B, int Y, int X,
                    int nlev, float omega, int nu_pre, int nu_post, int coarse_sweeps, unsigned flags,
                    hfm_stream_t stream);
