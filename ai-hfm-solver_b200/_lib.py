@@ -144,6 +144,7 @@ SIGNATURES = {
     "hfm_jacobi2d": (I, [I, P, P, P, F, P, P, I, I, I, F, U, P]),
     "hfm_residual2d": (I, [I, P, P, P, P, I, I, I, U, P]),
     "hfm_residual_restrict2d": (I, [I, P, P, P, P, I, I, I, U, P]),
+    "hfm_pre2_restrict2d": (I, [I, P, P, P, P, I, I, I, F, U, P]),
     "hfm_outer_residual2d": (I, [P, P, P, I, P, I, I, I, U, P, P, P]),
     "hfm_update2d": (I, [P, I, P, F, I64, P]),
     "hfm_coarse_jacobi2d": (I, [I, P, P, P, I, I, I, F, I, U, P]),

@@ -165,6 +165,88 @@ __global__ void __launch_bounds__(kT2) k2_two_sweeps_tile(W9 w, Src2<T> s, const
   }
 }
 
+// The down leg of a level with two pre-sweeps in one pass: phi = two Jacobi sweeps from zero
+// and the coarse rhs 0.25 * sum over 2 x 2 cells of (A phi - f).  A 32 x 8 tile holds the
+// first sweep on a two-cell ring, the second on a one-cell ring (each value computed and
+// rounded to T as the one-sweep launches store it) and the tile's residuals in shared memory;
+// the bits of hfm_jacobi2d (HFM_FLAG_TWO_SWEEPS) followed by hfm_residual_restrict2d.
+// Even extents: the tile's coarse cells lie inside the grid or wholly outside it.
+template <class T>
+__global__ void __launch_bounds__(kT2) k2_pre2_restrict(W9 w, Sweep1Src<T> s, T *__restrict__ phi,
+                                                        T *__restrict__ coarse) {
+  __shared__ float s1[kTwoTY + 4][kTwoTX + 4];
+  __shared__ float s2[kTwoTY + 2][kTwoTX + 2];
+  __shared__ float rr[kTwoTY][kTwoTX];
+  const int64_t b = blockIdx.z;
+  const int Y = s.Y, X = s.X;
+  const int x0 = blockIdx.x * kTwoTX, y0 = blockIdx.y * kTwoTY;
+  // first sweep on the tile and a two-cell ring (s(b, y, x) wraps or pads, -2 <= y - y0 <= 9)
+  for (int k = threadIdx.x; k < (kTwoTY + 4) * (kTwoTX + 4); k += blockDim.x) {
+    const int ty = k / (kTwoTX + 4), tx = k - ty * (kTwoTX + 4);
+    int y = y0 + ty - 2, x = x0 + tx - 2;
+    if (s.periodic) {  // a ring cell may lie more than one period out on a grid of 1 row
+      y = ((y % Y) + Y) % Y;
+      x = ((x % X) + X) % X;
+    }
+    s1[ty][tx] = s(b, y, x);
+  }
+  __syncthreads();
+  // second sweep on the tile and a one-cell ring
+  for (int k = threadIdx.x; k < (kTwoTY + 2) * (kTwoTX + 2); k += blockDim.x) {
+    const int ty = k / (kTwoTX + 2), tx = k - ty * (kTwoTX + 2);
+    int y = y0 + ty - 1, x = x0 + tx - 1;
+    bool live = true;
+    if (s.periodic) {
+      y = ((y % Y) + Y) % Y;
+      x = ((x % X) + X) % X;
+    } else {
+      live = y >= 0 && y < Y && x >= 0 && x < X;
+    }
+    float v = 0.f;
+    if (live) {
+      float acc = 0.f;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc += w.w[3 * a + c] * s1[ty + a][tx + c];
+      const float pc = s1[ty + 1][tx + 1];
+      const float fv = St<T>::ld(s.f + b * s.stride + (int64_t)y * X + x);
+      v = St<T>::to(St<T>::from(pc + s.omega * (fv - acc) / w.w[4]));
+    }
+    s2[ty][tx] = v;
+  }
+  __syncthreads();
+  {
+    const int tx = threadIdx.x % kTwoTX, ty = threadIdx.x / kTwoTX;
+    const int y = y0 + ty, x = x0 + tx;
+    if (y < Y && x < X) {
+      float acc = 0.f;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc += w.w[3 * a + c] * s2[ty + a][tx + c];
+      const int64_t i = b * s.stride + (int64_t)y * X + x;
+      phi[i] = St<T>::from(s2[ty + 1][tx + 1]);
+      float r = acc;
+      r -= St<T>::ld(s.f + i);
+      rr[ty][tx] = r;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < (kTwoTY / 2) * (kTwoTX / 2)) {
+    const int jy = threadIdx.x / (kTwoTX / 2), jx = threadIdx.x - jy * (kTwoTX / 2);
+    const int yc = y0 / 2 + jy, xc = x0 / 2 + jx, Yc = Y / 2, Xc = X / 2;
+    if (yc < Yc && xc < Xc) {
+      float sum = 0.f;
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) sum += rr[2 * jy + a][2 * jx + c];
+      coarse[b * (int64_t)Yc * Xc + (int64_t)yc * Xc + xc] = St<T>::from(0.25f * sum);
+    }
+  }
+}
+
 // Coarse cell (yc, xc) = 0.25 * sum over its 2x2 fine cells of (A phi - f); float32 phi and f
 // may be read while the coarse output is stored in T (TI = input storage).
 template <class TI, class TO>
@@ -858,6 +940,33 @@ int hfm_residual_restrict2d(int dtype, const float *w9_host, const void *phi, co
                      w9_of(w9_host), src2<T>(phi, nullptr, 0.f, Y, X, flags), (const T *)rhs,
                      (T *)r_coarse, nc)));
   HFM_CHECK_LAUNCH("k2_resid_restrict");
+  return HFM_OK;
+}
+
+int hfm_pre2_restrict2d(int dtype, const float *w9_host, const void *rhs, void *phi,
+                        void *coarse_rhs, int B, int Y, int X, float omega, unsigned flags,
+                        hfm_stream_t stream) {
+  int st;
+  if ((st = check2(B, Y, X)) || (st = check_dtype2(dtype))) return st;
+  if (!w9_host || !rhs || !phi || !coarse_rhs || rhs == phi || rhs == coarse_rhs || phi == coarse_rhs)
+    return fail(HFM_ERR_BAD_ARG, "hfm_pre2_restrict2d: NULL or aliased fields");
+  if (w9_host[4] == 0.f) return fail(HFM_ERR_BAD_ARG, "hfm_pre2_restrict2d: zero diagonal weight");
+  if ((Y | X) & 1) return fail(HFM_ERR_BAD_ARG, "hfm_pre2_restrict2d: extents must be even");
+  const dim3 grid((X + kTwoTX - 1) / kTwoTX, (Y + kTwoTY - 1) / kTwoTY, B);
+  if (grid.y > 65535) return fail(HFM_ERR_BAD_ARG, "hfm_pre2_restrict2d: Y too large");
+  HFM2_DT(dtype, {
+    Sweep1Src<T> s;
+    s.f = (const T *)rhs;
+    s.omega = omega;
+    s.diag = w9_host[4];
+    s.stride = (int64_t)Y * X;
+    s.Y = Y;
+    s.X = X;
+    s.periodic = (flags & HFM_FLAG_PERIODIC) ? 1 : 0;
+    k2_pre2_restrict<T><<<grid, kT2, 0, (cudaStream_t)stream>>>(w9_of(w9_host), s, (T *)phi,
+                                                               (T *)coarse_rhs);
+  });
+  HFM_CHECK_LAUNCH("k2_pre2_restrict");
   return HFM_OK;
 }
 

@@ -114,6 +114,12 @@ class Multigrid2D:
             return self.w[l]
         cur, oth = self.w[l], self.tmp[l]
         done = 1
+        if self.fused_pairs and self.nu_pre == 2 and Y % 2 == 0 and X % 2 == 0:
+            # both pre-sweeps, the residual and the restriction in one launch
+            L.call("hfm_pre2_restrict2d", self.code, self.ws[l], _p(self.rhs[l]), _p(oth),
+                   _p(self.rhs[l + 1]), self.slots, Y, X, self.omega, self.flags, _stream())
+            cur, oth = oth, cur
+            return self._up(l, cur, oth)
         if self.fused_pairs and self.nu_pre >= 2:
             L.call("hfm_jacobi2d", self.code, self.ws[l], None, None, 0.0, _p(self.rhs[l]), _p(oth),
                    self.slots, Y, X, self.omega, self.flags | L.FLAG_TWO_SWEEPS, _stream())
@@ -126,6 +132,12 @@ class Multigrid2D:
             cur, oth = oth, cur
         L.call("hfm_residual_restrict2d", self.code, self.ws[l], _p(cur), _p(self.rhs[l]),
                _p(self.rhs[l + 1]), self.slots, Y, X, self.flags, _stream())
+        return self._up(l, cur, oth)
+
+    def _up(self, l, cur, oth):
+        """The coarser levels' cycle, then the correction and post-sweeps of level l (its
+        iterate in ``cur``); returns the tensor holding level l's result."""
+        Y, X = self.shapes[l]
         wc = self._cycle(l + 1)
         # prolongation + correction w -= P w_c fused with the first post-sweep (and the second)
         if self.fused_pairs and self.nu_post >= 2:

@@ -382,6 +382,13 @@ int hfm_prolong_nearest2d(int dtype, const void *coarse, void *fine, int B, int 
 int hfm_jacobi2d(int dtype, const float *w9_host, const void *base, const void *coarse,
                  float coarse_sign, const void *rhs, void *out, int B, int Y, int X, float omega,
                  unsigned flags, hfm_stream_t stream);
+/* The down leg of a level with two pre-sweeps in one launch: phi = two Jacobi sweeps from
+ * zero on rhs, coarse_rhs = 2 x 2 average of (A phi - rhs) on the (Y/2, X/2) grid; the bits
+ * of hfm_jacobi2d with HFM_FLAG_TWO_SWEEPS followed by hfm_residual_restrict2d.  Even
+ * extents; rhs, phi and coarse_rhs distinct. */
+int hfm_pre2_restrict2d(int dtype, const float *w9_host, const void *rhs, void *phi,
+                        void *coarse_rhs, int B, int Y, int X, float omega, unsigned flags,
+                        hfm_stream_t stream);
 /* r = A phi - rhs (rhs NULL = 0): Multigrid_2D.ipynb#c18 `CNN3D_A_128(values) - b`. */
 int hfm_residual2d(int dtype, const float *w9_host, const void *phi, const void *rhs, void *r,
                    int B, int Y, int X, unsigned flags, hfm_stream_t stream);

@@ -220,6 +220,20 @@ def test_two_sweeps_flag_validates_without_gpu(lib, pkg):
     assert b"two sweeps" in lib.hfm_last_error()
 
 
+def test_pre2_restrict_validates_without_gpu(lib, pkg):
+    """hfm_pre2_restrict2d refuses odd extents, NULL and aliased fields on the host."""
+    L = pkg._lib
+    w = (C.c_float * 9)(0, -1, 0, -1, 4, -1, 0, -1, 0)
+    bufs = [(C.c_float * 64)() for _ in range(3)]
+    f, p, c = (C.c_void_p(C.addressof(b)) for b in bufs)
+    g = lambda *a: lib.hfm_pre2_restrict2d(L.F32, w, *a, 0.8, L.FLAG_PERIODIC, None)
+    assert g(f, p, c, 1, 7, 8) == L.ERR_BAD_ARG
+    assert b"even" in lib.hfm_last_error()
+    assert g(f, f, c, 1, 8, 8) == L.ERR_BAD_ARG
+    assert g(f, p, p, 1, 8, 8) == L.ERR_BAD_ARG
+    assert g(None, p, c, 1, 8, 8) == L.ERR_BAD_ARG
+
+
 def test_serve_config_and_validation_without_gpu(lib, pkg):
     """hfm_serve_*: the default configuration and the host-side checks that run before any
     device allocation."""

@@ -188,6 +188,38 @@ def test_two_sweeps_with_correction_same_bits(hfm, T, storage, periodic, shape):
 
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
 @pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("shape", [(1, 18, 44), (2, 2, 2), (3, 64, 48), (1, 512, 512)])
+def test_pre2_restrict_same_bits(hfm, T, storage, periodic, shape):
+    """hfm_pre2_restrict2d equals hfm_jacobi2d (two sweeps from zero) followed by
+    hfm_residual_restrict2d, bit for bit: the iterate and the coarse rhs; partial tiles and a
+    2 x 2 grid."""
+    L = hfm._lib
+    KM = hfm.kolmogorov
+    code, tdt = KM._DT[storage]
+    B, Y, X = shape
+    rng = np.random.default_rng(Y + X + B)
+    w = rng.standard_normal((3, 3))
+    w[1, 1] = 2.0 + np.abs(w).sum()
+    f = T.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda().to(tdt)
+    fl = L.FLAG_PERIODIC if periodic else 0
+    P = lambda t: C.c_void_p(t.data_ptr())
+    st = hfm.ops._stream()
+    phi_r, phi_f = T.empty_like(f), T.empty_like(f)
+    fc_r = T.empty((B, Y // 2, X // 2), dtype=tdt, device="cuda")
+    fc_f = T.empty_like(fc_r)
+    L.call("hfm_jacobi2d", code, _w9(w), None, None, 0.0, P(f), P(phi_r), B, Y, X, 0.8,
+           fl | L.FLAG_TWO_SWEEPS, st)
+    L.call("hfm_residual_restrict2d", code, _w9(w), P(phi_r), P(f), P(fc_r), B, Y, X, fl, st)
+    L.call("hfm_pre2_restrict2d", code, _w9(w), P(f), P(phi_f), P(fc_f), B, Y, X, 0.8, fl, st)
+    T.cuda.synchronize()
+    for a, r in ((phi_f, phi_r), (fc_f, fc_r)):
+        a, r = a.float().cpu().numpy(), r.float().cpu().numpy()
+        assert np.isfinite(a).all()
+        np.testing.assert_array_equal(a, r)
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+@pytest.mark.parametrize("periodic", [True, False])
 @pytest.mark.parametrize("nu", [(2, 2), (3, 3)])
 def test_fused_pairs_cycle_same_bits(hfm, T, storage, periodic, nu):
     """Outer iterations with and without the fused pairs of sweeps: the same bits."""
