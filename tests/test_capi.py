@@ -234,6 +234,27 @@ def test_pre2_restrict_validates_without_gpu(lib, pkg):
     assert g(None, p, c, 1, 8, 8) == L.ERR_BAD_ARG
 
 
+def test_multigrid2d_plan_without_gpu(pkg):
+    """Multigrid2D's plan on the host: the first level of at most 4096 cells starts the fused
+    coarse cycle, whose weights are the per-level weights in order; an odd extent above the
+    coarsest level or more than 8 fused levels keep one launch per level step."""
+    KM = pkg.kolmogorov
+    w = KM.laplace5(0.1)
+    mg = KM.Multigrid2D((512, 512), w, device="cpu")
+    assert mg.shapes[mg.l_sub] == (64, 64) and mg.L - mg.l_sub == 5 and mg.fused_coarse
+    assert mg.fused_pairs
+    ref = [v for l in range(mg.l_sub, mg.L) for v in mg.ws[l]]
+    assert list(mg.ws_sub) == ref
+    mg = KM.Multigrid2D((96, 80), w, device="cpu")
+    assert mg.shapes[mg.l_sub] == (48, 40) and mg.shapes[-1] == (6, 5) and mg.fused_coarse
+    mg = KM.Multigrid2D((100, 100), w, device="cpu")  # 25 x 25 above the coarsest level
+    assert not mg.fused_coarse
+    mg = KM.Multigrid2D((64, 64), w, min_edge=1, device="cpu")  # 64^2 .. 1^2: 7 levels
+    assert mg.l_sub == 0 and mg.fused_coarse
+    mg = KM.Multigrid2D((64, 64), w, device="cpu", fused_coarse=False, fused_pairs=False)
+    assert not mg.fused_coarse and not mg.fused_pairs
+
+
 def test_serve_config_and_validation_without_gpu(lib, pkg):
     """hfm_serve_*: the default configuration and the host-side checks that run before any
     device allocation."""
