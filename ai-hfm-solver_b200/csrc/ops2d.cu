@@ -383,13 +383,14 @@ __global__ void __launch_bounds__(kT2) k2_coarse_jacobi(W9 w, const T *__restric
 // ------------------------------------------------------------------ fused coarse cycle
 // The V-cycle of the levels of at most 4096 cells (64^2 .. 4^2 of a 512^2 grid) in one
 // launch: one 1024-thread block per instance, every field of those levels in shared memory
-// (float32), sweeps separated by __syncthreads(); a coarsest level of at most 32 cells runs on
-// one warp with its iterate in registers (shuffles, no barriers).  The steps and their arithmetic are those
-// of the per-level kernels (Multigrid2D._cycle): nu_pre sweeps from zero, residual + 2 x 2
-// averaging restriction (0.25 x the sum), recursion, `sweeps` sweeps from zero on the
-// coarsest level, then the nearest-prolongation correction phi - P w and nu_post sweeps;
-// iterates stay in float32 between sweeps (the per-level path stores them in the storage
-// type, so float32 storage gives the same bits).
+// (float32), sweeps separated by __syncthreads(); a coarsest level of at most 32 cells runs
+// on one warp with its iterate in registers (shuffles, no barriers).  The steps and their
+// arithmetic are those of the per-level kernels (hfm_jacobi2d, hfm_residual_restrict2d,
+// hfm_coarse_jacobi2d): nu_pre sweeps from zero, residual + 2 x 2 averaging restriction
+// (0.25 x the sum), recursion, coarse_sweeps sweeps from zero on the coarsest level, then
+// the nearest-prolongation correction phi - P w and nu_post sweeps; iterates stay in float32
+// between sweeps (the per-level path stores them in the storage type, so float32 storage
+// gives the same bits).
 constexpr int kSub2Levels = 8;
 constexpr int kSub2Threads = 1024;
 struct Sub2Args {
